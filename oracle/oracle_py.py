@@ -1,0 +1,344 @@
+"""ctypes bindings for the test-only CPU checkers (never imported by the product).
+
+* ``Ref``      -- the unmodified reference encoder built from its own sources
+                  (oracle/_ref/libevxref.so, see oracle/Makefile and
+                  oracle/ref_harness.cpp): stock public API and a staged
+                  per-frame driver with stage dumps.
+* ``Oracle``   -- this project's plain-C restatement (oracle/_build/liboracle.so).
+* ``plan_gop`` -- the frame-type / DPB-slot schedule of the reference encoder's
+                  GOP logic (src/video/evx3enc.cpp:105-414), restated in Python,
+                  used to drive the staged engines frame by frame.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import struct
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "libevxref.so")
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+
+BLOCK_DTYPE = np.dtype([
+    ("block_type", "<i4"), ("prediction_target", "u1"), ("pad0", "u1"),
+    ("motion_x", "<i2"), ("motion_y", "<i2"), ("sp_pred", "u1"), ("sp_amount", "u1"),
+    ("sp_index", "u1"), ("q_index", "u1"), ("intra_mode", "u1"), ("pad1", "u1"),
+    ("variance", "<i2"), ("prediction_mode", "u1"), ("prediction_target_b", "u1"),
+    ("motion_x_b", "<i2"), ("motion_y_b", "<i2"), ("sp_pred_b", "u1"), ("sp_amount_b", "u1"),
+    ("sp_index_b", "u1"), ("pad2", "u1")])
+assert BLOCK_DTYPE.itemsize == 28
+BLOCK_FIELDS = [n for n in BLOCK_DTYPE.names if not n.startswith("pad")]
+SAO_DTYPE = np.dtype([("merge_left", "u1"), ("merge_above", "u1"),
+                      ("l_type", "u1"), ("l_eo", "u1"), ("l_band", "u1"), ("l_off", "i1", 4),
+                      ("c_type", "u1"), ("c_eo", "u1"), ("c_band", "u1"), ("c_off", "i1", 4)])
+assert SAO_DTYPE.itemsize == 16
+
+FRAME_INTRA, FRAME_INTER, FRAME_BIDIR = 0, 1, 2
+
+
+def align16(v: int) -> int:
+    return (v + 15) & ~15
+
+
+def pack_frame(ftype, index, quality, display_order, is_reference, dpb_slot, ref_fwd, ref_bwd) -> bytes:
+    """18-byte evx_frame (src/video/common.h:72-87, pack(2))."""
+    return struct.pack("<iIHIBBBB", ftype, index, quality, display_order,
+                       is_reference, dpb_slot, ref_fwd, ref_bwd)
+
+
+def unpack_frame(b: bytes) -> dict:
+    t, i, q, d, r, s, f, bw = struct.unpack("<iIHIBBBB", bytes(b[:18]))
+    return dict(type=t, index=i, quality=q, display_order=d, is_reference=r,
+                dpb_slot=s, ref_fwd=f, ref_bwd=bw)
+
+
+def quality_to_qp(q: int) -> int:
+    """evx3_encoder::set_quality (src/video/evx3enc.cpp:64-82)."""
+    q = min(max(int(q), 1), 31)
+    qp = q if q <= 16 else q + ((q - 16) * (q - 16)) // 10
+    return min(qp, 63)
+
+
+def plan_gop(n_frames: int, quality: int = 8, intra_at=(), b_frames: int = 3):
+    """Yield (input_frame_index, frame18) in encode order, mirroring the
+    reference's reorder/GOP logic with the default EVX_B_FRAME_COUNT 3.
+    ``intra_at`` lists input indices before which insert_intra() is called."""
+    qp = quality_to_qp(quality)
+    st = dict(type=FRAME_INTRA, index=0, reorder=[], doc=0, ip=0, first=True)
+    out = []
+
+    def slot(ip):
+        return (ip & 0xFFFFFFFF) % 2
+
+    def gop():
+        r = st["reorder"]
+        p_in, p_do = r[-1]
+        out.append((p_in, pack_frame(FRAME_INTER, st["index"], qp, p_do, 1, slot(st["ip"]), slot(st["ip"] - 1), 0)))
+        st["index"] += 1
+        bc = len(r) - 1
+        if bc > 0:
+            ref = bc // 2
+            b_in, b_do = r[ref]
+            out.append((b_in, pack_frame(FRAME_BIDIR, st["index"], min(qp + 1, 31), b_do, 1, 2,
+                                         slot(st["ip"] - 1), slot(st["ip"]))))
+            st["index"] += 1
+            for bi in range(bc):
+                if bi == ref:
+                    continue
+                b_in, b_do = r[bi]
+                fw, bw = (slot(st["ip"] - 1), 2) if bi < ref else (2, slot(st["ip"]))
+                out.append((b_in, pack_frame(FRAME_BIDIR, st["index"], min(qp + 2, 31), b_do, 0, 3, fw, bw)))
+                st["index"] += 1
+        st["ip"] += 1
+        st["type"] = FRAME_INTER
+        st["reorder"] = []
+
+    for t in range(n_frames):
+        if t in intra_at:
+            st["type"] = FRAME_INTRA
+        if st["doc"] > 0 and st["doc"] % 3600 == 0:
+            if st["reorder"]:
+                gop()
+            st["type"] = FRAME_INTRA
+            st["ip"] = 0
+        as_intra = st["type"] == FRAME_INTRA
+        if as_intra and not st["first"] and st["reorder"]:
+            gop()
+            st["ip"] = 0
+        st["reorder"].append((t, st["doc"]))
+        st["doc"] += 1
+        if st["first"] or as_intra:
+            st["first"] = False
+            i_in, i_do = st["reorder"][0]
+            out.append((i_in, pack_frame(FRAME_INTRA, st["index"], qp, i_do, 1, slot(st["ip"]), 0, 0)))
+            st["ip"] += 1
+            st["type"] = FRAME_INTER
+            st["index"] += 1
+            st["reorder"] = []
+        elif len(st["reorder"]) == b_frames + 1:
+            gop()
+    # flush()
+    r = st["reorder"]
+    if len(r) == 1:
+        p_in, p_do = r[0]
+        out.append((p_in, pack_frame(FRAME_INTER, st["index"], qp, p_do, 1, slot(st["ip"]), slot(st["ip"] - 1), 0)))
+    elif len(r) > 1:
+        gop()
+    return out
+
+
+def split_stream(data: bytes):
+    """Split a stock .evx stream into (header, [frame payloads]); each payload
+    is frame18 + slice bytes (evx3enc.cpp:249-277)."""
+    hdr, pos, frames = bytes(data[:14]), 14, []
+    while pos < len(data):
+        (n,) = struct.unpack("<I", data[pos:pos + 4])
+        frames.append(bytes(data[pos + 4:pos + 4 + n]))
+        pos += 4 + n
+    return hdr, frames
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class StageDump:
+    """Per-frame stage buffers in the plane-set layout."""
+
+    def __init__(self, aw, ah):
+        n = aw * ah + 2 * (aw // 2) * (ah // 2)
+        nblk = (aw // 16) * (ah // 16)
+        self.src = np.zeros(n, np.int16)
+        self.blocks = np.zeros(nblk * 28, np.uint8)
+        self.levels = np.zeros(n, np.int16)
+        self.recon = np.zeros(n, np.int16)
+        self.deblock = np.zeros(n, np.int16)
+        self.sao = np.zeros(nblk * 16, np.uint8)
+        self.final = np.zeros(n, np.int16)
+
+    def block_table(self):
+        return self.blocks.view(BLOCK_DTYPE)
+
+    def sao_table(self):
+        return self.sao.view(SAO_DTYPE)
+
+
+class Ref:
+    """The unmodified reference library (built here from its own sources)."""
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"reference library not built: {path} (make -C oracle ref)")
+        L = self.lib = C.CDLL(path)
+        L.evxref_enc_create.restype = C.c_void_p
+        L.evxref_enc_create.argtypes = [C.c_uint32]
+        L.evxref_enc_destroy.argtypes = [C.c_void_p]
+        L.evxref_enc_set_quality.argtypes = [C.c_void_p, C.c_uint8]
+        L.evxref_enc_insert_intra.argtypes = [C.c_void_p]
+        L.evxref_enc_encode.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                        C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]
+        L.evxref_enc_flush.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]
+        L.evxref_ctx_create.restype = C.c_void_p
+        L.evxref_ctx_create.argtypes = [C.c_uint32, C.c_uint32]
+        L.evxref_ctx_destroy.argtypes = [C.c_void_p]
+        L.evxref_ctx_encode_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                              C.c_char_p, C.c_int] + [C.c_void_p] * 8 + \
+                                             [C.c_uint32, C.POINTER(C.c_uint32)]
+        L.evxref_ctx_serialize.argtypes = [C.c_void_p, C.c_char_p] + [C.c_void_p] * 5 + \
+                                          [C.c_uint32, C.POINTER(C.c_uint32)]
+        L.evxref_ctx_get_slot.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        L.evxref_lambda.restype = C.c_float
+        L.evxref_lambda.argtypes = [C.c_uint16]
+
+    # --- stock API ---
+    def encode_stream(self, frames: np.ndarray, quality: int = 8, intra_at=()) -> bytes:
+        """Encode (T,H,W,3) uint8 frames through create_encoder/encode/flush."""
+        T, H, W, _ = frames.shape
+        cap = max(1 << 22, W * H * 3 * 8)
+        h = self.lib.evxref_enc_create(cap)
+        buf = np.zeros(cap, np.uint8)
+        n = C.c_uint32(0)
+        out = bytearray()
+        try:
+            self.lib.evxref_enc_set_quality(h, quality)
+            for t in range(T):
+                if t in intra_at:
+                    self.lib.evxref_enc_insert_intra(h)
+                f = np.ascontiguousarray(frames[t])
+                rc = self.lib.evxref_enc_encode(h, _p(f), W, H, _p(buf), cap, C.byref(n))
+                if rc:
+                    raise RuntimeError(f"reference encode failed: {rc}")
+                out += buf[:n.value].tobytes()
+            rc = self.lib.evxref_enc_flush(h, _p(buf), cap, C.byref(n))
+            if rc:
+                raise RuntimeError(f"reference flush failed: {rc}")
+            out += buf[:n.value].tobytes()
+        finally:
+            self.lib.evxref_enc_destroy(h)
+        return bytes(out)
+
+    # --- staged engine ---
+    def context(self, width: int, height: int):
+        return RefContext(self, align16(width), align16(height))
+
+    def lam(self, q: int) -> float:
+        return self.lib.evxref_lambda(q)
+
+
+class RefContext:
+    def __init__(self, ref: Ref, aw: int, ah: int):
+        self.ref, self.aw, self.ah = ref, aw, ah
+        self.h = ref.lib.evxref_ctx_create(aw, ah)
+        self.cap = aw * ah * 8 + (1 << 20)
+        self.buf = np.zeros(self.cap, np.uint8)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.ref.lib.evxref_ctx_destroy(self.h)
+            self.h = None
+
+    def encode_frame(self, rgb: np.ndarray, frame18: bytes, wpp: bool = False):
+        H, W, _ = rgb.shape
+        d = StageDump(self.aw, self.ah)
+        n = C.c_uint32(0)
+        rgb = np.ascontiguousarray(rgb)
+        rc = self.ref.lib.evxref_ctx_encode_frame(
+            self.h, _p(rgb), W, H, frame18, int(wpp), _p(d.src), _p(d.blocks), _p(d.levels),
+            _p(d.recon), _p(d.deblock), _p(d.sao), _p(d.final), _p(self.buf), self.cap, C.byref(n))
+        if rc:
+            raise RuntimeError(f"reference staged encode failed: {rc}")
+        return d, self.buf[:n.value].tobytes()
+
+    def serialize(self, frame18: bytes, blocks, prev_blocks, sao, levels) -> bytes:
+        n = C.c_uint32(0)
+        rc = self.ref.lib.evxref_ctx_serialize(self.h, frame18, _p(blocks), _p(prev_blocks), _p(sao),
+                                               _p(levels), _p(self.buf), self.cap, C.byref(n))
+        if rc:
+            raise RuntimeError(f"reference serialize failed: {rc}")
+        return self.buf[:n.value].tobytes()
+
+    def slot(self, s: int) -> np.ndarray:
+        out = np.zeros(self.aw * self.ah * 3 // 2, np.int16)
+        self.ref.lib.evxref_ctx_get_slot(self.h, s, _p(out))
+        return out
+
+
+class Oracle:
+    """This project's plain-C restatement (test infrastructure)."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle not built: {path} (make -C oracle oracle)")
+        L = self.lib = C.CDLL(path)
+        L.orc_create.restype = C.c_void_p
+        L.orc_create.argtypes = [C.c_uint32, C.c_uint32]
+        L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_encode_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_char_p] + \
+                                      [C.c_void_p] * 7
+        for nm in ("orc_get_slot",):
+            getattr(L, nm).argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        L.orc_get_prev_blocks.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_get_levels.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_lambda.restype = C.c_float
+        L.orc_lambda.argtypes = [C.c_uint16]
+        L.orc_hadamard_4x4.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        L.orc_satd_16x16.restype = C.c_int32
+        L.orc_satd_16x16.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
+        L.orc_interpolate.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                      C.c_int16, C.c_int16, C.c_int32, C.c_void_p]
+        L.orc_fdct_8x8.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
+        L.orc_idct_8x8.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
+        L.orc_intra_predict.argtypes = [C.c_uint8, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                        C.c_int32, C.c_void_p]
+        L.orc_mv_predictor.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                       C.POINTER(C.c_int16), C.POINTER(C.c_int16)]
+        L.orc_deblock_strength.restype = C.c_uint8
+        L.orc_deblock_strength.argtypes = [C.c_int32, C.c_void_p, C.c_void_p]
+        L.orc_convert.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32]
+
+    def context(self, width: int, height: int):
+        return OracleContext(self, align16(width), align16(height))
+
+
+class OracleContext:
+    def __init__(self, orc: Oracle, aw: int, ah: int):
+        self.orc, self.aw, self.ah = orc, aw, ah
+        self.h = orc.lib.orc_create(aw, ah)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.orc.lib.orc_destroy(self.h)
+            self.h = None
+
+    def encode_frame(self, rgb: np.ndarray, frame18: bytes):
+        H, W, _ = rgb.shape
+        d = StageDump(self.aw, self.ah)
+        rgb = np.ascontiguousarray(rgb)
+        rc = self.orc.lib.orc_encode_frame(self.h, _p(rgb), W, H, frame18, _p(d.src), _p(d.blocks),
+                                           _p(d.levels), _p(d.recon), _p(d.deblock), _p(d.sao), _p(d.final))
+        if rc:
+            raise RuntimeError(f"oracle encode failed: {rc}")
+        return d
+
+    def prev_blocks(self) -> np.ndarray:
+        out = np.zeros((self.aw // 16) * (self.ah // 16) * 28, np.uint8)
+        self.orc.lib.orc_get_prev_blocks(self.h, _p(out))
+        return out
+
+    def levels(self) -> np.ndarray:
+        out = np.zeros(self.aw * self.ah * 3 // 2, np.int16)
+        self.orc.lib.orc_get_levels(self.h, _p(out))
+        return out
+
+
+def compare_blocks(a: np.ndarray, b: np.ndarray):
+    """Indices and field names where two block tables differ (padding ignored)."""
+    ta, tb = a.view(BLOCK_DTYPE), b.view(BLOCK_DTYPE)
+    bad = {}
+    for f in BLOCK_FIELDS:
+        idx = np.nonzero(ta[f] != tb[f])[0]
+        if idx.size:
+            bad[f] = idx
+    return bad
