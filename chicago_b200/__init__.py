@@ -1,0 +1,222 @@
+"""chicago_b200 -- B200 (sm_100a) EVX3 encoder pixel pipeline behind a C ABI.
+
+Python mirror of the C ABI in include/evxg.h over ctypes.  The CUDA library
+chicago_b200/libevxg.so is built in-tree (``python -m chicago_b200.build``);
+importing this package without it raises: there is no CPU fallback.
+
+* :class:`Stream`  -- one encoding context: ``encode_frame`` is the reference's
+  engine_encode_frame minus serialization (src/video/encode.cpp:945-998),
+  ``fetch_tables`` returns what the host entropy coder reads.
+* :class:`Encoder` -- the reference's evx3_encoder (src/video/evx3.h:67-100:
+  set_quality / insert_intra / encode / flush / clear) with its GOP logic,
+  emitting one record per encoded frame in bitstream order.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import struct
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libevxg.so")
+
+BLOCK_DTYPE = np.dtype([
+    ("block_type", "<i4"), ("prediction_target", "u1"), ("pad0", "u1"),
+    ("motion_x", "<i2"), ("motion_y", "<i2"), ("sp_pred", "u1"), ("sp_amount", "u1"),
+    ("sp_index", "u1"), ("q_index", "u1"), ("intra_mode", "u1"), ("pad1", "u1"),
+    ("variance", "<i2"), ("prediction_mode", "u1"), ("prediction_target_b", "u1"),
+    ("motion_x_b", "<i2"), ("motion_y_b", "<i2"), ("sp_pred_b", "u1"), ("sp_amount_b", "u1"),
+    ("sp_index_b", "u1"), ("pad2", "u1")])
+SAO_DTYPE = np.dtype([("merge_left", "u1"), ("merge_above", "u1"),
+                      ("l_type", "u1"), ("l_eo", "u1"), ("l_band", "u1"), ("l_off", "i1", 4),
+                      ("c_type", "u1"), ("c_eo", "u1"), ("c_band", "u1"), ("c_off", "i1", 4)])
+
+EVXG_SUCCESS = 0
+FRAME_INTRA, FRAME_INTER, FRAME_BIDIR = 0, 1, 2
+
+# Exported entry points, as declared in include/evxg.h.
+EXPORTS = [
+    "evxg_stream_create", "evxg_stream_destroy", "evxg_stream_dims", "evxg_encode_frame",
+    "evxg_fetch_tables", "evxg_fetch_planes", "evxg_stream_sync", "evxg_last_launch_count",
+    "evxg_lambda", "evxg_last_error", "evxg_encoder_create", "evxg_encoder_destroy",
+    "evxg_encoder_clear", "evxg_encoder_insert_intra", "evxg_encoder_set_quality",
+    "evxg_encoder_encode", "evxg_encoder_flush", "evxg_encoder_stream",
+]
+
+FRAME_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
+
+
+class EvxgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"evxg error {code}: {msg}")
+        self.code = code
+
+
+def _load(path: str = LIB_PATH) -> C.CDLL:
+    if not os.path.exists(path):
+        raise ImportError(f"CUDA library missing: {path}; build it with `python -m chicago_b200.build`")
+    L = C.CDLL(path)
+    vp, u32, i32 = C.c_void_p, C.c_uint32, C.c_int
+    L.evxg_stream_create.argtypes = [u32, u32, C.POINTER(vp)]
+    L.evxg_stream_destroy.argtypes = [vp]
+    L.evxg_stream_dims.argtypes = [vp] + [C.POINTER(u32)] * 4
+    L.evxg_encode_frame.argtypes = [vp, vp, i32, C.c_char_p, vp]
+    L.evxg_fetch_tables.argtypes = [vp, vp, vp, vp, vp, i32, vp]
+    L.evxg_fetch_planes.argtypes = [vp, u32, vp, i32, vp]
+    L.evxg_stream_sync.argtypes = [vp, vp]
+    L.evxg_last_launch_count.argtypes = [vp]
+    L.evxg_last_launch_count.restype = u32
+    L.evxg_lambda.argtypes = [C.c_uint16]
+    L.evxg_lambda.restype = C.c_float
+    L.evxg_last_error.restype = C.c_char_p
+    L.evxg_encoder_create.argtypes = [FRAME_CB, vp, C.POINTER(vp)]
+    for n in ("evxg_encoder_destroy", "evxg_encoder_clear", "evxg_encoder_insert_intra", "evxg_encoder_flush"):
+        getattr(L, n).argtypes = [vp]
+    L.evxg_encoder_set_quality.argtypes = [vp, C.c_uint8]
+    L.evxg_encoder_encode.argtypes = [vp, vp, u32, u32]
+    L.evxg_encoder_stream.argtypes = [vp]
+    L.evxg_encoder_stream.restype = vp
+    return L
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        _lib = _load()
+    return _lib
+
+
+def _check(rc: int):
+    if rc != EVXG_SUCCESS:
+        raise EvxgError(rc, lib().evxg_last_error().decode(errors="replace"))
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return C.c_void_p(a)
+    if hasattr(a, "data_ptr"):       # torch tensor
+        return C.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def lam(quality: int) -> float:
+    return lib().evxg_lambda(quality)
+
+
+def pack_frame(ftype, index, quality, display_order, is_reference, dpb_slot, ref_fwd, ref_bwd) -> bytes:
+    """18-byte evx_frame (reference src/video/common.h:72-87)."""
+    return struct.pack("<iIHIBBBB", ftype, index, quality, display_order, is_reference, dpb_slot, ref_fwd, ref_bwd)
+
+
+class Stream:
+    """One device encoding context (evx_context on the GPU)."""
+
+    def __init__(self, width: int, height: int):
+        self.width, self.height = int(width), int(height)
+        h = C.c_void_p()
+        _check(lib().evxg_stream_create(self.width, self.height, C.byref(h)))
+        self.h = h
+        d = [C.c_uint32() for _ in range(4)]
+        _check(lib().evxg_stream_dims(self.h, *[C.byref(x) for x in d]))
+        self.aw, self.ah, self.mbw, self.mbh = (x.value for x in d)
+        self.nblk = self.mbw * self.mbh
+        self.plane_elems = self.aw * self.ah + 2 * (self.aw // 2) * (self.ah // 2)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().evxg_stream_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def encode_frame(self, rgb, frame18: bytes, on_device: bool = False, cuda_stream=None):
+        """Asynchronously encode one RGB24 frame (host ndarray, or device pointer/tensor)."""
+        if not on_device:
+            rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+            if rgb.size != self.width * self.height * 3:
+                raise ValueError("rgb must hold width*height*3 bytes")
+        _check(lib().evxg_encode_frame(self.h, _ptr(rgb), int(on_device), frame18, _ptr(cuda_stream)))
+
+    def sync(self, cuda_stream=None):
+        _check(lib().evxg_stream_sync(self.h, _ptr(cuda_stream)))
+
+    def fetch_tables(self, cuda_stream=None):
+        bt = np.zeros(self.nblk * 28, np.uint8)
+        prev = np.zeros(self.nblk * 28, np.uint8)
+        sao = np.zeros(self.nblk * 16, np.uint8)
+        lev = np.zeros(self.plane_elems, np.int16)
+        _check(lib().evxg_fetch_tables(self.h, _ptr(bt), _ptr(prev), _ptr(sao), _ptr(lev), 0, _ptr(cuda_stream)))
+        return dict(blocks=bt, prev_blocks=prev, sao=sao, levels=lev)
+
+    def fetch_planes(self, slot: int, cuda_stream=None) -> np.ndarray:
+        out = np.zeros(self.plane_elems, np.int16)
+        _check(lib().evxg_fetch_planes(self.h, slot, _ptr(out), 0, _ptr(cuda_stream)))
+        return out
+
+    def launch_count(self) -> int:
+        return lib().evxg_last_launch_count(self.h)
+
+
+class Encoder:
+    """evx3_encoder mirror: frames in, per-frame table records out (bitstream order)."""
+
+    def __init__(self, quality: int | None = None):
+        self.records = []
+        self._cb = FRAME_CB(self._on_frame)
+        h = C.c_void_p()
+        _check(lib().evxg_encoder_create(self._cb, None, C.byref(h)))
+        self.h = h
+        if quality is not None:
+            self.set_quality(quality)
+
+    def _on_frame(self, user, frame, blocks, prev, sao, levels):
+        st = lib().evxg_encoder_stream(self.h)
+        d = [C.c_uint32() for _ in range(4)]
+        lib().evxg_stream_dims(st, *[C.byref(x) for x in d])
+        aw, ah, mbw, mbh = (x.value for x in d)
+        nblk, ne = mbw * mbh, aw * ah + 2 * (aw // 2) * (ah // 2)
+        self.records.append(dict(
+            frame18=C.string_at(frame, 18),
+            blocks=np.frombuffer(C.string_at(blocks, nblk * 28), np.uint8).copy(),
+            prev_blocks=np.frombuffer(C.string_at(prev, nblk * 28), np.uint8).copy(),
+            sao=np.frombuffer(C.string_at(sao, nblk * 16), np.uint8).copy(),
+            levels=np.frombuffer(C.string_at(levels, ne * 2), np.int16).copy()))
+
+    def set_quality(self, q: int):
+        _check(lib().evxg_encoder_set_quality(self.h, q))
+
+    def insert_intra(self):
+        _check(lib().evxg_encoder_insert_intra(self.h))
+
+    def encode(self, rgb: np.ndarray):
+        rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+        H, W = rgb.shape[:2]
+        _check(lib().evxg_encoder_encode(self.h, _ptr(rgb), W, H))
+
+    def flush(self):
+        _check(lib().evxg_encoder_flush(self.h))
+
+    def clear(self):
+        _check(lib().evxg_encoder_clear(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().evxg_encoder_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

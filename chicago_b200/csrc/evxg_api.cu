@@ -1,0 +1,443 @@
+// evxg_api.cu -- host side of the B200 EVX3 encoder pipeline: the C ABI of
+// include/evxg.h (per-stream device state, per-frame launch sequence, table
+// fetch) and the GOP-level encoder that mirrors the reference's evx3_encoder
+// (src/video/evx3enc.cpp:35-414) on top of it.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "evxg.h"
+#include "evxg_device.cuh"
+
+namespace evxg {
+__global__ void k_convert(FrameArgs a);
+__global__ void k_mb_wavefront(FrameArgs a);
+__global__ void k_deblock(FrameArgs a);
+__global__ void k_sao_rdo(FrameArgs a);
+__global__ void k_sao_merge(FrameArgs a);
+__global__ void k_sao_apply(FrameArgs a);
+size_t mb_shared_bytes();
+}  // namespace evxg
+
+using namespace evxg;
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const char *what)
+{
+    g_last_error = what;
+    return code;
+}
+static int cuda_fail(cudaError_t e, const char *where)
+{
+    g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? EVXG_ERROR_OUTOFMEMORY : EVXG_ERROR_EXECUTION_FAILURE;
+}
+#define CK(call)                                              \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+    } while (0)
+
+struct evxg_stream {
+    uint32_t vw, vh, W, H, mbw, mbh;
+    size_t plane_elems;                 // elements of one plane set
+    int16_t *src, *lev, *dpb[4];
+    evxg_block_desc *bt, *prev, *prev_ser;
+    evxg_sao_info *sao;
+    float *sao_cost;
+    uint8_t *rgb;
+    int *sync;                          // 3*mbh progress words, 4 counters, 1 error word
+    int mb_grid, num_sms;
+    uint32_t launches;
+    long long timeout_ns;
+};
+
+extern "C" {
+
+float evxg_lambda(uint16_t q) { return 0.85f * powf(2.0f, ((float)q - 12.0f) / 3.0f); }   // common.h:264-266
+
+const char *evxg_last_error(void) { return g_last_error.c_str(); }
+
+int evxg_stream_create(uint32_t width, uint32_t height, evxg_stream **out)
+{
+    if (!out || !width || !height || width > 65535 || height > 65535 || (width & 1) || (height & 1))
+        return fail(EVXG_ERROR_INVALIDARG, "evxg_stream_create: width/height must be even and in 2..65534");
+    *out = nullptr;
+    evxg_stream *s = new evxg_stream();
+    s->vw = width; s->vh = height;
+    s->W = (width + 15) & ~15u; s->H = (height + 15) & ~15u;
+    s->mbw = s->W / 16; s->mbh = s->H / 16;
+    s->plane_elems = (size_t)s->W * s->H + 2 * (size_t)(s->W / 2) * (s->H / 2);
+    const size_t pb = s->plane_elems * sizeof(int16_t), nblk = (size_t)s->mbw * s->mbh;
+    s->timeout_ns = 5000000000LL;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaMalloc(&s->src, pb);
+    if (e == cudaSuccess) e = cudaMalloc(&s->lev, pb);
+    for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaMalloc(&s->dpb[i], pb);
+    if (e == cudaSuccess) e = cudaMalloc(&s->bt, nblk * sizeof(evxg_block_desc));
+    if (e == cudaSuccess) e = cudaMalloc(&s->prev, nblk * sizeof(evxg_block_desc));
+    if (e == cudaSuccess) e = cudaMalloc(&s->prev_ser, nblk * sizeof(evxg_block_desc));
+    if (e == cudaSuccess) e = cudaMalloc(&s->sao, nblk * sizeof(evxg_sao_info));
+    if (e == cudaSuccess) e = cudaMalloc(&s->sao_cost, nblk * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&s->rgb, (size_t)width * height * 3);
+    if (e == cudaSuccess) e = cudaMalloc(&s->sync, (3 * s->mbh + 5) * sizeof(int));
+    // The reference zero-fills every image and table at allocation (image.cpp:89,
+    // common.cpp:167-187); stale-pixel reads of never-written DPB slots see zeros.
+    if (e == cudaSuccess) e = cudaMemset(s->src, 0, pb);
+    if (e == cudaSuccess) e = cudaMemset(s->lev, 0, pb);
+    for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaMemset(s->dpb[i], 0, pb);
+    if (e == cudaSuccess) e = cudaMemset(s->bt, 0, nblk * sizeof(evxg_block_desc));
+    if (e == cudaSuccess) e = cudaMemset(s->prev, 0, nblk * sizeof(evxg_block_desc));
+    if (e == cudaSuccess) e = cudaMemset(s->prev_ser, 0, nblk * sizeof(evxg_block_desc));
+    if (e == cudaSuccess) e = cudaMemset(s->sao, 0, nblk * sizeof(evxg_sao_info));
+    if (e == cudaSuccess) e = cudaMemset(s->sync, 0, (3 * s->mbh + 5) * sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_mb_wavefront, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mb_shared_bytes());
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        int rc = cuda_fail(e, "evxg_stream_create");
+        evxg_stream_destroy(s);
+        return rc;
+    }
+    s->mb_grid = (int)std::min<uint32_t>(s->mbh, (uint32_t)s->num_sms);
+    *out = s;
+    return EVXG_SUCCESS;
+}
+
+int evxg_stream_destroy(evxg_stream *s)
+{
+    if (!s) return EVXG_ERROR_INVALIDARG;
+    cudaFree(s->src); cudaFree(s->lev);
+    for (int i = 0; i < 4; i++) cudaFree(s->dpb[i]);
+    cudaFree(s->bt); cudaFree(s->prev); cudaFree(s->prev_ser);
+    cudaFree(s->sao); cudaFree(s->sao_cost); cudaFree(s->rgb); cudaFree(s->sync);
+    delete s;
+    return EVXG_SUCCESS;
+}
+
+int evxg_stream_dims(const evxg_stream *s, uint32_t *aw, uint32_t *ah, uint32_t *mbw, uint32_t *mbh)
+{
+    if (!s) return EVXG_ERROR_INVALIDARG;
+    if (aw) *aw = s->W;
+    if (ah) *ah = s->H;
+    if (mbw) *mbw = s->mbw;
+    if (mbh) *mbh = s->mbh;
+    return EVXG_SUCCESS;
+}
+
+uint32_t evxg_last_launch_count(const evxg_stream *s) { return s ? s->launches : 0; }
+
+int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, const evxg_frame *f, void *cuda_stream)
+{
+    if (!s || !rgb || !f) return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: null argument");
+    if (f->type < EVXG_FRAME_INTRA || f->type > EVXG_FRAME_BIDIR)
+        return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: bad frame type");
+    if (f->dpb_slot > 3 || f->ref_slot_fwd > 3 || f->ref_slot_bwd > 3)
+        return fail(EVXG_ERROR_INVALID_INDEX, "evxg_encode_frame: DPB slot out of range");
+    if (f->quality < 1 || f->quality > 63)
+        return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: quality (QP) must be 1..63");
+    if (f->type != EVXG_FRAME_INTRA && f->ref_slot_fwd == f->dpb_slot)
+        return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: forward reference equals the destination slot");
+    if (f->type == EVXG_FRAME_BIDIR && f->ref_slot_bwd == f->dpb_slot)
+        return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: backward reference equals the destination slot");
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    const uint8_t *drgb = rgb;
+    if (!rgb_on_device) {
+        CK(cudaMemcpyAsync(s->rgb, rgb, (size_t)s->vw * s->vh * 3, cudaMemcpyHostToDevice, st));
+        drgb = s->rgb;
+    }
+    FrameArgs a{};
+    a.W = (int)s->W; a.H = (int)s->H; a.mbw = (int)s->mbw; a.mbh = (int)s->mbh;
+    a.vis_w = (int)s->vw; a.vis_h = (int)s->vh;
+    a.type = f->type; a.quality = f->quality; a.dpb = f->dpb_slot;
+    a.ref_fwd = f->ref_slot_fwd; a.ref_bwd = f->ref_slot_bwd;
+    a.lambda = evxg_lambda(f->quality);
+    for (int i = 0; i < 4; i++) a.planes[i] = s->dpb[i];
+    a.src = s->src; a.lev = s->lev; a.bt = s->bt;
+    a.prev = f->type == EVXG_FRAME_INTER ? s->prev : nullptr;
+    a.sao = s->sao; a.sao_cost = s->sao_cost; a.rgb = drgb;
+    a.progress = s->sync; a.counters = s->sync + 3 * s->mbh; a.error = s->sync + 3 * s->mbh + 4;
+    a.timeout_ns = s->timeout_ns;
+    const size_t nblk = (size_t)s->mbw * s->mbh;
+    // the serializer of this frame reads the previous table before this frame's update
+    CK(cudaMemcpyAsync(s->prev_ser, s->prev, nblk * sizeof(evxg_block_desc), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemsetAsync(s->sync, 0xFF, 3 * s->mbh * sizeof(int), st));
+    CK(cudaMemsetAsync(s->sync + 3 * s->mbh, 0, 4 * sizeof(int), st));
+    const int cw = (int)std::min(s->vw, s->W), ch = (int)std::min(s->vh, s->H);
+    dim3 cg((cw / 2 + 127) / 128, ch / 2);
+    k_convert<<<cg, 128, 0, st>>>(a);
+    k_mb_wavefront<<<s->mb_grid, 256, mb_shared_bytes(), st>>>(a);
+    k_deblock<<<3, 1024, 0, st>>>(a);
+    k_sao_rdo<<<(unsigned)((nblk + 127) / 128), 128, 0, st>>>(a);
+    const unsigned wf = (s->mbh + 7) / 8;
+    k_sao_merge<<<wf, 256, 0, st>>>(a);
+    k_sao_apply<<<wf, 256, 0, st>>>(a);
+    s->launches = 6;
+    CK(cudaGetLastError());
+    if (f->type != EVXG_FRAME_BIDIR)   // temporal MV predictor table (encode.cpp:990-998)
+        CK(cudaMemcpyAsync(s->prev, s->bt, nblk * sizeof(evxg_block_desc), cudaMemcpyDeviceToDevice, st));
+    return EVXG_SUCCESS;
+}
+
+int evxg_stream_sync(evxg_stream *s, void *cuda_stream)
+{
+    if (!s) return EVXG_ERROR_INVALIDARG;
+    CK(cudaStreamSynchronize((cudaStream_t)cuda_stream));
+    int err = 0;
+    CK(cudaMemcpy(&err, s->sync + 3 * s->mbh + 4, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+        CK(cudaMemset(s->sync + 3 * s->mbh + 4, 0, sizeof(int)));
+        return fail(err, "device wavefront gave up waiting (timeout)");
+    }
+    return EVXG_SUCCESS;
+}
+
+static int copy_out(void *dst, const void *src, size_t n, int to_device, cudaStream_t st)
+{
+    if (!dst) return EVXG_SUCCESS;
+    CK(cudaMemcpyAsync(dst, src, n, to_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    return EVXG_SUCCESS;
+}
+
+int evxg_fetch_tables(evxg_stream *s, evxg_block_desc *blocks, evxg_block_desc *prev_blocks, evxg_sao_info *sao,
+                      int16_t *levels, int to_device, void *cuda_stream)
+{
+    if (!s) return EVXG_ERROR_INVALIDARG;
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    const size_t nblk = (size_t)s->mbw * s->mbh;
+    int rc;
+    if ((rc = copy_out(blocks, s->bt, nblk * sizeof(evxg_block_desc), to_device, st))) return rc;
+    if ((rc = copy_out(prev_blocks, s->prev_ser, nblk * sizeof(evxg_block_desc), to_device, st))) return rc;
+    if ((rc = copy_out(sao, s->sao, nblk * sizeof(evxg_sao_info), to_device, st))) return rc;
+    if ((rc = copy_out(levels, s->lev, s->plane_elems * sizeof(int16_t), to_device, st))) return rc;
+    if (!to_device) return evxg_stream_sync(s, cuda_stream);
+    return EVXG_SUCCESS;
+}
+
+int evxg_fetch_planes(evxg_stream *s, uint32_t slot, int16_t *out, int to_device, void *cuda_stream)
+{
+    if (!s || !out) return EVXG_ERROR_INVALIDARG;
+    if (slot > 4) return fail(EVXG_ERROR_INVALID_INDEX, "evxg_fetch_planes: slot must be 0..3 (DPB) or 4 (source)");
+    int rc = copy_out(out, slot == 4 ? s->src : s->dpb[slot], s->plane_elems * sizeof(int16_t), to_device,
+                      (cudaStream_t)cuda_stream);
+    if (rc) return rc;
+    if (!to_device) return evxg_stream_sync(s, cuda_stream);
+    return EVXG_SUCCESS;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ GOP encoder
+// Mirrors evx3_encoder_impl with EVX_ENABLE_B_FRAMES 1, EVX_B_FRAME_COUNT 3 and
+// EVX_PERIODIC_INTRA_RATE 3600 (config.h:41, :120-121): frame types, display
+// order, DPB slot assignment (common.cpp:256-283) and the hierarchical
+// P / reference-B / B reorder (evx3enc.cpp:279-383).
+struct evxg_encoder {
+    evxg_frame_callback cb = nullptr;
+    void *user = nullptr;
+    evxg_stream *stream = nullptr;
+    evxg_frame frame{};                 // the running frame state (clear_frame, common.cpp:48-66)
+    uint32_t width = 0, height = 0;
+    struct Buf { std::vector<uint8_t> px; uint32_t display_order; };
+    Buf reorder[4];
+    uint32_t reorder_count = 0, display_counter = 0, ip_index = 0;
+    bool first = true;
+    std::vector<evxg_block_desc> h_bt, h_prev;
+    std::vector<evxg_sao_info> h_sao;
+    std::vector<int16_t> h_lev;
+};
+
+static const uint32_t kBFrames = 3, kIntraRate = 3600;
+static uint8_t ip_slot(uint32_t ip) { return (uint8_t)(ip % 2); }
+
+static void clear_frame(evxg_frame &f)
+{
+    f = evxg_frame{};
+    f.type = EVXG_FRAME_INTRA;
+    f.quality = 8;   // EVX_DEFAULT_QUALITY_LEVEL
+}
+
+static int encode_one(evxg_encoder *e, const uint8_t *px, const evxg_frame &f)
+{
+    int rc = evxg_encode_frame(e->stream, px, 0, &f, nullptr);
+    if (rc) return rc;
+    rc = evxg_fetch_tables(e->stream, e->h_bt.data(), e->h_prev.data(), e->h_sao.data(), e->h_lev.data(), 0, nullptr);
+    if (rc) return rc;
+    if (e->cb) e->cb(e->user, &f, e->h_bt.data(), e->h_prev.data(), e->h_sao.data(), e->h_lev.data());
+    return EVXG_SUCCESS;
+}
+
+static int encode_gop(evxg_encoder *e)   // evx3enc.cpp:279-383
+{
+    const uint32_t p_idx = e->reorder_count - 1;
+    evxg_frame p = e->frame;
+    p.type = EVXG_FRAME_INTER;
+    p.display_order = e->reorder[p_idx].display_order;
+    p.dpb_slot = ip_slot(e->ip_index);
+    p.is_reference = 1;
+    p.ref_slot_fwd = ip_slot(e->ip_index - 1);
+    p.ref_slot_bwd = 0;
+    int rc = encode_one(e, e->reorder[p_idx].px.data(), p);
+    if (rc) return rc;
+    e->frame.index++;
+    const uint32_t b_count = e->reorder_count - 1;
+    if (b_count > 0) {
+        const uint32_t ref_b = b_count / 2;
+        evxg_frame b = e->frame;
+        b.type = EVXG_FRAME_BIDIR;
+        b.display_order = e->reorder[ref_b].display_order;
+        b.dpb_slot = 2;
+        b.is_reference = 1;
+        b.ref_slot_fwd = ip_slot(e->ip_index - 1);
+        b.ref_slot_bwd = ip_slot(e->ip_index);
+        b.quality = (uint16_t)std::min<int>(e->frame.quality + 1, 31);
+        if ((rc = encode_one(e, e->reorder[ref_b].px.data(), b))) return rc;
+        e->frame.index++;
+        for (uint32_t bi = 0; bi < b_count; bi++) {
+            if (bi == ref_b) continue;
+            evxg_frame nb = e->frame;
+            nb.type = EVXG_FRAME_BIDIR;
+            nb.display_order = e->reorder[bi].display_order;
+            nb.dpb_slot = 3;
+            nb.is_reference = 0;
+            nb.quality = (uint16_t)std::min<int>(e->frame.quality + 2, 31);
+            if (bi < ref_b) { nb.ref_slot_fwd = ip_slot(e->ip_index - 1); nb.ref_slot_bwd = 2; }
+            else { nb.ref_slot_fwd = 2; nb.ref_slot_bwd = ip_slot(e->ip_index); }
+            if ((rc = encode_one(e, e->reorder[bi].px.data(), nb))) return rc;
+            e->frame.index++;
+        }
+    }
+    e->ip_index++;
+    e->frame.type = EVXG_FRAME_INTER;
+    e->reorder_count = 0;
+    return EVXG_SUCCESS;
+}
+
+extern "C" {
+
+int evxg_encoder_create(evxg_frame_callback cb, void *user, evxg_encoder **out)
+{
+    if (!out) return EVXG_ERROR_INVALIDARG;
+    evxg_encoder *e = new evxg_encoder();
+    e->cb = cb; e->user = user;
+    clear_frame(e->frame);
+    *out = e;
+    return EVXG_SUCCESS;
+}
+
+int evxg_encoder_clear(evxg_encoder *e)   // evx3enc.cpp:35-55
+{
+    if (!e) return EVXG_ERROR_INVALIDARG;
+    if (e->stream) evxg_stream_destroy(e->stream);
+    e->stream = nullptr;
+    clear_frame(e->frame);
+    e->reorder_count = 0; e->display_counter = 0; e->ip_index = 0; e->first = true;
+    return EVXG_SUCCESS;
+}
+
+int evxg_encoder_destroy(evxg_encoder *e)
+{
+    if (!e) return EVXG_ERROR_INVALIDARG;
+    evxg_encoder_clear(e);
+    delete e;
+    return EVXG_SUCCESS;
+}
+
+int evxg_encoder_insert_intra(evxg_encoder *e)
+{
+    if (!e) return EVXG_ERROR_INVALIDARG;
+    e->frame.type = EVXG_FRAME_INTRA;
+    return EVXG_SUCCESS;
+}
+
+int evxg_encoder_set_quality(evxg_encoder *e, uint8_t q)   // evx3enc.cpp:64-82
+{
+    if (!e) return EVXG_ERROR_INVALIDARG;
+    int qq = std::min(std::max((int)q, 1), 31);
+    int qp = qq <= 16 ? qq : qq + ((qq - 16) * (qq - 16)) / 10;
+    e->frame.quality = (uint16_t)std::min(qp, 63);
+    return EVXG_SUCCESS;
+}
+
+evxg_stream *evxg_encoder_stream(evxg_encoder *e) { return e ? e->stream : nullptr; }
+
+int evxg_encoder_encode(evxg_encoder *e, const uint8_t *rgb, uint32_t width, uint32_t height)
+{
+    if (!e || !rgb || !width || !height) return fail(EVXG_ERROR_INVALIDARG, "evxg_encoder_encode: bad argument");
+    int rc;
+    if (!e->stream) {
+        if ((rc = evxg_stream_create(width, height, &e->stream))) return rc;
+        e->width = width; e->height = height;
+        const size_t nblk = (size_t)e->stream->mbw * e->stream->mbh;
+        e->h_bt.resize(nblk); e->h_prev.resize(nblk); e->h_sao.resize(nblk);
+        e->h_lev.resize(e->stream->plane_elems);
+        e->reorder_count = 0; e->display_counter = 0; e->ip_index = 0; e->first = true;
+    }
+    if (width != e->width || height != e->height)
+        return fail(EVXG_ERROR_INVALID_RESOURCE, "evxg_encoder_encode: frame size changed within a stream");
+    if (e->display_counter > 0 && e->display_counter % kIntraRate == 0) {   // periodic intra
+        if (e->reorder_count > 0 && (rc = encode_gop(e))) return rc;
+        e->frame.type = EVXG_FRAME_INTRA;
+        e->ip_index = 0;
+    }
+    const bool as_intra = e->frame.type == EVXG_FRAME_INTRA;
+    if (as_intra && !e->first && e->reorder_count > 0) {
+        if ((rc = encode_gop(e))) return rc;
+        e->ip_index = 0;
+    }
+    evxg_encoder::Buf &b = e->reorder[e->reorder_count];
+    b.px.assign(rgb, rgb + (size_t)width * height * 3);
+    b.display_order = e->display_counter;
+    e->reorder_count++;
+    e->display_counter++;
+    if (e->first || as_intra) {
+        e->first = false;
+        e->frame.type = EVXG_FRAME_INTRA;
+        evxg_frame i = e->frame;
+        i.display_order = e->reorder[0].display_order;
+        i.dpb_slot = ip_slot(e->ip_index);
+        i.is_reference = 1;
+        i.ref_slot_fwd = 0;
+        i.ref_slot_bwd = 0;
+        if ((rc = encode_one(e, e->reorder[0].px.data(), i))) return rc;
+        e->ip_index++;
+        e->frame.type = EVXG_FRAME_INTER;
+        e->frame.index++;
+        e->reorder_count = 0;
+    } else if (e->reorder_count == kBFrames + 1) {
+        if ((rc = encode_gop(e))) return rc;
+    }
+    return EVXG_SUCCESS;
+}
+
+int evxg_encoder_flush(evxg_encoder *e)   // evx3enc.cpp:385-414
+{
+    if (!e) return EVXG_ERROR_INVALIDARG;
+    if (e->reorder_count == 0) return EVXG_SUCCESS;
+    int rc;
+    if (e->reorder_count == 1) {
+        evxg_frame p = e->frame;
+        p.type = EVXG_FRAME_INTER;
+        p.display_order = e->reorder[0].display_order;
+        p.dpb_slot = ip_slot(e->ip_index);
+        p.is_reference = 1;
+        p.ref_slot_fwd = ip_slot(e->ip_index - 1);
+        p.ref_slot_bwd = 0;
+        if ((rc = encode_one(e, e->reorder[0].px.data(), p))) return rc;
+        e->frame.index++;
+        e->ip_index++;
+    } else if ((rc = encode_gop(e))) {
+        return rc;
+    }
+    e->reorder_count = 0;
+    return EVXG_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,105 @@
+// evxg_device.cuh -- device-side constants and exact-integer helpers shared by
+// the EVX3 encoder kernels (sm_100a).  Every helper keeps the reference's C
+// semantics: truncating division, int16 stores that wrap, int32 products that
+// wrap, IEEE single precision with round-to-nearest and no FMA contraction.
+#pragma once
+#include <cstdint>
+#include <climits>
+#include <cuda_runtime.h>
+#include "evxg.h"
+
+namespace evxg {
+
+// Block-type bits (reference src/video/types.h:63-91).
+constexpr int BT_INTRA = 1, BT_MOTION = 2, BT_COPY = 4;
+constexpr int INTRA_DEFAULT = 1, INTER_MOTION_DELTA = 2;
+constexpr int MODE_NONE = 7;
+constexpr int SAD_THRESHOLD = 8192;   // motion.cpp:24
+constexpr int SEARCH_RADIUS = 16;     // motion.cpp:29
+constexpr int MAXQ = 63;              // quantize.h:42 (levels - 1)
+
+// Search window in shared memory: a 16x16 block anywhere within +-31 px of a
+// base position, plus the 6-tap overshoot (-3 .. +18), clamped to the frame
+// the way interp.cpp:8-14 clamps its samples.
+constexpr int WL = 84;                // luma window side:  base-34 .. base+49
+constexpr int WC = 48;                // chroma window side: (base>>1)-19 .. +28
+constexpr int WL_OFF = 34, WC_OFF = 19;
+
+__device__ __forceinline__ int rdiv(int n, int d)   // rounded_div, evx_math.h:228-236
+{
+    return ((n < 0) != (d < 0)) ? (n - d / 2) / d : (n + d / 2) / d;
+}
+__device__ __forceinline__ int lg2u(unsigned v) { return v ? 31 - __clz((int)v) : 0; }  // evx_math.h:69-113
+__device__ __forceinline__ int req_bits8(int x) { return lg2u((unsigned)(x & 255)) + 1; }  // required_bits((uint8)x)
+__device__ __forceinline__ int iabs32(int v) { return v == INT_MIN ? INT_MAX : (v < 0 ? -v : v); }
+__device__ __forceinline__ int16_t iabs16(int16_t v) { return v == INT16_MIN ? (int16_t)INT16_MAX : (int16_t)(v < 0 ? -v : v); }
+__device__ __forceinline__ int16_t sgn16(int16_t v) { return (int16_t)((v > 0) - (v < 0)); }
+__device__ __forceinline__ int wmul(int a, int b) { return (int)((unsigned)a * (unsigned)b); }
+__device__ __forceinline__ int16_t tap6(int a, int b, int c, int d, int e, int f)   // interp.cpp:18-41
+{
+    return (int16_t)((a - 5 * b + 20 * c + 20 * d - 5 * e + f + 16) >> 5);
+}
+// cost = (float)a + lambda * (float)b, in that operation order.
+__device__ __forceinline__ float rd_cost(int a, float lambda, unsigned b)
+{
+    return __fadd_rn(__int2float_rn(a), __fmul_rn(lambda, __uint2float_rn(b)));
+}
+
+__device__ __forceinline__ int warp_sum(int v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ int warp_max(int v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ long long warp_sum64(long long v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// acquire / release on a progress word (gpu scope)
+__device__ __forceinline__ int ld_acquire(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v)
+{
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Per-frame parameters shared by all kernels of one encode step.
+struct FrameArgs {
+    int W, H, mbw, mbh;          // aligned context size and MB grid
+    int vis_w, vis_h;            // visible RGB size
+    int type, quality, dpb, ref_fwd, ref_bwd;
+    float lambda;
+    int16_t *planes[4];          // DPB plane sets
+    int16_t *src;                // converted source plane set
+    int16_t *lev;                // quantised level plane set (persistent)
+    evxg_block_desc *bt;         // block table of this frame
+    const evxg_block_desc *prev; // temporal MV predictor table (P frames), else null
+    evxg_sao_info *sao;          // final SAO table
+    float *sao_cost;             // per-MB own-parameter SAO cost (RDO -> merge)
+    const uint8_t *rgb;          // device RGB24 input
+    int *progress;               // per-MB-row progress words (wavefronts)
+    int *counters;               // [0] next MB row, [1] next SAO merge row, [2] next SAO apply row
+    int *error;                  // device error word (0 = ok)
+    long long timeout_ns;        // bound on every spin-wait
+};
+
+}  // namespace evxg

@@ -1,0 +1,1011 @@
+// evxg_mb.cu -- the macroblock wavefront kernel: per-MB mode decision, encode
+// and reconstruction of one EVX3 frame on sm_100a.
+//
+// Reference: src/video/encode.cpp:168-941 (classify_block, classify_block_bidir,
+// encode_block, encode_slice_wpp), src/video/motion.cpp:120-840 (searches),
+// src/video/decode.cpp:31-432 (decode_block), src/video/intra_pred.cpp,
+// src/video/transform.cpp, src/video/quantize.cpp, src/video/interp.cpp.
+//
+// Schedule.  A persistent grid of CTAs claims macroblock rows in order from an
+// atomic counter; a CTA processes its row left to right and, before MB (r,c),
+// waits until row r-1 has finished column min(c+4, cols-1): the reference's
+// WPP lag (encode.cpp:866-877).  With that lag every MB sees exactly the
+// reconstruction the sequential raster encoder sees: all raster-earlier MBs in
+// its search window are finished and no raster-later MB has been written, so
+// the stale pixels the intra block-copy search and the 6-tap overshoot read in
+// the destination DPB slot are the same.  Waits are bounded by a timeout that
+// sets the device error word.
+//
+// Inside an MB, 8 warps evaluate search candidates concurrently (one warp per
+// candidate: 16 lanes do 4x4 luma Hadamard/SAD/MAD, 16 lanes chroma MAD) and
+// one thread replays the reference's order-dependent acceptance rule; sub-pel
+// refinement runs one warp per direction (half and quarter from one 6-tap
+// pass); DCT, quantisation, trellis, dequantisation and IDCT of all RDO
+// candidates run thread-per-line over shared memory.
+#include "evxg_device.cuh"
+
+namespace evxg {
+
+__constant__ int16_t c_lut8[64] = {  // xftables.h:57-67 (cos table x128)
+    128, 128, 128, 128, 128, 128, 128, 128, 126, 106, 71, 25, -25, -71, -106, -126,
+    118, 49, -49, -118, -118, -49, 49, 118, 106, -25, -126, -71, 71, 126, 25, -106,
+    91, -91, -91, 91, 91, -91, -91, 91, 71, -126, 25, 106, -106, -25, 126, -71,
+    49, -118, 118, -49, -49, 118, -118, 49, 25, -71, 106, -126, 126, -106, 71, -25};
+__constant__ int16_t c_qm_intra[64] = {  // quantize.cpp:14-24
+    8, 10, 12, 15, 19, 23, 25, 27, 10, 12, 14, 17, 21, 25, 27, 28, 12, 14, 18, 21, 24, 26, 28, 30,
+    15, 17, 21, 24, 26, 28, 30, 32, 19, 21, 24, 26, 28, 30, 32, 35, 23, 25, 26, 28, 30, 32, 35, 38,
+    25, 27, 28, 30, 32, 35, 38, 41, 27, 28, 30, 32, 35, 38, 41, 45};
+__constant__ int16_t c_qm_inter[64] = {  // quantize.cpp:26-36
+    16, 17, 18, 19, 20, 21, 22, 23, 17, 18, 19, 20, 21, 22, 23, 24, 18, 19, 20, 21, 22, 23, 24, 25,
+    19, 20, 21, 22, 23, 24, 26, 27, 20, 21, 22, 23, 25, 26, 27, 28, 21, 22, 23, 24, 26, 27, 28, 30,
+    22, 23, 24, 26, 27, 28, 30, 31, 23, 24, 25, 27, 28, 30, 31, 33};
+__constant__ uint8_t c_dz_intra[64] = {  // quantize.cpp:42-52
+    0, 1, 1, 1, 1, 1, 2, 2, 1, 1, 1, 1, 1, 2, 2, 2, 1, 1, 1, 1, 2, 2, 2, 2, 1, 1, 1, 2, 2, 2, 2, 3,
+    1, 1, 2, 2, 2, 2, 3, 3, 1, 2, 2, 2, 2, 3, 3, 3, 2, 2, 2, 2, 3, 3, 3, 3, 2, 2, 2, 3, 3, 3, 3, 3};
+__constant__ uint8_t c_dz_inter[64] = {  // quantize.cpp:61-71
+    2, 2, 2, 3, 3, 3, 4, 4, 2, 2, 3, 3, 3, 4, 4, 4, 2, 3, 3, 3, 4, 4, 4, 4, 3, 3, 3, 4, 4, 4, 4, 4,
+    3, 3, 4, 4, 4, 4, 4, 4, 3, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4};
+__constant__ uint8_t c_zigzag[64] = {  // scan.h:60-70
+    0, 1, 8, 16, 9, 2, 3, 10, 17, 24, 32, 25, 18, 11, 4, 5, 12, 19, 26, 33, 40, 48, 41, 34,
+    27, 20, 13, 6, 7, 14, 21, 28, 35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23, 30, 37, 44, 51,
+    58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63};
+
+constexpr int NT = 256;        // threads per CTA
+constexpr int NW = NT / 32;
+constexpr int MB_N = 384;      // 16x16 luma + 2 x 8x8 chroma, MB buffer layout Y | U | V
+constexpr int MAXC = 5;        // RDO candidates (encode.cpp:279-364)
+
+struct Win {
+    int16_t y[WL * WL];
+    int16_t u[WC * WC];
+    int16_t v[WC * WC];
+    int ox, oy, cox, coy;      // origins in plane coordinates
+};
+struct Sel {                   // evx_motion_selection, motion.cpp:53-66
+    int bx, by, sad, mad, ssd;
+    float cost;
+    int sp_index, sp_amount, sp_enabled;
+};
+struct Nbr {                   // intra_pred.cpp:13-54
+    int16_t top[16], left[16];
+    int16_t corner;
+    int ht, hl, dc;
+};
+struct alignas(4) Desc { evxg_block_desc d; };   // 4-aligned so it can be copied as 7 words
+
+struct MbShared {
+    int16_t src[MB_N];
+    Win win[2];
+    int16_t pred[7][MB_N];     // 0 intra-BC, 1 inter/fwd, 2 bwd, 3 bi, 4..6 directional candidates
+    Nbr nb[3];
+    int lx[16], ly[16], n_list;
+    int m_sad[16], m_mad[16], m_satd[16];
+    int sdx[8], sdy[8], n_sp;
+    int spm[8][4];
+    Sel sel;
+    int thr, row_abort;
+    int pmx, pmy, qx, qy, has_pred, cur_win;
+    Desc ibc, fwd, bwd, best, cd[MAXC];
+    int ibc_sad, fwd_sad, bwd_sad, best_sad, ibc_has_pred;
+    int modes[3], dsad[3], dir_best, dir_sad;
+    int bi_sad;
+    int ncand, chosen, rdo;
+    int cpred[MAXC];
+    float cost[MAXC];
+    int16_t coef[MAXC][MB_N], lev[MAXC][MB_N], rec[MAXC][MB_N], tmp[MAXC][MB_N];
+};
+
+// ---------------------------------------------------------------- helpers
+
+__device__ __forceinline__ int mb_index(int b, int r, int c)   // element (r,c) of 8x8 block b of an MB buffer
+{
+    return b < 4 ? (((b >> 1) * 8 + r) * 16 + (b & 1) * 8 + c) : (256 + (b - 4) * 64 + r * 8 + c);
+}
+__device__ __forceinline__ void clear_desc(evxg_block_desc &d)   // common.cpp:76-94
+{
+    d = evxg_block_desc{};
+    d.block_type = INTRA_DEFAULT;
+    d.intra_mode = MODE_NONE;
+}
+__device__ __forceinline__ void dir_from_frac(int f, int &dx, int &dy)   // motion.cpp:93-116
+{
+    if (f <= 2) { dy = -1; dx = f - 1; }
+    else if (f == 3) { dx = -1; dy = 0; }
+    else if (f == 4) { dx = 1; dy = 0; }
+    else { dy = 1; dx = f - 6; }
+}
+__device__ __forceinline__ int frac_from_dir(int i, int j)   // motion.cpp:68-91
+{
+    i++; j++;
+    if (j == 0) return i;
+    if (j == 1) return i == 0 ? 3 : 4;
+    return i + 5;
+}
+
+// Load a clamped search window around luma base (bx, by) from a plane set.
+template <bool kCoherent>
+__device__ void load_window(Win &w, const int16_t *planes, int W, int H, int bx, int by)
+{
+    const int16_t *Y = planes, *U = planes + (size_t)W * H, *V = U + (size_t)(W / 2) * (H / 2);
+    const int cw = W / 2, ch = H / 2;
+    const int ox = bx - WL_OFF, oy = by - WL_OFF, cox = (bx >> 1) - WC_OFF, coy = (by >> 1) - WC_OFF;
+    if (threadIdx.x == 0) { w.ox = ox; w.oy = oy; w.cox = cox; w.coy = coy; }
+    for (int e = threadIdx.x; e < WL * WL; e += NT) {
+        int r = e / WL, c = e - r * WL;
+        int y = min(max(oy + r, 0), H - 1), x = min(max(ox + c, 0), W - 1);
+        const int16_t *p = Y + (size_t)y * W + x;
+        w.y[e] = kCoherent ? __ldcg(p) : __ldg(p);
+    }
+    for (int e = threadIdx.x; e < 2 * WC * WC; e += NT) {
+        int pl = e >= WC * WC, k = e - pl * WC * WC;
+        int r = k / WC, c = k - r * WC;
+        int y = min(max(coy + r, 0), ch - 1), x = min(max(cox + c, 0), cw - 1);
+        const int16_t *p = (pl ? V : U) + (size_t)y * cw + x;
+        (pl ? w.v : w.u)[k] = kCoherent ? __ldcg(p) : __ldg(p);
+    }
+}
+
+// SAD (luma), MAD (Y, U, V) and SATD (luma) of the 16x16 block at plane
+// position (x, y) against the source; one warp.  analysis.h:89-202.
+__device__ void warp_metrics(const int16_t *src, const Win &w, int x, int y, int lane,
+                             int *o_sad, int *o_mad, int *o_satd)
+{
+    int sad = 0, mad = 0, satd = 0;
+    if (lane < 16) {
+        const int lx = x - w.ox, ly = y - w.oy;
+        const int rr = (lane >> 2) * 4, cc = (lane & 3) * 4;
+        int d[16];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                int df = src[(rr + r) * 16 + cc + c] - w.y[(ly + rr + r) * WL + lx + cc + c];
+                int a = iabs32(df);
+                sad += a;
+                mad = max(mad, a);
+                d[r * 4 + c] = (int16_t)df;   // analysis.h:97 stores the difference as int16
+            }
+        int t[16];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {     // hadamard_4x4, analysis.h:44-85
+            int a = d[r * 4], b = d[r * 4 + 1], c = d[r * 4 + 2], e = d[r * 4 + 3];
+            t[r * 4 + 0] = (a + b) + (c + e); t[r * 4 + 1] = (a - b) + (c - e);
+            t[r * 4 + 2] = (a + b) - (c + e); t[r * 4 + 3] = (a - b) - (c - e);
+        }
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            int a = t[c], b = t[4 + c], cc2 = t[8 + c], e = t[12 + c];
+            satd += iabs32((a + b) + (cc2 + e)) + iabs32((a - b) + (cc2 - e)) +
+                    iabs32((a + b) - (cc2 + e)) + iabs32((a - b) - (cc2 - e));
+        }
+    } else {
+        const int k = lane - 16, pl = k >> 3, row = k & 7;
+        const int cx = (x >> 1) - w.cox, cy = (y >> 1) - w.coy;
+        const int16_t *pp = (pl ? w.v : w.u) + (cy + row) * WC + cx;
+        const int16_t *sp = src + 256 + pl * 64 + row * 8;
+#pragma unroll
+        for (int c = 0; c < 8; c++) mad = max(mad, iabs32(sp[c] - pp[c]));
+    }
+    sad = warp_sum(sad);
+    mad = warp_max(mad);
+    satd = warp_sum(satd);
+    if (lane == 0) { *o_sad = sad; *o_mad = mad; *o_satd = (satd + 1) >> 1; }
+}
+
+// One column of a 6-tap half-pel block (interp.cpp:52-164) plus its quarter-pel
+// average, accumulating SAD/MAD against the source column.
+template <int N>
+__device__ __forceinline__ void subpel_column(const int16_t *pl, int S, int bx, int by, int c, int dx, int dy,
+                                              const int16_t *scol, int ss, bool luma,
+                                              int &sad_h, int &mad_h, int &sad_q, int &mad_q,
+                                              int16_t *oh, int16_t *oq, int os)
+{
+    const int xo = dx > 0 ? 0 : -1, yo = dy > 0 ? 0 : -1;
+    int16_t hv[N + 5];
+    if (dx && dy) {
+#pragma unroll
+        for (int t = 0; t < N + 5; t++) {
+            const int16_t *rp = pl + (by + yo + t - 2) * S + bx + c + xo;
+            hv[t] = tap6(rp[-2], rp[-1], rp[0], rp[1], rp[2], rp[3]);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < N; r++) {
+        int16_t half;
+        if (dx && !dy) {
+            const int16_t *rp = pl + (by + r) * S + bx + c + xo;
+            half = tap6(rp[-2], rp[-1], rp[0], rp[1], rp[2], rp[3]);
+        } else if (!dx && dy) {
+            const int16_t *cp = pl + (by + r + yo) * S + bx + c;
+            half = tap6(cp[-2 * S], cp[-S], cp[0], cp[S], cp[2 * S], cp[3 * S]);
+        } else {
+            half = tap6(hv[r], hv[r + 1], hv[r + 2], hv[r + 3], hv[r + 4], hv[r + 5]);
+        }
+        const int full = pl[(by + r) * S + bx + c];
+        const int16_t q = (int16_t)((full + half + 1) >> 1);
+        const int s = scol[r * ss];
+        const int ah = iabs32(s - half), aq = iabs32(s - q);
+        if (luma) { sad_h += ah; sad_q += aq; }
+        mad_h = max(mad_h, ah);
+        mad_q = max(mad_q, aq);
+        if (oh) oh[r * os] = half;
+        if (oq) oq[r * os] = q;
+    }
+}
+
+// Half- and quarter-pel candidate in direction (dx, dy) around integer
+// position (x, y): metrics into out4 = {sad_h, mad_h, sad_q, mad_q}; optionally
+// stores the half (oh) or quarter (oq) block.  One warp, one column per lane.
+__device__ void warp_subpel(const int16_t *src, const Win &w, int x, int y, int dx, int dy, int lane,
+                            int *out4, int16_t *oh, int16_t *oq)
+{
+    int sh = 0, mh = 0, sq = 0, mq = 0;
+    if (lane < 16) {
+        subpel_column<16>(w.y, WL, x - w.ox, y - w.oy, lane, dx, dy, src + lane, 16, true, sh, mh, sq, mq,
+                          oh ? oh + lane : nullptr, oq ? oq + lane : nullptr, 16);
+    } else {
+        const int k = lane - 16, p = k >> 3, c = k & 7;
+        subpel_column<8>(p ? w.v : w.u, WC, (x >> 1) - w.cox, (y >> 1) - w.coy, c, dx, dy, src + 256 + p * 64 + c,
+                         8, false, sh, mh, sq, mq, oh ? oh + 256 + p * 64 + c : nullptr,
+                         oq ? oq + 256 + p * 64 + c : nullptr, 8);
+    }
+    sh = warp_sum(sh); mh = warp_max(mh); sq = warp_sum(sq); mq = warp_max(mq);
+    if (out4 && lane == 0) { out4[0] = sh; out4[1] = mh; out4[2] = sq; out4[3] = mq; }
+}
+
+// Integer candidate acceptance (motion.cpp:148-177), replayed by one thread.
+__device__ void accept_int(Sel &s, int x, int y, int sad, int mad, int satd, int px, int py, int thr, float lambda)
+{
+    const int ssd = (x - px) * (x - px) + (y - py) * (y - py);
+    const int16_t mx = (int16_t)(x - px), my = (int16_t)(y - py);
+    const float cost = rd_cost(satd, lambda, (unsigned)(iabs16(mx) + iabs16(my) + 1));
+    bool take;
+    if (s.mad < thr) take = mad < s.mad || (mad == s.mad && ssd < s.ssd);
+    else take = (cost < s.cost || ((cost == s.cost && ssd < s.ssd) && sad < SAD_THRESHOLD)) || mad < thr;
+    if (take) { s.bx = x; s.by = y; s.sad = sad; s.ssd = ssd; s.mad = mad; s.cost = cost; }
+}
+
+// One pattern step (perform_intra/inter_motion_search, motion.cpp:348-406).
+__device__ void run_step(MbShared &S, const Win &w, bool intra, int l, int t, int r, int b, int st,
+                         int px, int py, int W, int H, float lambda)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        int n = 0;
+        const int bx = S.sel.bx, by = S.sel.by;
+        for (int j = t; j <= b; j += st)
+            for (int i = l; i <= r; i += st) {
+                const int x = bx + i, y = by + j;
+                if (intra && y > py - 16 && x > px - 16) continue;   // not yet reconstructed
+                if (x < 0 || x > W - 16 || y < 0 || y > H - 16) continue;
+                S.lx[n] = x; S.ly[n] = y; n++;
+            }
+        S.n_list = n;
+    }
+    __syncthreads();
+    const int n = S.n_list;
+    for (int k = warp; k < n; k += NW) warp_metrics(S.src, w, S.lx[k], S.ly[k], lane, &S.m_sad[k], &S.m_mad[k], &S.m_satd[k]);
+    __syncthreads();
+    if (tid == 0)
+        for (int k = 0; k < n; k++) {
+            accept_int(S.sel, S.lx[k], S.ly[k], S.m_sad[k], S.m_mad[k], S.m_satd[k], px, py, S.thr, lambda);
+            if (S.sel.mad < S.thr) break;   // early exit on a copy-quality match
+        }
+    __syncthreads();
+}
+
+// Sub-pel refinement around the selection (motion.cpp:180-261, :408-483).
+__device__ void run_subpel(MbShared &S, const Win &w, bool intra, int px, int py, int W, int H)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        S.sel.sp_index = 0; S.sel.sp_amount = 0; S.sel.sp_enabled = 0;
+        int n = 0;
+        for (int j = -1; j <= 1; j++)
+            for (int i = -1; i <= 1; i++) {
+                if (!i && !j) continue;
+                const int x = S.sel.bx + i, y = S.sel.by + j;
+                if (intra && y > py - 16 && x > px - 16) continue;
+                if (x < 0 || x > W - 16 || y < 0 || y > H - 16) continue;
+                S.sdx[n] = i; S.sdy[n] = j; n++;
+            }
+        S.n_sp = n;
+    }
+    __syncthreads();
+    if (warp < S.n_sp) warp_subpel(S.src, w, S.sel.bx, S.sel.by, S.sdx[warp], S.sdy[warp], lane, S.spm[warp], nullptr, nullptr);
+    __syncthreads();
+    if (tid == 0) {
+        Sel &s = S.sel;
+        for (int k = 0; k < S.n_sp; k++)
+            for (int q = 0; q < 2; q++) {
+                const int sad = S.spm[k][q * 2], mad = S.spm[k][q * 2 + 1];
+                const bool take = s.mad < S.thr ? (mad < s.mad)
+                                                : ((sad < s.sad && sad < SAD_THRESHOLD) || mad < S.thr);
+                if (take) {
+                    s.sp_enabled = 1; s.sp_amount = q; s.sp_index = frac_from_dir(S.sdx[k], S.sdy[k]);
+                    s.sad = sad; s.mad = mad;
+                }
+            }
+    }
+    __syncthreads();
+}
+
+// Prediction block of a search result into out: integer block or half/quarter-pel.
+__device__ void materialize(const MbShared &S, const Win &w, int x, int y, int spp, int spa, int spi, int16_t *out)
+{
+    const int tid = threadIdx.x;
+    if (spp) {
+        if ((tid >> 5) == 0) {
+            int dx, dy;
+            dir_from_frac(spi, dx, dy);
+            warp_subpel(S.src, w, x, y, dx, dy, tid & 31, nullptr, spa ? nullptr : out, spa ? out : nullptr);
+        }
+    } else {
+        const int lx = x - w.ox, ly = y - w.oy;
+        out[tid] = w.y[(ly + (tid >> 4)) * WL + lx + (tid & 15)];
+        if (tid < 128) {
+            const int p = tid >> 6, k = tid & 63;
+            const int cx = (x >> 1) - w.cox, cy = (y >> 1) - w.coy;
+            out[256 + tid] = (p ? w.v : w.u)[(cy + (k >> 3)) * WC + cx + (k & 7)];
+        }
+    }
+}
+
+__device__ void fill_desc(const Sel &s, int px, int py, bool intra, int thr, evxg_block_desc &o)   // motion.cpp:542-564
+{
+    clear_desc(o);
+    o.block_type = intra ? BT_INTRA : 0;
+    if (s.bx != px || s.by != py || s.sp_enabled) o.block_type |= BT_MOTION;
+    if (s.mad < thr) o.block_type |= BT_COPY;
+    o.motion_x = (int16_t)(s.bx - px);
+    o.motion_y = (int16_t)(s.by - py);
+    o.sp_pred = (uint8_t)s.sp_enabled;
+    o.sp_amount = (uint8_t)s.sp_amount;
+    o.sp_index = (uint8_t)s.sp_index;
+}
+
+// Directional intra predictor value at (x, y) of an N x N block (intra_pred.cpp:60-174).
+__device__ __forceinline__ int16_t intra_px(int mode, const Nbr &nb, int n, int x, int y)
+{
+    auto ref = [&](int i) -> int { return i < n ? nb.left[n - 1 - i] : (i == n ? nb.corner : nb.top[i - n - 1]); };
+    switch (mode) {
+    case 0: return (int16_t)nb.dc;
+    case 1: return nb.top[x];
+    case 2: return nb.left[y];
+    case 3: {
+        const int k = x + y;
+        return (int16_t)((nb.top[min(k, n - 1)] + 2 * nb.top[min(k + 1, n - 1)] + nb.top[min(k + 2, n - 1)] + 2) >> 2);
+    }
+    case 4: { const int d = x - y + n; return (int16_t)((ref(d - 1) + 2 * ref(d) + ref(d + 1) + 2) >> 2); }
+    case 5: {
+        const int d = min(max(x - (y >> 1) + n, 1), 2 * n - 1);
+        return (y & 1) ? (int16_t)((ref(d - 1) + 2 * ref(d) + ref(d + 1) + 2) >> 2) : (int16_t)((ref(d) + ref(d + 1) + 1) >> 1);
+    }
+    case 6: {
+        const int d = min(max((x >> 1) - y + n, 1), 2 * n - 1);
+        return (x & 1) ? (int16_t)((ref(d - 1) + 2 * ref(d) + ref(d + 1) + 2) >> 2) : (int16_t)((ref(d) + ref(d + 1) + 1) >> 1);
+    }
+    default: return 128;
+    }
+}
+
+// --------------------------------------------------- transform / quantisation
+
+__device__ __forceinline__ int16_t luma_dc_scale(int qp)   // quantize.cpp:74-83
+{
+    if (qp < 5) return (int16_t)max(qp << 1, 2);
+    if (qp < 9) return (int16_t)(qp << 1);
+    if (qp < 25) return (int16_t)(qp + 8);
+    return (int16_t)((qp << 1) - 16);
+}
+__device__ __forceinline__ int16_t chroma_dc_scale(int qp)   // quantize.cpp:85-92
+{
+    if (qp < 5) return (int16_t)max(qp << 1, 2);
+    if (qp < 25) return (int16_t)((qp + 13) >> 1);
+    return (int16_t)(qp - 6);
+}
+__device__ __forceinline__ int16_t quant_coeff(int16_t sv, int qp, int o, bool intra, bool chroma)   // quantize.cpp:120-252
+{
+    if (intra) {
+        if (o == 0) return (int16_t)rdiv(sv, chroma ? chroma_dc_scale(qp) : luma_dc_scale(qp));
+        int16_t qf = (int16_t)rdiv(sv * 16, c_qm_intra[o]);
+        if (qp >= 16) qf = (int16_t)(qf - (int16_t)((sgn16(qf) * qp * c_dz_intra[o]) >> 1));
+        return (int16_t)rdiv(qf, qp << 1);
+    }
+    const int16_t qf = (int16_t)rdiv(sv * 16, c_qm_inter[o]);
+    int wgt = c_dz_inter[o];
+    if (qp >= 16) wgt = min(wgt + 1, 6);
+    const int16_t dz = (int16_t)((sgn16(qf) * qp * wgt) >> 1);
+    return (int16_t)rdiv(qf - dz, qp << 1);
+}
+__device__ __forceinline__ int16_t dequant_coeff(int16_t lv, int qp, int o, bool intra, bool chroma)   // quantize.cpp:271-332
+{
+    if (intra && o == 0) return (int16_t)(lv * (chroma ? chroma_dc_scale(qp) : luma_dc_scale(qp)));
+    return (int16_t)((2 * lv * (intra ? c_qm_intra[o] : c_qm_inter[o]) * qp) / 16);
+}
+__device__ __forceinline__ unsigned coeff_bits(int16_t lv)   // quantize.cpp:517-532
+{
+    if (lv == 0) return 1;
+    const int a = min((int)iabs16(lv), 255);
+    unsigned b = 2;
+    if (a > 1) b += 1;
+    if (a > 2) b += 1 + 2 * req_bits8(a - 3 + 1);
+    else b += 1;
+    return b;
+}
+__device__ __forceinline__ int scan_pos(int mode, int p)   // scan.h:125-159
+{
+    if (mode == 1 || mode == 5) return p;
+    if (mode == 2 || mode == 6) return (p & 7) * 8 + (p >> 3);
+    return c_zigzag[p];
+}
+// forward 8-point line (transform.cpp:264-284)
+__device__ __forceinline__ void fdct8_line(const int in[8], int16_t out[8])
+{
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        int t = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) t += in[k] * c_lut8[i * 8 + k];
+        t = i == 0 ? (t * 45) / 128 : t / 2;
+        out[i] = (int16_t)rdiv(t, 128);
+    }
+}
+// inverse 8-point line, per-term truncation (transform.cpp:330-349)
+__device__ __forceinline__ void idct8_line(const int in[8], int out[8])
+{
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        int t = ((in[0] * c_lut8[i]) * 45) / 128;
+#pragma unroll
+        for (int k = 1; k < 8; k++) t += (in[k] * c_lut8[k * 8 + i]) / 2;
+        out[i] = rdiv(t, 128);
+    }
+}
+__device__ __forceinline__ bool intra_quant(int bt) { return (bt & BT_INTRA) && !(bt & BT_MOTION); }   // quantize.cpp:457
+
+// Trellis of one 8x8 block (quantize.cpp:536-613) in place on an MB buffer.
+__device__ void trellis_block(int16_t *lev, const int16_t *coef, int b, int qp, bool intra, int mode, float lambda)
+{
+    const bool chroma = b >= 4;
+    int last = -1;
+    for (int p = 63; p >= 0; p--) {
+        const int o = scan_pos(mode, p);
+        if (lev[mb_index(b, o >> 3, o & 7)]) { last = p; break; }
+    }
+    if (last < 0) return;
+    for (int p = last; p >= 1; p--) {
+        const int o = scan_pos(mode, p), e = mb_index(b, o >> 3, o & 7);
+        const int16_t l = lev[e];
+        if (!l) continue;
+        const int dk = (int)coef[e] - (int)dequant_coeff(l, qp, o, intra, chroma), dz = coef[e];
+        const float ck = __fadd_rn(__int2float_rn(wmul(dk, dk)), __fmul_rn(lambda, __uint2float_rn(coeff_bits(l))));
+        const float cz = __fadd_rn(__int2float_rn(wmul(dz, dz)), __fmul_rn(lambda, __uint2float_rn(coeff_bits(0))));
+        if (cz <= ck) lev[e] = 0;
+        else break;
+    }
+    last = -1;
+    for (int p = 63; p >= 0; p--) {
+        const int o = scan_pos(mode, p);
+        if (lev[mb_index(b, o >> 3, o & 7)]) { last = p; break; }
+    }
+    if (last < 0) return;
+    for (int p = 1; p <= last; p++) {
+        const int o = scan_pos(mode, p), e = mb_index(b, o >> 3, o & 7);
+        const int16_t l = lev[e];
+        if (!l) continue;
+        const int16_t rl = (int16_t)(l - sgn16(l));
+        const int dk = (int)coef[e] - (int)dequant_coeff(l, qp, o, intra, chroma);
+        const int dr = (int)coef[e] - (int)dequant_coeff(rl, qp, o, intra, chroma);
+        const float ck = __fadd_rn(__int2float_rn(wmul(dk, dk)), __fmul_rn(lambda, __uint2float_rn(coeff_bits(l))));
+        const float cr = __fadd_rn(__int2float_rn(wmul(dr, dr)), __fmul_rn(lambda, __uint2float_rn(coeff_bits(rl))));
+        if (cr < ck) lev[e] = rl;
+    }
+}
+
+// encode_block + decode_block for S.ncand candidates (encode.cpp:481-750,
+// decode.cpp:31-432); with S.rdo set also the RD cost (encode.cpp:39-164).
+__device__ void encode_candidates(MbShared &S, const FrameArgs &a)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nc = S.ncand;
+    // forward DCT, rows (thread per candidate x block x row)
+    if (tid < nc * 48) {
+        const int k = tid / 48, rem = tid - k * 48, b = rem >> 3, r = rem & 7;
+        if (!(S.cd[k].d.block_type & BT_COPY)) {
+            const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
+            int in[8];
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                const int e = mb_index(b, r, c);
+                in[c] = (int16_t)(pr ? S.src[e] - pr[e] : S.src[e]);
+            }
+            int16_t out[8];
+            fdct8_line(in, out);
+#pragma unroll
+            for (int c = 0; c < 8; c++) S.tmp[k][mb_index(b, r, c)] = out[c];
+        }
+    }
+    __syncthreads();
+    if (tid < nc * 48) {   // columns
+        const int k = tid / 48, rem = tid - k * 48, b = rem >> 3, c = rem & 7;
+        if (!(S.cd[k].d.block_type & BT_COPY)) {
+            int in[8];
+#pragma unroll
+            for (int r = 0; r < 8; r++) in[r] = S.tmp[k][mb_index(b, r, c)];
+            int16_t out[8];
+            fdct8_line(in, out);
+#pragma unroll
+            for (int r = 0; r < 8; r++) S.coef[k][mb_index(b, r, c)] = out[r];
+        }
+    }
+    __syncthreads();
+    // adaptive QP from the luma coefficients' variance (quantize.cpp:97-118, analysis.h:251-275)
+    if (warp < nc && !(S.cd[warp].d.block_type & BT_COPY)) {
+        unsigned sum = 0, sq = 0, cnt = 0;
+        for (int e = lane; e < 256; e += 32) {
+            if (e == 0) continue;
+            const int t = S.coef[warp][e];
+            if (t) { sum += (unsigned)t; sq += (unsigned)wmul(t, t); cnt++; }
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            sq += __shfl_xor_sync(0xffffffffu, sq, o);
+            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        }
+        if (lane == 0) {
+            const int var = cnt > 0 ? (int)(sq - (unsigned)rdiv(wmul((int)sum, (int)sum), (int)cnt)) : 0;
+            const int idx = min(max(lg2u((unsigned)var) >> 1, 1), MAXQ);
+            int delta = (int16_t)((int16_t)idx - (int16_t)a.quality) >> 1;
+            delta = min(max(delta, -6), 6);
+            S.cd[warp].d.q_index = (uint8_t)min(max(a.quality + delta, 1), MAXQ);
+            S.cd[warp].d.variance = (int16_t)var;
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < nc * MB_N; e += NT) {   // quantise
+        const int k = e / MB_N, p = e - k * MB_N;
+        const int bt = S.cd[k].d.block_type;
+        if (bt & BT_COPY) continue;
+        const bool chroma = p >= 256;
+        const int qp = chroma ? min(S.cd[k].d.q_index + 2, MAXQ) : S.cd[k].d.q_index;
+        const int o = chroma ? (p & 63) : (((p >> 4) & 7) * 8 + (p & 7));
+        S.lev[k][p] = quant_coeff(S.coef[k][p], qp, o, intra_quant(bt), chroma);
+    }
+    __syncthreads();
+    if (tid < nc * 6) {   // trellis, one thread per 8x8 block
+        const int k = tid / 6, b = tid - k * 6;
+        const int bt = S.cd[k].d.block_type;
+        if (!(bt & BT_COPY)) {
+            const int qp = b >= 4 ? min(S.cd[k].d.q_index + 2, MAXQ) : S.cd[k].d.q_index;
+            trellis_block(S.lev[k], S.coef[k], b, qp, intra_quant(bt), S.cd[k].d.intra_mode, a.lambda);
+        }
+    }
+    __syncthreads();
+    if (tid < nc * 48) {   // dequantise + inverse DCT, columns
+        const int k = tid / 48, rem = tid - k * 48, b = rem >> 3, c = rem & 7;
+        const int bt = S.cd[k].d.block_type;
+        if (!(bt & BT_COPY)) {
+            const int qp = b >= 4 ? min(S.cd[k].d.q_index + 2, MAXQ) : S.cd[k].d.q_index;
+            int in[8], out[8];
+#pragma unroll
+            for (int r = 0; r < 8; r++) in[r] = dequant_coeff(S.lev[k][mb_index(b, r, c)], qp, r * 8 + c, intra_quant(bt), b >= 4);
+            idct8_line(in, out);
+#pragma unroll
+            for (int r = 0; r < 8; r++) S.tmp[k][mb_index(b, r, c)] = (int16_t)out[r];
+        }
+    }
+    __syncthreads();
+    if (tid < nc * 48) {   // inverse DCT rows + prediction
+        const int k = tid / 48, rem = tid - k * 48, b = rem >> 3, r = rem & 7;
+        const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
+        if (S.cd[k].d.block_type & BT_COPY) {
+#pragma unroll
+            for (int c = 0; c < 8; c++) S.rec[k][mb_index(b, r, c)] = pr ? pr[mb_index(b, r, c)] : (int16_t)0;
+        } else {
+            int in[8], out[8];
+#pragma unroll
+            for (int c = 0; c < 8; c++) in[c] = S.tmp[k][mb_index(b, r, c)];
+            idct8_line(in, out);
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                const int e = mb_index(b, r, c);
+                S.rec[k][e] = (int16_t)(pr ? out[c] + pr[e] : out[c]);
+            }
+        }
+    }
+    __syncthreads();
+    if (S.rdo && warp < nc) {   // J = (float)SSD_y + lambda * (float)bits
+        const evxg_block_desc &d = S.cd[warp].d;
+        const int bt = d.block_type;
+        int ssd = 0;
+        for (int e = lane; e < 256; e += 32) {
+            const int df = S.src[e] - S.rec[warp][e];
+            ssd = (int)((unsigned)ssd + (unsigned)wmul(df, df));
+        }
+        ssd = warp_sum(ssd);
+        // Rate of the residual: the reference's quantised and reconstructed
+        // blocks share one staging buffer (encode.cpp:151, :158), so the
+        // estimate reads the reconstruction.
+        unsigned nz = 0, cb = 0;
+        if (!(bt & BT_COPY)) {
+            const int b = lane >> 3, r = lane & 7;
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                const int16_t v = S.rec[warp][mb_index(b, r, c)];
+                if (v) {
+                    nz++;
+                    const int av = min((int)iabs16(v), 255);
+                    cb += 2;
+                    if (av > 1) cb += 1;
+                    if (av > 2) cb += 1 + 2 * req_bits8(av - 3 + 1);
+                    else cb += 1;
+                }
+            }
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1) {
+                nz += __shfl_xor_sync(0xffffffffu, nz, o);
+                cb += __shfl_xor_sync(0xffffffffu, cb, o);
+            }
+        }
+        unsigned blkbits = ((lane & 7) == 0 && !(bt & BT_COPY)) ? (unsigned)(req_bits8(nz + 1) * 2 + 1) + cb : 0;
+        blkbits += __shfl_xor_sync(0xffffffffu, blkbits, 8);
+        blkbits += __shfl_xor_sync(0xffffffffu, blkbits, 16);
+        if (lane == 0) {   // estimate_block_bits header part (encode.cpp:39-78)
+            unsigned bits = 3;
+            if (!(bt & BT_INTRA)) bits += 2;
+            if (bt & BT_MOTION) {
+                bits += 2 * req_bits8(iabs16(d.motion_x) + 1) + 2 * req_bits8(iabs16(d.motion_y) + 1);
+                bits += d.sp_pred ? 5 : 1;
+            }
+            if (!(bt & BT_COPY)) {
+                if (bt == INTRA_DEFAULT) bits += 3;
+                bits += 2 * req_bits8(iabs32(d.q_index) + 1);
+                bits += blkbits;
+            }
+            S.cost[warp] = rd_cost(ssd, a.lambda, bits);
+        }
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------------- searches
+
+// Intra block-copy search in the current frame (motion.cpp:485-565).
+__device__ void intra_bc_search(MbShared &S, const FrameArgs &a, int px, int py)
+{
+    const int tid = threadIdx.x;
+    const Win &w = S.win[0];
+    if (tid < 32) {   // best_sad starts at the source's own SAD (analysis.h:133-145)
+        int s = 0;
+        for (int e = tid; e < 256; e += 32) s += iabs16(S.src[e]);
+        s = warp_sum(s);
+        if (tid == 0) {
+            S.sel.bx = px; S.sel.by = py; S.sel.sad = s; S.sel.mad = INT_MAX; S.sel.ssd = INT_MAX;
+            S.sel.cost = __int2float_rn(s); S.sel.sp_index = 0; S.sel.sp_amount = 0; S.sel.sp_enabled = 0;
+        }
+    }
+    __syncthreads();
+    run_step(S, w, true, -SEARCH_RADIUS, -(SEARCH_RADIUS << 1), SEARCH_RADIUS, 0, SEARCH_RADIUS, px, py, a.W, a.H, a.lambda);
+    if (S.sel.mad >= S.thr)
+        for (int st = SEARCH_RADIUS >> 1; st > 0; st >>= 1) {
+            run_step(S, w, true, -st, -st, st, st, st, px, py, a.W, a.H, a.lambda);
+            if (S.sel.mad < S.thr) break;
+        }
+    run_subpel(S, w, true, px, py, a.W, a.H);
+    if (tid == 0) {
+        fill_desc(S.sel, px, py, true, S.thr, S.ibc.d);
+        S.ibc_sad = S.sel.sad;
+        S.ibc_has_pred = (S.ibc.d.block_type & BT_MOTION) != 0;
+    }
+    __syncthreads();
+    if (S.ibc_has_pred) materialize(S, w, S.sel.bx, S.sel.by, S.sel.sp_enabled, S.sel.sp_amount, S.sel.sp_index, S.pred[0]);
+    __syncthreads();
+}
+
+// MV predictor (motion.cpp:271-346) from the live block table and, for P
+// frames, the previous frame's table.
+__device__ void mv_predictor(const FrameArgs &a, int idx, bool temporal, int &ox, int &oy)
+{
+    const int mbw = a.mbw, bx = idx % mbw, by = idx / mbw;
+    int mx[3], my[3], n = 0;
+    auto motion = [&](int i) { return (__ldcg(&a.bt[i].block_type) & BT_MOTION) != 0; };
+    auto take = [&](int i) { mx[n] = __ldcg(&a.bt[i].motion_x); my[n] = __ldcg(&a.bt[i].motion_y); n++; };
+    if (bx > 0 && motion(idx - 1)) take(idx - 1);
+    if (by > 0 && motion(idx - mbw)) take(idx - mbw);
+    if (by > 0 && bx + 1 < mbw && motion(idx - mbw + 1)) take(idx - mbw + 1);
+    else if (by > 0 && bx > 0 && motion(idx - mbw - 1)) take(idx - mbw - 1);
+    if (n < 3 && temporal && (a.prev[idx].block_type & BT_MOTION)) { mx[n] = a.prev[idx].motion_x; my[n] = a.prev[idx].motion_y; n++; }
+    if (n == 0) { ox = 0; oy = 0; }
+    else if (n == 1) { ox = mx[0]; oy = my[0]; }
+    else if (n == 2) { ox = (int16_t)((mx[0] + mx[1]) / 2); oy = (int16_t)((my[0] + my[1]) / 2); }
+    else {
+        int v[2];
+        for (int k = 0; k < 2; k++) {
+            int p = k ? my[0] : mx[0], q = k ? my[1] : mx[1], r = k ? my[2] : mx[2], t;
+            if (p > q) { t = p; p = q; q = t; }
+            if (q > r) q = r;
+            if (p > q) q = p;
+            v[k] = q;
+        }
+        ox = v[0]; oy = v[1];
+    }
+}
+
+// Inter search against one DPB slot (motion.cpp:567-679); result descriptor,
+// SAD and prediction block.
+__device__ void inter_search(MbShared &S, const FrameArgs &a, int slot, bool temporal, int px, int py, int idx,
+                             evxg_block_desc &out, int &out_sad, int16_t *pred_out)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        int pmx, pmy;
+        mv_predictor(a, idx, temporal, pmx, pmy);
+        S.has_pred = (pmx || pmy);
+        int qx = min(max(px + pmx, 0), a.W - 16), qy = min(max(py + pmy, 0), a.H - 16);
+        S.qx = qx; S.qy = qy;
+        S.cur_win = 0;
+    }
+    __syncthreads();
+    const bool sep = S.has_pred && (S.qx != px || S.qy != py);
+    load_window<false>(S.win[0], a.planes[slot], a.W, a.H, px, py);
+    if (sep) load_window<false>(S.win[1], a.planes[slot], a.W, a.H, S.qx, S.qy);
+    __syncthreads();
+    if (warp == 0) warp_metrics(S.src, S.win[0], px, py, lane, &S.m_sad[0], &S.m_mad[0], &S.m_satd[0]);
+    if (warp == 1 && S.has_pred) warp_metrics(S.src, S.win[sep ? 1 : 0], S.qx, S.qy, lane, &S.m_sad[1], &S.m_mad[1], &S.m_satd[1]);
+    __syncthreads();
+    if (tid == 0) {
+        Sel &s = S.sel;
+        s.bx = px; s.by = py; s.sad = S.m_sad[0]; s.mad = S.m_mad[0]; s.ssd = INT_MAX;
+        s.cost = rd_cost(S.m_satd[0], a.lambda, 1u);
+        s.sp_index = 0; s.sp_amount = 0; s.sp_enabled = 0;
+        if (S.has_pred) accept_int(s, S.qx, S.qy, S.m_sad[1], S.m_mad[1], S.m_satd[1], px, py, S.thr, a.lambda);
+        S.cur_win = (sep && s.bx == S.qx && s.by == S.qy) ? 1 : 0;
+    }
+    __syncthreads();
+    const Win &w = S.win[S.cur_win];
+    if (S.sel.mad >= S.thr) {
+        int r = SEARCH_RADIUS;   // adaptive radius, motion.cpp:640-646
+        if (S.sel.sad < SAD_THRESHOLD / 4) r = SEARCH_RADIUS / 4;
+        else if (S.sel.sad < SAD_THRESHOLD / 2) r = SEARCH_RADIUS / 2;
+        for (int st = r; st > 0; st >>= 1) {
+            run_step(S, w, false, -st, -st, st, st, st, px, py, a.W, a.H, a.lambda);
+            if (S.sel.mad < S.thr) break;
+        }
+        run_subpel(S, w, false, px, py, a.W, a.H);
+    }
+    materialize(S, w, S.sel.bx, S.sel.by, S.sel.sp_enabled, S.sel.sp_amount, S.sel.sp_index, pred_out);
+    if (tid == 0) {
+        fill_desc(S.sel, px, py, false, S.thr, out);
+        out_sad = S.sel.sad;
+    }
+    __syncthreads();
+}
+
+// Neighbours of the MB for directional intra, from the intra window (base (px, py-16)).
+__device__ void extract_neighbours(MbShared &S, int px, int py)
+{
+    const int tid = threadIdx.x;
+    const Win &w = S.win[0];
+    if (tid < 3) {
+        Nbr &nb = S.nb[tid];
+        const int n = tid ? 8 : 16;
+        const int16_t *pl = tid == 0 ? w.y : (tid == 1 ? w.u : w.v);
+        const int S_ = tid ? WC : WL;
+        const int trow = tid ? 26 : 49, tcol = tid ? 19 : 34;   // window coordinates of (cy-1, cx)
+        nb.ht = py > 0; nb.hl = px > 0;
+        for (int i = 0; i < n; i++) {
+            nb.top[i] = nb.ht ? pl[trow * S_ + tcol + i] : (int16_t)128;
+            nb.left[i] = nb.hl ? pl[(trow + 1 + i) * S_ + tcol - 1] : (int16_t)128;
+        }
+        if (nb.ht && nb.hl) nb.corner = pl[trow * S_ + tcol - 1];
+        else if (nb.ht) nb.corner = nb.top[0];
+        else if (nb.hl) nb.corner = nb.left[0];
+        else nb.corner = 128;
+        int sum = 0, cnt = 0;
+        if (nb.ht) { for (int i = 0; i < n; i++) sum += nb.top[i]; cnt += n; }
+        if (nb.hl) { for (int i = 0; i < n; i++) sum += nb.left[i]; cnt += n; }
+        nb.dc = cnt > 0 ? (int16_t)((sum + cnt / 2) / cnt) : 128;
+    }
+    __syncthreads();
+    if (tid == 0) {   // gradient-pruned candidates (intra_pred.cpp:225-260)
+        const Nbr &nb = S.nb[0];
+        int gh = 0, gv = 0;
+        if (nb.ht) for (int i = 1; i < 16; i++) gh += iabs32(nb.top[i] - nb.top[i - 1]);
+        if (nb.hl) for (int i = 1; i < 16; i++) gv += iabs32(nb.left[i] - nb.left[i - 1]);
+        S.modes[0] = 0;
+        if (gv > gh * 3 / 2) { S.modes[1] = 2; S.modes[2] = 6; }
+        else if (gh > gv * 3 / 2) { S.modes[1] = 1; S.modes[2] = 5; }
+        else { S.modes[1] = 3; S.modes[2] = 4; }
+    }
+    __syncthreads();
+}
+
+// Directional intra: 3 predictions and the best by luma SAD (intra_pred.cpp:219-289).
+__device__ void directional_intra(MbShared &S)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int e = tid; e < 3 * MB_N; e += NT) {
+        const int m = e / MB_N, p = e - m * MB_N;
+        int16_t v;
+        if (p < 256) v = intra_px(S.modes[m], S.nb[0], 16, p & 15, p >> 4);
+        else { const int q = p - 256, pl = q >> 6, k = q & 63; v = intra_px(S.modes[m], S.nb[1 + pl], 8, k & 7, k >> 3); }
+        S.pred[4 + m][p] = v;
+    }
+    __syncthreads();
+    if (warp < 3) {
+        int s = 0;
+        for (int e = lane; e < 256; e += 32) s += iabs32(S.src[e] - S.pred[4 + warp][e]);
+        s = warp_sum(s);
+        if (lane == 0) S.dsad[warp] = s;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int best = INT_MAX, bm = 0;
+        for (int m = 0; m < 3; m++) if (S.dsad[m] < best) { best = S.dsad[m]; bm = m; }
+        S.dir_best = bm; S.dir_sad = best;
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------------- per MB
+
+__device__ void process_mb(MbShared &S, const FrameArgs &a, int row, int col)
+{
+    const int tid = threadIdx.x;
+    const int px = col * 16, py = row * 16, idx = row * a.mbw + col;
+    const int16_t *srcY = a.src, *srcU = a.src + (size_t)a.W * a.H, *srcV = srcU + (size_t)(a.W / 2) * (a.H / 2);
+    int16_t *dst = a.planes[a.dpb];
+
+    S.src[tid] = __ldg(srcY + (size_t)(py + (tid >> 4)) * a.W + px + (tid & 15));
+    if (tid < 128) {
+        const int pl = tid >> 6, k = tid & 63;
+        S.src[256 + tid] = __ldg((pl ? srcV : srcU) + (size_t)((py >> 1) + (k >> 3)) * (a.W / 2) + (px >> 1) + (k & 7));
+    }
+    if (tid == 0) S.thr = (a.quality >> 2) + 1;   // mad_skip_threshold, motion.cpp:501
+    load_window<true>(S.win[0], dst, a.W, a.H, px, py - 16);
+    __syncthreads();
+    extract_neighbours(S, px, py);
+    intra_bc_search(S, a, px, py);
+
+    if (a.type == EVXG_FRAME_INTER) {
+        inter_search(S, a, a.ref_fwd, true, px, py, idx, S.fwd.d, S.fwd_sad, S.pred[1]);
+    } else if (a.type == EVXG_FRAME_BIDIR) {
+        inter_search(S, a, a.ref_fwd, false, px, py, idx, S.fwd.d, S.fwd_sad, S.pred[1]);
+        inter_search(S, a, a.ref_bwd, false, px, py, idx, S.bwd.d, S.bwd_sad, S.pred[2]);
+        // bi-prediction: (f + b + 1) >> 1, SAD over Y, U and V (motion.cpp:778-813)
+        int s = 0;
+        for (int e = tid; e < MB_N; e += NT) {
+            const int av = (S.pred[1][e] + S.pred[2][e] + 1) >> 1;
+            S.pred[3][e] = (int16_t)av;
+            s += iabs32(S.src[e] - av);
+        }
+        s = warp_sum(s);
+        if ((tid & 31) == 0) S.m_sad[tid >> 5] = s;
+        __syncthreads();
+        if (tid == 0) {
+            int t = 0;
+            for (int k = 0; k < NW; k++) t += S.m_sad[k];
+            S.bi_sad = t;
+        }
+    }
+    directional_intra(S);
+
+    if (tid == 0) {   // candidate decision (encode.cpp:168-277, :374-470)
+        evxg_block_desc best = S.ibc.d;
+        int bsad = S.ibc_sad, bpred = S.ibc_has_pred ? 0 : -1;
+        if (a.type == EVXG_FRAME_INTER) {
+            evxg_block_desc in = S.fwd.d;
+            in.prediction_target = (uint8_t)a.ref_fwd;
+            const bool ci = in.block_type & BT_COPY, cb = best.block_type & BT_COPY;
+            if (ci != cb) { if (ci) { best = in; bsad = S.fwd_sad; bpred = 1; } }
+            else if (S.fwd_sad < bsad) { best = in; bsad = S.fwd_sad; bpred = 1; }
+        } else if (a.type == EVXG_FRAME_BIDIR) {
+            evxg_block_desc f = S.fwd.d, b = S.bwd.d;
+            f.prediction_mode = 0; f.prediction_target = (uint8_t)a.ref_fwd;
+            b.prediction_mode = 1; b.prediction_target = (uint8_t)a.ref_bwd;
+            if (S.fwd_sad < bsad) { best = f; bsad = S.fwd_sad; bpred = 1; }
+            if (S.bwd_sad < bsad) { best = b; bsad = S.bwd_sad; bpred = 2; }
+            const int bias = __float2int_rz(__fmul_rn(a.lambda, 8.0f));
+            if (S.bi_sad + bias < bsad) {
+                evxg_block_desc bi;
+                clear_desc(bi);
+                bi.block_type = INTER_MOTION_DELTA; bi.prediction_mode = 2;
+                bi.prediction_target = (uint8_t)a.ref_fwd;
+                bi.motion_x = f.motion_x; bi.motion_y = f.motion_y;
+                bi.sp_pred = f.sp_pred; bi.sp_amount = f.sp_amount; bi.sp_index = f.sp_index;
+                bi.prediction_target_b = (uint8_t)a.ref_bwd;
+                bi.motion_x_b = b.motion_x; bi.motion_y_b = b.motion_y;
+                bi.sp_pred_b = b.sp_pred; bi.sp_amount_b = b.sp_amount; bi.sp_index_b = b.sp_index;
+                best = bi; bsad = S.bi_sad; bpred = 3;
+            }
+        }
+        if (S.dir_sad < bsad) {
+            clear_desc(best);
+            best.intra_mode = (uint8_t)S.modes[S.dir_best];
+            bsad = S.dir_sad;
+            bpred = 4 + S.dir_best;
+        }
+        int n = 0;
+        S.cd[n].d = best; S.cpred[n++] = bpred;
+        S.rdo = (a.type == EVXG_FRAME_INTER);
+        if (S.rdo) {   // RDO candidates (encode.cpp:279-364)
+            if (best.block_type != INTRA_DEFAULT) { clear_desc(S.cd[n].d); S.cpred[n++] = -1; }
+            for (int m = 0; m < 3; m++) { clear_desc(S.cd[n].d); S.cd[n].d.intra_mode = (uint8_t)S.modes[m]; S.cpred[n++] = 4 + m; }
+        }
+        S.ncand = n;
+    }
+    __syncthreads();
+    encode_candidates(S, a);
+    if (tid == 0) {
+        int ch = 0;
+        if (S.rdo)
+            for (int k = 1; k < S.ncand; k++) if (S.cost[k] < S.cost[ch]) ch = k;
+        S.chosen = ch;
+    }
+    __syncthreads();
+    // write-back: reconstruction into the DPB slot, levels (non-copy), descriptor
+    const int ch = S.chosen;
+    const bool copy = S.cd[ch].d.block_type & BT_COPY;
+    int16_t *dU = dst + (size_t)a.W * a.H, *dV = dU + (size_t)(a.W / 2) * (a.H / 2);
+    int16_t *lY = a.lev, *lU = a.lev + (size_t)a.W * a.H, *lV = lU + (size_t)(a.W / 2) * (a.H / 2);
+    {
+        const size_t o = (size_t)(py + (tid >> 4)) * a.W + px + (tid & 15);
+        dst[o] = S.rec[ch][tid];
+        if (!copy) lY[o] = S.lev[ch][tid];
+        if (tid < 128) {
+            const int pl = tid >> 6, k = tid & 63;
+            const size_t oc = (size_t)((py >> 1) + (k >> 3)) * (a.W / 2) + (px >> 1) + (k & 7);
+            (pl ? dV : dU)[oc] = S.rec[ch][256 + tid];
+            if (!copy) (pl ? lV : lU)[oc] = S.lev[ch][256 + tid];
+        }
+        if (tid < 7) reinterpret_cast<int *>(a.bt + idx)[tid] = reinterpret_cast<const int *>(&S.cd[ch].d)[tid];
+    }
+    __threadfence();   // every writer orders its stores before the row's progress release
+}
+
+__global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MbShared &S = *reinterpret_cast<MbShared *>(smem_raw);
+    __shared__ int s_row;
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_row = atomicAdd(&a.counters[0], 1);
+        __syncthreads();
+        const int row = s_row;
+        if (row >= a.mbh) return;
+        for (int col = 0; col < a.mbw; ++col) {
+            if (tid == 0) {
+                S.row_abort = 0;
+                if (row > 0) {   // WPP dependency: row above finished column min(c+4, cols-1)
+                    const int need = min(col + 4, a.mbw - 1);
+                    const unsigned long long t0 = globaltimer_ns();
+                    while (ld_acquire(&a.progress[row - 1]) < need) {
+                        if (*(volatile int *)a.error) { S.row_abort = 1; break; }
+                        if ((long long)(globaltimer_ns() - t0) > a.timeout_ns) {
+                            atomicCAS(a.error, 0, EVXG_ERROR_OPERATION_TIMEDOUT);
+                            S.row_abort = 1;
+                            break;
+                        }
+                        __nanosleep(128);
+                    }
+                }
+            }
+            __syncthreads();
+            if (S.row_abort) return;
+            process_mb(S, a, row, col);
+            __syncthreads();
+            if (tid == 0) {
+                __threadfence();
+                st_release(&a.progress[row], col);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+size_t mb_shared_bytes() { return sizeof(MbShared); }
+
+}  // namespace evxg

@@ -1,0 +1,177 @@
+/*
+ * evxg.h -- C ABI of the B200 (sm_100a) EVX3 encoder pixel pipeline.
+ *
+ * The GPU path replaces the reference encoder's per-frame pixel pipeline,
+ * engine_encode_frame() minus serialize_slice() (reference
+ * src/video/encode.cpp:945-1001): RGB->YUV 4:2:0 conversion, per-macroblock
+ * mode decision (intra block copy, inter and bidirectional motion search with
+ * 6-tap sub-pel refinement, directional intra, RDO), DCT / adaptive
+ * quantisation / trellis, reconstruction, deblocking and SAO.  The outputs are
+ * exactly the tables the reference's host entropy coder reads
+ * (serialize.cpp:151-314, :564-686): the block table, the previous block
+ * table, the SAO table and the quantised level planes, byte-identical to the
+ * reference's for the same inputs.
+ *
+ * All entry points return an evx_status-compatible code (reference
+ * src/base.h:168-185); no exceptions cross the ABI.  One stream handle is one
+ * encoder context (reference evx_context, common.h:209-240); a handle is not
+ * thread-safe and needs external synchronisation, like the reference encoder.
+ * Pointers are plain host or device pointers; cuda_stream is a cudaStream_t
+ * passed as void* (NULL = the legacy default stream).
+ */
+#ifndef EVXG_H
+#define EVXG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: same values as the reference's evx_status (base.h:168-185). */
+#define EVXG_SUCCESS              0
+#define EVXG_ERROR_INVALIDARG     1
+#define EVXG_ERROR_OUTOFMEMORY    3
+#define EVXG_ERROR_INVALID_INDEX  6
+#define EVXG_ERROR_CAPACITY_LIMIT 7
+#define EVXG_ERROR_INVALID_RESOURCE 8
+#define EVXG_ERROR_OPERATION_TIMEDOUT 9
+#define EVXG_ERROR_EXECUTION_FAILURE 10
+
+/* Frame types (reference types.h:45-53). */
+#define EVXG_FRAME_INTRA 0
+#define EVXG_FRAME_INTER 1
+#define EVXG_FRAME_BIDIR 2
+
+#pragma pack(push, 2)
+/* Same byte layout as the reference's evx_frame (common.h:72-87, pack(2), 18 B). */
+typedef struct evxg_frame {
+    int32_t type;
+    uint32_t index;
+    uint16_t quality;          /* internal QP, 1..63 (evx3enc.cpp:64-82) */
+    uint32_t display_order;
+    uint8_t is_reference;
+    uint8_t dpb_slot;          /* DPB slot reconstructed into (0..3) */
+    uint8_t ref_slot_fwd;
+    uint8_t ref_slot_bwd;
+} evxg_frame;
+
+/* Same byte layout as the reference's evx_block_desc (common.h:91-115, pack(2), 28 B). */
+typedef struct evxg_block_desc {
+    int32_t block_type;        /* bit0 intra, bit1 motion, bit2 copy (types.h:63-91) */
+    uint8_t prediction_target;
+    uint8_t pad0;
+    int16_t motion_x;
+    int16_t motion_y;
+    uint8_t sp_pred;
+    uint8_t sp_amount;
+    uint8_t sp_index;
+    uint8_t q_index;
+    uint8_t intra_mode;        /* 0..6 directional, 7 none */
+    uint8_t pad1;
+    int16_t variance;
+    uint8_t prediction_mode;   /* 0 fwd, 1 bwd, 2 bi */
+    uint8_t prediction_target_b;
+    int16_t motion_x_b;
+    int16_t motion_y_b;
+    uint8_t sp_pred_b;
+    uint8_t sp_amount_b;
+    uint8_t sp_index_b;
+    uint8_t pad2;
+} evxg_block_desc;
+#pragma pack(pop)
+
+/* Same byte layout as the reference's evx_sao_params / evx_sao_info (sao.h:66-78, 16 B). */
+typedef struct evxg_sao_params {
+    uint8_t type;              /* 0 off, 1 edge, 2 band */
+    uint8_t eo_class;
+    uint8_t band_position;
+    int8_t offsets[4];
+} evxg_sao_params;
+typedef struct evxg_sao_info {
+    uint8_t merge_left;
+    uint8_t merge_above;
+    evxg_sao_params luma;
+    evxg_sao_params chroma;
+} evxg_sao_info;
+
+typedef struct evxg_stream evxg_stream;
+
+/*
+ * Create the device state of one encoding stream for frames of width x height
+ * (visible size; the context is 16-aligned like initialize_context,
+ * common.cpp:106-202): source, level and 4 DPB plane sets, block / previous
+ * block / SAO tables, all zero-initialised.  Replaces evx3_encoder_impl::
+ * initialize (evx3enc.cpp:84-103) on the device side.
+ */
+int evxg_stream_create(uint32_t width, uint32_t height, evxg_stream **out);
+int evxg_stream_destroy(evxg_stream *s);
+
+/* Aligned context size and macroblock grid of a stream. */
+int evxg_stream_dims(const evxg_stream *s, uint32_t *aligned_w, uint32_t *aligned_h,
+                     uint32_t *mb_w, uint32_t *mb_h);
+
+/*
+ * engine_encode_frame minus serialize_slice (encode.cpp:945-998): convert the
+ * packed RGB24 frame (width*height*3 bytes; rgb_on_device != 0 if it is a
+ * device pointer), run the macroblock wavefront (classify, encode, reconstruct
+ * into DPB[frame->dpb_slot]), deblock, SAO, and update the previous block
+ * table for non-B frames.  Asynchronous on cuda_stream.  frame is the
+ * reference's evx_frame as chosen by its GOP logic (evx3enc.cpp:105-414).
+ */
+int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device,
+                      const evxg_frame *frame, void *cuda_stream);
+
+/*
+ * Copy the tables the host serializer reads (serialize_slice,
+ * serialize.cpp:624-686) to host or device memory (to_device != 0).  Any
+ * pointer may be NULL.  Plane sets are int16, Y (aw*ah) then U then V
+ * ((aw/2)*(ah/2) each).  The previous block table returned is the one the
+ * serializer of the frame just encoded must see, i.e. as it was BEFORE that
+ * frame's update (encode.cpp:985-998 serializes before the copy).
+ */
+int evxg_fetch_tables(evxg_stream *s, evxg_block_desc *blocks, evxg_block_desc *prev_blocks,
+                      evxg_sao_info *sao, int16_t *levels, int to_device, void *cuda_stream);
+
+/* Copy one DPB slot (plane-set layout) or the converted source
+ * (slot = 4) out; supports the reference's peek() views (evx3enc.cpp:417-547). */
+int evxg_fetch_planes(evxg_stream *s, uint32_t slot, int16_t *out, int to_device, void *cuda_stream);
+
+/* Wait for the stream's work; returns the device error word if a kernel gave
+ * up waiting (EVXG_ERROR_OPERATION_TIMEDOUT) or a launch failed. */
+int evxg_stream_sync(evxg_stream *s, void *cuda_stream);
+
+/* Number of kernels launched by the last evxg_encode_frame call. */
+uint32_t evxg_last_launch_count(const evxg_stream *s);
+
+/* lambda = 0.85 * 2^((q-12)/3) in float, as the reference computes it (common.h:264-266). */
+float evxg_lambda(uint16_t quality);
+
+/* Human-readable text of the last error on this thread. */
+const char *evxg_last_error(void);
+
+/* ---- GOP-level encoder: evx3_encoder (evx3.h:67-100) over the stream API ---- */
+
+typedef struct evxg_encoder evxg_encoder;
+
+/* Called once per encoded frame, in bitstream order, after the frame's GPU
+ * work has completed and its tables were copied to host memory. */
+typedef void (*evxg_frame_callback)(void *user, const evxg_frame *frame,
+                                    const evxg_block_desc *blocks, const evxg_block_desc *prev_blocks,
+                                    const evxg_sao_info *sao, const int16_t *levels);
+
+int evxg_encoder_create(evxg_frame_callback cb, void *user, evxg_encoder **out);
+int evxg_encoder_destroy(evxg_encoder *e);
+int evxg_encoder_clear(evxg_encoder *e);                     /* evx3enc.cpp:35-55 */
+int evxg_encoder_insert_intra(evxg_encoder *e);              /* evx3enc.cpp:57-62 */
+int evxg_encoder_set_quality(evxg_encoder *e, uint8_t q);    /* evx3enc.cpp:64-82 */
+/* evx3enc.cpp:105-234: buffer / encode one RGB24 host frame. */
+int evxg_encoder_encode(evxg_encoder *e, const uint8_t *rgb, uint32_t width, uint32_t height);
+int evxg_encoder_flush(evxg_encoder *e);                     /* evx3enc.cpp:385-414 */
+/* The stream under an encoder (NULL before the first frame). */
+evxg_stream *evxg_encoder_stream(evxg_encoder *e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
