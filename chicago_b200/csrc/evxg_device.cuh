@@ -21,8 +21,13 @@ constexpr int MAXQ = 63;              // quantize.h:42 (levels - 1)
 // Search window in shared memory: a 16x16 block anywhere within +-31 px of a
 // base position, plus the 6-tap overshoot (-3 .. +18), clamped to the frame
 // the way interp.cpp:8-14 clamps its samples.
-constexpr int WL = 84;                // luma window side:  base-34 .. base+49
-constexpr int WC = 48;                // chroma window side: (base>>1)-19 .. +28
+// The window's left edge is rounded down to a multiple of 8 samples so rows
+// are copied as aligned 16-byte chunks; a chunk is then either entirely
+// inside the plane or entirely outside it (plane widths are multiples of 8).
+constexpr int WL_ROWS = 84;           // luma rows:  base-34 .. base+49
+constexpr int WL = 96;                // luma row stride: 12 chunks cover base-41 .. base+54
+constexpr int WC_ROWS = 48;           // chroma rows: (base>>1)-19 .. +28
+constexpr int WC = 56;                // chroma row stride: 7 chunks
 constexpr int WL_OFF = 34, WC_OFF = 19;
 
 __device__ __forceinline__ int rdiv(int n, int d)   // rounded_div, evx_math.h:228-236

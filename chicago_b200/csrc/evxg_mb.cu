@@ -55,11 +55,11 @@ constexpr int NW = NT / 32;
 constexpr int MB_N = 384;      // 16x16 luma + 2 x 8x8 chroma, MB buffer layout Y | U | V
 constexpr int MAXC = 5;        // RDO candidates (encode.cpp:279-364)
 
-struct Win {
-    int16_t y[WL * WL];
-    int16_t u[WC * WC];
-    int16_t v[WC * WC];
-    int ox, oy, cox, coy;      // origins in plane coordinates
+struct alignas(16) Win {
+    int16_t y[WL_ROWS * WL];
+    int16_t u[WC_ROWS * WC];
+    int16_t v[WC_ROWS * WC];
+    int ox, oy, cox, coy;      // plane coordinates of window element (0, 0)
 };
 struct Sel {                   // evx_motion_selection, motion.cpp:53-66
     int bx, by, sad, mad, ssd;
@@ -122,26 +122,70 @@ __device__ __forceinline__ int frac_from_dir(int i, int j)   // motion.cpp:68-91
     return i + 5;
 }
 
-// Load a clamped search window around luma base (bx, by) from a plane set.
+// Load a clamped search window around luma base (bx, by) from a plane set:
+// aligned 16-byte chunks, all loads of a thread issued before its stores.
+// Rows are clamped to the plane; chunks left/right of the plane are filled
+// with the edge sample, which is the clamping of interp.cpp:8-14.
 template <bool kCoherent>
-__device__ void load_window(Win &w, const int16_t *planes, int W, int H, int bx, int by)
+__device__ __forceinline__ uint4 ld16(const int16_t *p)
+{
+    return kCoherent ? __ldcg(reinterpret_cast<const uint4 *>(p)) : __ldg(reinterpret_cast<const uint4 *>(p));
+}
+template <bool kCoherent>
+__device__ __forceinline__ uint4 edge16(const int16_t *p)
+{
+    const unsigned v = (unsigned short)(kCoherent ? __ldcg(p) : __ldg(p));
+    const unsigned w2 = v | (v << 16);
+    return make_uint4(w2, w2, w2, w2);
+}
+template <bool kCoherent>
+__device__ __noinline__ void load_window(Win &w, const int16_t *planes, int W, int H, int bx, int by)
 {
     const int16_t *Y = planes, *U = planes + (size_t)W * H, *V = U + (size_t)(W / 2) * (H / 2);
     const int cw = W / 2, ch = H / 2;
-    const int ox = bx - WL_OFF, oy = by - WL_OFF, cox = (bx >> 1) - WC_OFF, coy = (by >> 1) - WC_OFF;
+    const int ox = ((bx - WL_OFF) >> 3) << 3, oy = by - WL_OFF;
+    const int cox = (((bx >> 1) - WC_OFF) >> 3) << 3, coy = (by >> 1) - WC_OFF;
     if (threadIdx.x == 0) { w.ox = ox; w.oy = oy; w.cox = cox; w.coy = coy; }
-    for (int e = threadIdx.x; e < WL * WL; e += NT) {
-        int r = e / WL, c = e - r * WL;
-        int y = min(max(oy + r, 0), H - 1), x = min(max(ox + c, 0), W - 1);
-        const int16_t *p = Y + (size_t)y * W + x;
-        w.y[e] = kCoherent ? __ldcg(p) : __ldg(p);
+    constexpr int NLC = WL / 8, NL = WL_ROWS * NLC, KL = (NL + NT - 1) / NT;
+    constexpr int NCC = WC / 8, NCH = 2 * WC_ROWS * NCC, KC = (NCH + NT - 1) / NT;
+    uint4 v[KL + KC];
+#pragma unroll
+    for (int i = 0; i < KL; i++) {
+        const int e = threadIdx.x + i * NT;
+        if (e < NL) {
+            const int r = e / NLC, k = e - r * NLC;
+            const int y = min(max(oy + r, 0), H - 1), x = ox + 8 * k;
+            const int16_t *row = Y + (size_t)y * W;
+            v[i] = (x >= 0 && x + 8 <= W) ? ld16<kCoherent>(row + x) : edge16<kCoherent>(row + (x < 0 ? 0 : W - 1));
+        }
     }
-    for (int e = threadIdx.x; e < 2 * WC * WC; e += NT) {
-        int pl = e >= WC * WC, k = e - pl * WC * WC;
-        int r = k / WC, c = k - r * WC;
-        int y = min(max(coy + r, 0), ch - 1), x = min(max(cox + c, 0), cw - 1);
-        const int16_t *p = (pl ? V : U) + (size_t)y * cw + x;
-        (pl ? w.v : w.u)[k] = kCoherent ? __ldcg(p) : __ldg(p);
+#pragma unroll
+    for (int i = 0; i < KC; i++) {
+        const int e = threadIdx.x + i * NT;
+        if (e < NCH) {
+            const int pl = e >= WC_ROWS * NCC, q = e - pl * WC_ROWS * NCC;
+            const int r = q / NCC, k = q - r * NCC;
+            const int y = min(max(coy + r, 0), ch - 1), x = cox + 8 * k;
+            const int16_t *row = (pl ? V : U) + (size_t)y * cw;
+            v[KL + i] = (x >= 0 && x + 8 <= cw) ? ld16<kCoherent>(row + x) : edge16<kCoherent>(row + (x < 0 ? 0 : cw - 1));
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < KL; i++) {
+        const int e = threadIdx.x + i * NT;
+        if (e < NL) {
+            const int r = e / NLC, k = e - r * NLC;
+            *reinterpret_cast<uint4 *>(&w.y[r * WL + 8 * k]) = v[i];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < KC; i++) {
+        const int e = threadIdx.x + i * NT;
+        if (e < NCH) {
+            const int pl = e >= WC_ROWS * NCC, q = e - pl * WC_ROWS * NCC;
+            const int r = q / NCC, k = q - r * NCC;
+            *reinterpret_cast<uint4 *>(&(pl ? w.v : w.u)[r * WC + 8 * k]) = v[KL + i];
+        }
     }
 }
 
@@ -266,7 +310,7 @@ __device__ void accept_int(Sel &s, int x, int y, int sad, int mad, int satd, int
 }
 
 // One pattern step (perform_intra/inter_motion_search, motion.cpp:348-406).
-__device__ void run_step(MbShared &S, const Win &w, bool intra, int l, int t, int r, int b, int st,
+__device__ __noinline__ void run_step(MbShared &S, const Win &w, bool intra, int l, int t, int r, int b, int st,
                          int px, int py, int W, int H, float lambda)
 {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -295,7 +339,7 @@ __device__ void run_step(MbShared &S, const Win &w, bool intra, int l, int t, in
 }
 
 // Sub-pel refinement around the selection (motion.cpp:180-261, :408-483).
-__device__ void run_subpel(MbShared &S, const Win &w, bool intra, int px, int py, int W, int H)
+__device__ __noinline__ void run_subpel(MbShared &S, const Win &w, bool intra, int px, int py, int W, int H)
 {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
@@ -505,7 +549,7 @@ __device__ void trellis_block(int16_t *lev, const int16_t *coef, int b, int qp, 
 
 // encode_block + decode_block for S.ncand candidates (encode.cpp:481-750,
 // decode.cpp:31-432); with S.rdo set also the RD cost (encode.cpp:39-164).
-__device__ void encode_candidates(MbShared &S, const FrameArgs &a)
+__device__ __noinline__ void encode_candidates(MbShared &S, const FrameArgs &a)
 {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nc = S.ncand;
@@ -673,7 +717,7 @@ __device__ void encode_candidates(MbShared &S, const FrameArgs &a)
 // ------------------------------------------------------------- searches
 
 // Intra block-copy search in the current frame (motion.cpp:485-565).
-__device__ void intra_bc_search(MbShared &S, const FrameArgs &a, int px, int py)
+__device__ __noinline__ void intra_bc_search(MbShared &S, const FrameArgs &a, int px, int py)
 {
     const int tid = threadIdx.x;
     const Win &w = S.win[0];
@@ -735,7 +779,7 @@ __device__ void mv_predictor(const FrameArgs &a, int idx, bool temporal, int &ox
 
 // Inter search against one DPB slot (motion.cpp:567-679); result descriptor,
 // SAD and prediction block.
-__device__ void inter_search(MbShared &S, const FrameArgs &a, int slot, bool temporal, int px, int py, int idx,
+__device__ __noinline__ void inter_search(MbShared &S, const FrameArgs &a, int slot, bool temporal, int px, int py, int idx,
                              evxg_block_desc &out, int &out_sad, int16_t *pred_out)
 {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -784,7 +828,7 @@ __device__ void inter_search(MbShared &S, const FrameArgs &a, int slot, bool tem
 }
 
 // Neighbours of the MB for directional intra, from the intra window (base (px, py-16)).
-__device__ void extract_neighbours(MbShared &S, int px, int py)
+__device__ __noinline__ void extract_neighbours(MbShared &S, int px, int py)
 {
     const int tid = threadIdx.x;
     const Win &w = S.win[0];
@@ -793,7 +837,8 @@ __device__ void extract_neighbours(MbShared &S, int px, int py)
         const int n = tid ? 8 : 16;
         const int16_t *pl = tid == 0 ? w.y : (tid == 1 ? w.u : w.v);
         const int S_ = tid ? WC : WL;
-        const int trow = tid ? 26 : 49, tcol = tid ? 19 : 34;   // window coordinates of (cy-1, cx)
+        const int trow = tid ? (py >> 1) - 1 - w.coy : py - 1 - w.oy;   // window coordinates of (cy-1, cx)
+        const int tcol = tid ? (px >> 1) - w.cox : px - w.ox;
         nb.ht = py > 0; nb.hl = px > 0;
         for (int i = 0; i < n; i++) {
             nb.top[i] = nb.ht ? pl[trow * S_ + tcol + i] : (int16_t)128;
@@ -823,7 +868,7 @@ __device__ void extract_neighbours(MbShared &S, int px, int py)
 }
 
 // Directional intra: 3 predictions and the best by luma SAD (intra_pred.cpp:219-289).
-__device__ void directional_intra(MbShared &S)
+__device__ __noinline__ void directional_intra(MbShared &S)
 {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for (int e = tid; e < 3 * MB_N; e += NT) {
