@@ -1,0 +1,304 @@
+"""Benchmark of the EVX3 encoder pixel pipeline on B200.
+
+Workload (the plain one-stream configuration): a seeded 1920x1080 RGB24
+sequence of 120 frames (sinusoid background, global pan with per-frame
+velocity in [-24, 24] px at quarter-pel, moving textured rectangles, noise
+sigma 3, scene cut at frame 60 where insert_intra() starts a new GOP),
+quality 8, deblocking and SAO on, encoded with the reference encoder's own GOP
+structure (I, then hierarchical P / reference-B / B groups of 4).
+
+A step is one frame of engine_encode_frame minus serialization in encode
+order: RGB->YUV, the macroblock wavefront (mode decision, transform,
+quantisation, trellis, reconstruction), deblocking, SAO.  `value` times the
+steps on the device with the RGB frames already resident in HBM and L2
+flushed between steps; `e2e` times the same steps through the C ABI with
+pinned host RGB in and the serializer's tables (block, previous block, SAO
+tables and level planes) out, copies inside the timed region.
+
+Multi-GPU (torchrun): every rank encodes its own stream (own seed), no
+collective on the data path (weak scaling); time is the max over ranks.
+`--impl reference` times the unmodified reference encoder (oracle/_ref, built
+from the reference's sources) through its public API on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "1080p-eq frames/s & p99 frame latency, batched vs plain GPU, bit-exact output"
+UNIT = "1080p-eq frames/s"
+W, H, FRAMES, QUALITY, VMAX, CUT = 1920, 1080, 120, 8, 24.0, 60
+EQ = (W * H) / (1920 * 1080)
+HBM_PEAK_FALLBACK = 6650.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_PEAK_FALLBACK, "fallback"
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def plan(seed_offset: int):
+    from chicago_b200.gop import plan as gop_plan
+    return gop_plan(FRAMES, quality=QUALITY, intra_at=(CUT,))
+
+
+def frames_for(rank: int):
+    from chicago_b200.synth import generate
+    return generate(W, H, FRAMES, seed=1000 + rank, vmax=VMAX, n_rects=4, cut_at=CUT)
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.p = None
+        self.path = f"/tmp/evxg_clocks_{os.getpid()}.csv"
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(index), "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(ftype: int, aw: int, ah: int) -> int:
+    """Compulsory HBM bytes of one macroblock-wavefront launch: the source plane
+    set read once, every reference slot read once (the intra block-copy search
+    reads the destination slot too), reconstruction and levels written once,
+    block table written (28 B per MB)."""
+    planeset = (aw * ah + 2 * (aw // 2) * (ah // 2)) * 2
+    refs = {0: 1, 1: 2, 2: 3}[ftype]
+    return planeset * (1 + refs + 2) + (aw // 16) * (ah // 16) * 28
+
+
+def run_gpu(args):
+    import torch
+    import chicago_b200 as cb
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=600))
+    sched = plan(rank)
+    K = min(args.steps, len(sched) - args.warmup)
+    frames = frames_for(rank)
+    dev_frames = torch.from_numpy(frames).cuda()                       # 746 MB resident in HBM
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")   # > 126 MB L2
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    st = cb.Stream(W, H)
+    st.profile(True)
+    from chicago_b200.gop import unpack_frame
+    # warm-up steps, then K timed steps; state (DPB, tables) carries across steps
+    order = sched[:args.warmup + K]
+    for ti, f18 in order[:args.warmup]:
+        st.encode_frame(dev_frames[ti].data_ptr(), f18, on_device=True, cuda_stream=sp)
+    st.sync(sp)
+    clocks = Clocks(local)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    step_ms, mb_ms, mb_bytes = [], [], 0
+    kernel_tot = {k: 0.0 for k in cb.Stream.KERNELS}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for ti, f18 in order[args.warmup:]:
+        flush.zero_()
+        ev0.record(stream)
+        st.encode_frame(dev_frames[ti].data_ptr(), f18, on_device=True, cuda_stream=sp)
+        ev1.record(stream)
+        ev1.synchronize()
+        step_ms.append(ev0.elapsed_time(ev1))
+        km = st.kernel_ms()
+        for k, v in km.items():
+            kernel_tot[k] += v
+        mb_ms.append(km["mb_wavefront"])
+        mb_bytes += algorithmic_bytes(unpack_frame(f18)["type"], st.aw, st.ah)
+    st.sync(sp)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * K * EQ / (total_ms / 1e3)
+
+    # end to end through the C ABI: pinned host RGB in, serializer tables out
+    nblk = st.mbw * st.mbh
+    host_rgb = torch.from_numpy(frames).pin_memory()
+    out_bt = torch.empty(nblk * 28, dtype=torch.uint8).pin_memory()
+    out_prev = torch.empty(nblk * 28, dtype=torch.uint8).pin_memory()
+    out_sao = torch.empty(nblk * 16, dtype=torch.uint8).pin_memory()
+    out_lev = torch.empty(st.plane_elems, dtype=torch.int16).pin_memory()
+    st2 = cb.Stream(W, H)
+    L = cb.lib()
+    import ctypes as C
+    e2e_ms = []
+    for i, (ti, f18) in enumerate(order):
+        ev0.record(stream)
+        cb._check(L.evxg_encode_frame(st2.h, C.c_void_p(host_rgb[ti].data_ptr()), 0, f18, C.c_void_p(sp)))
+        cb._check(L.evxg_fetch_tables(st2.h, C.c_void_p(out_bt.data_ptr()), C.c_void_p(out_prev.data_ptr()),
+                                      C.c_void_p(out_sao.data_ptr()), C.c_void_p(out_lev.data_ptr()), 0, C.c_void_p(sp)))
+        ev1.record(stream)
+        ev1.synchronize()
+        if i >= args.warmup:
+            e2e_ms.append(ev0.elapsed_time(ev1))
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_total], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * K * EQ / (e2e_total / 1e3)
+    h2d = W * H * 3
+    d2h = nblk * 28 * 2 + nblk * 16 + st.plane_elems * 2
+
+    peak, peak_kind = peaks()
+    achieved = mb_bytes / (sum(mb_ms) / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / K, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic (seeded generator)",
+        "config": {"workload": "plain GPU path, one stream per GPU: 1920x1080 RGB24, 120 frames, pan +-24 px, "
+                               "scene cut at 60, quality 8, reference GOP (I + hierarchical P/B of 4), deblock+SAO",
+                   "frames": FRAMES, "quality": QUALITY, "l2": "flushed (256 MB write) between timed steps",
+                   "parallelism": f"{world} independent streams, no collective"},
+        "p50_frame_ms": round(float(np.percentile(step_ms, 50)), 3),
+        "p99_frame_ms": round(float(np.percentile(step_ms, 99)), 3),
+        "kernel_ms_per_step": {k: round(v / K, 4) for k, v in kernel_tot.items()},
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"kernel": "k_mb_wavefront", "bound": "hbm", "achieved": round(achieved, 3), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 6), "traffic": None,
+                     "peak_source": f"{peak_kind} hbm_gbs",
+                     "note": "dependency-latency bound: lag-4 macroblock wavefront, see DESIGN.md"},
+        "gpu_launches": st.launch_count() * K,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def cpu_baseline(n_frames: int = 8):
+    """The unmodified reference encoder (built here from its sources) with its
+    WPP threads on all host cores, on the first n_frames of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from chicago_b200.synth import generate
+    from oracle_py import Ref
+    frames = generate(W, H, n_frames, seed=1000, vmax=VMAX)
+    ref = Ref()
+    t0 = time.perf_counter()
+    ref.encode_stream(frames, quality=QUALITY)
+    dt = time.perf_counter() - t0
+    return {"value": round(n_frames * EQ / dt, 4), "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"first {n_frames} frames of the workload through create_encoder/encode/flush (WPP threads)"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle_py import REF_SO, Ref
+    if not os.path.exists(REF_SO):
+        print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref/libevxref.so not built"}))
+        return
+    import ctypes as C
+    ref = Ref()
+    K = min(args.steps, FRAMES - args.warmup)
+    frames = frames_for(0)[:args.warmup + K]
+    L = ref.lib
+    cap = W * H * 3 * 8
+    h = L.evxref_enc_create(cap)
+    buf = np.zeros(cap, np.uint8)
+    n = C.c_uint32(0)
+    L.evxref_enc_set_quality(h, QUALITY)
+    for t in range(args.warmup):
+        if t == CUT:
+            L.evxref_enc_insert_intra(h)
+        L.evxref_enc_encode(h, frames[t].ctypes.data_as(C.c_void_p), W, H, buf.ctypes.data_as(C.c_void_p), cap, C.byref(n))
+    t0 = time.perf_counter()
+    for t in range(args.warmup, args.warmup + K):
+        if t == CUT:
+            L.evxref_enc_insert_intra(h)
+        L.evxref_enc_encode(h, frames[t].ctypes.data_as(C.c_void_p), W, H, buf.ctypes.data_as(C.c_void_p), cap, C.byref(n))
+    L.evxref_enc_flush(h, buf.ctypes.data_as(C.c_void_p), cap, C.byref(n))
+    dt = time.perf_counter() - t0
+    L.evxref_enc_destroy(h)
+    value = K * EQ / dt
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
+            "steps": K, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / K, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic (seeded generator)",
+            "config": {"workload": "same sequence as the GPU arm, stream 0", "frames": FRAMES, "quality": QUALITY},
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                             "sample": f"{K} frames after {args.warmup} warm-up frames, WPP threads"},
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=117)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

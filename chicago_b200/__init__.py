@@ -40,7 +40,7 @@ FRAME_INTRA, FRAME_INTER, FRAME_BIDIR = 0, 1, 2
 EXPORTS = [
     "evxg_stream_create", "evxg_stream_destroy", "evxg_stream_dims", "evxg_encode_frame",
     "evxg_fetch_tables", "evxg_fetch_planes", "evxg_stream_sync", "evxg_last_launch_count",
-    "evxg_lambda", "evxg_last_error", "evxg_encoder_create", "evxg_encoder_destroy",
+    "evxg_lambda", "evxg_last_error", "evxg_stream_profile", "evxg_stream_kernel_ms", "evxg_encoder_create", "evxg_encoder_destroy",
     "evxg_encoder_clear", "evxg_encoder_insert_intra", "evxg_encoder_set_quality",
     "evxg_encoder_encode", "evxg_encoder_flush", "evxg_encoder_stream",
 ]
@@ -68,6 +68,8 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_stream_sync.argtypes = [vp, vp]
     L.evxg_last_launch_count.argtypes = [vp]
     L.evxg_last_launch_count.restype = u32
+    L.evxg_stream_profile.argtypes = [vp, i32]
+    L.evxg_stream_kernel_ms.argtypes = [vp, C.POINTER(C.c_float), u32]
     L.evxg_lambda.argtypes = [C.c_uint16]
     L.evxg_lambda.restype = C.c_float
     L.evxg_last_error.restype = C.c_char_p
@@ -163,6 +165,18 @@ class Stream:
         out = np.zeros(self.plane_elems, np.int16)
         _check(lib().evxg_fetch_planes(self.h, slot, _ptr(out), 0, _ptr(cuda_stream)))
         return out
+
+    KERNELS = ("convert", "mb_wavefront", "deblock", "sao_rdo", "sao_merge", "sao_apply")
+
+    def profile(self, enable: bool = True):
+        _check(lib().evxg_stream_profile(self.h, int(enable)))
+
+    def kernel_ms(self) -> dict:
+        buf = (C.c_float * 6)()
+        n = lib().evxg_stream_kernel_ms(self.h, buf, 6)
+        if n < 0:
+            raise EvxgError(-n, "kernel timing failed")
+        return {self.KERNELS[i]: buf[i] for i in range(n)}
 
     def launch_count(self) -> int:
         return lib().evxg_last_launch_count(self.h)

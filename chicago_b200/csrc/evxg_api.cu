@@ -55,6 +55,8 @@ struct evxg_stream {
     int mb_grid, num_sms;
     uint32_t launches;
     long long timeout_ns;
+    bool profile;
+    cudaEvent_t ev[7];
 };
 
 extern "C" {
@@ -118,6 +120,8 @@ int evxg_stream_destroy(evxg_stream *s)
     for (int i = 0; i < 4; i++) cudaFree(s->dpb[i]);
     cudaFree(s->bt); cudaFree(s->prev); cudaFree(s->prev_ser);
     cudaFree(s->sao); cudaFree(s->sao_cost); cudaFree(s->rgb); cudaFree(s->sync);
+    if (s->profile)
+        for (int i = 0; i < 7; i++) cudaEventDestroy(s->ev[i]);
     delete s;
     return EVXG_SUCCESS;
 }
@@ -172,18 +176,48 @@ int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, con
     CK(cudaMemsetAsync(s->sync + 3 * s->mbh, 0, 4 * sizeof(int), st));
     const int cw = (int)std::min(s->vw, s->W), ch = (int)std::min(s->vh, s->H);
     dim3 cg((cw / 2 + 127) / 128, ch / 2);
-    k_convert<<<cg, 128, 0, st>>>(a);
-    k_mb_wavefront<<<s->mb_grid, 256, mb_shared_bytes(), st>>>(a);
-    k_deblock<<<3, 1024, 0, st>>>(a);
-    k_sao_rdo<<<(unsigned)((nblk + 127) / 128), 128, 0, st>>>(a);
     const unsigned wf = (s->mbh + 7) / 8;
+    auto mark = [&](int i) { if (s->profile) cudaEventRecord(s->ev[i], st); };
+    mark(0);
+    k_convert<<<cg, 128, 0, st>>>(a);
+    mark(1);
+    k_mb_wavefront<<<s->mb_grid, 256, mb_shared_bytes(), st>>>(a);
+    mark(2);
+    k_deblock<<<3, 1024, 0, st>>>(a);
+    mark(3);
+    k_sao_rdo<<<(unsigned)((nblk + 127) / 128), 128, 0, st>>>(a);
+    mark(4);
     k_sao_merge<<<wf, 256, 0, st>>>(a);
+    mark(5);
     k_sao_apply<<<wf, 256, 0, st>>>(a);
+    mark(6);
     s->launches = 6;
     CK(cudaGetLastError());
     if (f->type != EVXG_FRAME_BIDIR)   // temporal MV predictor table (encode.cpp:990-998)
         CK(cudaMemcpyAsync(s->prev, s->bt, nblk * sizeof(evxg_block_desc), cudaMemcpyDeviceToDevice, st));
     return EVXG_SUCCESS;
+}
+
+int evxg_stream_profile(evxg_stream *s, int enable)
+{
+    if (!s) return EVXG_ERROR_INVALIDARG;
+    if (enable && !s->profile)
+        for (int i = 0; i < 7; i++) CK(cudaEventCreate(&s->ev[i]));
+    if (!enable && s->profile)
+        for (int i = 0; i < 7; i++) cudaEventDestroy(s->ev[i]);
+    s->profile = enable != 0;
+    return EVXG_SUCCESS;
+}
+
+int evxg_stream_kernel_ms(evxg_stream *s, float *out, uint32_t n)
+{
+    if (!s || !out) return -EVXG_ERROR_INVALIDARG;
+    if (!s->profile) return 0;
+    if (cudaEventSynchronize(s->ev[6]) != cudaSuccess) return -EVXG_ERROR_EXECUTION_FAILURE;
+    uint32_t k = 0;
+    for (; k < n && k < 6; k++)
+        if (cudaEventElapsedTime(&out[k], s->ev[k], s->ev[k + 1]) != cudaSuccess) return -EVXG_ERROR_EXECUTION_FAILURE;
+    return (int)k;
 }
 
 int evxg_stream_sync(evxg_stream *s, void *cuda_stream)

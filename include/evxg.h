@@ -144,6 +144,14 @@ int evxg_stream_sync(evxg_stream *s, void *cuda_stream);
 /* Number of kernels launched by the last evxg_encode_frame call. */
 uint32_t evxg_last_launch_count(const evxg_stream *s);
 
+/* Kernel timing (no counterpart in the reference, which has no device work):
+ * when enabled, evxg_encode_frame records a CUDA event around each of its
+ * kernels; evxg_stream_kernel_ms waits for the last frame and writes up to n
+ * durations in milliseconds, in launch order: convert, macroblock wavefront,
+ * deblock, SAO RDO, SAO merge, SAO apply.  Returns the number written. */
+int evxg_stream_profile(evxg_stream *s, int enable);
+int evxg_stream_kernel_ms(evxg_stream *s, float *out_ms, uint32_t n);
+
 /* lambda = 0.85 * 2^((q-12)/3) in float, as the reference computes it (common.h:264-266). */
 float evxg_lambda(uint16_t quality);
 

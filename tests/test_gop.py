@@ -30,3 +30,9 @@ def test_insert_intra_flushes_gop():
 
 def test_quality_mapping():
     assert [quality_to_qp(q) for q in (0, 1, 8, 16, 17, 31, 40)] == [1, 1, 8, 16, 17, 53, 53]
+
+
+def test_product_schedule_equals_restatement():
+    from chicago_b200.gop import plan
+    for T, q, cuts in [(1, 8, ()), (2, 8, ()), (9, 8, ()), (13, 20, (5,)), (30, 4, (3, 4, 17)), (120, 8, (60,))]:
+        assert plan(T, q, cuts) == plan_gop(T, quality=q, intra_at=cuts)
