@@ -50,6 +50,13 @@ __constant__ uint8_t c_zigzag[64] = {  // scan.h:60-70
     27, 20, 13, 6, 7, 14, 21, 28, 35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23, 30, 37, 44, 51,
     58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63};
 
+// Per-CTA shared copies of the tables indexed by coefficient position (a
+// different position per thread), filled once at kernel start: divergent
+// __constant__ reads would serialise.
+__shared__ int16_t s_qm[2][64];      // 0 intra, 1 inter
+__shared__ uint8_t s_dz[2][64];
+__shared__ uint8_t s_scan[3][64];    // 0 zigzag, 1 row-first (vertical modes), 2 column-first (horizontal modes)
+
 constexpr int NT = 256;        // threads per CTA
 constexpr int NW = NT / 32;
 constexpr int MB_N = 384;      // 16x16 luma + 2 x 8x8 chroma, MB buffer layout Y | U | V
@@ -452,12 +459,12 @@ __device__ __forceinline__ int16_t quant_coeff(int16_t sv, int qp, int o, bool i
 {
     if (intra) {
         if (o == 0) return (int16_t)rdiv(sv, chroma ? chroma_dc_scale(qp) : luma_dc_scale(qp));
-        int16_t qf = (int16_t)rdiv(sv * 16, c_qm_intra[o]);
-        if (qp >= 16) qf = (int16_t)(qf - (int16_t)((sgn16(qf) * qp * c_dz_intra[o]) >> 1));
+        int16_t qf = (int16_t)rdiv(sv * 16, s_qm[0][o]);
+        if (qp >= 16) qf = (int16_t)(qf - (int16_t)((sgn16(qf) * qp * s_dz[0][o]) >> 1));
         return (int16_t)rdiv(qf, qp << 1);
     }
-    const int16_t qf = (int16_t)rdiv(sv * 16, c_qm_inter[o]);
-    int wgt = c_dz_inter[o];
+    const int16_t qf = (int16_t)rdiv(sv * 16, s_qm[1][o]);
+    int wgt = s_dz[1][o];
     if (qp >= 16) wgt = min(wgt + 1, 6);
     const int16_t dz = (int16_t)((sgn16(qf) * qp * wgt) >> 1);
     return (int16_t)rdiv(qf - dz, qp << 1);
@@ -465,7 +472,7 @@ __device__ __forceinline__ int16_t quant_coeff(int16_t sv, int qp, int o, bool i
 __device__ __forceinline__ int16_t dequant_coeff(int16_t lv, int qp, int o, bool intra, bool chroma)   // quantize.cpp:271-332
 {
     if (intra && o == 0) return (int16_t)(lv * (chroma ? chroma_dc_scale(qp) : luma_dc_scale(qp)));
-    return (int16_t)((2 * lv * (intra ? c_qm_intra[o] : c_qm_inter[o]) * qp) / 16);
+    return (int16_t)((2 * lv * s_qm[intra ? 0 : 1][o] * qp) / 16);
 }
 __device__ __forceinline__ unsigned coeff_bits(int16_t lv)   // quantize.cpp:517-532
 {
@@ -477,11 +484,9 @@ __device__ __forceinline__ unsigned coeff_bits(int16_t lv)   // quantize.cpp:517
     else b += 1;
     return b;
 }
-__device__ __forceinline__ int scan_pos(int mode, int p)   // scan.h:125-159
+__device__ __forceinline__ int scan_kind(int mode)   // scan.h:154-159
 {
-    if (mode == 1 || mode == 5) return p;
-    if (mode == 2 || mode == 6) return (p & 7) * 8 + (p >> 3);
-    return c_zigzag[p];
+    return (mode == 1 || mode == 5) ? 1 : ((mode == 2 || mode == 6) ? 2 : 0);
 }
 // forward 8-point line (transform.cpp:264-284)
 __device__ __forceinline__ void fdct8_line(const int in[8], int16_t out[8])
@@ -508,42 +513,64 @@ __device__ __forceinline__ void idct8_line(const int in[8], int out[8])
 }
 __device__ __forceinline__ bool intra_quant(int bt) { return (bt & BT_INTRA) && !(bt & BT_MOTION); }   // quantize.cpp:457
 
-// Trellis of one 8x8 block (quantize.cpp:536-613) in place on an MB buffer.
-__device__ void trellis_block(int16_t *lev, const int16_t *coef, int b, int qp, bool intra, int mode, float lambda)
+// Trellis of one 8x8 block (quantize.cpp:536-613) in place on an MB buffer,
+// one warp: lane l owns scan positions l and l+32.  The reference's tail trim
+// walks down from the last significant position zeroing levels until the
+// first one worth keeping, so it zeroes every nonzero level above the highest
+// "keep" position; the forward refinement decides each position on its own.
+// Both become per-position RD tests plus ballots.
+__device__ void trellis_warp(int16_t *lev, const int16_t *coef, int b, int qp, bool intra, int mode, float lambda,
+                             int lane)
 {
     const bool chroma = b >= 4;
-    int last = -1;
-    for (int p = 63; p >= 0; p--) {
-        const int o = scan_pos(mode, p);
-        if (lev[mb_index(b, o >> 3, o & 7)]) { last = p; break; }
+    const uint8_t *scan = s_scan[scan_kind(mode)];
+    int o[2], e[2], c[2];
+    int16_t l[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        o[h] = scan[lane + 32 * h];
+        e[h] = mb_index(b, o[h] >> 3, o[h] & 7);
+        l[h] = lev[e[h]];
+        c[h] = coef[e[h]];
     }
+    auto last_sig = [&]() {
+        const unsigned n0 = __ballot_sync(0xffffffffu, l[0] != 0), n1 = __ballot_sync(0xffffffffu, l[1] != 0);
+        return n1 ? 63 - __clz((int)n1) : (n0 ? 31 - __clz((int)n0) : -1);
+    };
+    int last = last_sig();
     if (last < 0) return;
-    for (int p = last; p >= 1; p--) {
-        const int o = scan_pos(mode, p), e = mb_index(b, o >> 3, o & 7);
-        const int16_t l = lev[e];
-        if (!l) continue;
-        const int dk = (int)coef[e] - (int)dequant_coeff(l, qp, o, intra, chroma), dz = coef[e];
-        const float ck = __fadd_rn(__int2float_rn(wmul(dk, dk)), __fmul_rn(lambda, __uint2float_rn(coeff_bits(l))));
-        const float cz = __fadd_rn(__int2float_rn(wmul(dz, dz)), __fmul_rn(lambda, __uint2float_rn(coeff_bits(0))));
-        if (cz <= ck) lev[e] = 0;
-        else break;
+    bool keep[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int p = lane + 32 * h;
+        keep[h] = false;
+        if (l[h] != 0 && p >= 1 && p <= last) {
+            const int dk = c[h] - (int)dequant_coeff(l[h], qp, o[h], intra, chroma), dz = c[h];
+            const float ck = __fadd_rn(__int2float_rn(wmul(dk, dk)), __fmul_rn(lambda, __uint2float_rn(coeff_bits(l[h]))));
+            const float cz = __fadd_rn(__int2float_rn(wmul(dz, dz)), __fmul_rn(lambda, __uint2float_rn(coeff_bits(0))));
+            keep[h] = !(cz <= ck);
+        }
     }
-    last = -1;
-    for (int p = 63; p >= 0; p--) {
-        const int o = scan_pos(mode, p);
-        if (lev[mb_index(b, o >> 3, o & 7)]) { last = p; break; }
+    const unsigned k0 = __ballot_sync(0xffffffffu, keep[0]), k1 = __ballot_sync(0xffffffffu, keep[1]);
+    const int stop = k1 ? 63 - __clz((int)k1) : (k0 ? 31 - __clz((int)k0) : 0);
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int p = lane + 32 * h;
+        if (l[h] != 0 && p > stop && p <= last) l[h] = 0;
     }
-    if (last < 0) return;
-    for (int p = 1; p <= last; p++) {
-        const int o = scan_pos(mode, p), e = mb_index(b, o >> 3, o & 7);
-        const int16_t l = lev[e];
-        if (!l) continue;
-        const int16_t rl = (int16_t)(l - sgn16(l));
-        const int dk = (int)coef[e] - (int)dequant_coeff(l, qp, o, intra, chroma);
-        const int dr = (int)coef[e] - (int)dequant_coeff(rl, qp, o, intra, chroma);
-        const float ck = __fadd_rn(__int2float_rn(wmul(dk, dk)), __fmul_rn(lambda, __uint2float_rn(coeff_bits(l))));
-        const float cr = __fadd_rn(__int2float_rn(wmul(dr, dr)), __fmul_rn(lambda, __uint2float_rn(coeff_bits(rl))));
-        if (cr < ck) lev[e] = rl;
+    last = last_sig();
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int p = lane + 32 * h;
+        if (last >= 1 && l[h] != 0 && p >= 1 && p <= last) {
+            const int16_t rl = (int16_t)(l[h] - sgn16(l[h]));
+            const int dk = c[h] - (int)dequant_coeff(l[h], qp, o[h], intra, chroma);
+            const int dr = c[h] - (int)dequant_coeff(rl, qp, o[h], intra, chroma);
+            const float ck = __fadd_rn(__int2float_rn(wmul(dk, dk)), __fmul_rn(lambda, __uint2float_rn(coeff_bits(l[h]))));
+            const float cr = __fadd_rn(__int2float_rn(wmul(dr, dr)), __fmul_rn(lambda, __uint2float_rn(coeff_bits(rl))));
+            if (cr < ck) l[h] = rl;
+        }
+        lev[e[h]] = l[h];
     }
 }
 
@@ -618,12 +645,12 @@ __device__ __noinline__ void encode_candidates(MbShared &S, const FrameArgs &a)
         S.lev[k][p] = quant_coeff(S.coef[k][p], qp, o, intra_quant(bt), chroma);
     }
     __syncthreads();
-    if (tid < nc * 6) {   // trellis, one thread per 8x8 block
-        const int k = tid / 6, b = tid - k * 6;
+    for (int j = warp; j < nc * 6; j += NW) {   // trellis, one warp per 8x8 block
+        const int k = j / 6, b = j - k * 6;
         const int bt = S.cd[k].d.block_type;
         if (!(bt & BT_COPY)) {
             const int qp = b >= 4 ? min(S.cd[k].d.q_index + 2, MAXQ) : S.cd[k].d.q_index;
-            trellis_block(S.lev[k], S.coef[k], b, qp, intra_quant(bt), S.cd[k].d.intra_mode, a.lambda);
+            trellis_warp(S.lev[k], S.coef[k], b, qp, intra_quant(bt), S.cd[k].d.intra_mode, a.lambda, lane);
         }
     }
     __syncthreads();
@@ -1016,6 +1043,14 @@ __global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a)
     MbShared &S = *reinterpret_cast<MbShared *>(smem_raw);
     __shared__ int s_row;
     const int tid = threadIdx.x;
+    if (tid < 64) {
+        s_qm[0][tid] = c_qm_intra[tid]; s_qm[1][tid] = c_qm_inter[tid];
+        s_dz[0][tid] = c_dz_intra[tid]; s_dz[1][tid] = c_dz_inter[tid];
+        s_scan[0][tid] = c_zigzag[tid];
+        s_scan[1][tid] = (uint8_t)tid;
+        s_scan[2][tid] = (uint8_t)((tid & 7) * 8 + (tid >> 3));
+    }
+    __syncthreads();
     for (;;) {
         if (tid == 0) s_row = atomicAdd(&a.counters[0], 1);
         __syncthreads();
