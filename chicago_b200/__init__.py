@@ -42,7 +42,7 @@ EXPORTS = [
     "evxg_fetch_tables", "evxg_fetch_planes", "evxg_stream_sync", "evxg_last_launch_count",
     "evxg_lambda", "evxg_last_error", "evxg_stream_profile", "evxg_stream_kernel_ms", "evxg_encoder_create", "evxg_encoder_destroy",
     "evxg_encoder_clear", "evxg_encoder_insert_intra", "evxg_encoder_set_quality",
-    "evxg_encoder_encode", "evxg_encoder_flush", "evxg_encoder_stream",
+    "evxg_encoder_encode", "evxg_encoder_flush", "evxg_encoder_stream", "evxg_mb_pass_noalloc",
 ]
 
 FRAME_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
@@ -80,6 +80,7 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_encoder_encode.argtypes = [vp, vp, u32, u32]
     L.evxg_encoder_stream.argtypes = [vp]
     L.evxg_encoder_stream.restype = vp
+    L.evxg_mb_pass_noalloc.argtypes = [u32, u32, C.c_char_p, vp, C.POINTER(vp), vp, vp, vp, vp]
     return L
 
 

@@ -1,0 +1,103 @@
+// evxg_noalloc.cu -- an allocation-free entry point for the macroblock pass.
+//
+// Some callers cannot allocate device memory at the time they encode: a host
+// that manages one fixed device arena itself (a plugin in a media server or a
+// capture pipeline that gets all of its buffers from the host application), a
+// caller running inside a section where allocation would synchronise the
+// device or fail, or one whose memory budget is fixed at start-up.  Such a
+// caller already owns every input and output buffer; what the macroblock
+// wavefront kernel needs beyond them is a small scratch area (one progress
+// word per macroblock row, a row counter and an error word).  Here that
+// scratch lives in a fixed array in the library's device image, so this entry
+// point calls no allocator at all.
+#include <cuda_runtime.h>
+
+#include "evxg.h"
+#include "evxg_device.cuh"
+
+namespace evxg {
+__global__ void k_mb_wavefront(FrameArgs a);
+size_t mb_shared_bytes();
+}  // namespace evxg
+
+using namespace evxg;
+
+// Scratch words: [0, rows) row progress, then 4 counters, then the error word.
+// Every GPU that loads this library holds these 16 KiB until the process exits.
+static __device__ __align__(256) int g_noalloc_scratch[EVXG_NOALLOC_MAX_MB_ROWS + 5];
+
+namespace {
+constexpr int kMaxDevices = 64;
+int *g_scratch_ptr[kMaxDevices];   // device address of g_noalloc_scratch, per device
+int g_num_sms[kMaxDevices];
+
+// Once per device, with that device current: translate the array's host-side
+// name into its device address and allow the kernel's shared-memory size.
+int setup_device(int dev)
+{
+    if (g_scratch_ptr[dev]) return EVXG_SUCCESS;
+    int *p = nullptr;
+    if (cudaGetSymbolAddress((void **)&p, g_noalloc_scratch) != cudaSuccess || !p)
+        return EVXG_ERROR_EXECUTION_FAILURE;
+    if (cudaDeviceGetAttribute(&g_num_sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return EVXG_ERROR_EXECUTION_FAILURE;
+    if (cudaFuncSetAttribute(k_mb_wavefront, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mb_shared_bytes()) !=
+        cudaSuccess)
+        return EVXG_ERROR_EXECUTION_FAILURE;
+    g_scratch_ptr[dev] = p;
+    return EVXG_SUCCESS;
+}
+}  // namespace
+
+extern "C" int evxg_mb_pass_noalloc(uint32_t aligned_w, uint32_t aligned_h, const evxg_frame *f, const int16_t *src,
+                                    int16_t *const dpb[4], int16_t *levels, evxg_block_desc *blocks,
+                                    const evxg_block_desc *prev_blocks, void *cuda_stream)
+{
+    if (!f || !src || !dpb || !levels || !blocks) return EVXG_ERROR_INVALIDARG;
+    if (!aligned_w || !aligned_h || (aligned_w & 15) || (aligned_h & 15) || aligned_w > 65520)
+        return EVXG_ERROR_INVALIDARG;
+    const uint32_t mbw = aligned_w / 16, mbh = aligned_h / 16;
+    if (mbh > EVXG_NOALLOC_MAX_MB_ROWS) return EVXG_ERROR_CAPACITY_LIMIT;
+    if (f->type < EVXG_FRAME_INTRA || f->type > EVXG_FRAME_BIDIR || f->quality < 1 || f->quality > 63)
+        return EVXG_ERROR_INVALIDARG;
+    if (f->dpb_slot > 3 || f->ref_slot_fwd > 3 || f->ref_slot_bwd > 3) return EVXG_ERROR_INVALID_INDEX;
+    if (f->type != EVXG_FRAME_INTRA && f->ref_slot_fwd == f->dpb_slot) return EVXG_ERROR_INVALIDARG;
+    if (f->type == EVXG_FRAME_BIDIR && f->ref_slot_bwd == f->dpb_slot) return EVXG_ERROR_INVALIDARG;
+    if (f->type == EVXG_FRAME_INTER && !prev_blocks) return EVXG_ERROR_INVALIDARG;
+    for (int i = 0; i < 4; i++)
+        if (!dpb[i]) return EVXG_ERROR_INVALIDARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return EVXG_ERROR_EXECUTION_FAILURE;
+    int rc = setup_device(dev);
+    if (rc) return rc;
+    int *scratch = g_scratch_ptr[dev];
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+
+    FrameArgs a{};
+    a.W = (int)aligned_w; a.H = (int)aligned_h; a.mbw = (int)mbw; a.mbh = (int)mbh;
+    a.vis_w = a.W; a.vis_h = a.H;
+    a.type = f->type; a.quality = f->quality; a.dpb = f->dpb_slot;
+    a.ref_fwd = f->ref_slot_fwd; a.ref_bwd = f->ref_slot_bwd;
+    a.lambda = evxg_lambda(f->quality);
+    for (int i = 0; i < 4; i++) a.planes[i] = dpb[i];
+    a.src = const_cast<int16_t *>(src);
+    a.lev = levels;
+    a.bt = blocks;
+    a.prev = f->type == EVXG_FRAME_INTER ? prev_blocks : nullptr;
+    a.progress = scratch;
+    a.counters = scratch + mbh;
+    a.error = scratch + mbh + 4;
+    a.timeout_ns = 5000000000LL;
+    // The array keeps whatever the previous call left: progress words start at
+    // -1, the row counter and the error word at 0.
+    if (cudaMemsetAsync(scratch, 0xFF, mbh * sizeof(int), st) != cudaSuccess) return EVXG_ERROR_EXECUTION_FAILURE;
+    if (cudaMemsetAsync(scratch + mbh, 0, 5 * sizeof(int), st) != cudaSuccess) return EVXG_ERROR_EXECUTION_FAILURE;
+    const int grid = (int)(mbh < (uint32_t)g_num_sms[dev] ? mbh : (uint32_t)g_num_sms[dev]);
+    k_mb_wavefront<<<grid, 256, mb_shared_bytes(), st>>>(a);
+    if (cudaGetLastError() != cudaSuccess) return EVXG_ERROR_EXECUTION_FAILURE;
+    int err = 0;
+    if (cudaMemcpyAsync(&err, scratch + mbh + 4, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return EVXG_ERROR_EXECUTION_FAILURE;
+    return err ? err : EVXG_SUCCESS;
+}

@@ -158,6 +158,35 @@ float evxg_lambda(uint16_t quality);
 /* Human-readable text of the last error on this thread. */
 const char *evxg_last_error(void);
 
+/* ---- Allocation-free macroblock pass ----
+ *
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they encode (a plugin that must take every buffer from a host
+ * application's own arena, code running where an allocation would stall or
+ * fail, a process with a device budget fixed at start-up): runs only the
+ * macroblock wavefront of one frame -- classify, encode and reconstruct every
+ * macroblock into dpb[frame->dpb_slot], writing the block table and the level
+ * planes -- on buffers the caller owns, and allocates nothing.
+ *
+ * Layouts are those of the stream API: src, levels and each dpb[i] are int16
+ * plane sets of the 16-aligned size (Y, then U, then V); blocks and
+ * prev_blocks hold (aligned_w/16)*(aligned_h/16) descriptors; prev_blocks is
+ * read for P frames only.  All pointers are device pointers.
+ *
+ * Its scratch (a progress word per macroblock row, a row counter and an error
+ * word) is a fixed array in the library's device image: at most
+ * EVXG_NOALLOC_MAX_MB_ROWS macroblock rows, i.e. aligned_h <= 65408; larger
+ * frames are refused with EVXG_ERROR_CAPACITY_LIMIT.  The first call on a
+ * device looks up that array's device address; make that first call before
+ * any stream capture.  Every call on a device shares the one array and
+ * re-initialises it, so calls whose work overlaps on the GPU race: issue them
+ * one after another.  The call waits for its work on cuda_stream and returns
+ * EVXG_ERROR_OPERATION_TIMEDOUT if the wavefront gave up waiting. */
+#define EVXG_NOALLOC_MAX_MB_ROWS 4088
+int evxg_mb_pass_noalloc(uint32_t aligned_w, uint32_t aligned_h, const evxg_frame *frame, const int16_t *src,
+                         int16_t *const dpb[4], int16_t *levels, evxg_block_desc *blocks,
+                         const evxg_block_desc *prev_blocks, void *cuda_stream);
+
 /* ---- GOP-level encoder: evx3_encoder (evx3.h:67-100) over the stream API ---- */
 
 typedef struct evxg_encoder evxg_encoder;
