@@ -21,6 +21,7 @@ __global__ void k_sao_rdo(FrameArgs a);
 __global__ void k_sao_merge(FrameArgs a);
 __global__ void k_sao_apply(FrameArgs a);
 size_t mb_shared_bytes();
+int mb_threads();
 }  // namespace evxg
 
 using namespace evxg;
@@ -181,7 +182,7 @@ int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, con
     mark(0);
     k_convert<<<cg, 128, 0, st>>>(a);
     mark(1);
-    k_mb_wavefront<<<s->mb_grid, 256, mb_shared_bytes(), st>>>(a);
+    k_mb_wavefront<<<s->mb_grid, mb_threads(), mb_shared_bytes(), st>>>(a);
     mark(2);
     k_deblock<<<3, 1024, 0, st>>>(a);
     mark(3);

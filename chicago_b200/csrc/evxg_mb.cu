@@ -16,12 +16,15 @@
 // the destination DPB slot are the same.  Waits are bounded by a timeout that
 // sets the device error word.
 //
-// Inside an MB, 8 warps evaluate search candidates concurrently (one warp per
-// candidate: 16 lanes do 4x4 luma Hadamard/SAD/MAD, 16 lanes chroma MAD) and
-// one thread replays the reference's order-dependent acceptance rule; sub-pel
-// refinement runs one warp per direction (half and quarter from one 6-tap
-// pass); DCT, quantisation, trellis, dequantisation and IDCT of all RDO
-// candidates run thread-per-line over shared memory.
+// Inside an MB, three groups of four warps run the independent work at the
+// same time: the intra block-copy search, the forward (P: the only) inter
+// search, and the backward search (B) or the intra RDO candidates (P).  In a
+// search step every warp evaluates candidates of the 3x3 pattern (16 lanes do
+// 4x4 luma Hadamard/SAD/MAD, 16 lanes chroma MAD) and the group leader
+// replays the reference's order-dependent acceptance rule; sub-pel refinement
+// runs one warp per direction (half and quarter from one 6-tap pass); DCT,
+// quantisation, dequantisation and IDCT run thread-per-line and the trellis
+// warp-per-block over shared memory.
 #include "evxg_device.cuh"
 
 namespace evxg {
@@ -57,10 +60,12 @@ __shared__ int16_t s_qm[2][64];      // 0 intra, 1 inter
 __shared__ uint8_t s_dz[2][64];
 __shared__ uint8_t s_scan[3][64];    // 0 zigzag, 1 row-first (vertical modes), 2 column-first (horizontal modes)
 
-constexpr int NT = 256;        // threads per CTA
+constexpr int NT = 384;        // threads per CTA: three groups of four warps
 constexpr int NW = NT / 32;
+constexpr int GT = 128;        // threads per warp group
 constexpr int MB_N = 384;      // 16x16 luma + 2 x 8x8 chroma, MB buffer layout Y | U | V
 constexpr int MAXC = 5;        // RDO candidates (encode.cpp:279-364)
+constexpr int NWIN = 5;        // 0 intra (destination slot), 1/2 forward at MB / predictor, 3/4 backward
 
 struct alignas(16) Win {
     int16_t y[WL_ROWS * WL];
@@ -80,27 +85,43 @@ struct Nbr {                   // intra_pred.cpp:13-54
 };
 struct alignas(4) Desc { evxg_block_desc d; };   // 4-aligned so it can be copied as 7 words
 
-struct MbShared {
-    int16_t src[MB_N];
-    Win win[2];
-    int16_t pred[7][MB_N];     // 0 intra-BC, 1 inter/fwd, 2 bwd, 3 bi, 4..6 directional candidates
-    Nbr nb[3];
-    int lx[16], ly[16], n_list;
-    int m_sad[16], m_mad[16], m_satd[16];
-    int sdx[8], sdy[8], n_sp;
+// State of one motion search, owned by one warp group.
+struct Srch {
+    int m_sad[9], m_mad[9], m_satd[9], valid[9];
     int spm[8][4];
     Sel sel;
+    int cur;                   // window the search runs in
+    Desc out;
+    int out_sad;
+};
+
+struct MbShared {
+    int16_t src[MB_N];
+    Win win[NWIN];
+    int16_t pred[7][MB_N];     // 0 intra-BC, 1 inter/fwd, 2 bwd, 3 bi, 4..6 directional candidates
+    Nbr nb[3];
+    Srch srch[3];              // 0 intra block copy, 1 forward / P inter, 2 backward
     int thr, row_abort;
-    int pmx, pmy, qx, qy, has_pred, cur_win;
-    Desc ibc, fwd, bwd, best, cd[MAXC];
-    int ibc_sad, fwd_sad, bwd_sad, best_sad, ibc_has_pred;
+    int has_pred, sep, qx, qy;
     int modes[3], dsad[3], dir_best, dir_sad;
-    int bi_sad;
-    int ncand, chosen, rdo;
-    int cpred[MAXC];
+    int bi_sad, part[NW];
+    int cpred[MAXC], win_k, need_encode, chosen, rdo;
+    Desc cd[MAXC];             // 0 intra (no prediction), 1..3 directional modes, 4 SAD winner / final
     float cost[MAXC];
     int16_t coef[MAXC][MB_N], lev[MAXC][MB_N], rec[MAXC][MB_N], tmp[MAXC][MB_N];
 };
+
+extern __shared__ __align__(16) unsigned char g_smem[];
+__device__ __forceinline__ MbShared &SM() { return *reinterpret_cast<MbShared *>(g_smem); }
+
+// A warp group: named barrier id, first thread, thread count.  Group 0 is the
+// whole CTA (barrier 0 = __syncthreads).
+struct Grp {
+    int bar, t0, nt;
+};
+__device__ __forceinline__ void gsync(const Grp &g) { asm volatile("bar.sync %0, %1;" ::"r"(g.bar), "r"(g.nt) : "memory"); }
+constexpr Grp G_ALL{0, 0, NT};
+__device__ __forceinline__ Grp group(int k) { return Grp{1 + k, k * GT, GT}; }
 
 // ---------------------------------------------------------------- helpers
 
@@ -316,88 +337,94 @@ __device__ void accept_int(Sel &s, int x, int y, int sad, int mad, int satd, int
     if (take) { s.bx = x; s.by = y; s.sad = sad; s.ssd = ssd; s.mad = mad; s.cost = cost; }
 }
 
-// One pattern step (perform_intra/inter_motion_search, motion.cpp:348-406).
-__device__ __noinline__ void run_step(MbShared &S, const Win &w, bool intra, int l, int t, int r, int b, int st,
-                         int px, int py, int W, int H, float lambda)
+// One pattern step (perform_intra/inter_motion_search, motion.cpp:348-406) on
+// a warp group: every warp evaluates slots of the 3x3 pattern (validity is
+// decided identically by all lanes), then the group leader replays the
+// reference's loop order in registers, with its early exit.
+__device__ __noinline__ void run_step(const Grp g, int si, int wi, bool intra, int l, int t, int st, int px, int py,
+                                      int W, int H, float lambda)
 {
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (tid == 0) {
-        int n = 0;
-        const int bx = S.sel.bx, by = S.sel.by;
-        for (int j = t; j <= b; j += st)
-            for (int i = l; i <= r; i += st) {
-                const int x = bx + i, y = by + j;
-                if (intra && y > py - 16 && x > px - 16) continue;   // not yet reconstructed
-                if (x < 0 || x > W - 16 || y < 0 || y > H - 16) continue;
-                S.lx[n] = x; S.ly[n] = y; n++;
-            }
-        S.n_list = n;
+    MbShared &S = SM();
+    Srch &sr = S.srch[si];
+    const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31, nw = g.nt >> 5;
+    const int bx = sr.sel.bx, by = sr.sel.by;
+    for (int k = gw; k < 9; k += nw) {
+        const int x = bx + l + (k % 3) * st, y = by + t + (k / 3) * st;
+        const bool ok = !(intra && y > py - 16 && x > px - 16) && !(x < 0 || x > W - 16 || y < 0 || y > H - 16);
+        if (lane == 0) sr.valid[k] = ok;
+        if (ok) warp_metrics(S.src, S.win[wi], x, y, lane, &sr.m_sad[k], &sr.m_mad[k], &sr.m_satd[k]);
     }
-    __syncthreads();
-    const int n = S.n_list;
-    for (int k = warp; k < n; k += NW) warp_metrics(S.src, w, S.lx[k], S.ly[k], lane, &S.m_sad[k], &S.m_mad[k], &S.m_satd[k]);
-    __syncthreads();
-    if (tid == 0)
-        for (int k = 0; k < n; k++) {
-            accept_int(S.sel, S.lx[k], S.ly[k], S.m_sad[k], S.m_mad[k], S.m_satd[k], px, py, S.thr, lambda);
-            if (S.sel.mad < S.thr) break;   // early exit on a copy-quality match
+    gsync(g);
+    if (gt == 0) {
+        Sel s = sr.sel;
+        const int thr = S.thr;
+        for (int k = 0; k < 9; k++) {
+            if (!sr.valid[k]) continue;
+            accept_int(s, bx + l + (k % 3) * st, by + t + (k / 3) * st, sr.m_sad[k], sr.m_mad[k], sr.m_satd[k], px, py,
+                       thr, lambda);
+            if (s.mad < thr) break;   // early exit on a copy-quality match
         }
-    __syncthreads();
+        sr.sel = s;
+    }
+    gsync(g);
 }
 
 // Sub-pel refinement around the selection (motion.cpp:180-261, :408-483).
-__device__ __noinline__ void run_subpel(MbShared &S, const Win &w, bool intra, int px, int py, int W, int H)
+__device__ __noinline__ void run_subpel(const Grp g, int si, int wi, bool intra, int px, int py, int W, int H)
 {
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (tid == 0) {
-        S.sel.sp_index = 0; S.sel.sp_amount = 0; S.sel.sp_enabled = 0;
-        int n = 0;
-        for (int j = -1; j <= 1; j++)
-            for (int i = -1; i <= 1; i++) {
-                if (!i && !j) continue;
-                const int x = S.sel.bx + i, y = S.sel.by + j;
-                if (intra && y > py - 16 && x > px - 16) continue;
-                if (x < 0 || x > W - 16 || y < 0 || y > H - 16) continue;
-                S.sdx[n] = i; S.sdy[n] = j; n++;
-            }
-        S.n_sp = n;
+    MbShared &S = SM();
+    Srch &sr = S.srch[si];
+    const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31, nw = g.nt >> 5;
+    const int bx = sr.sel.bx, by = sr.sel.by;
+    for (int k = gw; k < 8; k += nw) {
+        const int r = k < 4 ? k : k + 1, i = r % 3 - 1, j = r / 3 - 1;
+        const int x = bx + i, y = by + j;
+        const bool ok = !(intra && y > py - 16 && x > px - 16) && !(x < 0 || x > W - 16 || y < 0 || y > H - 16);
+        if (lane == 0) sr.valid[k] = ok;
+        if (ok) warp_subpel(S.src, S.win[wi], bx, by, i, j, lane, sr.spm[k], nullptr, nullptr);
     }
-    __syncthreads();
-    if (warp < S.n_sp) warp_subpel(S.src, w, S.sel.bx, S.sel.by, S.sdx[warp], S.sdy[warp], lane, S.spm[warp], nullptr, nullptr);
-    __syncthreads();
-    if (tid == 0) {
-        Sel &s = S.sel;
-        for (int k = 0; k < S.n_sp; k++)
+    gsync(g);
+    if (gt == 0) {
+        Sel s = sr.sel;
+        const int thr = S.thr;
+        s.sp_index = 0; s.sp_amount = 0; s.sp_enabled = 0;
+        for (int k = 0; k < 8; k++) {
+            if (!sr.valid[k]) continue;
+            const int r = k < 4 ? k : k + 1;
             for (int q = 0; q < 2; q++) {
-                const int sad = S.spm[k][q * 2], mad = S.spm[k][q * 2 + 1];
-                const bool take = s.mad < S.thr ? (mad < s.mad)
-                                                : ((sad < s.sad && sad < SAD_THRESHOLD) || mad < S.thr);
+                const int sad = sr.spm[k][q * 2], mad = sr.spm[k][q * 2 + 1];
+                const bool take = s.mad < thr ? (mad < s.mad) : ((sad < s.sad && sad < SAD_THRESHOLD) || mad < thr);
                 if (take) {
-                    s.sp_enabled = 1; s.sp_amount = q; s.sp_index = frac_from_dir(S.sdx[k], S.sdy[k]);
+                    s.sp_enabled = 1; s.sp_amount = q; s.sp_index = frac_from_dir(r % 3 - 1, r / 3 - 1);
                     s.sad = sad; s.mad = mad;
                 }
             }
+        }
+        sr.sel = s;
     }
-    __syncthreads();
+    gsync(g);
 }
 
 // Prediction block of a search result into out: integer block or half/quarter-pel.
-__device__ void materialize(const MbShared &S, const Win &w, int x, int y, int spp, int spa, int spi, int16_t *out)
+__device__ void materialize(const Grp g, int wi, int x, int y, int spp, int spa, int spi, int16_t *out)
 {
-    const int tid = threadIdx.x;
+    MbShared &S = SM();
+    const Win &w = S.win[wi];
+    const int gt = threadIdx.x - g.t0;
     if (spp) {
-        if ((tid >> 5) == 0) {
+        if ((gt >> 5) == 0) {
             int dx, dy;
             dir_from_frac(spi, dx, dy);
-            warp_subpel(S.src, w, x, y, dx, dy, tid & 31, nullptr, spa ? nullptr : out, spa ? out : nullptr);
+            warp_subpel(S.src, w, x, y, dx, dy, gt & 31, nullptr, spa ? nullptr : out, spa ? out : nullptr);
         }
     } else {
-        const int lx = x - w.ox, ly = y - w.oy;
-        out[tid] = w.y[(ly + (tid >> 4)) * WL + lx + (tid & 15)];
-        if (tid < 128) {
-            const int p = tid >> 6, k = tid & 63;
-            const int cx = (x >> 1) - w.cox, cy = (y >> 1) - w.coy;
-            out[256 + tid] = (p ? w.v : w.u)[(cy + (k >> 3)) * WC + cx + (k & 7)];
+        const int lx = x - w.ox, ly = y - w.oy, cx = (x >> 1) - w.cox, cy = (y >> 1) - w.coy;
+        for (int e = gt; e < MB_N; e += g.nt) {
+            if (e < 256) out[e] = w.y[(ly + (e >> 4)) * WL + lx + (e & 15)];
+            else {
+                const int p = (e - 256) >> 6, k = (e - 256) & 63;
+                out[e] = (p ? w.v : w.u)[(cy + (k >> 3)) * WC + cx + (k & 7)];
+            }
         }
     }
 }
@@ -576,47 +603,49 @@ __device__ void trellis_warp(int16_t *lev, const int16_t *coef, int b, int qp, b
 
 // encode_block + decode_block for S.ncand candidates (encode.cpp:481-750,
 // decode.cpp:31-432); with S.rdo set also the RD cost (encode.cpp:39-164).
-__device__ __noinline__ void encode_candidates(MbShared &S, const FrameArgs &a)
+// encode_block + decode_block for candidates k0 .. k0+nc-1 on a warp group
+// (encode.cpp:481-750, decode.cpp:31-432); with S.rdo set also their RD cost
+// (encode.cpp:39-164).
+__device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, int k0, int nc)
 {
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nc = S.ncand;
-    // forward DCT, rows (thread per candidate x block x row)
-    if (tid < nc * 48) {
-        const int k = tid / 48, rem = tid - k * 48, b = rem >> 3, r = rem & 7;
-        if (!(S.cd[k].d.block_type & BT_COPY)) {
-            const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
-            int in[8];
+    MbShared &S = SM();
+    const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31, nw = g.nt >> 5;
+    for (int j = gt; j < nc * 48; j += g.nt) {   // forward DCT, rows
+        const int k = k0 + j / 48, rem = j % 48, b = rem >> 3, r = rem & 7;
+        if (S.cd[k].d.block_type & BT_COPY) continue;
+        const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
+        int in[8];
 #pragma unroll
-            for (int c = 0; c < 8; c++) {
-                const int e = mb_index(b, r, c);
-                in[c] = (int16_t)(pr ? S.src[e] - pr[e] : S.src[e]);
-            }
-            int16_t out[8];
-            fdct8_line(in, out);
-#pragma unroll
-            for (int c = 0; c < 8; c++) S.tmp[k][mb_index(b, r, c)] = out[c];
+        for (int c = 0; c < 8; c++) {
+            const int e = mb_index(b, r, c);
+            in[c] = (int16_t)(pr ? S.src[e] - pr[e] : S.src[e]);
         }
-    }
-    __syncthreads();
-    if (tid < nc * 48) {   // columns
-        const int k = tid / 48, rem = tid - k * 48, b = rem >> 3, c = rem & 7;
-        if (!(S.cd[k].d.block_type & BT_COPY)) {
-            int in[8];
+        int16_t out[8];
+        fdct8_line(in, out);
 #pragma unroll
-            for (int r = 0; r < 8; r++) in[r] = S.tmp[k][mb_index(b, r, c)];
-            int16_t out[8];
-            fdct8_line(in, out);
-#pragma unroll
-            for (int r = 0; r < 8; r++) S.coef[k][mb_index(b, r, c)] = out[r];
-        }
+        for (int c = 0; c < 8; c++) S.tmp[k][mb_index(b, r, c)] = out[c];
     }
-    __syncthreads();
+    gsync(g);
+    for (int j = gt; j < nc * 48; j += g.nt) {   // columns
+        const int k = k0 + j / 48, rem = j % 48, b = rem >> 3, c = rem & 7;
+        if (S.cd[k].d.block_type & BT_COPY) continue;
+        int in[8];
+#pragma unroll
+        for (int r = 0; r < 8; r++) in[r] = S.tmp[k][mb_index(b, r, c)];
+        int16_t out[8];
+        fdct8_line(in, out);
+#pragma unroll
+        for (int r = 0; r < 8; r++) S.coef[k][mb_index(b, r, c)] = out[r];
+    }
+    gsync(g);
     // adaptive QP from the luma coefficients' variance (quantize.cpp:97-118, analysis.h:251-275)
-    if (warp < nc && !(S.cd[warp].d.block_type & BT_COPY)) {
+    for (int ci = gw; ci < nc; ci += nw) {
+        const int k = k0 + ci;
+        if (S.cd[k].d.block_type & BT_COPY) continue;
         unsigned sum = 0, sq = 0, cnt = 0;
         for (int e = lane; e < 256; e += 32) {
             if (e == 0) continue;
-            const int t = S.coef[warp][e];
+            const int t = S.coef[k][e];
             if (t) { sum += (unsigned)t; sq += (unsigned)wmul(t, t); cnt++; }
         }
 #pragma unroll
@@ -630,13 +659,13 @@ __device__ __noinline__ void encode_candidates(MbShared &S, const FrameArgs &a)
             const int idx = min(max(lg2u((unsigned)var) >> 1, 1), MAXQ);
             int delta = (int16_t)((int16_t)idx - (int16_t)a.quality) >> 1;
             delta = min(max(delta, -6), 6);
-            S.cd[warp].d.q_index = (uint8_t)min(max(a.quality + delta, 1), MAXQ);
-            S.cd[warp].d.variance = (int16_t)var;
+            S.cd[k].d.q_index = (uint8_t)min(max(a.quality + delta, 1), MAXQ);
+            S.cd[k].d.variance = (int16_t)var;
         }
     }
-    __syncthreads();
-    for (int e = tid; e < nc * MB_N; e += NT) {   // quantise
-        const int k = e / MB_N, p = e - k * MB_N;
+    gsync(g);
+    for (int e = gt; e < nc * MB_N; e += g.nt) {   // quantise
+        const int k = k0 + e / MB_N, p = e % MB_N;
         const int bt = S.cd[k].d.block_type;
         if (bt & BT_COPY) continue;
         const bool chroma = p >= 256;
@@ -644,32 +673,30 @@ __device__ __noinline__ void encode_candidates(MbShared &S, const FrameArgs &a)
         const int o = chroma ? (p & 63) : (((p >> 4) & 7) * 8 + (p & 7));
         S.lev[k][p] = quant_coeff(S.coef[k][p], qp, o, intra_quant(bt), chroma);
     }
-    __syncthreads();
-    for (int j = warp; j < nc * 6; j += NW) {   // trellis, one warp per 8x8 block
-        const int k = j / 6, b = j - k * 6;
+    gsync(g);
+    for (int j = gw; j < nc * 6; j += nw) {   // trellis, one warp per 8x8 block
+        const int k = k0 + j / 6, b = j % 6;
         const int bt = S.cd[k].d.block_type;
-        if (!(bt & BT_COPY)) {
-            const int qp = b >= 4 ? min(S.cd[k].d.q_index + 2, MAXQ) : S.cd[k].d.q_index;
-            trellis_warp(S.lev[k], S.coef[k], b, qp, intra_quant(bt), S.cd[k].d.intra_mode, a.lambda, lane);
-        }
+        if (bt & BT_COPY) continue;
+        const int qp = b >= 4 ? min(S.cd[k].d.q_index + 2, MAXQ) : S.cd[k].d.q_index;
+        trellis_warp(S.lev[k], S.coef[k], b, qp, intra_quant(bt), S.cd[k].d.intra_mode, a.lambda, lane);
     }
-    __syncthreads();
-    if (tid < nc * 48) {   // dequantise + inverse DCT, columns
-        const int k = tid / 48, rem = tid - k * 48, b = rem >> 3, c = rem & 7;
+    gsync(g);
+    for (int j = gt; j < nc * 48; j += g.nt) {   // dequantise + inverse DCT, columns
+        const int k = k0 + j / 48, rem = j % 48, b = rem >> 3, c = rem & 7;
         const int bt = S.cd[k].d.block_type;
-        if (!(bt & BT_COPY)) {
-            const int qp = b >= 4 ? min(S.cd[k].d.q_index + 2, MAXQ) : S.cd[k].d.q_index;
-            int in[8], out[8];
+        if (bt & BT_COPY) continue;
+        const int qp = b >= 4 ? min(S.cd[k].d.q_index + 2, MAXQ) : S.cd[k].d.q_index;
+        int in[8], out[8];
 #pragma unroll
-            for (int r = 0; r < 8; r++) in[r] = dequant_coeff(S.lev[k][mb_index(b, r, c)], qp, r * 8 + c, intra_quant(bt), b >= 4);
-            idct8_line(in, out);
+        for (int r = 0; r < 8; r++) in[r] = dequant_coeff(S.lev[k][mb_index(b, r, c)], qp, r * 8 + c, intra_quant(bt), b >= 4);
+        idct8_line(in, out);
 #pragma unroll
-            for (int r = 0; r < 8; r++) S.tmp[k][mb_index(b, r, c)] = (int16_t)out[r];
-        }
+        for (int r = 0; r < 8; r++) S.tmp[k][mb_index(b, r, c)] = (int16_t)out[r];
     }
-    __syncthreads();
-    if (tid < nc * 48) {   // inverse DCT rows + prediction
-        const int k = tid / 48, rem = tid - k * 48, b = rem >> 3, r = rem & 7;
+    gsync(g);
+    for (int j = gt; j < nc * 48; j += g.nt) {   // inverse DCT rows + prediction
+        const int k = k0 + j / 48, rem = j % 48, b = rem >> 3, r = rem & 7;
         const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
         if (S.cd[k].d.block_type & BT_COPY) {
 #pragma unroll
@@ -686,93 +713,96 @@ __device__ __noinline__ void encode_candidates(MbShared &S, const FrameArgs &a)
             }
         }
     }
-    __syncthreads();
-    if (S.rdo && warp < nc) {   // J = (float)SSD_y + lambda * (float)bits
-        const evxg_block_desc &d = S.cd[warp].d;
-        const int bt = d.block_type;
-        int ssd = 0;
-        for (int e = lane; e < 256; e += 32) {
-            const int df = S.src[e] - S.rec[warp][e];
-            ssd = (int)((unsigned)ssd + (unsigned)wmul(df, df));
-        }
-        ssd = warp_sum(ssd);
-        // Rate of the residual: the reference's quantised and reconstructed
-        // blocks share one staging buffer (encode.cpp:151, :158), so the
-        // estimate reads the reconstruction.
-        unsigned nz = 0, cb = 0;
-        if (!(bt & BT_COPY)) {
-            const int b = lane >> 3, r = lane & 7;
+    gsync(g);
+    if (S.rdo)
+        for (int ci = gw; ci < nc; ci += nw) {   // J = (float)SSD_y + lambda * (float)bits
+            const int k = k0 + ci;
+            const evxg_block_desc &d = S.cd[k].d;
+            const int bt = d.block_type;
+            int ssd = 0;
+            for (int e = lane; e < 256; e += 32) {
+                const int df = S.src[e] - S.rec[k][e];
+                ssd = (int)((unsigned)ssd + (unsigned)wmul(df, df));
+            }
+            ssd = warp_sum(ssd);
+            // Rate of the residual: the reference's quantised and reconstructed
+            // blocks share one staging buffer (encode.cpp:151, :158), so the
+            // estimate reads the reconstruction.
+            unsigned nz = 0, cb = 0;
+            if (!(bt & BT_COPY)) {
+                const int b = lane >> 3, r = lane & 7;
 #pragma unroll
-            for (int c = 0; c < 8; c++) {
-                const int16_t v = S.rec[warp][mb_index(b, r, c)];
-                if (v) {
-                    nz++;
-                    const int av = min((int)iabs16(v), 255);
-                    cb += 2;
-                    if (av > 1) cb += 1;
-                    if (av > 2) cb += 1 + 2 * req_bits8(av - 3 + 1);
-                    else cb += 1;
+                for (int c = 0; c < 8; c++) {
+                    const int16_t v = S.rec[k][mb_index(b, r, c)];
+                    if (v) {
+                        nz++;
+                        const int av = min((int)iabs16(v), 255);
+                        cb += 2;
+                        if (av > 1) cb += 1;
+                        if (av > 2) cb += 1 + 2 * req_bits8(av - 3 + 1);
+                        else cb += 1;
+                    }
+                }
+#pragma unroll
+                for (int o = 1; o < 8; o <<= 1) {
+                    nz += __shfl_xor_sync(0xffffffffu, nz, o);
+                    cb += __shfl_xor_sync(0xffffffffu, cb, o);
                 }
             }
-#pragma unroll
-            for (int o = 1; o < 8; o <<= 1) {
-                nz += __shfl_xor_sync(0xffffffffu, nz, o);
-                cb += __shfl_xor_sync(0xffffffffu, cb, o);
+            unsigned blkbits = ((lane & 7) == 0 && !(bt & BT_COPY)) ? (unsigned)(req_bits8(nz + 1) * 2 + 1) + cb : 0;
+            blkbits += __shfl_xor_sync(0xffffffffu, blkbits, 8);
+            blkbits += __shfl_xor_sync(0xffffffffu, blkbits, 16);
+            if (lane == 0) {   // estimate_block_bits header part (encode.cpp:39-78)
+                unsigned bits = 3;
+                if (!(bt & BT_INTRA)) bits += 2;
+                if (bt & BT_MOTION) {
+                    bits += 2 * req_bits8(iabs16(d.motion_x) + 1) + 2 * req_bits8(iabs16(d.motion_y) + 1);
+                    bits += d.sp_pred ? 5 : 1;
+                }
+                if (!(bt & BT_COPY)) {
+                    if (bt == INTRA_DEFAULT) bits += 3;
+                    bits += 2 * req_bits8(iabs32(d.q_index) + 1);
+                    bits += blkbits;
+                }
+                S.cost[k] = rd_cost(ssd, a.lambda, bits);
             }
         }
-        unsigned blkbits = ((lane & 7) == 0 && !(bt & BT_COPY)) ? (unsigned)(req_bits8(nz + 1) * 2 + 1) + cb : 0;
-        blkbits += __shfl_xor_sync(0xffffffffu, blkbits, 8);
-        blkbits += __shfl_xor_sync(0xffffffffu, blkbits, 16);
-        if (lane == 0) {   // estimate_block_bits header part (encode.cpp:39-78)
-            unsigned bits = 3;
-            if (!(bt & BT_INTRA)) bits += 2;
-            if (bt & BT_MOTION) {
-                bits += 2 * req_bits8(iabs16(d.motion_x) + 1) + 2 * req_bits8(iabs16(d.motion_y) + 1);
-                bits += d.sp_pred ? 5 : 1;
-            }
-            if (!(bt & BT_COPY)) {
-                if (bt == INTRA_DEFAULT) bits += 3;
-                bits += 2 * req_bits8(iabs32(d.q_index) + 1);
-                bits += blkbits;
-            }
-            S.cost[warp] = rd_cost(ssd, a.lambda, bits);
-        }
-    }
-    __syncthreads();
+    gsync(g);
 }
 
 // ------------------------------------------------------------- searches
 
-// Intra block-copy search in the current frame (motion.cpp:485-565).
-__device__ __noinline__ void intra_bc_search(MbShared &S, const FrameArgs &a, int px, int py)
+// Intra block-copy search in the current frame (motion.cpp:485-565), window 0.
+__device__ __noinline__ void intra_bc_search(const Grp g, const FrameArgs &a, int px, int py)
 {
-    const int tid = threadIdx.x;
-    const Win &w = S.win[0];
-    if (tid < 32) {   // best_sad starts at the source's own SAD (analysis.h:133-145)
+    MbShared &S = SM();
+    Srch &sr = S.srch[0];
+    const int gt = threadIdx.x - g.t0;
+    if (gt < 32) {   // best_sad starts at the source's own SAD (analysis.h:133-145)
         int s = 0;
-        for (int e = tid; e < 256; e += 32) s += iabs16(S.src[e]);
+        for (int e = gt; e < 256; e += 32) s += iabs16(S.src[e]);
         s = warp_sum(s);
-        if (tid == 0) {
-            S.sel.bx = px; S.sel.by = py; S.sel.sad = s; S.sel.mad = INT_MAX; S.sel.ssd = INT_MAX;
-            S.sel.cost = __int2float_rn(s); S.sel.sp_index = 0; S.sel.sp_amount = 0; S.sel.sp_enabled = 0;
+        if (gt == 0) {
+            sr.sel.bx = px; sr.sel.by = py; sr.sel.sad = s; sr.sel.mad = INT_MAX; sr.sel.ssd = INT_MAX;
+            sr.sel.cost = __int2float_rn(s); sr.sel.sp_index = 0; sr.sel.sp_amount = 0; sr.sel.sp_enabled = 0;
         }
     }
-    __syncthreads();
-    run_step(S, w, true, -SEARCH_RADIUS, -(SEARCH_RADIUS << 1), SEARCH_RADIUS, 0, SEARCH_RADIUS, px, py, a.W, a.H, a.lambda);
-    if (S.sel.mad >= S.thr)
+    gsync(g);
+    run_step(g, 0, 0, true, -SEARCH_RADIUS, -(SEARCH_RADIUS << 1), SEARCH_RADIUS, px, py, a.W, a.H, a.lambda);
+    if (sr.sel.mad >= S.thr)
         for (int st = SEARCH_RADIUS >> 1; st > 0; st >>= 1) {
-            run_step(S, w, true, -st, -st, st, st, st, px, py, a.W, a.H, a.lambda);
-            if (S.sel.mad < S.thr) break;
+            run_step(g, 0, 0, true, -st, -st, st, px, py, a.W, a.H, a.lambda);
+            if (sr.sel.mad < S.thr) break;
         }
-    run_subpel(S, w, true, px, py, a.W, a.H);
-    if (tid == 0) {
-        fill_desc(S.sel, px, py, true, S.thr, S.ibc.d);
-        S.ibc_sad = S.sel.sad;
-        S.ibc_has_pred = (S.ibc.d.block_type & BT_MOTION) != 0;
+    run_subpel(g, 0, 0, true, px, py, a.W, a.H);
+    if (gt == 0) {
+        fill_desc(sr.sel, px, py, true, S.thr, sr.out.d);
+        sr.out_sad = sr.sel.sad;
     }
-    __syncthreads();
-    if (S.ibc_has_pred) materialize(S, w, S.sel.bx, S.sel.by, S.sel.sp_enabled, S.sel.sp_amount, S.sel.sp_index, S.pred[0]);
-    __syncthreads();
+    gsync(g);
+    if (sr.out.d.block_type & BT_MOTION)
+        materialize(g, 0, sr.sel.bx, sr.sel.by, sr.sel.sp_enabled, sr.sel.sp_amount, sr.sel.sp_index, S.pred[0]);
+    gsync(g);
 }
 
 // MV predictor (motion.cpp:271-346) from the live block table and, for P
@@ -804,62 +834,118 @@ __device__ void mv_predictor(const FrameArgs &a, int idx, bool temporal, int &ox
     }
 }
 
-// Inter search against one DPB slot (motion.cpp:567-679); result descriptor,
-// SAD and prediction block.
-__device__ __noinline__ void inter_search(MbShared &S, const FrameArgs &a, int slot, bool temporal, int px, int py, int idx,
-                             evxg_block_desc &out, int &out_sad, int16_t *pred_out)
+// Inter search (motion.cpp:567-679) on one warp group: window wa holds the
+// reference around the MB, wb around the predictor when that differs.
+__device__ __noinline__ void inter_search(const Grp g, const FrameArgs &a, int si, int wa, int wb, int px, int py,
+                                          int16_t *pred_out)
 {
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (tid == 0) {
-        int pmx, pmy;
-        mv_predictor(a, idx, temporal, pmx, pmy);
-        S.has_pred = (pmx || pmy);
-        int qx = min(max(px + pmx, 0), a.W - 16), qy = min(max(py + pmy, 0), a.H - 16);
-        S.qx = qx; S.qy = qy;
-        S.cur_win = 0;
-    }
-    __syncthreads();
-    const bool sep = S.has_pred && (S.qx != px || S.qy != py);
-    load_window<false>(S.win[0], a.planes[slot], a.W, a.H, px, py);
-    if (sep) load_window<false>(S.win[1], a.planes[slot], a.W, a.H, S.qx, S.qy);
-    __syncthreads();
-    if (warp == 0) warp_metrics(S.src, S.win[0], px, py, lane, &S.m_sad[0], &S.m_mad[0], &S.m_satd[0]);
-    if (warp == 1 && S.has_pred) warp_metrics(S.src, S.win[sep ? 1 : 0], S.qx, S.qy, lane, &S.m_sad[1], &S.m_mad[1], &S.m_satd[1]);
-    __syncthreads();
-    if (tid == 0) {
-        Sel &s = S.sel;
-        s.bx = px; s.by = py; s.sad = S.m_sad[0]; s.mad = S.m_mad[0]; s.ssd = INT_MAX;
-        s.cost = rd_cost(S.m_satd[0], a.lambda, 1u);
+    MbShared &S = SM();
+    Srch &sr = S.srch[si];
+    const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31;
+    if (gw == 0) warp_metrics(S.src, S.win[wa], px, py, lane, &sr.m_sad[0], &sr.m_mad[0], &sr.m_satd[0]);
+    if (gw == 1 && S.has_pred)
+        warp_metrics(S.src, S.win[S.sep ? wb : wa], S.qx, S.qy, lane, &sr.m_sad[1], &sr.m_mad[1], &sr.m_satd[1]);
+    gsync(g);
+    if (gt == 0) {
+        Sel s;
+        s.bx = px; s.by = py; s.sad = sr.m_sad[0]; s.mad = sr.m_mad[0]; s.ssd = INT_MAX;
+        s.cost = rd_cost(sr.m_satd[0], a.lambda, 1u);
         s.sp_index = 0; s.sp_amount = 0; s.sp_enabled = 0;
-        if (S.has_pred) accept_int(s, S.qx, S.qy, S.m_sad[1], S.m_mad[1], S.m_satd[1], px, py, S.thr, a.lambda);
-        S.cur_win = (sep && s.bx == S.qx && s.by == S.qy) ? 1 : 0;
+        if (S.has_pred) accept_int(s, S.qx, S.qy, sr.m_sad[1], sr.m_mad[1], sr.m_satd[1], px, py, S.thr, a.lambda);
+        sr.sel = s;
+        sr.cur = (S.sep && s.bx == S.qx && s.by == S.qy) ? wb : wa;
     }
-    __syncthreads();
-    const Win &w = S.win[S.cur_win];
-    if (S.sel.mad >= S.thr) {
+    gsync(g);
+    const int wi = sr.cur;
+    if (sr.sel.mad >= S.thr) {
         int r = SEARCH_RADIUS;   // adaptive radius, motion.cpp:640-646
-        if (S.sel.sad < SAD_THRESHOLD / 4) r = SEARCH_RADIUS / 4;
-        else if (S.sel.sad < SAD_THRESHOLD / 2) r = SEARCH_RADIUS / 2;
+        if (sr.sel.sad < SAD_THRESHOLD / 4) r = SEARCH_RADIUS / 4;
+        else if (sr.sel.sad < SAD_THRESHOLD / 2) r = SEARCH_RADIUS / 2;
         for (int st = r; st > 0; st >>= 1) {
-            run_step(S, w, false, -st, -st, st, st, st, px, py, a.W, a.H, a.lambda);
-            if (S.sel.mad < S.thr) break;
+            run_step(g, si, wi, false, -st, -st, st, px, py, a.W, a.H, a.lambda);
+            if (sr.sel.mad < S.thr) break;
         }
-        run_subpel(S, w, false, px, py, a.W, a.H);
+        run_subpel(g, si, wi, false, px, py, a.W, a.H);
     }
-    materialize(S, w, S.sel.bx, S.sel.by, S.sel.sp_enabled, S.sel.sp_amount, S.sel.sp_index, pred_out);
-    if (tid == 0) {
-        fill_desc(S.sel, px, py, false, S.thr, out);
-        out_sad = S.sel.sad;
+    materialize(g, wi, sr.sel.bx, sr.sel.by, sr.sel.sp_enabled, sr.sel.sp_amount, sr.sel.sp_index, pred_out);
+    if (gt == 0) {
+        fill_desc(sr.sel, px, py, false, S.thr, sr.out.d);
+        sr.out_sad = sr.sel.sad;
     }
-    __syncthreads();
+    gsync(g);
 }
 
-// Neighbours of the MB for directional intra, from the intra window (base (px, py-16)).
-__device__ __noinline__ void extract_neighbours(MbShared &S, int px, int py)
+// Directional intra: 3 predictions and the best by luma SAD (intra_pred.cpp:219-289).
+__device__ __noinline__ void directional_intra(const Grp g)
 {
+    MbShared &S = SM();
+    const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31;
+    for (int e = gt; e < 3 * MB_N; e += g.nt) {
+        const int m = e / MB_N, p = e % MB_N;
+        int16_t v;
+        if (p < 256) v = intra_px(S.modes[m], S.nb[0], 16, p & 15, p >> 4);
+        else { const int q = p - 256, pl = q >> 6, k = q & 63; v = intra_px(S.modes[m], S.nb[1 + pl], 8, k & 7, k >> 3); }
+        S.pred[4 + m][p] = v;
+    }
+    gsync(g);
+    if (gw < 3) {
+        int s = 0;
+        for (int e = lane; e < 256; e += 32) s += iabs32(S.src[e] - S.pred[4 + gw][e]);
+        s = warp_sum(s);
+        if (lane == 0) S.dsad[gw] = s;
+    }
+    gsync(g);
+    if (gt == 0) {
+        int best = INT_MAX, bm = 0;
+        for (int m = 0; m < 3; m++) if (S.dsad[m] < best) { best = S.dsad[m]; bm = m; }
+        S.dir_best = bm; S.dir_sad = best;
+    }
+    gsync(g);
+}
+
+// ------------------------------------------------------------- per MB
+
+__device__ void process_mb(const FrameArgs &a, int row, int col)
+{
+    MbShared &S = SM();
     const int tid = threadIdx.x;
-    const Win &w = S.win[0];
-    if (tid < 3) {
+    const int px = col * 16, py = row * 16, idx = row * a.mbw + col;
+    const int16_t *srcY = a.src, *srcU = a.src + (size_t)a.W * a.H, *srcV = srcU + (size_t)(a.W / 2) * (a.H / 2);
+    int16_t *dst = a.planes[a.dpb];
+
+    for (int e = tid; e < MB_N; e += NT) {
+        if (e < 256) S.src[e] = __ldg(srcY + (size_t)(py + (e >> 4)) * a.W + px + (e & 15));
+        else {
+            const int pl = (e - 256) >> 6, k = (e - 256) & 63;
+            S.src[e] = __ldg((pl ? srcV : srcU) + (size_t)((py >> 1) + (k >> 3)) * (a.W / 2) + (px >> 1) + (k & 7));
+        }
+    }
+    if (tid == 0) {
+        S.thr = (a.quality >> 2) + 1;   // mad_skip_threshold, motion.cpp:501
+        S.rdo = a.type == EVXG_FRAME_INTER;
+        S.has_pred = 0; S.sep = 0; S.qx = px; S.qy = py;
+        if (a.type != EVXG_FRAME_INTRA) {   // one predictor serves every search of this MB
+            int pmx, pmy;
+            mv_predictor(a, idx, a.type == EVXG_FRAME_INTER, pmx, pmy);
+            S.has_pred = (pmx || pmy);
+            S.qx = min(max(px + pmx, 0), a.W - 16);
+            S.qy = min(max(py + pmy, 0), a.H - 16);
+            S.sep = S.has_pred && (S.qx != px || S.qy != py);
+        }
+    }
+    __syncthreads();
+    load_window<true>(S.win[0], dst, a.W, a.H, px, py - 16);
+    if (a.type != EVXG_FRAME_INTRA) {
+        load_window<false>(S.win[1], a.planes[a.ref_fwd], a.W, a.H, px, py);
+        if (S.sep) load_window<false>(S.win[2], a.planes[a.ref_fwd], a.W, a.H, S.qx, S.qy);
+    }
+    if (a.type == EVXG_FRAME_BIDIR) {
+        load_window<false>(S.win[3], a.planes[a.ref_bwd], a.W, a.H, px, py);
+        if (S.sep) load_window<false>(S.win[4], a.planes[a.ref_bwd], a.W, a.H, S.qx, S.qy);
+    }
+    __syncthreads();
+    if (tid < 3) {   // neighbours for directional intra, from window 0 (intra_pred.cpp:13-54)
+        const Win &w = S.win[0];
         Nbr &nb = S.nb[tid];
         const int n = tid ? 8 : 16;
         const int16_t *pl = tid == 0 ? w.y : (tid == 1 ? w.u : w.v);
@@ -892,61 +978,33 @@ __device__ __noinline__ void extract_neighbours(MbShared &S, int px, int py)
         else { S.modes[1] = 3; S.modes[2] = 4; }
     }
     __syncthreads();
-}
 
-// Directional intra: 3 predictions and the best by luma SAD (intra_pred.cpp:219-289).
-__device__ __noinline__ void directional_intra(MbShared &S)
-{
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    for (int e = tid; e < 3 * MB_N; e += NT) {
-        const int m = e / MB_N, p = e - m * MB_N;
-        int16_t v;
-        if (p < 256) v = intra_px(S.modes[m], S.nb[0], 16, p & 15, p >> 4);
-        else { const int q = p - 256, pl = q >> 6, k = q & 63; v = intra_px(S.modes[m], S.nb[1 + pl], 8, k & 7, k >> 3); }
-        S.pred[4 + m][p] = v;
+    // Independent work runs concurrently on three warp groups.
+    const int gi = tid / GT;
+    const Grp g = group(gi);
+    if (gi == 0) {
+        intra_bc_search(g, a, px, py);
+        if (a.type == EVXG_FRAME_BIDIR) directional_intra(g);
+    } else if (gi == 1) {
+        if (a.type == EVXG_FRAME_INTRA) directional_intra(g);
+        else inter_search(g, a, 1, 1, 2, px, py, S.pred[1]);
+    } else {
+        if (a.type == EVXG_FRAME_BIDIR) {
+            inter_search(g, a, 2, 3, 4, px, py, S.pred[2]);
+        } else if (a.type == EVXG_FRAME_INTER) {
+            // The intra RDO candidates do not depend on the searches
+            // (encode.cpp:295-336): encode them while the searches run.
+            directional_intra(g);
+            if (tid - g.t0 == 0) {
+                clear_desc(S.cd[0].d); S.cpred[0] = -1;
+                for (int m = 0; m < 3; m++) { clear_desc(S.cd[1 + m].d); S.cd[1 + m].d.intra_mode = (uint8_t)S.modes[m]; S.cpred[1 + m] = 4 + m; }
+            }
+            gsync(g);
+            encode_candidates(g, a, 0, 4);
+        }
     }
     __syncthreads();
-    if (warp < 3) {
-        int s = 0;
-        for (int e = lane; e < 256; e += 32) s += iabs32(S.src[e] - S.pred[4 + warp][e]);
-        s = warp_sum(s);
-        if (lane == 0) S.dsad[warp] = s;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        int best = INT_MAX, bm = 0;
-        for (int m = 0; m < 3; m++) if (S.dsad[m] < best) { best = S.dsad[m]; bm = m; }
-        S.dir_best = bm; S.dir_sad = best;
-    }
-    __syncthreads();
-}
-
-// ------------------------------------------------------------- per MB
-
-__device__ void process_mb(MbShared &S, const FrameArgs &a, int row, int col)
-{
-    const int tid = threadIdx.x;
-    const int px = col * 16, py = row * 16, idx = row * a.mbw + col;
-    const int16_t *srcY = a.src, *srcU = a.src + (size_t)a.W * a.H, *srcV = srcU + (size_t)(a.W / 2) * (a.H / 2);
-    int16_t *dst = a.planes[a.dpb];
-
-    S.src[tid] = __ldg(srcY + (size_t)(py + (tid >> 4)) * a.W + px + (tid & 15));
-    if (tid < 128) {
-        const int pl = tid >> 6, k = tid & 63;
-        S.src[256 + tid] = __ldg((pl ? srcV : srcU) + (size_t)((py >> 1) + (k >> 3)) * (a.W / 2) + (px >> 1) + (k & 7));
-    }
-    if (tid == 0) S.thr = (a.quality >> 2) + 1;   // mad_skip_threshold, motion.cpp:501
-    load_window<true>(S.win[0], dst, a.W, a.H, px, py - 16);
-    __syncthreads();
-    extract_neighbours(S, px, py);
-    intra_bc_search(S, a, px, py);
-
-    if (a.type == EVXG_FRAME_INTER) {
-        inter_search(S, a, a.ref_fwd, true, px, py, idx, S.fwd.d, S.fwd_sad, S.pred[1]);
-    } else if (a.type == EVXG_FRAME_BIDIR) {
-        inter_search(S, a, a.ref_fwd, false, px, py, idx, S.fwd.d, S.fwd_sad, S.pred[1]);
-        inter_search(S, a, a.ref_bwd, false, px, py, idx, S.bwd.d, S.bwd_sad, S.pred[2]);
-        // bi-prediction: (f + b + 1) >> 1, SAD over Y, U and V (motion.cpp:778-813)
+    if (a.type == EVXG_FRAME_BIDIR) {   // bi-prediction: (f + b + 1) >> 1, SAD over Y, U, V (motion.cpp:778-813)
         int s = 0;
         for (int e = tid; e < MB_N; e += NT) {
             const int av = (S.pred[1][e] + S.pred[2][e] + 1) >> 1;
@@ -954,31 +1012,29 @@ __device__ void process_mb(MbShared &S, const FrameArgs &a, int row, int col)
             s += iabs32(S.src[e] - av);
         }
         s = warp_sum(s);
-        if ((tid & 31) == 0) S.m_sad[tid >> 5] = s;
+        if ((tid & 31) == 0) S.part[tid >> 5] = s;
         __syncthreads();
         if (tid == 0) {
             int t = 0;
-            for (int k = 0; k < NW; k++) t += S.m_sad[k];
+            for (int k = 0; k < NW; k++) t += S.part[k];
             S.bi_sad = t;
         }
     }
-    directional_intra(S);
-
     if (tid == 0) {   // candidate decision (encode.cpp:168-277, :374-470)
-        evxg_block_desc best = S.ibc.d;
-        int bsad = S.ibc_sad, bpred = S.ibc_has_pred ? 0 : -1;
+        evxg_block_desc best = S.srch[0].out.d;
+        int bsad = S.srch[0].out_sad, bpred = (best.block_type & BT_MOTION) ? 0 : -1;
         if (a.type == EVXG_FRAME_INTER) {
-            evxg_block_desc in = S.fwd.d;
+            evxg_block_desc in = S.srch[1].out.d;
             in.prediction_target = (uint8_t)a.ref_fwd;
             const bool ci = in.block_type & BT_COPY, cb = best.block_type & BT_COPY;
-            if (ci != cb) { if (ci) { best = in; bsad = S.fwd_sad; bpred = 1; } }
-            else if (S.fwd_sad < bsad) { best = in; bsad = S.fwd_sad; bpred = 1; }
+            if (ci != cb) { if (ci) { best = in; bsad = S.srch[1].out_sad; bpred = 1; } }
+            else if (S.srch[1].out_sad < bsad) { best = in; bsad = S.srch[1].out_sad; bpred = 1; }
         } else if (a.type == EVXG_FRAME_BIDIR) {
-            evxg_block_desc f = S.fwd.d, b = S.bwd.d;
+            evxg_block_desc f = S.srch[1].out.d, b = S.srch[2].out.d;
             f.prediction_mode = 0; f.prediction_target = (uint8_t)a.ref_fwd;
             b.prediction_mode = 1; b.prediction_target = (uint8_t)a.ref_bwd;
-            if (S.fwd_sad < bsad) { best = f; bsad = S.fwd_sad; bpred = 1; }
-            if (S.bwd_sad < bsad) { best = b; bsad = S.bwd_sad; bpred = 2; }
+            if (S.srch[1].out_sad < bsad) { best = f; bsad = S.srch[1].out_sad; bpred = 1; }
+            if (S.srch[2].out_sad < bsad) { best = b; bsad = S.srch[2].out_sad; bpred = 2; }
             const int bias = __float2int_rz(__fmul_rn(a.lambda, 8.0f));
             if (S.bi_sad + bias < bsad) {
                 evxg_block_desc bi;
@@ -993,27 +1049,32 @@ __device__ void process_mb(MbShared &S, const FrameArgs &a, int row, int col)
                 best = bi; bsad = S.bi_sad; bpred = 3;
             }
         }
+        int dir_k = -1;
         if (S.dir_sad < bsad) {
             clear_desc(best);
             best.intra_mode = (uint8_t)S.modes[S.dir_best];
             bsad = S.dir_sad;
             bpred = 4 + S.dir_best;
+            dir_k = 1 + S.dir_best;
         }
-        int n = 0;
-        S.cd[n].d = best; S.cpred[n++] = bpred;
-        S.rdo = (a.type == EVXG_FRAME_INTER);
-        if (S.rdo) {   // RDO candidates (encode.cpp:279-364)
-            if (best.block_type != INTRA_DEFAULT) { clear_desc(S.cd[n].d); S.cpred[n++] = -1; }
-            for (int m = 0; m < 3; m++) { clear_desc(S.cd[n].d); S.cd[n].d.intra_mode = (uint8_t)S.modes[m]; S.cpred[n++] = 4 + m; }
+        if (a.type == EVXG_FRAME_INTER && best.block_type == INTRA_DEFAULT) {
+            // already encoded with the intra RDO candidates
+            S.win_k = best.intra_mode == MODE_NONE ? 0 : dir_k;
+            S.need_encode = 0;
+        } else {
+            S.cd[4].d = best; S.cpred[4] = bpred;
+            S.win_k = 4; S.need_encode = 1;
         }
-        S.ncand = n;
     }
     __syncthreads();
-    encode_candidates(S, a);
+    if (S.need_encode) encode_candidates(G_ALL, a, 4, 1);
     if (tid == 0) {
-        int ch = 0;
-        if (S.rdo)
-            for (int k = 1; k < S.ncand; k++) if (S.cost[k] < S.cost[ch]) ch = k;
+        int ch = S.win_k;
+        if (S.rdo) {   // RDO order: SAD winner, intra default (if the winner is not), the 3 modes (encode.cpp:279-336)
+            float bc = S.cost[ch];
+            if (S.cd[S.win_k].d.block_type != INTRA_DEFAULT && S.cost[0] < bc) { ch = 0; bc = S.cost[0]; }
+            for (int k = 1; k <= 3; k++) if (S.cost[k] < bc) { ch = k; bc = S.cost[k]; }
+        }
         S.chosen = ch;
     }
     __syncthreads();
@@ -1022,25 +1083,25 @@ __device__ void process_mb(MbShared &S, const FrameArgs &a, int row, int col)
     const bool copy = S.cd[ch].d.block_type & BT_COPY;
     int16_t *dU = dst + (size_t)a.W * a.H, *dV = dU + (size_t)(a.W / 2) * (a.H / 2);
     int16_t *lY = a.lev, *lU = a.lev + (size_t)a.W * a.H, *lV = lU + (size_t)(a.W / 2) * (a.H / 2);
-    {
-        const size_t o = (size_t)(py + (tid >> 4)) * a.W + px + (tid & 15);
-        dst[o] = S.rec[ch][tid];
-        if (!copy) lY[o] = S.lev[ch][tid];
-        if (tid < 128) {
-            const int pl = tid >> 6, k = tid & 63;
+    for (int e = tid; e < MB_N; e += NT) {
+        if (e < 256) {
+            const size_t o = (size_t)(py + (e >> 4)) * a.W + px + (e & 15);
+            dst[o] = S.rec[ch][e];
+            if (!copy) lY[o] = S.lev[ch][e];
+        } else {
+            const int pl = (e - 256) >> 6, k = (e - 256) & 63;
             const size_t oc = (size_t)((py >> 1) + (k >> 3)) * (a.W / 2) + (px >> 1) + (k & 7);
-            (pl ? dV : dU)[oc] = S.rec[ch][256 + tid];
-            if (!copy) (pl ? lV : lU)[oc] = S.lev[ch][256 + tid];
+            (pl ? dV : dU)[oc] = S.rec[ch][e];
+            if (!copy) (pl ? lV : lU)[oc] = S.lev[ch][e];
         }
-        if (tid < 7) reinterpret_cast<int *>(a.bt + idx)[tid] = reinterpret_cast<const int *>(&S.cd[ch].d)[tid];
     }
+    if (tid < 7) reinterpret_cast<int *>(a.bt + idx)[tid] = reinterpret_cast<const int *>(&S.cd[ch].d)[tid];
     __threadfence();   // every writer orders its stores before the row's progress release
 }
 
 __global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    MbShared &S = *reinterpret_cast<MbShared *>(smem_raw);
+    MbShared &S = SM();
     __shared__ int s_row;
     const int tid = threadIdx.x;
     if (tid < 64) {
@@ -1069,23 +1130,21 @@ __global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a)
                             S.row_abort = 1;
                             break;
                         }
-                        __nanosleep(128);
+                        __nanosleep(64);
                     }
                 }
             }
             __syncthreads();
             if (S.row_abort) return;
-            process_mb(S, a, row, col);
+            process_mb(a, row, col);
             __syncthreads();
-            if (tid == 0) {
-                __threadfence();
-                st_release(&a.progress[row], col);
-            }
+            if (tid == 0) st_release(&a.progress[row], col);
         }
         __syncthreads();
     }
 }
 
 size_t mb_shared_bytes() { return sizeof(MbShared); }
+int mb_threads() { return NT; }
 
 }  // namespace evxg

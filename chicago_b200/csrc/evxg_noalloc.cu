@@ -18,6 +18,7 @@
 namespace evxg {
 __global__ void k_mb_wavefront(FrameArgs a);
 size_t mb_shared_bytes();
+int mb_threads();
 }  // namespace evxg
 
 using namespace evxg;
@@ -93,7 +94,7 @@ extern "C" int evxg_mb_pass_noalloc(uint32_t aligned_w, uint32_t aligned_h, cons
     if (cudaMemsetAsync(scratch, 0xFF, mbh * sizeof(int), st) != cudaSuccess) return EVXG_ERROR_EXECUTION_FAILURE;
     if (cudaMemsetAsync(scratch + mbh, 0, 5 * sizeof(int), st) != cudaSuccess) return EVXG_ERROR_EXECUTION_FAILURE;
     const int grid = (int)(mbh < (uint32_t)g_num_sms[dev] ? mbh : (uint32_t)g_num_sms[dev]);
-    k_mb_wavefront<<<grid, 256, mb_shared_bytes(), st>>>(a);
+    k_mb_wavefront<<<grid, mb_threads(), mb_shared_bytes(), st>>>(a);
     if (cudaGetLastError() != cudaSuccess) return EVXG_ERROR_EXECUTION_FAILURE;
     int err = 0;
     if (cudaMemcpyAsync(&err, scratch + mbh + 4, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
