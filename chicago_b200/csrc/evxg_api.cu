@@ -19,7 +19,9 @@ __global__ void k_mb_wavefront(FrameArgs a);
 __global__ void k_deblock(FrameArgs a);
 __global__ void k_sao_rdo(FrameArgs a);
 __global__ void k_sao_merge(FrameArgs a);
-__global__ void k_sao_apply(FrameArgs a);
+__global__ void k_sao_fix(FrameArgs a, int pass);
+__global__ void k_sao_restore(FrameArgs a, int last_pass);
+__global__ void k_sao_apply(FrameArgs a, int last_pass);
 size_t mb_shared_bytes();
 int mb_threads();
 }  // namespace evxg
@@ -27,6 +29,9 @@ int mb_threads();
 using namespace evxg;
 
 static thread_local std::string g_last_error;
+// Fixed-point passes of the SAO application (evxg_filters.cu); the chains they
+// resolve are a few pixels long, the last pass only confirms.
+static const int kSaoPasses = 8;
 
 static int fail(int code, const char *what)
 {
@@ -51,6 +56,8 @@ struct evxg_stream {
     evxg_block_desc *bt, *prev, *prev_ser;
     evxg_sao_info *sao;
     float *sao_cost;
+    int16_t *sao_orig;                  // pristine copy for the SAO fixed-point passes
+    int *sao_flags;
     uint8_t *rgb;
     int *sync;                          // 3*mbh progress words, 4 counters, 1 error word
     int mb_grid, num_sms;
@@ -89,6 +96,8 @@ int evxg_stream_create(uint32_t width, uint32_t height, evxg_stream **out)
     if (e == cudaSuccess) e = cudaMalloc(&s->prev_ser, nblk * sizeof(evxg_block_desc));
     if (e == cudaSuccess) e = cudaMalloc(&s->sao, nblk * sizeof(evxg_sao_info));
     if (e == cudaSuccess) e = cudaMalloc(&s->sao_cost, nblk * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&s->sao_orig, pb);
+    if (e == cudaSuccess) e = cudaMalloc(&s->sao_flags, kSaoPasses * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&s->rgb, (size_t)width * height * 3);
     if (e == cudaSuccess) e = cudaMalloc(&s->sync, (3 * s->mbh + 5) * sizeof(int));
     // The reference zero-fills every image and table at allocation (image.cpp:89,
@@ -121,6 +130,7 @@ int evxg_stream_destroy(evxg_stream *s)
     for (int i = 0; i < 4; i++) cudaFree(s->dpb[i]);
     cudaFree(s->bt); cudaFree(s->prev); cudaFree(s->prev_ser);
     cudaFree(s->sao); cudaFree(s->sao_cost); cudaFree(s->rgb); cudaFree(s->sync);
+    cudaFree(s->sao_orig); cudaFree(s->sao_flags);
     if (s->profile)
         for (int i = 0; i < 7; i++) cudaEventDestroy(s->ev[i]);
     delete s;
@@ -168,6 +178,7 @@ int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, con
     a.src = s->src; a.lev = s->lev; a.bt = s->bt;
     a.prev = f->type == EVXG_FRAME_INTER ? s->prev : nullptr;
     a.sao = s->sao; a.sao_cost = s->sao_cost; a.rgb = drgb;
+    a.sao_orig = s->sao_orig; a.sao_flags = s->sao_flags;
     a.progress = s->sync; a.counters = s->sync + 3 * s->mbh; a.error = s->sync + 3 * s->mbh + 4;
     a.timeout_ns = s->timeout_ns;
     const size_t nblk = (size_t)s->mbw * s->mbh;
@@ -186,13 +197,17 @@ int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, con
     mark(2);
     k_deblock<<<3, 1024, 0, st>>>(a);
     mark(3);
+    CK(cudaMemcpyAsync(s->sao_orig, s->dpb[f->dpb_slot], s->plane_elems * sizeof(int16_t), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemsetAsync(s->sao_flags, 0, kSaoPasses * sizeof(int), st));
     k_sao_rdo<<<(unsigned)((nblk + 127) / 128), 128, 0, st>>>(a);
     mark(4);
     k_sao_merge<<<wf, 256, 0, st>>>(a);
     mark(5);
-    k_sao_apply<<<wf, 256, 0, st>>>(a);
+    for (int p = 0; p < kSaoPasses; p++) k_sao_fix<<<s->num_sms * 8, 256, 0, st>>>(a, p);
+    k_sao_restore<<<s->num_sms * 4, 256, 0, st>>>(a, kSaoPasses - 1);
+    k_sao_apply<<<wf, 256, 0, st>>>(a, kSaoPasses - 1);
     mark(6);
-    s->launches = 6;
+    s->launches = 7 + kSaoPasses;
     CK(cudaGetLastError());
     if (f->type != EVXG_FRAME_BIDIR)   // temporal MV predictor table (encode.cpp:990-998)
         CK(cudaMemcpyAsync(s->prev, s->bt, nblk * sizeof(evxg_block_desc), cudaMemcpyDeviceToDevice, st));

@@ -100,6 +100,8 @@ struct FrameArgs {
     const evxg_block_desc *prev; // temporal MV predictor table (P frames), else null
     evxg_sao_info *sao;          // final SAO table
     float *sao_cost;             // per-MB own-parameter SAO cost (RDO -> merge)
+    int16_t *sao_orig;           // deblocked, not yet SAO-filtered copy of the destination slot
+    int *sao_flags;              // per fixed-point pass: 1 if the pass changed a pixel
     const uint8_t *rgb;          // device RGB24 input
     int *progress;               // per-MB-row progress words (wavefronts)
     int *counters;               // [0] next MB row, [1] next SAO merge row, [2] next SAO apply row

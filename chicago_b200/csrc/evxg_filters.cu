@@ -300,68 +300,200 @@ __device__ bool wait_row(const FrameArgs &a, const int *progress, int row, int n
     return __shfl_sync(0xffffffffu, ok, 0);
 }
 
-// Luma SSD of MB m under params p, one warp (sao.cpp:346-387 without the rate).
-__device__ long long warp_sao_ssd(const FrameArgs &a, int bx, int by, const evxg_sao_params &p)
+// ---- merge decisions (sao.cpp:559-586) ----
+// One warp per MB row in a wavefront: MB (r, c) needs the final parameters of
+// (r-1, c) and (r, c-1).  Merge costs read the deblocked, not yet filtered
+// frame, which does not change during this kernel, so each warp prefetches
+// the next MB's tile (recon rows y0-1..y0+16, columns x0-2..x0+17, and the
+// source block) into registers while it waits for the row above.
+constexpr int MT_W = 20, MT_H = 18;   // recon tile, 10 words per row
+struct MergeTile {
+    int16_t rec[MT_H * MT_W];
+    int16_t src[256];
+};
+struct TileRegs {
+    unsigned r[6], s[4];
+};
+
+__device__ __forceinline__ void tile_load(const FrameArgs &a, int c, int row, int lane, TileRegs &t)
 {
-    const int lane = threadIdx.x & 31;
     const int16_t *rec = a.planes[a.dpb];
-    const int y = by * 16 + (lane >> 1), x0 = bx * 16 + (lane & 1) * 8;
+    const int x0 = c * 16 - 2, y0 = row * 16 - 1;
+#pragma unroll
+    for (int i = 0; i < 6; i++) {   // 180 words of the recon tile
+        const int wi = lane + 32 * i;
+        if (wi < MT_H * MT_W / 2) {
+            const int ty = wi / (MT_W / 2), tx = 2 * (wi % (MT_W / 2));
+            const int y = min(max(y0 + ty, 0), a.H - 1), x = min(max(x0 + tx, 0), a.W - 2);
+            t.r[i] = __ldg(reinterpret_cast<const unsigned *>(rec + (size_t)y * a.W + x));
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {   // 128 words of the source block
+        const int wi = lane + 32 * i;
+        const int ty = wi >> 3, tx = 2 * (wi & 7);
+        t.s[i] = __ldg(reinterpret_cast<const unsigned *>(a.src + (size_t)(row * 16 + ty) * a.W + c * 16 + tx));
+    }
+}
+__device__ __forceinline__ void tile_store(MergeTile &m, int lane, const TileRegs &t)
+{
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        const int wi = lane + 32 * i;
+        if (wi < MT_H * MT_W / 2) reinterpret_cast<unsigned *>(m.rec)[wi] = t.r[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) reinterpret_cast<unsigned *>(m.src)[lane + 32 * i] = t.s[i];
+}
+// Luma SSD of the tile's MB under p, one warp (sao.cpp:346-387 without the rate).
+__device__ long long tile_sao_ssd(const FrameArgs &a, const MergeTile &m, int c, int row, int lane, const evxg_sao_params &p)
+{
+    const int ty = lane >> 1, tx0 = (lane & 1) * 8;
+    const int y = row * 16 + ty;
     long long acc = 0;
+#pragma unroll
     for (int i = 0; i < 8; i++) {
-        const int x = x0 + i;
-        const int d = a.src[(size_t)y * a.W + x] - sao_px(rec, a.W, a.H, x, y, p);
+        const int tx = tx0 + i, x = c * 16 + tx;
+        const int v = m.rec[(ty + 1) * MT_W + tx + 2];
+        int corr = v;
+        if (p.type == 2) {
+            const int idx = (sclamp(v) >> 3) - p.band_position;
+            if (idx >= 0 && idx < 4) corr = sclamp(v + p.offsets[idx]);
+        } else if (p.type == 1) {
+            const int dxa = c_eo[p.eo_class][0], dya = c_eo[p.eo_class][1], dxb = c_eo[p.eo_class][2], dyb = c_eo[p.eo_class][3];
+            const int ax = x + dxa, ay = y + dya, bx = x + dxb, by = y + dyb;
+            if (ax >= 0 && ax < a.W && ay >= 0 && ay < a.H && bx >= 0 && bx < a.W && by >= 0 && by < a.H) {
+                const int ct = eo_cat(v, m.rec[(ty + 1 + dya) * MT_W + tx + 2 + dxa], m.rec[(ty + 1 + dyb) * MT_W + tx + 2 + dxb]);
+                if (ct < 4) corr = sclamp(v + p.offsets[ct]);
+            }
+        }
+        const int d = m.src[ty * 16 + tx] - corr;
         acc += (long long)(d * d);
     }
     return warp_sum64(acc);
 }
-
-// Merge decisions: one warp per MB row in a wavefront, MB (r, c) after the
-// final parameters of (r-1, c) and (r, c-1) exist (sao.cpp:559-586).
-__global__ void k_sao_merge(FrameArgs a)
+__device__ __forceinline__ evxg_sao_info ld_info_cg(const evxg_sao_info *p)
 {
-    const int lane = threadIdx.x & 31;
+    const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(p));
+    evxg_sao_info r;
+    memcpy(&r, &v, sizeof r);
+    return r;
+}
+
+__global__ void __launch_bounds__(256) k_sao_merge(FrameArgs a)
+{
+    __shared__ MergeTile tiles[8][2];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int *progress = a.progress + a.mbh;
     for (;;) {
         int row = 0;
         if (lane == 0) row = atomicAdd(&a.counters[1], 1);
         row = __shfl_sync(0xffffffffu, row, 0);
         if (row >= a.mbh) return;
+        TileRegs t;
+        tile_load(a, 0, row, lane, t);
+        tile_store(tiles[w][0], lane, t);
+        evxg_sao_info left{};
         for (int c = 0; c < a.mbw; c++) {
+            if (c + 1 < a.mbw) tile_load(a, c + 1, row, lane, t);   // in flight during the wait
             if (row > 0 && !wait_row(a, progress, row - 1, c)) return;
+            __syncwarp();
+            const MergeTile &mt = tiles[w][c & 1];
             const int m = row * a.mbw + c;
-            evxg_sao_info info;
-            info.merge_left = 0; info.merge_above = 0;
-            info.luma = ld_params_cg(&a.sao[m].luma);
-            info.chroma = ld_params_cg(&a.sao[m].chroma);
+            evxg_sao_info info = ld_info_cg(&a.sao[m]);   // own RDO parameters
             float cur = __ldcg(&a.sao_cost[m]);
-            if (c > 0) {
-                const evxg_sao_params lp = ld_params_cg(&a.sao[m - 1].luma), lc = ld_params_cg(&a.sao[m - 1].chroma);
-                if (lp.type != 0) {
-                    const float mc = __fadd_rn(__ll2float_rn(warp_sao_ssd(a, c, row, lp)), __fmul_rn(a.lambda, 1.0f));
-                    if (mc < cur) { info.merge_left = 1; info.luma = lp; info.chroma = lc; cur = mc; }
-                }
+            if (c > 0 && left.luma.type != 0) {
+                const float mc = __fadd_rn(__ll2float_rn(tile_sao_ssd(a, mt, c, row, lane, left.luma)), __fmul_rn(a.lambda, 1.0f));
+                if (mc < cur) { info.merge_left = 1; info.luma = left.luma; info.chroma = left.chroma; cur = mc; }
             }
             if (!info.merge_left && row > 0) {
-                const evxg_sao_params ap = ld_params_cg(&a.sao[m - a.mbw].luma);
-                if (ap.type != 0) {
-                    const float mc = __fadd_rn(__ll2float_rn(warp_sao_ssd(a, c, row, ap)), __fmul_rn(a.lambda, 1.0f));
-                    if (mc < cur) { info.merge_above = 1; info.luma = ap; info.chroma = ld_params_cg(&a.sao[m - a.mbw].chroma); }
+                const evxg_sao_info above = ld_info_cg(&a.sao[m - a.mbw]);
+                if (above.luma.type != 0) {
+                    const float mc = __fadd_rn(__ll2float_rn(tile_sao_ssd(a, mt, c, row, lane, above.luma)), __fmul_rn(a.lambda, 1.0f));
+                    if (mc < cur) { info.merge_above = 1; info.luma = above.luma; info.chroma = above.chroma; }
                 }
             }
-            if (lane == 0) a.sao[m] = info;
+            left = info;
+            if (lane == 0) *reinterpret_cast<uint4 *>(&a.sao[m]) = *reinterpret_cast<const uint4 *>(&info);
             __threadfence();
             __syncwarp();
             if (lane == 0) st_release(&progress[row], c);
-            __syncwarp();
+            if (c + 1 < a.mbw) tile_store(tiles[w][(c + 1) & 1], lane, t);
         }
     }
 }
 
-// In-place application in raster order (sao.cpp:99-146): edge classes read
-// neighbours that raster-earlier MBs already modified, so MB (r, c) runs after
-// (r-1, c+1) and before anything of row r+1 at columns >= c-1.
-__global__ void k_sao_apply(FrameArgs a)
+// ---- application (sao.cpp:99-146) ----
+// The reference applies offsets MB by MB in raster order, in place: a pixel's
+// edge class reads its own MB's and raster-later MBs' pixels unfiltered and
+// raster-earlier MBs' pixels already filtered.  Writing F for that rule, the
+// filtered frame is the unique fixed point x = F(x) (every dependency points
+// to an earlier MB, so there are no cycles), and the dependency chains are a
+// few pixels long: they only pass through MB borders.  k_sao_fix evaluates F
+// for every pixel in parallel, in place, reading unfiltered values from the
+// pristine copy a.sao_orig and earlier MBs' values from the frame itself, and
+// flags any change; once a pass changes nothing the frame is exactly x = F(x).
+// Passes after a quiet pass return at once; if the last pass still changed a
+// pixel, k_sao_restore and k_sao_apply redo the frame in raster wavefront order.
+__global__ void __launch_bounds__(256) k_sao_fix(FrameArgs a, int pass)
 {
+    if (pass > 0 && __ldcg(&a.sao_flags[pass - 1]) == 0) return;
+    const int cw = a.W / 2, ch = a.H / 2;
+    const size_t ny = (size_t)a.W * a.H, nc = (size_t)cw * ch;
+    bool changed = false;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < ny + 2 * nc; i += (size_t)gridDim.x * blockDim.x) {
+        const int pl = i < ny ? 0 : (i < ny + nc ? 1 : 2);
+        const size_t k = pl == 0 ? i : (pl == 1 ? i - ny : i - ny - nc);
+        const int w = pl ? cw : a.W, h = pl ? ch : a.H, n = pl ? 8 : 16;
+        const int y = (int)(k / w), x = (int)(k % w);
+        const int m = (y / n) * a.mbw + x / n;
+        const evxg_sao_params p = pl ? a.sao[m].chroma : a.sao[m].luma;
+        if (p.type == 0) continue;
+        const size_t off = pl == 0 ? 0 : (pl == 1 ? ny : ny + nc);
+        const int16_t *orig = a.sao_orig + off;
+        int16_t *img = a.planes[a.dpb] + off;
+        const int v = orig[k];
+        int corr = v;
+        if (p.type == 2) {
+            const int idx = (sclamp(v) >> 3) - p.band_position;
+            if (idx >= 0 && idx < 4) corr = sclamp(v + p.offsets[idx]);
+        } else {
+            const int ax = x + c_eo[p.eo_class][0], ay = y + c_eo[p.eo_class][1];
+            const int bx = x + c_eo[p.eo_class][2], by = y + c_eo[p.eo_class][3];
+            if (ax >= 0 && ax < w && ay >= 0 && ay < h && bx >= 0 && bx < w && by >= 0 && by < h) {
+                const int ma = (ay / n) * a.mbw + ax / n, mb = (by / n) * a.mbw + bx / n;
+                const size_t ka = (size_t)ay * w + ax, kb = (size_t)by * w + bx;
+                const int va = ma < m ? __ldcg(img + ka) : orig[ka];
+                const int vb = mb < m ? __ldcg(img + kb) : orig[kb];
+                const int ct = eo_cat(v, va, vb);
+                if (ct < 4) corr = sclamp(v + p.offsets[ct]);
+            }
+        }
+        if (__ldcg(img + k) != corr) {
+            img[k] = (int16_t)corr;
+            changed = true;
+        }
+    }
+    if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) atomicOr(&a.sao_flags[pass], 1);
+}
+
+// Fallback when the fixed point was not reached within the pass budget:
+// restore the unfiltered frame, then the raster wavefront below.
+__global__ void k_sao_restore(FrameArgs a, int last_pass)
+{
+    if (__ldcg(&a.sao_flags[last_pass]) == 0) return;
+    const size_t n = (size_t)a.W * a.H + 2 * (size_t)(a.W / 2) * (a.H / 2);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        a.planes[a.dpb][i] = a.sao_orig[i];
+}
+
+// In-place application in raster order, one warp per MB row: MB (r, c) runs
+// after (r-1, c+1) and before anything of row r+1 at columns >= c-1.  Runs
+// only when the fixed-point passes did not converge.
+__global__ void k_sao_apply(FrameArgs a, int last_pass)
+{
+    if (__ldcg(&a.sao_flags[last_pass]) == 0) return;
+
     const int lane = threadIdx.x & 31;
     int *progress = a.progress + 2 * a.mbh;
     int16_t *Y = a.planes[a.dpb], *U = Y + (size_t)a.W * a.H, *V = U + (size_t)(a.W / 2) * (a.H / 2);
