@@ -118,7 +118,10 @@ int evxg_stream_create(uint32_t width, uint32_t height, evxg_stream **out)
         evxg_stream_destroy(s);
         return rc;
     }
-    s->mb_grid = (int)std::min<uint32_t>(s->mbh, (uint32_t)s->num_sms);
+    // The lag-4 wavefront keeps at most about cols/4 + 1 rows busy at once; a
+    // few more CTAs than that hide row hand-over, the rest would only spin,
+    // and leaving SMs free lets other streams' frames run beside this one.
+    s->mb_grid = (int)std::min<uint32_t>(std::min<uint32_t>(s->mbh, (uint32_t)s->num_sms), s->mbw / 4 + 4);
     *out = s;
     return EVXG_SUCCESS;
 }

@@ -25,7 +25,7 @@ constexpr int MAXQ = 63;              // quantize.h:42 (levels - 1)
 // are copied as aligned 16-byte chunks; a chunk is then either entirely
 // inside the plane or entirely outside it (plane widths are multiples of 8).
 constexpr int WL_ROWS = 84;           // luma rows:  base-34 .. base+49
-constexpr int WL = 96;                // luma row stride: 12 chunks cover base-41 .. base+54
+constexpr int WL = 104;               // luma row stride: 13 chunks cover base-41 .. base+62 (stride avoids 4-way bank conflicts)
 constexpr int WC_ROWS = 48;           // chroma rows: (base>>1)-19 .. +28
 constexpr int WC = 56;                // chroma row stride: 7 chunks
 constexpr int WL_OFF = 34, WC_OFF = 19;

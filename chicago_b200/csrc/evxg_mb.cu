@@ -166,53 +166,69 @@ __device__ __forceinline__ uint4 edge16(const int16_t *p)
     const unsigned w2 = v | (v << 16);
     return make_uint4(w2, w2, w2, w2);
 }
-template <bool kCoherent>
-__device__ __noinline__ void load_window(Win &w, const int16_t *planes, int W, int H, int bx, int by)
+// Several windows at once: every thread issues up to 8 chunk loads before
+// storing them, so the five windows of a B-frame macroblock need three
+// load round trips instead of ten.  Window k of the list is loaded into
+// S.win[wi[k]] from plane set pl[k] around (bx[k], by[k]); coherent[k]
+// selects L2-only loads for the slot being reconstructed.
+struct WinReq {
+    int n;
+    int wi[NWIN], bx[NWIN], by[NWIN], coherent[NWIN];
+    const int16_t *pl[NWIN];
+};
+__device__ __noinline__ void load_windows(const WinReq &q, int W, int H)
 {
-    const int16_t *Y = planes, *U = planes + (size_t)W * H, *V = U + (size_t)(W / 2) * (H / 2);
+    MbShared &S = SM();
+    constexpr int NLC = WL / 8, NL = WL_ROWS * NLC, NCC = WC / 8, NCH = 2 * WC_ROWS * NCC, PER = NL + NCH;
     const int cw = W / 2, ch = H / 2;
-    const int ox = ((bx - WL_OFF) >> 3) << 3, oy = by - WL_OFF;
-    const int cox = (((bx >> 1) - WC_OFF) >> 3) << 3, coy = (by >> 1) - WC_OFF;
-    if (threadIdx.x == 0) { w.ox = ox; w.oy = oy; w.cox = cox; w.coy = coy; }
-    constexpr int NLC = WL / 8, NL = WL_ROWS * NLC, KL = (NL + NT - 1) / NT;
-    constexpr int NCC = WC / 8, NCH = 2 * WC_ROWS * NCC, KC = (NCH + NT - 1) / NT;
-    uint4 v[KL + KC];
-#pragma unroll
-    for (int i = 0; i < KL; i++) {
-        const int e = threadIdx.x + i * NT;
-        if (e < NL) {
-            const int r = e / NLC, k = e - r * NLC;
-            const int y = min(max(oy + r, 0), H - 1), x = ox + 8 * k;
-            const int16_t *row = Y + (size_t)y * W;
-            v[i] = (x >= 0 && x + 8 <= W) ? ld16<kCoherent>(row + x) : edge16<kCoherent>(row + (x < 0 ? 0 : W - 1));
-        }
+    if (threadIdx.x < q.n) {
+        const int k = threadIdx.x;
+        Win &w = S.win[q.wi[k]];
+        w.ox = ((q.bx[k] - WL_OFF) >> 3) << 3; w.oy = q.by[k] - WL_OFF;
+        w.cox = (((q.bx[k] >> 1) - WC_OFF) >> 3) << 3; w.coy = (q.by[k] >> 1) - WC_OFF;
     }
+    const int total = q.n * PER;
+    constexpr int B = 8;
+    for (int base = 0; base < total; base += B * NT) {
+        uint4 v[B];
 #pragma unroll
-    for (int i = 0; i < KC; i++) {
-        const int e = threadIdx.x + i * NT;
-        if (e < NCH) {
-            const int pl = e >= WC_ROWS * NCC, q = e - pl * WC_ROWS * NCC;
-            const int r = q / NCC, k = q - r * NCC;
-            const int y = min(max(coy + r, 0), ch - 1), x = cox + 8 * k;
-            const int16_t *row = (pl ? V : U) + (size_t)y * cw;
-            v[KL + i] = (x >= 0 && x + 8 <= cw) ? ld16<kCoherent>(row + x) : edge16<kCoherent>(row + (x < 0 ? 0 : cw - 1));
+        for (int i = 0; i < B; i++) {
+            const int e = base + threadIdx.x + i * NT;
+            if (e < total) {
+                const int k = e / PER, c = e - k * PER;
+                const int16_t *Y = q.pl[k], *U = Y + (size_t)W * H, *V = U + (size_t)cw * ch;
+                const bool coh = q.coherent[k];
+                if (c < NL) {
+                    const int r = c / NLC, kk = c - r * NLC;
+                    const int y = min(max(q.by[k] - WL_OFF + r, 0), H - 1), x = (((q.bx[k] - WL_OFF) >> 3) << 3) + 8 * kk;
+                    const int16_t *row = Y + (size_t)y * W;
+                    v[i] = (x >= 0 && x + 8 <= W) ? (coh ? ld16<true>(row + x) : ld16<false>(row + x))
+                                                  : (coh ? edge16<true>(row + (x < 0 ? 0 : W - 1)) : edge16<false>(row + (x < 0 ? 0 : W - 1)));
+                } else {
+                    const int cc = c - NL, pl = cc >= WC_ROWS * NCC, qq = cc - pl * WC_ROWS * NCC;
+                    const int r = qq / NCC, kk = qq - r * NCC;
+                    const int y = min(max((q.by[k] >> 1) - WC_OFF + r, 0), ch - 1), x = ((((q.bx[k] >> 1) - WC_OFF) >> 3) << 3) + 8 * kk;
+                    const int16_t *row = (pl ? V : U) + (size_t)y * cw;
+                    v[i] = (x >= 0 && x + 8 <= cw) ? (coh ? ld16<true>(row + x) : ld16<false>(row + x))
+                                                   : (coh ? edge16<true>(row + (x < 0 ? 0 : cw - 1)) : edge16<false>(row + (x < 0 ? 0 : cw - 1)));
+                }
+            }
         }
-    }
 #pragma unroll
-    for (int i = 0; i < KL; i++) {
-        const int e = threadIdx.x + i * NT;
-        if (e < NL) {
-            const int r = e / NLC, k = e - r * NLC;
-            *reinterpret_cast<uint4 *>(&w.y[r * WL + 8 * k]) = v[i];
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < KC; i++) {
-        const int e = threadIdx.x + i * NT;
-        if (e < NCH) {
-            const int pl = e >= WC_ROWS * NCC, q = e - pl * WC_ROWS * NCC;
-            const int r = q / NCC, k = q - r * NCC;
-            *reinterpret_cast<uint4 *>(&(pl ? w.v : w.u)[r * WC + 8 * k]) = v[KL + i];
+        for (int i = 0; i < B; i++) {
+            const int e = base + threadIdx.x + i * NT;
+            if (e < total) {
+                const int k = e / PER, c = e - k * PER;
+                Win &w = S.win[q.wi[k]];
+                if (c < NL) {
+                    const int r = c / NLC, kk = c - r * NLC;
+                    *reinterpret_cast<uint4 *>(&w.y[r * WL + 8 * kk]) = v[i];
+                } else {
+                    const int cc = c - NL, pl = cc >= WC_ROWS * NCC, qq = cc - pl * WC_ROWS * NCC;
+                    const int r = qq / NCC, kk = qq - r * NCC;
+                    *reinterpret_cast<uint4 *>(&(pl ? w.v : w.u)[r * WC + 8 * kk]) = v[i];
+                }
+            }
         }
     }
 }
@@ -308,7 +324,7 @@ __device__ __forceinline__ void subpel_column(const int16_t *pl, int S, int bx, 
 // Half- and quarter-pel candidate in direction (dx, dy) around integer
 // position (x, y): metrics into out4 = {sad_h, mad_h, sad_q, mad_q}; optionally
 // stores the half (oh) or quarter (oq) block.  One warp, one column per lane.
-__device__ void warp_subpel(const int16_t *src, const Win &w, int x, int y, int dx, int dy, int lane,
+__device__ __noinline__ void warp_subpel(const int16_t *src, const Win &w, int x, int y, int dx, int dy, int lane,
                             int *out4, int16_t *oh, int16_t *oq)
 {
     int sh = 0, mh = 0, sq = 0, mq = 0;
@@ -934,14 +950,22 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
         }
     }
     __syncthreads();
-    load_window<true>(S.win[0], dst, a.W, a.H, px, py - 16);
-    if (a.type != EVXG_FRAME_INTRA) {
-        load_window<false>(S.win[1], a.planes[a.ref_fwd], a.W, a.H, px, py);
-        if (S.sep) load_window<false>(S.win[2], a.planes[a.ref_fwd], a.W, a.H, S.qx, S.qy);
-    }
-    if (a.type == EVXG_FRAME_BIDIR) {
-        load_window<false>(S.win[3], a.planes[a.ref_bwd], a.W, a.H, px, py);
-        if (S.sep) load_window<false>(S.win[4], a.planes[a.ref_bwd], a.W, a.H, S.qx, S.qy);
+    {
+        WinReq q;
+        q.n = 0;
+        auto add = [&](int wi, const int16_t *pl, int bx, int by, int coh) {
+            q.wi[q.n] = wi; q.pl[q.n] = pl; q.bx[q.n] = bx; q.by[q.n] = by; q.coherent[q.n] = coh; q.n++;
+        };
+        add(0, dst, px, py - 16, 1);   // intra window: the slot being reconstructed
+        if (a.type != EVXG_FRAME_INTRA) {
+            add(1, a.planes[a.ref_fwd], px, py, 0);
+            if (S.sep) add(2, a.planes[a.ref_fwd], S.qx, S.qy, 0);
+        }
+        if (a.type == EVXG_FRAME_BIDIR) {
+            add(3, a.planes[a.ref_bwd], px, py, 0);
+            if (S.sep) add(4, a.planes[a.ref_bwd], S.qx, S.qy, 0);
+        }
+        load_windows(q, a.W, a.H);
     }
     __syncthreads();
     if (tid < 3) {   // neighbours for directional intra, from window 0 (intra_pred.cpp:13-54)
