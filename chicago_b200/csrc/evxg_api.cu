@@ -58,6 +58,8 @@ struct evxg_stream {
     float *sao_cost;
     int16_t *sao_orig;                  // pristine copy for the SAO fixed-point passes
     int *sao_flags;
+    unsigned long long *sao_mail;       // SAO merge hand-over words, epoch-tagged
+    int epoch;
     uint8_t *rgb;
     int *sync;                          // 3*mbh progress words, 4 counters, 1 error word
     int mb_grid, num_sms;
@@ -98,6 +100,8 @@ int evxg_stream_create(uint32_t width, uint32_t height, evxg_stream **out)
     if (e == cudaSuccess) e = cudaMalloc(&s->sao_cost, nblk * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&s->sao_orig, pb);
     if (e == cudaSuccess) e = cudaMalloc(&s->sao_flags, kSaoPasses * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&s->sao_mail, nblk * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(s->sao_mail, 0, nblk * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&s->rgb, (size_t)width * height * 3);
     if (e == cudaSuccess) e = cudaMalloc(&s->sync, (3 * s->mbh + 5) * sizeof(int));
     // The reference zero-fills every image and table at allocation (image.cpp:89,
@@ -133,7 +137,7 @@ int evxg_stream_destroy(evxg_stream *s)
     for (int i = 0; i < 4; i++) cudaFree(s->dpb[i]);
     cudaFree(s->bt); cudaFree(s->prev); cudaFree(s->prev_ser);
     cudaFree(s->sao); cudaFree(s->sao_cost); cudaFree(s->rgb); cudaFree(s->sync);
-    cudaFree(s->sao_orig); cudaFree(s->sao_flags);
+    cudaFree(s->sao_orig); cudaFree(s->sao_flags); cudaFree(s->sao_mail);
     if (s->profile)
         for (int i = 0; i < 7; i++) cudaEventDestroy(s->ev[i]);
     delete s;
@@ -181,7 +185,9 @@ int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, con
     a.src = s->src; a.lev = s->lev; a.bt = s->bt;
     a.prev = f->type == EVXG_FRAME_INTER ? s->prev : nullptr;
     a.sao = s->sao; a.sao_cost = s->sao_cost; a.rgb = drgb;
-    a.sao_orig = s->sao_orig; a.sao_flags = s->sao_flags;
+    a.sao_orig = s->sao_orig; a.sao_flags = s->sao_flags; a.sao_mail = s->sao_mail;
+    s->epoch = s->epoch % 255 + 1;
+    a.epoch = s->epoch;
     a.progress = s->sync; a.counters = s->sync + 3 * s->mbh; a.error = s->sync + 3 * s->mbh + 4;
     a.timeout_ns = s->timeout_ns;
     const size_t nblk = (size_t)s->mbw * s->mbh;

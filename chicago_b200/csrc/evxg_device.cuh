@@ -80,6 +80,16 @@ __device__ __forceinline__ void st_release(int *p, int v)
 {
     asm volatile("st.release.gpu.global.s32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release64(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
 __device__ __forceinline__ unsigned long long globaltimer_ns()
 {
     unsigned long long t;
@@ -102,6 +112,8 @@ struct FrameArgs {
     float *sao_cost;             // per-MB own-parameter SAO cost (RDO -> merge)
     int16_t *sao_orig;           // deblocked, not yet SAO-filtered copy of the destination slot
     int *sao_flags;              // per fixed-point pass: 1 if the pass changed a pixel
+    unsigned long long *sao_mail;// per MB: final SAO parameters of this frame, tagged with epoch
+    int epoch;                   // 1..255, differs from the previous frame's
     const uint8_t *rgb;          // device RGB24 input
     int *progress;               // per-MB-row progress words (wavefronts)
     int *counters;               // [0] next MB row, [1] next SAO merge row, [2] next SAO apply row

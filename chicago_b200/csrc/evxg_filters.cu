@@ -380,11 +380,29 @@ __device__ __forceinline__ evxg_sao_info ld_info_cg(const evxg_sao_info *p)
     return r;
 }
 
+// Final parameters travel between rows in one tagged 64-bit word per MB:
+// 25 bits per plane (type, class, band position, four offsets + 8) and the
+// frame epoch in the low byte, so a waiting row polls the word it needs.
+__device__ __forceinline__ unsigned long long pack_params(const evxg_sao_params &p)
+{
+    unsigned long long v = (unsigned long long)p.type | ((unsigned long long)p.eo_class << 2) |
+                           ((unsigned long long)p.band_position << 4);
+    for (int i = 0; i < 4; i++) v |= (unsigned long long)(p.offsets[i] + 8) << (9 + 4 * i);
+    return v;
+}
+__device__ __forceinline__ evxg_sao_params unpack_params(unsigned long long v)
+{
+    evxg_sao_params p;
+    p.type = (uint8_t)(v & 3); p.eo_class = (uint8_t)((v >> 2) & 3); p.band_position = (uint8_t)((v >> 4) & 31);
+    for (int i = 0; i < 4; i++) p.offsets[i] = (int8_t)((int)((v >> (9 + 4 * i)) & 15) - 8);
+    return p;
+}
+
 __global__ void __launch_bounds__(256) k_sao_merge(FrameArgs a)
 {
     __shared__ MergeTile tiles[8][2];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int *progress = a.progress + a.mbh;
+    const unsigned long long ep = (unsigned long long)a.epoch;
     for (;;) {
         int row = 0;
         if (lane == 0) row = atomicAdd(&a.counters[1], 1);
@@ -393,31 +411,56 @@ __global__ void __launch_bounds__(256) k_sao_merge(FrameArgs a)
         TileRegs t;
         tile_load(a, 0, row, lane, t);
         tile_store(tiles[w][0], lane, t);
+        evxg_sao_info own = ld_info_cg(&a.sao[row * a.mbw]);
+        float own_cost = __ldcg(&a.sao_cost[row * a.mbw]);
         evxg_sao_info left{};
         for (int c = 0; c < a.mbw; c++) {
-            if (c + 1 < a.mbw) tile_load(a, c + 1, row, lane, t);   // in flight during the wait
-            if (row > 0 && !wait_row(a, progress, row - 1, c)) return;
+            const int m = row * a.mbw + c;
+            evxg_sao_info info = own;   // own RDO parameters, prefetched
+            float cur = own_cost;
+            if (c + 1 < a.mbw) {        // next MB's data is in flight while this one waits
+                tile_load(a, c + 1, row, lane, t);
+                own = ld_info_cg(&a.sao[m + 1]);
+                own_cost = __ldcg(&a.sao_cost[m + 1]);
+            }
+            unsigned long long above = 0;
+            if (row > 0) {   // bounded wait for the final parameters of (r-1, c)
+                bool ok = true;
+                if (lane == 0) {
+                    const unsigned long long t0 = globaltimer_ns();
+                    for (;;) {
+                        above = ld_acquire64(&a.sao_mail[m - a.mbw]);
+                        if ((above & 0xFF) == ep) break;
+                        if (*(volatile int *)a.error) { ok = false; break; }
+                        if ((long long)(globaltimer_ns() - t0) > a.timeout_ns) {
+                            atomicCAS(a.error, 0, EVXG_ERROR_OPERATION_TIMEDOUT);
+                            ok = false;
+                            break;
+                        }
+                    }
+                }
+                if (!__shfl_sync(0xffffffffu, ok, 0)) return;
+                above = __shfl_sync(0xffffffffu, above, 0);
+            }
             __syncwarp();
             const MergeTile &mt = tiles[w][c & 1];
-            const int m = row * a.mbw + c;
-            evxg_sao_info info = ld_info_cg(&a.sao[m]);   // own RDO parameters
-            float cur = __ldcg(&a.sao_cost[m]);
             if (c > 0 && left.luma.type != 0) {
                 const float mc = __fadd_rn(__ll2float_rn(tile_sao_ssd(a, mt, c, row, lane, left.luma)), __fmul_rn(a.lambda, 1.0f));
                 if (mc < cur) { info.merge_left = 1; info.luma = left.luma; info.chroma = left.chroma; cur = mc; }
             }
             if (!info.merge_left && row > 0) {
-                const evxg_sao_info above = ld_info_cg(&a.sao[m - a.mbw]);
-                if (above.luma.type != 0) {
-                    const float mc = __fadd_rn(__ll2float_rn(tile_sao_ssd(a, mt, c, row, lane, above.luma)), __fmul_rn(a.lambda, 1.0f));
-                    if (mc < cur) { info.merge_above = 1; info.luma = above.luma; info.chroma = above.chroma; }
+                const evxg_sao_params al = unpack_params(above >> 8), ac = unpack_params(above >> 33);
+                if (al.type != 0) {
+                    const float mc = __fadd_rn(__ll2float_rn(tile_sao_ssd(a, mt, c, row, lane, al)), __fmul_rn(a.lambda, 1.0f));
+                    if (mc < cur) { info.merge_above = 1; info.luma = al; info.chroma = ac; }
                 }
             }
             left = info;
-            if (lane == 0) *reinterpret_cast<uint4 *>(&a.sao[m]) = *reinterpret_cast<const uint4 *>(&info);
-            __threadfence();
+            if (lane == 0) {
+                *reinterpret_cast<uint4 *>(&a.sao[m]) = *reinterpret_cast<const uint4 *>(&info);
+                st_release64(&a.sao_mail[m], ep | (pack_params(info.luma) << 8) | (pack_params(info.chroma) << 33));
+            }
             __syncwarp();
-            if (lane == 0) st_release(&progress[row], c);
             if (c + 1 < a.mbw) tile_store(tiles[w][(c + 1) & 1], lane, t);
         }
     }

@@ -86,7 +86,20 @@ struct Nbr {                   // intra_pred.cpp:13-54
 struct alignas(4) Desc { evxg_block_desc d; };   // 4-aligned so it can be copied as 7 words
 
 // State of one motion search, owned by one warp group.
+// Half-pel planes around a selection (luma 16x16 + two 8x8 chroma blocks):
+// HH = horizontal 6-tap at column centres x-1 .. x+15 for rows y-3 .. y+18,
+// VV = vertical 6-tap at row centres y-1 .. y+15, DD = vertical 6-tap over HH
+// (the diagonal).  Every direction's half-pel block is a sub-window of one of
+// them.
+template <int N>
+struct HalfPlanes {
+    int16_t hh[(N + 6) * (N + 1)];
+    int16_t vv[(N + 1) * N];
+    int16_t dd[(N + 1) * (N + 1)];
+};
 struct Srch {
+    HalfPlanes<16> hy;
+    HalfPlanes<8> hu, hv;
     int m_sad[9], m_mad[9], m_satd[9], valid[9];
     int spm[8][4];
     Sel sel;
@@ -385,19 +398,93 @@ __device__ __noinline__ void run_step(const Grp g, int si, int wi, bool intra, i
     gsync(g);
 }
 
+// Half-pel planes for one plane block (window plane pl, stride S, selection at
+// window coordinates (lx, ly)), computed by the group's threads.
+template <int N>
+__device__ __forceinline__ void half_planes_a(HalfPlanes<N> &hp, const int16_t *pl, int S, int lx, int ly, int gt, int nt)
+{
+    constexpr int NH = (N + 6) * (N + 1), NV = (N + 1) * N;
+    for (int e = gt; e < NH + NV; e += nt) {
+        if (e < NH) {
+            const int t = e / (N + 1), c = e % (N + 1);
+            const int16_t *rp = pl + (ly - 3 + t) * S + lx - 1 + c;
+            hp.hh[e] = tap6(rp[-2], rp[-1], rp[0], rp[1], rp[2], rp[3]);
+        } else {
+            const int k = e - NH, r = k / N, c = k % N;
+            const int16_t *cp = pl + (ly - 1 + r) * S + lx + c;
+            hp.vv[k] = tap6(cp[-2 * S], cp[-S], cp[0], cp[S], cp[2 * S], cp[3 * S]);
+        }
+    }
+}
+template <int N>
+__device__ __forceinline__ void half_planes_b(HalfPlanes<N> &hp, int gt, int nt)
+{
+    for (int e = gt; e < (N + 1) * (N + 1); e += nt) {
+        const int r = e / (N + 1), c = e % (N + 1);
+        const int16_t *h = hp.hh + r * (N + 1) + c;
+        hp.dd[e] = tap6(h[0], h[N + 1], h[2 * (N + 1)], h[3 * (N + 1)], h[4 * (N + 1)], h[5 * (N + 1)]);
+    }
+}
+// Half-pel sample (r, c) of direction (dx, dy) from the planes (interp.cpp:52-164).
+template <int N>
+__device__ __forceinline__ int half_at(const HalfPlanes<N> &hp, int dx, int dy, int r, int c)
+{
+    const int cx = c + (dx > 0), ry = r + (dy > 0);
+    if (dx && !dy) return hp.hh[(r + 3) * (N + 1) + cx];
+    if (!dx && dy) return hp.vv[ry * N + c];
+    return hp.dd[ry * (N + 1) + cx];
+}
+
 // Sub-pel refinement around the selection (motion.cpp:180-261, :408-483).
+// The interpolation reads only the selection, which the refinement does not
+// move, so the three half-pel planes are built once and each direction's
+// half and quarter blocks (quarter = (full + half + 1) >> 1) are read from them.
 __device__ __noinline__ void run_subpel(const Grp g, int si, int wi, bool intra, int px, int py, int W, int H)
 {
     MbShared &S = SM();
     Srch &sr = S.srch[si];
+    const Win &w = S.win[wi];
     const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31, nw = g.nt >> 5;
     const int bx = sr.sel.bx, by = sr.sel.by;
+    const int lx = bx - w.ox, ly = by - w.oy, cx = (bx >> 1) - w.cox, cy = (by >> 1) - w.coy;
+    half_planes_a<16>(sr.hy, w.y, WL, lx, ly, gt, g.nt);
+    half_planes_a<8>(sr.hu, w.u, WC, cx, cy, gt, g.nt);
+    half_planes_a<8>(sr.hv, w.v, WC, cx, cy, gt, g.nt);
+    gsync(g);
+    half_planes_b<16>(sr.hy, gt, g.nt);
+    half_planes_b<8>(sr.hu, gt, g.nt);
+    half_planes_b<8>(sr.hv, gt, g.nt);
+    gsync(g);
     for (int k = gw; k < 8; k += nw) {
         const int r = k < 4 ? k : k + 1, i = r % 3 - 1, j = r / 3 - 1;
         const int x = bx + i, y = by + j;
         const bool ok = !(intra && y > py - 16 && x > px - 16) && !(x < 0 || x > W - 16 || y < 0 || y > H - 16);
         if (lane == 0) sr.valid[k] = ok;
-        if (ok) warp_subpel(S.src, S.win[wi], bx, by, i, j, lane, sr.spm[k], nullptr, nullptr);
+        if (!ok) continue;
+        int sh = 0, mh = 0, sq = 0, mq = 0;
+        if (lane < 16) {   // luma column
+            for (int rr = 0; rr < 16; rr++) {
+                const int half = half_at<16>(sr.hy, i, j, rr, lane);
+                const int full = w.y[(ly + rr) * WL + lx + lane];
+                const int q = (int16_t)((full + half + 1) >> 1);
+                const int s0 = S.src[rr * 16 + lane];
+                const int ah = iabs32(s0 - half), aq = iabs32(s0 - q);
+                sh += ah; sq += aq; mh = max(mh, ah); mq = max(mq, aq);
+            }
+        } else {           // chroma column
+            const int kk = lane - 16, pl = kk >> 3, c = kk & 7;
+            const HalfPlanes<8> &hp = pl ? sr.hv : sr.hu;
+            const int16_t *fp = pl ? w.v : w.u;
+            for (int rr = 0; rr < 8; rr++) {
+                const int half = half_at<8>(hp, i, j, rr, c);
+                const int full = fp[(cy + rr) * WC + cx + c];
+                const int q = (int16_t)((full + half + 1) >> 1);
+                const int s0 = S.src[256 + pl * 64 + rr * 8 + c];
+                mh = max(mh, iabs32(s0 - half)); mq = max(mq, iabs32(s0 - q));
+            }
+        }
+        sh = warp_sum(sh); mh = warp_max(mh); sq = warp_sum(sq); mq = warp_max(mq);
+        if (lane == 0) { sr.spm[k][0] = sh; sr.spm[k][1] = mh; sr.spm[k][2] = sq; sr.spm[k][3] = mq; }
     }
     gsync(g);
     if (gt == 0) {
@@ -1144,8 +1231,15 @@ __global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a)
         for (int col = 0; col < a.mbw; ++col) {
             if (tid == 0) {
                 S.row_abort = 0;
-                if (row > 0) {   // WPP dependency: row above finished column min(c+4, cols-1)
-                    const int need = min(col + 4, a.mbw - 1);
+                if (row > 0) {
+                    // Row r-1 must have finished column c+3: the reads of MB (r,c)
+                    // (intra block-copy candidates x in [px-31, px+31], 6-tap
+                    // overshoot -3..+18) reach columns c-3 .. c+3.  Rows below
+                    // then trail by three columns too, so row r+1 has finished at
+                    // most column c-4 and the stale pixels MB (r,c) reads there
+                    // (columns >= c-3) are still unwritten.  The reference waits
+                    // for c+4 (encode.cpp:866-877); c+3 gives the same pixels.
+                    const int need = min(col + 3, a.mbw - 1);
                     const unsigned long long t0 = globaltimer_ns();
                     while (ld_acquire(&a.progress[row - 1]) < need) {
                         if (*(volatile int *)a.error) { S.row_abort = 1; break; }
