@@ -40,6 +40,9 @@ UNIT = "1080p-eq frames/s"
 W, H, FRAMES, QUALITY, VMAX, CUT = 1920, 1080, 120, 8, 24.0, 60
 EQ = (W * H) / (1920 * 1080)
 HBM_PEAK_FALLBACK = 6650.0
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_mb_wavefront launch
+# (a 1080p B frame of this workload), profiles/mb_wavefront_1080p.md
+MB_TRAFFIC_BYTES = 25_676_032 + 488_960
 
 
 def peaks():
@@ -243,9 +246,9 @@ def run_gpu(args):
         "kernel_ms_per_step": {k: round(v / K, 4) for k, v in kernel_tot.items()},
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"kernel": "k_mb_wavefront", "bound": "hbm", "achieved": round(achieved, 3), "peak": peak,
-                     "unit": "GB/s", "frac": round(achieved / peak, 6), "traffic": None,
+                     "unit": "GB/s", "frac": round(achieved / peak, 6), "traffic": MB_TRAFFIC_BYTES,
                      "peak_source": f"{peak_kind} hbm_gbs",
-                     "note": "dependency-latency bound: lag-4 macroblock wavefront, see DESIGN.md"},
+                     "note": "dependency-latency bound: lag-3 macroblock wavefront (critical path of cols + 3*(rows-1) MB steps)"},
         "gpu_launches": st.launch_count() * K,
         "batched": batched,
         "clocks": clk,
