@@ -59,6 +59,7 @@ __constant__ uint8_t c_zigzag[64] = {  // scan.h:60-70
 __shared__ int16_t s_qm[2][64];      // 0 intra, 1 inter
 __shared__ uint8_t s_dz[2][64];
 __shared__ uint8_t s_scan[3][64];    // 0 zigzag, 1 row-first (vertical modes), 2 column-first (horizontal modes)
+__shared__ int16_t s_lut8[64];       // cosine table, read at a different row per thread
 
 constexpr int NT = 384;        // threads per CTA: three groups of four warps
 constexpr int NW = NT / 32;
@@ -72,6 +73,16 @@ struct alignas(16) Win {
     int16_t u[WC_ROWS * WC];
     int16_t v[WC_ROWS * WC];
     int ox, oy, cox, coy;      // plane coordinates of window element (0, 0)
+    const int16_t *pl;         // plane set the window holds
+    int valid;                 // 0: contents undefined (start of a row)
+};
+// Windows requested for one MB: window wi[k] around luma (bx[k], by[k]) of
+// plane set pl[k]; coherent[k] selects L2-only loads (the slot being
+// reconstructed); mode[k] is decided by load_windows.
+struct WinReq {
+    int n;
+    int wi[5], bx[5], by[5], coherent[5], mode[5];
+    const int16_t *pl[5];
 };
 struct Sel {                   // evx_motion_selection, motion.cpp:53-66
     int bx, by, sad, mad, ssd;
@@ -100,7 +111,8 @@ struct HalfPlanes {
 struct Srch {
     HalfPlanes<16> hy;
     HalfPlanes<8> hu, hv;
-    int m_sad[9], m_mad[9], m_satd[9], valid[9];
+    int m_sad[9], m_mad[9], valid[9];
+    float m_cost[9];           // RD cost of each pattern slot
     int spm[8][4];
     Sel sel;
     int cur;                   // window the search runs in
@@ -119,6 +131,7 @@ struct MbShared {
     int modes[3], dsad[3], dir_best, dir_sad;
     int bi_sad, part[NW];
     int cpred[MAXC], win_k, need_encode, chosen, rdo;
+    WinReq req;
     Desc cd[MAXC];             // 0 intra (no prediction), 1..3 directional modes, 4 SAD winner / final
     float cost[MAXC];
     int16_t coef[MAXC][MB_N], lev[MAXC][MB_N], rec[MAXC][MB_N], tmp[MAXC][MB_N];
@@ -179,28 +192,57 @@ __device__ __forceinline__ uint4 edge16(const int16_t *p)
     const unsigned w2 = v | (v << 16);
     return make_uint4(w2, w2, w2, w2);
 }
-// Several windows at once: every thread issues up to 8 chunk loads before
-// storing them, so the five windows of a B-frame macroblock need three
-// load round trips instead of ten.  Window k of the list is loaded into
-// S.win[wi[k]] from plane set pl[k] around (bx[k], by[k]); coherent[k]
-// selects L2-only loads for the slot being reconstructed.
-struct WinReq {
-    int n;
-    int wi[NWIN], bx[NWIN], by[NWIN], coherent[NWIN];
-    const int16_t *pl[NWIN];
-};
-__device__ __noinline__ void load_windows(const WinReq &q, int W, int H)
+// Window origin for a luma position: 8-aligned columns (16-byte chunks).
+__device__ __forceinline__ int win_ox(int bx) { return ((bx - WL_OFF) >> 3) << 3; }
+__device__ __forceinline__ int win_cox(int bx) { return (((bx >> 1) - WC_OFF) >> 3) << 3; }
+
+// One 16-byte chunk of window row r (luma: plane row by-WL_OFF+r, columns
+// x0 .. x0+7; chroma likewise), rows clamped to the plane and columns outside
+// it filled with the edge sample -- the clamping of interp.cpp:8-14.
+__device__ __forceinline__ uint4 win_chunk(const int16_t *plane, int S, int rows, int y, int x0, bool coh)
+{
+    const int16_t *row = plane + (size_t)min(max(y, 0), rows - 1) * S;
+    if (x0 >= 0 && x0 + 8 <= S) return coh ? ld16<true>(row + x0) : ld16<false>(row + x0);
+    const int16_t *e = row + (x0 < 0 ? 0 : S - 1);
+    return coh ? edge16<true>(e) : edge16<false>(e);
+}
+
+// Fill the requested windows (S.req, built by thread 0).  A window whose
+// plane set and origin are unchanged is kept; one that moved right by one
+// macroblock (16 luma / 8 chroma columns, same rows) -- the next MB of a row
+// -- is shifted in shared memory and only its new strip is read from memory,
+// one thread per window row; every other window is loaded whole, every thread
+// issuing up to 8 chunk loads before storing them.  A shifted window holds
+// what a fresh load would: reference slots do not change during a frame, and
+// for the slot being reconstructed the caller patches each finished MB into
+// window 0, while no other MB writes the retained columns before this MB
+// (rows above finished them before the previous MB began; rows below trail
+// by more than the window's reach).
+__device__ __noinline__ void load_windows(int W, int H)
 {
     MbShared &S = SM();
+    WinReq &q = S.req;
     constexpr int NLC = WL / 8, NL = WL_ROWS * NLC, NCC = WC / 8, NCH = 2 * WC_ROWS * NCC, PER = NL + NCH;
     const int cw = W / 2, ch = H / 2;
     if (threadIdx.x < q.n) {
         const int k = threadIdx.x;
         Win &w = S.win[q.wi[k]];
-        w.ox = ((q.bx[k] - WL_OFF) >> 3) << 3; w.oy = q.by[k] - WL_OFF;
-        w.cox = (((q.bx[k] >> 1) - WC_OFF) >> 3) << 3; w.coy = (q.by[k] >> 1) - WC_OFF;
+        const int ox = win_ox(q.bx[k]), oy = q.by[k] - WL_OFF, cox = win_cox(q.bx[k]), coy = (q.by[k] >> 1) - WC_OFF;
+        int mode = 0;   // 0 full load, 1 keep, 2 shift by one MB
+        if (w.valid && w.pl == q.pl[k] && w.oy == oy && w.coy == coy) {
+            if (w.ox == ox && w.cox == cox) mode = 1;
+            else if (w.ox + 16 == ox && w.cox + 8 == cox) mode = 2;
+        }
+        q.mode[k] = mode;
+        w.ox = ox; w.oy = oy; w.cox = cox; w.coy = coy; w.pl = q.pl[k]; w.valid = 1;
     }
-    const int total = q.n * PER;
+    __syncthreads();
+    int full[5], nf = 0, shift[5], ns = 0;
+    for (int k = 0; k < q.n; k++) {
+        if (q.mode[k] == 0) full[nf++] = k;
+        else if (q.mode[k] == 2) shift[ns++] = k;
+    }
+    const int total = nf * PER;
     constexpr int B = 8;
     for (int base = 0; base < total; base += B * NT) {
         uint4 v[B];
@@ -208,22 +250,16 @@ __device__ __noinline__ void load_windows(const WinReq &q, int W, int H)
         for (int i = 0; i < B; i++) {
             const int e = base + threadIdx.x + i * NT;
             if (e < total) {
-                const int k = e / PER, c = e - k * PER;
+                const int k = full[e / PER], c = e % PER;
+                const Win &w = S.win[q.wi[k]];
                 const int16_t *Y = q.pl[k], *U = Y + (size_t)W * H, *V = U + (size_t)cw * ch;
-                const bool coh = q.coherent[k];
                 if (c < NL) {
                     const int r = c / NLC, kk = c - r * NLC;
-                    const int y = min(max(q.by[k] - WL_OFF + r, 0), H - 1), x = (((q.bx[k] - WL_OFF) >> 3) << 3) + 8 * kk;
-                    const int16_t *row = Y + (size_t)y * W;
-                    v[i] = (x >= 0 && x + 8 <= W) ? (coh ? ld16<true>(row + x) : ld16<false>(row + x))
-                                                  : (coh ? edge16<true>(row + (x < 0 ? 0 : W - 1)) : edge16<false>(row + (x < 0 ? 0 : W - 1)));
+                    v[i] = win_chunk(Y, W, H, w.oy + r, w.ox + 8 * kk, q.coherent[k]);
                 } else {
                     const int cc = c - NL, pl = cc >= WC_ROWS * NCC, qq = cc - pl * WC_ROWS * NCC;
                     const int r = qq / NCC, kk = qq - r * NCC;
-                    const int y = min(max((q.by[k] >> 1) - WC_OFF + r, 0), ch - 1), x = ((((q.bx[k] >> 1) - WC_OFF) >> 3) << 3) + 8 * kk;
-                    const int16_t *row = (pl ? V : U) + (size_t)y * cw;
-                    v[i] = (x >= 0 && x + 8 <= cw) ? (coh ? ld16<true>(row + x) : ld16<false>(row + x))
-                                                   : (coh ? edge16<true>(row + (x < 0 ? 0 : cw - 1)) : edge16<false>(row + (x < 0 ? 0 : cw - 1)));
+                    v[i] = win_chunk(pl ? V : U, cw, ch, w.coy + r, w.cox + 8 * kk, q.coherent[k]);
                 }
             }
         }
@@ -231,7 +267,7 @@ __device__ __noinline__ void load_windows(const WinReq &q, int W, int H)
         for (int i = 0; i < B; i++) {
             const int e = base + threadIdx.x + i * NT;
             if (e < total) {
-                const int k = e / PER, c = e - k * PER;
+                const int k = full[e / PER], c = e % PER;
                 Win &w = S.win[q.wi[k]];
                 if (c < NL) {
                     const int r = c / NLC, kk = c - r * NLC;
@@ -244,12 +280,46 @@ __device__ __noinline__ void load_windows(const WinReq &q, int W, int H)
             }
         }
     }
+    // Shifts: one thread per window row; the row's new chunks are requested
+    // first, then the row moves left in registers.
+    constexpr int RT = WL_ROWS + 2 * WC_ROWS;
+    for (int e = threadIdx.x; e < ns * RT; e += NT) {
+        const int k = shift[e / RT], r = e % RT;
+        Win &w = S.win[q.wi[k]];
+        const bool coh = q.coherent[k];
+        if (r < WL_ROWS) {
+            int16_t *row = w.y + r * WL;
+            const uint4 n0 = win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 16, coh);
+            const uint4 n1 = win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 8, coh);
+            uint4 t[NLC - 2];
+#pragma unroll
+            for (int j = 0; j < NLC - 2; j++) t[j] = *reinterpret_cast<const uint4 *>(row + 16 + 8 * j);
+#pragma unroll
+            for (int j = 0; j < NLC - 2; j++) *reinterpret_cast<uint4 *>(row + 8 * j) = t[j];
+            *reinterpret_cast<uint4 *>(row + WL - 16) = n0;
+            *reinterpret_cast<uint4 *>(row + WL - 8) = n1;
+        } else {
+            const int rr = r - WL_ROWS, pl = rr >= WC_ROWS, cr = rr - pl * WC_ROWS;
+            const int16_t *U = q.pl[k] + (size_t)W * H, *V = U + (size_t)cw * ch;
+            int16_t *row = (pl ? w.v : w.u) + cr * WC;
+            const uint4 n0 = win_chunk(pl ? V : U, cw, ch, w.coy + cr, w.cox + WC - 8, coh);
+            uint4 t[NCC - 1];
+#pragma unroll
+            for (int j = 0; j < NCC - 1; j++) t[j] = *reinterpret_cast<const uint4 *>(row + 8 + 8 * j);
+#pragma unroll
+            for (int j = 0; j < NCC - 1; j++) *reinterpret_cast<uint4 *>(row + 8 * j) = t[j];
+            *reinterpret_cast<uint4 *>(row + WC - 8) = n0;
+        }
+    }
 }
 
 // SAD (luma), MAD (Y, U, V) and SATD (luma) of the 16x16 block at plane
-// position (x, y) against the source; one warp.  analysis.h:89-202.
-__device__ void warp_metrics(const int16_t *src, const Win &w, int x, int y, int lane,
-                             int *o_sad, int *o_mad, int *o_satd)
+// position (x, y) against the source; one warp, every lane gets the sums.
+// analysis.h:89-202.
+struct Metrics {
+    int sad, mad, satd;
+};
+__device__ Metrics warp_metrics(const int16_t *src, const Win &w, int x, int y, int lane)
 {
     int sad = 0, mad = 0, satd = 0;
     if (lane < 16) {
@@ -287,10 +357,14 @@ __device__ void warp_metrics(const int16_t *src, const Win &w, int x, int y, int
 #pragma unroll
         for (int c = 0; c < 8; c++) mad = max(mad, iabs32(sp[c] - pp[c]));
     }
-    sad = warp_sum(sad);
-    mad = warp_max(mad);
-    satd = warp_sum(satd);
-    if (lane == 0) { *o_sad = sad; *o_mad = mad; *o_satd = (satd + 1) >> 1; }
+    return Metrics{warp_sum(sad), warp_max(mad), (warp_sum(satd) + 1) >> 1};
+}
+// RD cost of an integer candidate: (float)satd + lambda * (|mvx| + |mvy| + 1)
+// with the motion vector taken as int16 (motion.cpp:136-146).
+__device__ __forceinline__ float cand_cost(int satd, int x, int y, int px, int py, float lambda)
+{
+    const int16_t mx = (int16_t)(x - px), my = (int16_t)(y - py);
+    return rd_cost(satd, lambda, (unsigned)(iabs16(mx) + iabs16(my) + 1));
 }
 
 // One column of a 6-tap half-pel block (interp.cpp:52-164) plus its quarter-pel
@@ -354,12 +428,11 @@ __device__ __noinline__ void warp_subpel(const int16_t *src, const Win &w, int x
     if (out4 && lane == 0) { out4[0] = sh; out4[1] = mh; out4[2] = sq; out4[3] = mq; }
 }
 
-// Integer candidate acceptance (motion.cpp:148-177), replayed by one thread.
-__device__ void accept_int(Sel &s, int x, int y, int sad, int mad, int satd, int px, int py, int thr, float lambda)
+// Integer candidate acceptance (motion.cpp:148-177), replayed by one thread;
+// the candidate's cost comes from cand_cost.
+__device__ __forceinline__ void accept_int(Sel &s, int x, int y, int sad, int mad, float cost, int px, int py, int thr)
 {
     const int ssd = (x - px) * (x - px) + (y - py) * (y - py);
-    const int16_t mx = (int16_t)(x - px), my = (int16_t)(y - py);
-    const float cost = rd_cost(satd, lambda, (unsigned)(iabs16(mx) + iabs16(my) + 1));
     bool take;
     if (s.mad < thr) take = mad < s.mad || (mad == s.mad && ssd < s.ssd);
     else take = (cost < s.cost || ((cost == s.cost && ssd < s.ssd) && sad < SAD_THRESHOLD)) || mad < thr;
@@ -370,6 +443,13 @@ __device__ void accept_int(Sel &s, int x, int y, int sad, int mad, int satd, int
 // a warp group: every warp evaluates slots of the 3x3 pattern (validity is
 // decided identically by all lanes), then the group leader replays the
 // reference's loop order in registers, with its early exit.
+//
+// When the pattern is centred on the selection (l = t = -st) its centre slot
+// is the selection itself, whose SAD, MAD and cost are already in sr.sel:
+// every selection but the intra search's starting point was accepted from a
+// candidate evaluation (its stored sad/mad/cost are that candidate's), and
+// that starting point lies in the excluded region, so it is never valid.
+// The eight remaining slots take two rounds on four warps instead of three.
 __device__ __noinline__ void run_step(const Grp g, int si, int wi, bool intra, int l, int t, int st, int px, int py,
                                       int W, int H, float lambda)
 {
@@ -377,20 +457,32 @@ __device__ __noinline__ void run_step(const Grp g, int si, int wi, bool intra, i
     Srch &sr = S.srch[si];
     const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31, nw = g.nt >> 5;
     const int bx = sr.sel.bx, by = sr.sel.by;
-    for (int k = gw; k < 9; k += nw) {
+    const bool centred = l == -st && t == -st;
+    const int n = centred ? 8 : 9;
+    for (int j = gw; j < n; j += nw) {
+        const int k = centred && j >= 4 ? j + 1 : j;
         const int x = bx + l + (k % 3) * st, y = by + t + (k / 3) * st;
         const bool ok = !(intra && y > py - 16 && x > px - 16) && !(x < 0 || x > W - 16 || y < 0 || y > H - 16);
         if (lane == 0) sr.valid[k] = ok;
-        if (ok) warp_metrics(S.src, S.win[wi], x, y, lane, &sr.m_sad[k], &sr.m_mad[k], &sr.m_satd[k]);
+        if (ok) {
+            const Metrics m = warp_metrics(S.src, S.win[wi], x, y, lane);
+            if (lane == 0) { sr.m_sad[k] = m.sad; sr.m_mad[k] = m.mad; sr.m_cost[k] = cand_cost(m.satd, x, y, px, py, lambda); }
+        }
     }
     gsync(g);
     if (gt == 0) {
         Sel s = sr.sel;
+        const Sel s0 = s;
         const int thr = S.thr;
         for (int k = 0; k < 9; k++) {
-            if (!sr.valid[k]) continue;
-            accept_int(s, bx + l + (k % 3) * st, by + t + (k / 3) * st, sr.m_sad[k], sr.m_mad[k], sr.m_satd[k], px, py,
-                       thr, lambda);
+            const int x = bx + l + (k % 3) * st, y = by + t + (k / 3) * st;
+            if (centred && k == 4) {
+                if (intra && y > py - 16 && x > px - 16) continue;   // the intra search's starting point
+                accept_int(s, x, y, s0.sad, s0.mad, s0.cost, px, py, thr);
+            } else {
+                if (!sr.valid[k]) continue;
+                accept_int(s, x, y, sr.m_sad[k], sr.m_mad[k], sr.m_cost[k], px, py, thr);
+            }
             if (s.mad < thr) break;   // early exit on a copy-quality match
         }
         sr.sel = s;
@@ -618,27 +710,32 @@ __device__ __forceinline__ int scan_kind(int mode)   // scan.h:154-159
 {
     return (mode == 1 || mode == 5) ? 1 : ((mode == 2 || mode == 6) ? 2 : 0);
 }
-// forward 8-point line (transform.cpp:264-284)
-__device__ __forceinline__ void fdct8_line(const int in[8], int16_t out[8])
+// Outputs i0 .. i0+NO-1 of a forward 8-point line (transform.cpp:264-284).
+template <int NO>
+__device__ __forceinline__ void fdct8_part(const int in[8], int i0, int16_t out[NO])
 {
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
+    for (int q = 0; q < NO; q++) {
+        const int i = i0 + q;
         int t = 0;
 #pragma unroll
-        for (int k = 0; k < 8; k++) t += in[k] * c_lut8[i * 8 + k];
+        for (int k = 0; k < 8; k++) t += in[k] * s_lut8[i * 8 + k];
         t = i == 0 ? (t * 45) / 128 : t / 2;
-        out[i] = (int16_t)rdiv(t, 128);
+        out[q] = (int16_t)rdiv(t, 128);
     }
 }
-// inverse 8-point line, per-term truncation (transform.cpp:330-349)
-__device__ __forceinline__ void idct8_line(const int in[8], int out[8])
+// Outputs i0 .. i0+NO-1 of an inverse 8-point line, per-term truncation
+// (transform.cpp:330-349).
+template <int NO>
+__device__ __forceinline__ void idct8_part(const int in[8], int i0, int out[NO])
 {
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-        int t = ((in[0] * c_lut8[i]) * 45) / 128;
+    for (int q = 0; q < NO; q++) {
+        const int i = i0 + q;
+        int t = ((in[0] * s_lut8[i]) * 45) / 128;
 #pragma unroll
-        for (int k = 1; k < 8; k++) t += (in[k] * c_lut8[k * 8 + i]) / 2;
-        out[i] = rdiv(t, 128);
+        for (int k = 1; k < 8; k++) t += (in[k] * s_lut8[k * 8 + i]) / 2;
+        out[q] = rdiv(t, 128);
     }
 }
 __device__ __forceinline__ bool intra_quant(int bt) { return (bt & BT_INTRA) && !(bt & BT_MOTION); }   // quantize.cpp:457
@@ -704,17 +801,21 @@ __device__ void trellis_warp(int16_t *lev, const int16_t *coef, int b, int qp, b
     }
 }
 
-// encode_block + decode_block for S.ncand candidates (encode.cpp:481-750,
-// decode.cpp:31-432); with S.rdo set also the RD cost (encode.cpp:39-164).
 // encode_block + decode_block for candidates k0 .. k0+nc-1 on a warp group
 // (encode.cpp:481-750, decode.cpp:31-432); with S.rdo set also their RD cost
-// (encode.cpp:39-164).
+// (encode.cpp:39-164).  The transforms give each thread NO outputs of one
+// 8-point line: 8 when the group has few threads per line (several
+// candidates on one group), 1 when it has eight or more (one candidate on
+// the whole CTA), which shortens each transform pass eightfold.
+template <int NO>
 __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, int k0, int nc)
 {
     MbShared &S = SM();
     const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31, nw = g.nt >> 5;
-    for (int j = gt; j < nc * 48; j += g.nt) {   // forward DCT, rows
-        const int k = k0 + j / 48, rem = j % 48, b = rem >> 3, r = rem & 7;
+    constexpr int PER = 8 / NO;   // work items per line
+    for (int j = gt; j < nc * 48 * PER; j += g.nt) {   // forward DCT, rows
+        const int line = j / PER, i0 = (j % PER) * NO;
+        const int k = k0 + line / 48, rem = line % 48, b = rem >> 3, r = rem & 7;
         if (S.cd[k].d.block_type & BT_COPY) continue;
         const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
         int in[8];
@@ -723,22 +824,23 @@ __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, 
             const int e = mb_index(b, r, c);
             in[c] = (int16_t)(pr ? S.src[e] - pr[e] : S.src[e]);
         }
-        int16_t out[8];
-        fdct8_line(in, out);
+        int16_t out[NO];
+        fdct8_part<NO>(in, i0, out);
 #pragma unroll
-        for (int c = 0; c < 8; c++) S.tmp[k][mb_index(b, r, c)] = out[c];
+        for (int q = 0; q < NO; q++) S.tmp[k][mb_index(b, r, i0 + q)] = out[q];
     }
     gsync(g);
-    for (int j = gt; j < nc * 48; j += g.nt) {   // columns
-        const int k = k0 + j / 48, rem = j % 48, b = rem >> 3, c = rem & 7;
+    for (int j = gt; j < nc * 48 * PER; j += g.nt) {   // columns
+        const int line = j / PER, i0 = (j % PER) * NO;
+        const int k = k0 + line / 48, rem = line % 48, b = rem >> 3, c = rem & 7;
         if (S.cd[k].d.block_type & BT_COPY) continue;
         int in[8];
 #pragma unroll
         for (int r = 0; r < 8; r++) in[r] = S.tmp[k][mb_index(b, r, c)];
-        int16_t out[8];
-        fdct8_line(in, out);
+        int16_t out[NO];
+        fdct8_part<NO>(in, i0, out);
 #pragma unroll
-        for (int r = 0; r < 8; r++) S.coef[k][mb_index(b, r, c)] = out[r];
+        for (int q = 0; q < NO; q++) S.coef[k][mb_index(b, i0 + q, c)] = out[q];
     }
     gsync(g);
     // adaptive QP from the luma coefficients' variance (quantize.cpp:97-118, analysis.h:251-275)
@@ -785,34 +887,36 @@ __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, 
         trellis_warp(S.lev[k], S.coef[k], b, qp, intra_quant(bt), S.cd[k].d.intra_mode, a.lambda, lane);
     }
     gsync(g);
-    for (int j = gt; j < nc * 48; j += g.nt) {   // dequantise + inverse DCT, columns
-        const int k = k0 + j / 48, rem = j % 48, b = rem >> 3, c = rem & 7;
+    for (int j = gt; j < nc * 48 * PER; j += g.nt) {   // dequantise + inverse DCT, columns
+        const int line = j / PER, i0 = (j % PER) * NO;
+        const int k = k0 + line / 48, rem = line % 48, b = rem >> 3, c = rem & 7;
         const int bt = S.cd[k].d.block_type;
         if (bt & BT_COPY) continue;
         const int qp = b >= 4 ? min(S.cd[k].d.q_index + 2, MAXQ) : S.cd[k].d.q_index;
-        int in[8], out[8];
+        int in[8], out[NO];
 #pragma unroll
         for (int r = 0; r < 8; r++) in[r] = dequant_coeff(S.lev[k][mb_index(b, r, c)], qp, r * 8 + c, intra_quant(bt), b >= 4);
-        idct8_line(in, out);
+        idct8_part<NO>(in, i0, out);
 #pragma unroll
-        for (int r = 0; r < 8; r++) S.tmp[k][mb_index(b, r, c)] = (int16_t)out[r];
+        for (int q = 0; q < NO; q++) S.tmp[k][mb_index(b, i0 + q, c)] = (int16_t)out[q];
     }
     gsync(g);
-    for (int j = gt; j < nc * 48; j += g.nt) {   // inverse DCT rows + prediction
-        const int k = k0 + j / 48, rem = j % 48, b = rem >> 3, r = rem & 7;
+    for (int j = gt; j < nc * 48 * PER; j += g.nt) {   // inverse DCT rows + prediction
+        const int line = j / PER, i0 = (j % PER) * NO;
+        const int k = k0 + line / 48, rem = line % 48, b = rem >> 3, r = rem & 7;
         const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
         if (S.cd[k].d.block_type & BT_COPY) {
 #pragma unroll
-            for (int c = 0; c < 8; c++) S.rec[k][mb_index(b, r, c)] = pr ? pr[mb_index(b, r, c)] : (int16_t)0;
+            for (int q = 0; q < NO; q++) S.rec[k][mb_index(b, r, i0 + q)] = pr ? pr[mb_index(b, r, i0 + q)] : (int16_t)0;
         } else {
-            int in[8], out[8];
+            int in[8], out[NO];
 #pragma unroll
             for (int c = 0; c < 8; c++) in[c] = S.tmp[k][mb_index(b, r, c)];
-            idct8_line(in, out);
+            idct8_part<NO>(in, i0, out);
 #pragma unroll
-            for (int c = 0; c < 8; c++) {
-                const int e = mb_index(b, r, c);
-                S.rec[k][e] = (int16_t)(pr ? out[c] + pr[e] : out[c]);
+            for (int q = 0; q < NO; q++) {
+                const int e = mb_index(b, r, i0 + q);
+                S.rec[k][e] = (int16_t)(pr ? out[q] + pr[e] : out[q]);
             }
         }
     }
@@ -945,16 +1049,21 @@ __device__ __noinline__ void inter_search(const Grp g, const FrameArgs &a, int s
     MbShared &S = SM();
     Srch &sr = S.srch[si];
     const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31;
-    if (gw == 0) warp_metrics(S.src, S.win[wa], px, py, lane, &sr.m_sad[0], &sr.m_mad[0], &sr.m_satd[0]);
-    if (gw == 1 && S.has_pred)
-        warp_metrics(S.src, S.win[S.sep ? wb : wa], S.qx, S.qy, lane, &sr.m_sad[1], &sr.m_mad[1], &sr.m_satd[1]);
+    if (gw == 0) {
+        const Metrics m = warp_metrics(S.src, S.win[wa], px, py, lane);
+        if (lane == 0) { sr.m_sad[0] = m.sad; sr.m_mad[0] = m.mad; sr.m_cost[0] = rd_cost(m.satd, a.lambda, 1u); }
+    }
+    if (gw == 1 && S.has_pred) {
+        const Metrics m = warp_metrics(S.src, S.win[S.sep ? wb : wa], S.qx, S.qy, lane);
+        if (lane == 0) { sr.m_sad[1] = m.sad; sr.m_mad[1] = m.mad; sr.m_cost[1] = cand_cost(m.satd, S.qx, S.qy, px, py, a.lambda); }
+    }
     gsync(g);
     if (gt == 0) {
         Sel s;
         s.bx = px; s.by = py; s.sad = sr.m_sad[0]; s.mad = sr.m_mad[0]; s.ssd = INT_MAX;
-        s.cost = rd_cost(sr.m_satd[0], a.lambda, 1u);
+        s.cost = sr.m_cost[0];
         s.sp_index = 0; s.sp_amount = 0; s.sp_enabled = 0;
-        if (S.has_pred) accept_int(s, S.qx, S.qy, sr.m_sad[1], sr.m_mad[1], sr.m_satd[1], px, py, S.thr, a.lambda);
+        if (S.has_pred) accept_int(s, S.qx, S.qy, sr.m_sad[1], sr.m_mad[1], sr.m_cost[1], px, py, S.thr);
         sr.sel = s;
         sr.cur = (S.sep && s.bx == S.qx && s.by == S.qy) ? wb : wa;
     }
@@ -1035,10 +1144,7 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
             S.qy = min(max(py + pmy, 0), a.H - 16);
             S.sep = S.has_pred && (S.qx != px || S.qy != py);
         }
-    }
-    __syncthreads();
-    {
-        WinReq q;
+        WinReq &q = S.req;
         q.n = 0;
         auto add = [&](int wi, const int16_t *pl, int bx, int by, int coh) {
             q.wi[q.n] = wi; q.pl[q.n] = pl; q.bx[q.n] = bx; q.by[q.n] = by; q.coherent[q.n] = coh; q.n++;
@@ -1052,8 +1158,9 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
             add(3, a.planes[a.ref_bwd], px, py, 0);
             if (S.sep) add(4, a.planes[a.ref_bwd], S.qx, S.qy, 0);
         }
-        load_windows(q, a.W, a.H);
     }
+    __syncthreads();
+    load_windows(a.W, a.H);
     __syncthreads();
     if (tid < 3) {   // neighbours for directional intra, from window 0 (intra_pred.cpp:13-54)
         const Win &w = S.win[0];
@@ -1111,7 +1218,7 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
                 for (int m = 0; m < 3; m++) { clear_desc(S.cd[1 + m].d); S.cd[1 + m].d.intra_mode = (uint8_t)S.modes[m]; S.cpred[1 + m] = 4 + m; }
             }
             gsync(g);
-            encode_candidates(g, a, 0, 4);
+            encode_candidates<8>(g, a, 0, 4);
         }
     }
     __syncthreads();
@@ -1178,7 +1285,7 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
         }
     }
     __syncthreads();
-    if (S.need_encode) encode_candidates(G_ALL, a, 4, 1);
+    if (S.need_encode) encode_candidates<1>(G_ALL, a, 4, 1);
     if (tid == 0) {
         int ch = S.win_k;
         if (S.rdo) {   // RDO order: SAD winner, intra default (if the winner is not), the 3 modes (encode.cpp:279-336)
@@ -1194,18 +1301,27 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
     const bool copy = S.cd[ch].d.block_type & BT_COPY;
     int16_t *dU = dst + (size_t)a.W * a.H, *dV = dU + (size_t)(a.W / 2) * (a.H / 2);
     int16_t *lY = a.lev, *lU = a.lev + (size_t)a.W * a.H, *lV = lU + (size_t)(a.W / 2) * (a.H / 2);
+    Win &w0 = S.win[0];   // the next MB's window 0 is this one shifted: keep it equal to the slot
     for (int e = tid; e < MB_N; e += NT) {
+        const int16_t rv = S.rec[ch][e];
         if (e < 256) {
-            const size_t o = (size_t)(py + (e >> 4)) * a.W + px + (e & 15);
-            dst[o] = S.rec[ch][e];
+            const int r = e >> 4, c = e & 15;
+            const size_t o = (size_t)(py + r) * a.W + px + c;
+            dst[o] = rv;
             if (!copy) lY[o] = S.lev[ch][e];
+            w0.y[(py + r - w0.oy) * WL + px + c - w0.ox] = rv;
         } else {
-            const int pl = (e - 256) >> 6, k = (e - 256) & 63;
-            const size_t oc = (size_t)((py >> 1) + (k >> 3)) * (a.W / 2) + (px >> 1) + (k & 7);
-            (pl ? dV : dU)[oc] = S.rec[ch][e];
+            const int pl = (e - 256) >> 6, k = (e - 256) & 63, r = k >> 3, c = k & 7;
+            const size_t oc = (size_t)((py >> 1) + r) * (a.W / 2) + (px >> 1) + c;
+            (pl ? dV : dU)[oc] = rv;
             if (!copy) (pl ? lV : lU)[oc] = S.lev[ch][e];
+            (pl ? w0.v : w0.u)[((py >> 1) + r - w0.coy) * WC + (px >> 1) + c - w0.cox] = rv;
         }
     }
+    // Window rows clamped to plane row 0 or H-1 and chunks left of the plane
+    // hold copies of edge pixels that the patch above does not update: after
+    // an MB on the top, bottom or left edge the next MB loads window 0 afresh.
+    if (tid == 0 && (px == 0 || py == 0 || py + 16 == a.H)) w0.valid = 0;
     if (tid < 7) reinterpret_cast<int *>(a.bt + idx)[tid] = reinterpret_cast<const int *>(&S.cd[ch].d)[tid];
     __threadfence();   // every writer orders its stores before the row's progress release
 }
@@ -1221,10 +1337,12 @@ __global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a)
         s_scan[0][tid] = c_zigzag[tid];
         s_scan[1][tid] = (uint8_t)tid;
         s_scan[2][tid] = (uint8_t)((tid & 7) * 8 + (tid >> 3));
+        s_lut8[tid] = c_lut8[tid];
     }
     __syncthreads();
     for (;;) {
         if (tid == 0) s_row = atomicAdd(&a.counters[0], 1);
+        if (tid < NWIN) S.win[tid].valid = 0;   // windows are reused only along a row
         __syncthreads();
         const int row = s_row;
         if (row >= a.mbh) return;
