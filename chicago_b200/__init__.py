@@ -43,7 +43,9 @@ EXPORTS = [
     "evxg_lambda", "evxg_last_error", "evxg_stream_profile", "evxg_stream_kernel_ms", "evxg_encoder_create", "evxg_encoder_destroy",
     "evxg_encoder_clear", "evxg_encoder_insert_intra", "evxg_encoder_set_quality",
     "evxg_encoder_encode", "evxg_encoder_flush", "evxg_encoder_stream", "evxg_mb_pass_noalloc",
+    "evxg_stream_set_mb_form", "evxg_stream_mb_form",
 ]
+MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
 
 FRAME_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
 
@@ -81,6 +83,8 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_encoder_stream.argtypes = [vp]
     L.evxg_encoder_stream.restype = vp
     L.evxg_mb_pass_noalloc.argtypes = [u32, u32, C.c_char_p, vp, C.POINTER(vp), vp, vp, vp, vp]
+    L.evxg_stream_set_mb_form.argtypes = [vp, i32]
+    L.evxg_stream_mb_form.argtypes = [vp]
     return L
 
 
@@ -181,6 +185,15 @@ class Stream:
 
     def launch_count(self) -> int:
         return lib().evxg_last_launch_count(self.h)
+
+    @property
+    def mb_form(self) -> int:
+        """MB_FORM_CLUSTER (three CTAs per macroblock row) or MB_FORM_SINGLE (one)."""
+        return lib().evxg_stream_mb_form(self.h)
+
+    @mb_form.setter
+    def mb_form(self, form: int):
+        _check(lib().evxg_stream_set_mb_form(self.h, int(form)))
 
 
 class Encoder:

@@ -16,6 +16,7 @@
 namespace evxg {
 __global__ void k_convert(FrameArgs a);
 __global__ void k_mb_wavefront(FrameArgs a);
+__global__ void k_mb_cluster(FrameArgs a);
 __global__ void k_deblock(FrameArgs a);
 __global__ void k_sao_rdo(FrameArgs a);
 __global__ void k_sao_merge(FrameArgs a);
@@ -63,6 +64,7 @@ struct evxg_stream {
     uint8_t *rgb;
     int *sync;                          // 3*mbh progress words, 4 counters, 1 error word
     int mb_grid, num_sms;
+    int mb_form, mb_clusters;          // macroblock pass shape; clusters launched in the cluster form
     uint32_t launches;
     long long timeout_ns;
     bool profile;
@@ -116,16 +118,35 @@ int evxg_stream_create(uint32_t width, uint32_t height, evxg_stream **out)
     if (e == cudaSuccess) e = cudaMemset(s->sync, 0, (3 * s->mbh + 5) * sizeof(int));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_mb_wavefront, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mb_shared_bytes());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_mb_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mb_shared_bytes());
+    int max_clusters = 0;
+    if (e == cudaSuccess) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 3; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(3); cfg.blockDim = dim3(mb_threads()); cfg.dynamicSmemBytes = mb_shared_bytes();
+        cfg.attrs = at; cfg.numAttrs = 1;
+        if (cudaOccupancyMaxActiveClusters(&max_clusters, (void *)k_mb_cluster, &cfg) != cudaSuccess) {
+            cudaGetLastError();   // the cluster form is optional: fall back to one CTA per row
+            max_clusters = 0;
+        }
+    }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         int rc = cuda_fail(e, "evxg_stream_create");
         evxg_stream_destroy(s);
         return rc;
     }
-    // The lag-4 wavefront keeps at most about cols/4 + 1 rows busy at once; a
-    // few more CTAs than that hide row hand-over, the rest would only spin,
-    // and leaving SMs free lets other streams' frames run beside this one.
-    s->mb_grid = (int)std::min<uint32_t>(std::min<uint32_t>(s->mbh, (uint32_t)s->num_sms), s->mbw / 4 + 4);
+    // The wavefront (row r trails row r-1 by four MBs) keeps at most about
+    // cols/4 + 1 rows busy at once; a few more rows than that hide the row
+    // hand-over, more would only spin, and leaving SMs free lets other
+    // streams' frames run beside this one.
+    const uint32_t rows_busy = std::min<uint32_t>(s->mbh, s->mbw / 4 + 4);
+    s->mb_grid = (int)std::min<uint32_t>(rows_busy, (uint32_t)s->num_sms);
+    s->mb_clusters = (int)std::min<uint32_t>(rows_busy, (uint32_t)max_clusters);
+    s->mb_form = s->mb_clusters > 0 ? EVXG_MB_FORM_CLUSTER : EVXG_MB_FORM_SINGLE;
     *out = s;
     return EVXG_SUCCESS;
 }
@@ -155,6 +176,18 @@ int evxg_stream_dims(const evxg_stream *s, uint32_t *aw, uint32_t *ah, uint32_t 
 }
 
 uint32_t evxg_last_launch_count(const evxg_stream *s) { return s ? s->launches : 0; }
+
+int evxg_stream_set_mb_form(evxg_stream *s, int form)
+{
+    if (!s || (form != EVXG_MB_FORM_SINGLE && form != EVXG_MB_FORM_CLUSTER))
+        return fail(EVXG_ERROR_INVALIDARG, "evxg_stream_set_mb_form: unknown form");
+    if (form == EVXG_MB_FORM_CLUSTER && s->mb_clusters <= 0)
+        return fail(EVXG_ERROR_INVALID_RESOURCE, "evxg_stream_set_mb_form: the device cannot run the cluster form");
+    s->mb_form = form;
+    return EVXG_SUCCESS;
+}
+
+int evxg_stream_mb_form(const evxg_stream *s) { return s ? s->mb_form : -EVXG_ERROR_INVALIDARG; }
 
 int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, const evxg_frame *f, void *cuda_stream)
 {
@@ -202,7 +235,10 @@ int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, con
     mark(0);
     k_convert<<<cg, 128, 0, st>>>(a);
     mark(1);
-    k_mb_wavefront<<<s->mb_grid, mb_threads(), mb_shared_bytes(), st>>>(a);
+    if (s->mb_form == EVXG_MB_FORM_CLUSTER)
+        k_mb_cluster<<<3 * s->mb_clusters, mb_threads(), mb_shared_bytes(), st>>>(a);
+    else
+        k_mb_wavefront<<<s->mb_grid, mb_threads(), mb_shared_bytes(), st>>>(a);
     mark(2);
     k_deblock<<<3, 1024, 0, st>>>(a);
     mark(3);

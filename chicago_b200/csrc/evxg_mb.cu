@@ -120,6 +120,25 @@ struct Srch {
     int out_sad;
 };
 
+// Cluster form (three CTAs per macroblock row): what ranks 1 and 2 hand the
+// leader for one MB, and the sequence flags the CTAs exchange.  Every field
+// of Mail is written by exactly one other CTA of the cluster.
+struct alignas(16) Inbox {
+    int16_t f_pred[MB_N], b_pred[MB_N], d_pred[MB_N];   // forward, backward, best directional prediction
+    Desc f_out, b_out, cd[4];
+    int f_sad, b_sad, dir_best, dir_sad, modes[3];
+    float cost[4];             // P: RD costs of the intra candidates cd[0..3]
+};
+struct Mail {
+    Inbox in;                  // leader: results for the current MB
+    Desc left;                 // ranks 1, 2: the leader's final descriptor of the previous MB
+    int row_val;               // ranks 1, 2: row of the latest assignment (-1: no rows left)
+    int row_seq;               // ranks 1, 2: number of row assignments made
+    int dec_seq;               // ranks 1, 2: MBs whose descriptor the leader has published
+    int wr_seq;                // rank 2: MBs the leader has written back to the slot
+    int f_seq, d_seq;          // leader: MBs whose rank-1 / rank-2 results are in the inbox
+};
+
 struct MbShared {
     int16_t src[MB_N];
     Win win[NWIN];
@@ -135,6 +154,7 @@ struct MbShared {
     Desc cd[MAXC];             // 0 intra (no prediction), 1..3 directional modes, 4 SAD winner / final
     float cost[MAXC];
     int16_t coef[MAXC][MB_N], lev[MAXC][MB_N], rec[MAXC][MB_N], tmp[MAXC][MB_N];
+    Mail mail;
 };
 
 extern __shared__ __align__(16) unsigned char g_smem[];
@@ -1013,14 +1033,22 @@ __device__ __noinline__ void intra_bc_search(const Grp g, const FrameArgs &a, in
 }
 
 // MV predictor (motion.cpp:271-346) from the live block table and, for P
-// frames, the previous frame's table.
-__device__ void mv_predictor(const FrameArgs &a, int idx, bool temporal, int &ox, int &oy)
+// frames, the previous frame's table.  left, when given, replaces the table
+// entry of the left neighbour (the cluster form hands it over in shared
+// memory before the leader writes the table).
+__device__ void mv_predictor(const FrameArgs &a, int idx, bool temporal, const evxg_block_desc *left, int &ox, int &oy)
 {
     const int mbw = a.mbw, bx = idx % mbw, by = idx / mbw;
     int mx[3], my[3], n = 0;
     auto motion = [&](int i) { return (__ldcg(&a.bt[i].block_type) & BT_MOTION) != 0; };
     auto take = [&](int i) { mx[n] = __ldcg(&a.bt[i].motion_x); my[n] = __ldcg(&a.bt[i].motion_y); n++; };
-    if (bx > 0 && motion(idx - 1)) take(idx - 1);
+    if (bx > 0) {
+        if (left) {
+            if (left->block_type & BT_MOTION) { mx[n] = left->motion_x; my[n] = left->motion_y; n++; }
+        } else if (motion(idx - 1)) {
+            take(idx - 1);
+        }
+    }
     if (by > 0 && motion(idx - mbw)) take(idx - mbw);
     if (by > 0 && bx + 1 < mbw && motion(idx - mbw + 1)) take(idx - mbw + 1);
     else if (by > 0 && bx > 0 && motion(idx - mbw - 1)) take(idx - mbw - 1);
@@ -1115,86 +1143,280 @@ __device__ __noinline__ void directional_intra(const Grp g)
     gsync(g);
 }
 
-// ------------------------------------------------------------- per MB
+// ------------------------------------------------------------- per-MB steps
 
-__device__ void process_mb(const FrameArgs &a, int row, int col)
+__device__ void load_src(const FrameArgs &a, int px, int py)   // whole CTA
 {
     MbShared &S = SM();
-    const int tid = threadIdx.x;
-    const int px = col * 16, py = row * 16, idx = row * a.mbw + col;
     const int16_t *srcY = a.src, *srcU = a.src + (size_t)a.W * a.H, *srcV = srcU + (size_t)(a.W / 2) * (a.H / 2);
-    int16_t *dst = a.planes[a.dpb];
-
-    for (int e = tid; e < MB_N; e += NT) {
+    for (int e = threadIdx.x; e < MB_N; e += NT) {
         if (e < 256) S.src[e] = __ldg(srcY + (size_t)(py + (e >> 4)) * a.W + px + (e & 15));
         else {
             const int pl = (e - 256) >> 6, k = (e - 256) & 63;
             S.src[e] = __ldg((pl ? srcV : srcU) + (size_t)((py >> 1) + (k >> 3)) * (a.W / 2) + (px >> 1) + (k & 7));
         }
     }
+}
+
+// One thread: copy threshold (motion.cpp:501), RDO flag and, when searches
+// follow, the MV predictor, which serves every search of the MB.  Clears the
+// window request list.
+__device__ void setup_mb(const FrameArgs &a, int idx, int px, int py, bool need_pred, const evxg_block_desc *left)
+{
+    MbShared &S = SM();
+    S.thr = (a.quality >> 2) + 1;
+    S.rdo = a.type == EVXG_FRAME_INTER;
+    S.has_pred = 0; S.sep = 0; S.qx = px; S.qy = py;
+    if (need_pred) {
+        int pmx, pmy;
+        mv_predictor(a, idx, a.type == EVXG_FRAME_INTER, left, pmx, pmy);
+        S.has_pred = (pmx || pmy);
+        S.qx = min(max(px + pmx, 0), a.W - 16);
+        S.qy = min(max(py + pmy, 0), a.H - 16);
+        S.sep = S.has_pred && (S.qx != px || S.qy != py);
+    }
+    S.req.n = 0;
+}
+__device__ void req_window(int wi, const int16_t *pl, int bx, int by, int coh)   // one thread
+{
+    WinReq &q = SM().req;
+    q.wi[q.n] = wi; q.pl[q.n] = pl; q.bx[q.n] = bx; q.by[q.n] = by; q.coherent[q.n] = coh; q.n++;
+}
+
+// Neighbours for directional intra (intra_pred.cpp:13-54), threads 0..2 for
+// Y, U, V; sample(p, y, x) returns plane p's sample at plane coordinates.
+template <class F>
+__device__ void extract_nbr(int px, int py, F sample)
+{
+    MbShared &S = SM();
+    const int p = threadIdx.x;
+    if (p >= 3) return;
+    Nbr &nb = S.nb[p];
+    const int n = p ? 8 : 16, cy = p ? py >> 1 : py, cx = p ? px >> 1 : px;
+    nb.ht = py > 0; nb.hl = px > 0;
+    for (int i = 0; i < n; i++) {
+        nb.top[i] = nb.ht ? sample(p, cy - 1, cx + i) : (int16_t)128;
+        nb.left[i] = nb.hl ? sample(p, cy + i, cx - 1) : (int16_t)128;
+    }
+    if (nb.ht && nb.hl) nb.corner = sample(p, cy - 1, cx - 1);
+    else if (nb.ht) nb.corner = nb.top[0];
+    else if (nb.hl) nb.corner = nb.left[0];
+    else nb.corner = 128;
+    int sum = 0, cnt = 0;
+    if (nb.ht) { for (int i = 0; i < n; i++) sum += nb.top[i]; cnt += n; }
+    if (nb.hl) { for (int i = 0; i < n; i++) sum += nb.left[i]; cnt += n; }
+    nb.dc = cnt > 0 ? (int16_t)((sum + cnt / 2) / cnt) : 128;
+}
+
+__device__ void choose_modes()   // one thread: gradient-pruned candidates (intra_pred.cpp:225-260)
+{
+    MbShared &S = SM();
+    const Nbr &nb = S.nb[0];
+    int gh = 0, gv = 0;
+    if (nb.ht) for (int i = 1; i < 16; i++) gh += iabs32(nb.top[i] - nb.top[i - 1]);
+    if (nb.hl) for (int i = 1; i < 16; i++) gv += iabs32(nb.left[i] - nb.left[i - 1]);
+    S.modes[0] = 0;
+    if (gv > gh * 3 / 2) { S.modes[1] = 2; S.modes[2] = 6; }
+    else if (gh > gv * 3 / 2) { S.modes[1] = 1; S.modes[2] = 5; }
+    else { S.modes[1] = 3; S.modes[2] = 4; }
+}
+
+// P frames: the intra RDO candidates -- intra without prediction and the
+// three directional modes (encode.cpp:295-336); one thread.
+__device__ void intra_candidates()
+{
+    MbShared &S = SM();
+    clear_desc(S.cd[0].d); S.cpred[0] = -1;
+    for (int m = 0; m < 3; m++) {
+        clear_desc(S.cd[1 + m].d);
+        S.cd[1 + m].d.intra_mode = (uint8_t)S.modes[m];
+        S.cpred[1 + m] = 4 + m;
+    }
+}
+
+// B frames: bi-prediction (f + b + 1) >> 1 into pred[3] and its SAD over Y,
+// U and V (motion.cpp:778-813); whole CTA, ends with thread 0 holding bi_sad.
+__device__ void bi_prediction()
+{
+    MbShared &S = SM();
+    const int tid = threadIdx.x;
+    int s = 0;
+    for (int e = tid; e < MB_N; e += NT) {
+        const int av = (S.pred[1][e] + S.pred[2][e] + 1) >> 1;
+        S.pred[3][e] = (int16_t)av;
+        s += iabs32(S.src[e] - av);
+    }
+    s = warp_sum(s);
+    if ((tid & 31) == 0) S.part[tid >> 5] = s;
+    __syncthreads();
     if (tid == 0) {
-        S.thr = (a.quality >> 2) + 1;   // mad_skip_threshold, motion.cpp:501
-        S.rdo = a.type == EVXG_FRAME_INTER;
-        S.has_pred = 0; S.sep = 0; S.qx = px; S.qy = py;
-        if (a.type != EVXG_FRAME_INTRA) {   // one predictor serves every search of this MB
-            int pmx, pmy;
-            mv_predictor(a, idx, a.type == EVXG_FRAME_INTER, pmx, pmy);
-            S.has_pred = (pmx || pmy);
-            S.qx = min(max(px + pmx, 0), a.W - 16);
-            S.qy = min(max(py + pmy, 0), a.H - 16);
-            S.sep = S.has_pred && (S.qx != px || S.qy != py);
+        int t = 0;
+        for (int k = 0; k < NW; k++) t += S.part[k];
+        S.bi_sad = t;
+    }
+}
+
+// Candidate decision by SAD (encode.cpp:168-277, :374-470); one thread.
+// Sets cd[4]/cpred[4] to the winner and need_encode, or (P frames whose winner
+// is an intra candidate, already encoded) points win_k at that candidate.
+__device__ void decide(const FrameArgs &a)
+{
+    MbShared &S = SM();
+    evxg_block_desc best = S.srch[0].out.d;
+    int bsad = S.srch[0].out_sad, bpred = (best.block_type & BT_MOTION) ? 0 : -1;
+    if (a.type == EVXG_FRAME_INTER) {
+        evxg_block_desc in = S.srch[1].out.d;
+        in.prediction_target = (uint8_t)a.ref_fwd;
+        const bool ci = in.block_type & BT_COPY, cb = best.block_type & BT_COPY;
+        if (ci != cb) { if (ci) { best = in; bsad = S.srch[1].out_sad; bpred = 1; } }
+        else if (S.srch[1].out_sad < bsad) { best = in; bsad = S.srch[1].out_sad; bpred = 1; }
+    } else if (a.type == EVXG_FRAME_BIDIR) {
+        evxg_block_desc f = S.srch[1].out.d, b = S.srch[2].out.d;
+        f.prediction_mode = 0; f.prediction_target = (uint8_t)a.ref_fwd;
+        b.prediction_mode = 1; b.prediction_target = (uint8_t)a.ref_bwd;
+        if (S.srch[1].out_sad < bsad) { best = f; bsad = S.srch[1].out_sad; bpred = 1; }
+        if (S.srch[2].out_sad < bsad) { best = b; bsad = S.srch[2].out_sad; bpred = 2; }
+        const int bias = __float2int_rz(__fmul_rn(a.lambda, 8.0f));
+        if (S.bi_sad + bias < bsad) {
+            evxg_block_desc bi;
+            clear_desc(bi);
+            bi.block_type = INTER_MOTION_DELTA; bi.prediction_mode = 2;
+            bi.prediction_target = (uint8_t)a.ref_fwd;
+            bi.motion_x = f.motion_x; bi.motion_y = f.motion_y;
+            bi.sp_pred = f.sp_pred; bi.sp_amount = f.sp_amount; bi.sp_index = f.sp_index;
+            bi.prediction_target_b = (uint8_t)a.ref_bwd;
+            bi.motion_x_b = b.motion_x; bi.motion_y_b = b.motion_y;
+            bi.sp_pred_b = b.sp_pred; bi.sp_amount_b = b.sp_amount; bi.sp_index_b = b.sp_index;
+            best = bi; bsad = S.bi_sad; bpred = 3;
         }
-        WinReq &q = S.req;
-        q.n = 0;
-        auto add = [&](int wi, const int16_t *pl, int bx, int by, int coh) {
-            q.wi[q.n] = wi; q.pl[q.n] = pl; q.bx[q.n] = bx; q.by[q.n] = by; q.coherent[q.n] = coh; q.n++;
-        };
-        add(0, dst, px, py - 16, 1);   // intra window: the slot being reconstructed
+    }
+    int dir_k = -1;
+    if (S.dir_sad < bsad) {
+        clear_desc(best);
+        best.intra_mode = (uint8_t)S.modes[S.dir_best];
+        bsad = S.dir_sad;
+        bpred = 4 + S.dir_best;
+        dir_k = 1 + S.dir_best;
+    }
+    if (a.type == EVXG_FRAME_INTER && best.block_type == INTRA_DEFAULT) {
+        // already encoded with the intra RDO candidates
+        S.win_k = best.intra_mode == MODE_NONE ? 0 : dir_k;
+        S.need_encode = 0;
+    } else {
+        S.cd[4].d = best; S.cpred[4] = bpred;
+        S.win_k = 4; S.need_encode = 1;
+    }
+}
+
+__device__ void rdo_choose()   // one thread: RDO order -- SAD winner, intra default, the 3 modes (encode.cpp:279-336)
+{
+    MbShared &S = SM();
+    int ch = S.win_k;
+    if (S.rdo) {
+        float bc = S.cost[ch];
+        if (S.cd[S.win_k].d.block_type != INTRA_DEFAULT && S.cost[0] < bc) { ch = 0; bc = S.cost[0]; }
+        for (int k = 1; k <= 3; k++) if (S.cost[k] < bc) { ch = k; bc = S.cost[k]; }
+    }
+    S.chosen = ch;
+}
+
+// Write-back of the chosen candidate (rec / lev, possibly another CTA's shared
+// memory): reconstruction into the DPB slot and window 0, levels (non-copy
+// blocks), descriptor; whole CTA, ends with a fence before the progress release.
+__device__ void write_back(const FrameArgs &a, int px, int py, int idx, const int16_t *rec, const int16_t *lev)
+{
+    MbShared &S = SM();
+    const int tid = threadIdx.x;
+    const int ch = S.chosen;
+    const bool copy = S.cd[ch].d.block_type & BT_COPY;
+    int16_t *dst = a.planes[a.dpb];
+    int16_t *dU = dst + (size_t)a.W * a.H, *dV = dU + (size_t)(a.W / 2) * (a.H / 2);
+    int16_t *lY = a.lev, *lU = a.lev + (size_t)a.W * a.H, *lV = lU + (size_t)(a.W / 2) * (a.H / 2);
+    Win &w0 = S.win[0];   // the next MB's window 0 is this one shifted: keep it equal to the slot
+    for (int e = tid; e < MB_N; e += NT) {
+        const int16_t rv = rec[e];
+        if (e < 256) {
+            const int r = e >> 4, c = e & 15;
+            const size_t o = (size_t)(py + r) * a.W + px + c;
+            dst[o] = rv;
+            if (!copy) lY[o] = lev[e];
+            w0.y[(py + r - w0.oy) * WL + px + c - w0.ox] = rv;
+        } else {
+            const int pl = (e - 256) >> 6, k = (e - 256) & 63, r = k >> 3, c = k & 7;
+            const size_t oc = (size_t)((py >> 1) + r) * (a.W / 2) + (px >> 1) + c;
+            (pl ? dV : dU)[oc] = rv;
+            if (!copy) (pl ? lV : lU)[oc] = lev[e];
+            (pl ? w0.v : w0.u)[((py >> 1) + r - w0.coy) * WC + (px >> 1) + c - w0.cox] = rv;
+        }
+    }
+    // Window rows clamped to plane row 0 or H-1 and chunks left of the plane
+    // hold copies of edge pixels that the patch above does not update: after
+    // an MB on the top, bottom or left edge the next MB loads window 0 afresh.
+    if (tid == 0 && (px == 0 || py == 0 || py + 16 == a.H)) w0.valid = 0;
+    if (tid < 7) reinterpret_cast<int *>(a.bt + idx)[tid] = reinterpret_cast<const int *>(&S.cd[ch].d)[tid];
+    __threadfence();   // every writer orders its stores before the row's progress release
+}
+
+// Thread 0: wait until row r has finished column need (the wavefront's
+// progress words); false once the error word is set or the wait times out.
+__device__ bool wait_progress(const FrameArgs &a, int r, int need)
+{
+    const unsigned long long t0 = globaltimer_ns();
+    while (ld_acquire(&a.progress[r]) < need) {
+        if (*(volatile int *)a.error) return false;
+        if ((long long)(globaltimer_ns() - t0) > a.timeout_ns) {
+            atomicCAS(a.error, 0, EVXG_ERROR_OPERATION_TIMEDOUT);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    return true;
+}
+
+__device__ void init_tables()
+{
+    const int tid = threadIdx.x;
+    if (tid < 64) {
+        s_qm[0][tid] = c_qm_intra[tid]; s_qm[1][tid] = c_qm_inter[tid];
+        s_dz[0][tid] = c_dz_intra[tid]; s_dz[1][tid] = c_dz_inter[tid];
+        s_scan[0][tid] = c_zigzag[tid];
+        s_scan[1][tid] = (uint8_t)tid;
+        s_scan[2][tid] = (uint8_t)((tid & 7) * 8 + (tid >> 3));
+        s_lut8[tid] = c_lut8[tid];
+    }
+}
+
+// ------------------------------------------------- single-CTA form, per MB
+
+__device__ void process_mb(const FrameArgs &a, int row, int col)
+{
+    MbShared &S = SM();
+    const int tid = threadIdx.x;
+    const int px = col * 16, py = row * 16, idx = row * a.mbw + col;
+    int16_t *dst = a.planes[a.dpb];
+
+    load_src(a, px, py);
+    if (tid == 0) {
+        setup_mb(a, idx, px, py, a.type != EVXG_FRAME_INTRA, nullptr);
+        req_window(0, dst, px, py - 16, 1);   // intra window: the slot being reconstructed
         if (a.type != EVXG_FRAME_INTRA) {
-            add(1, a.planes[a.ref_fwd], px, py, 0);
-            if (S.sep) add(2, a.planes[a.ref_fwd], S.qx, S.qy, 0);
+            req_window(1, a.planes[a.ref_fwd], px, py, 0);
+            if (S.sep) req_window(2, a.planes[a.ref_fwd], S.qx, S.qy, 0);
         }
         if (a.type == EVXG_FRAME_BIDIR) {
-            add(3, a.planes[a.ref_bwd], px, py, 0);
-            if (S.sep) add(4, a.planes[a.ref_bwd], S.qx, S.qy, 0);
+            req_window(3, a.planes[a.ref_bwd], px, py, 0);
+            if (S.sep) req_window(4, a.planes[a.ref_bwd], S.qx, S.qy, 0);
         }
     }
     __syncthreads();
     load_windows(a.W, a.H);
     __syncthreads();
-    if (tid < 3) {   // neighbours for directional intra, from window 0 (intra_pred.cpp:13-54)
+    extract_nbr(px, py, [&](int p, int y, int x) -> int16_t {   // from window 0
         const Win &w = S.win[0];
-        Nbr &nb = S.nb[tid];
-        const int n = tid ? 8 : 16;
-        const int16_t *pl = tid == 0 ? w.y : (tid == 1 ? w.u : w.v);
-        const int S_ = tid ? WC : WL;
-        const int trow = tid ? (py >> 1) - 1 - w.coy : py - 1 - w.oy;   // window coordinates of (cy-1, cx)
-        const int tcol = tid ? (px >> 1) - w.cox : px - w.ox;
-        nb.ht = py > 0; nb.hl = px > 0;
-        for (int i = 0; i < n; i++) {
-            nb.top[i] = nb.ht ? pl[trow * S_ + tcol + i] : (int16_t)128;
-            nb.left[i] = nb.hl ? pl[(trow + 1 + i) * S_ + tcol - 1] : (int16_t)128;
-        }
-        if (nb.ht && nb.hl) nb.corner = pl[trow * S_ + tcol - 1];
-        else if (nb.ht) nb.corner = nb.top[0];
-        else if (nb.hl) nb.corner = nb.left[0];
-        else nb.corner = 128;
-        int sum = 0, cnt = 0;
-        if (nb.ht) { for (int i = 0; i < n; i++) sum += nb.top[i]; cnt += n; }
-        if (nb.hl) { for (int i = 0; i < n; i++) sum += nb.left[i]; cnt += n; }
-        nb.dc = cnt > 0 ? (int16_t)((sum + cnt / 2) / cnt) : 128;
-    }
+        return p == 0 ? w.y[(y - w.oy) * WL + x - w.ox] : (p == 1 ? w.u : w.v)[(y - w.coy) * WC + x - w.cox];
+    });
     __syncthreads();
-    if (tid == 0) {   // gradient-pruned candidates (intra_pred.cpp:225-260)
-        const Nbr &nb = S.nb[0];
-        int gh = 0, gv = 0;
-        if (nb.ht) for (int i = 1; i < 16; i++) gh += iabs32(nb.top[i] - nb.top[i - 1]);
-        if (nb.hl) for (int i = 1; i < 16; i++) gv += iabs32(nb.left[i] - nb.left[i - 1]);
-        S.modes[0] = 0;
-        if (gv > gh * 3 / 2) { S.modes[1] = 2; S.modes[2] = 6; }
-        else if (gh > gv * 3 / 2) { S.modes[1] = 1; S.modes[2] = 5; }
-        else { S.modes[1] = 3; S.modes[2] = 4; }
-    }
+    if (tid == 0) choose_modes();
     __syncthreads();
 
     // Independent work runs concurrently on three warp groups.
@@ -1213,117 +1435,19 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
             // The intra RDO candidates do not depend on the searches
             // (encode.cpp:295-336): encode them while the searches run.
             directional_intra(g);
-            if (tid - g.t0 == 0) {
-                clear_desc(S.cd[0].d); S.cpred[0] = -1;
-                for (int m = 0; m < 3; m++) { clear_desc(S.cd[1 + m].d); S.cd[1 + m].d.intra_mode = (uint8_t)S.modes[m]; S.cpred[1 + m] = 4 + m; }
-            }
+            if (tid - g.t0 == 0) intra_candidates();
             gsync(g);
             encode_candidates<8>(g, a, 0, 4);
         }
     }
     __syncthreads();
-    if (a.type == EVXG_FRAME_BIDIR) {   // bi-prediction: (f + b + 1) >> 1, SAD over Y, U, V (motion.cpp:778-813)
-        int s = 0;
-        for (int e = tid; e < MB_N; e += NT) {
-            const int av = (S.pred[1][e] + S.pred[2][e] + 1) >> 1;
-            S.pred[3][e] = (int16_t)av;
-            s += iabs32(S.src[e] - av);
-        }
-        s = warp_sum(s);
-        if ((tid & 31) == 0) S.part[tid >> 5] = s;
-        __syncthreads();
-        if (tid == 0) {
-            int t = 0;
-            for (int k = 0; k < NW; k++) t += S.part[k];
-            S.bi_sad = t;
-        }
-    }
-    if (tid == 0) {   // candidate decision (encode.cpp:168-277, :374-470)
-        evxg_block_desc best = S.srch[0].out.d;
-        int bsad = S.srch[0].out_sad, bpred = (best.block_type & BT_MOTION) ? 0 : -1;
-        if (a.type == EVXG_FRAME_INTER) {
-            evxg_block_desc in = S.srch[1].out.d;
-            in.prediction_target = (uint8_t)a.ref_fwd;
-            const bool ci = in.block_type & BT_COPY, cb = best.block_type & BT_COPY;
-            if (ci != cb) { if (ci) { best = in; bsad = S.srch[1].out_sad; bpred = 1; } }
-            else if (S.srch[1].out_sad < bsad) { best = in; bsad = S.srch[1].out_sad; bpred = 1; }
-        } else if (a.type == EVXG_FRAME_BIDIR) {
-            evxg_block_desc f = S.srch[1].out.d, b = S.srch[2].out.d;
-            f.prediction_mode = 0; f.prediction_target = (uint8_t)a.ref_fwd;
-            b.prediction_mode = 1; b.prediction_target = (uint8_t)a.ref_bwd;
-            if (S.srch[1].out_sad < bsad) { best = f; bsad = S.srch[1].out_sad; bpred = 1; }
-            if (S.srch[2].out_sad < bsad) { best = b; bsad = S.srch[2].out_sad; bpred = 2; }
-            const int bias = __float2int_rz(__fmul_rn(a.lambda, 8.0f));
-            if (S.bi_sad + bias < bsad) {
-                evxg_block_desc bi;
-                clear_desc(bi);
-                bi.block_type = INTER_MOTION_DELTA; bi.prediction_mode = 2;
-                bi.prediction_target = (uint8_t)a.ref_fwd;
-                bi.motion_x = f.motion_x; bi.motion_y = f.motion_y;
-                bi.sp_pred = f.sp_pred; bi.sp_amount = f.sp_amount; bi.sp_index = f.sp_index;
-                bi.prediction_target_b = (uint8_t)a.ref_bwd;
-                bi.motion_x_b = b.motion_x; bi.motion_y_b = b.motion_y;
-                bi.sp_pred_b = b.sp_pred; bi.sp_amount_b = b.sp_amount; bi.sp_index_b = b.sp_index;
-                best = bi; bsad = S.bi_sad; bpred = 3;
-            }
-        }
-        int dir_k = -1;
-        if (S.dir_sad < bsad) {
-            clear_desc(best);
-            best.intra_mode = (uint8_t)S.modes[S.dir_best];
-            bsad = S.dir_sad;
-            bpred = 4 + S.dir_best;
-            dir_k = 1 + S.dir_best;
-        }
-        if (a.type == EVXG_FRAME_INTER && best.block_type == INTRA_DEFAULT) {
-            // already encoded with the intra RDO candidates
-            S.win_k = best.intra_mode == MODE_NONE ? 0 : dir_k;
-            S.need_encode = 0;
-        } else {
-            S.cd[4].d = best; S.cpred[4] = bpred;
-            S.win_k = 4; S.need_encode = 1;
-        }
-    }
+    if (a.type == EVXG_FRAME_BIDIR) bi_prediction();
+    if (tid == 0) decide(a);
     __syncthreads();
     if (S.need_encode) encode_candidates<1>(G_ALL, a, 4, 1);
-    if (tid == 0) {
-        int ch = S.win_k;
-        if (S.rdo) {   // RDO order: SAD winner, intra default (if the winner is not), the 3 modes (encode.cpp:279-336)
-            float bc = S.cost[ch];
-            if (S.cd[S.win_k].d.block_type != INTRA_DEFAULT && S.cost[0] < bc) { ch = 0; bc = S.cost[0]; }
-            for (int k = 1; k <= 3; k++) if (S.cost[k] < bc) { ch = k; bc = S.cost[k]; }
-        }
-        S.chosen = ch;
-    }
+    if (tid == 0) rdo_choose();
     __syncthreads();
-    // write-back: reconstruction into the DPB slot, levels (non-copy), descriptor
-    const int ch = S.chosen;
-    const bool copy = S.cd[ch].d.block_type & BT_COPY;
-    int16_t *dU = dst + (size_t)a.W * a.H, *dV = dU + (size_t)(a.W / 2) * (a.H / 2);
-    int16_t *lY = a.lev, *lU = a.lev + (size_t)a.W * a.H, *lV = lU + (size_t)(a.W / 2) * (a.H / 2);
-    Win &w0 = S.win[0];   // the next MB's window 0 is this one shifted: keep it equal to the slot
-    for (int e = tid; e < MB_N; e += NT) {
-        const int16_t rv = S.rec[ch][e];
-        if (e < 256) {
-            const int r = e >> 4, c = e & 15;
-            const size_t o = (size_t)(py + r) * a.W + px + c;
-            dst[o] = rv;
-            if (!copy) lY[o] = S.lev[ch][e];
-            w0.y[(py + r - w0.oy) * WL + px + c - w0.ox] = rv;
-        } else {
-            const int pl = (e - 256) >> 6, k = (e - 256) & 63, r = k >> 3, c = k & 7;
-            const size_t oc = (size_t)((py >> 1) + r) * (a.W / 2) + (px >> 1) + c;
-            (pl ? dV : dU)[oc] = rv;
-            if (!copy) (pl ? lV : lU)[oc] = S.lev[ch][e];
-            (pl ? w0.v : w0.u)[((py >> 1) + r - w0.coy) * WC + (px >> 1) + c - w0.cox] = rv;
-        }
-    }
-    // Window rows clamped to plane row 0 or H-1 and chunks left of the plane
-    // hold copies of edge pixels that the patch above does not update: after
-    // an MB on the top, bottom or left edge the next MB loads window 0 afresh.
-    if (tid == 0 && (px == 0 || py == 0 || py + 16 == a.H)) w0.valid = 0;
-    if (tid < 7) reinterpret_cast<int *>(a.bt + idx)[tid] = reinterpret_cast<const int *>(&S.cd[ch].d)[tid];
-    __threadfence();   // every writer orders its stores before the row's progress release
+    write_back(a, px, py, idx, S.rec[S.chosen], S.lev[S.chosen]);
 }
 
 __global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a)
@@ -1331,14 +1455,7 @@ __global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a)
     MbShared &S = SM();
     __shared__ int s_row;
     const int tid = threadIdx.x;
-    if (tid < 64) {
-        s_qm[0][tid] = c_qm_intra[tid]; s_qm[1][tid] = c_qm_inter[tid];
-        s_dz[0][tid] = c_dz_intra[tid]; s_dz[1][tid] = c_dz_inter[tid];
-        s_scan[0][tid] = c_zigzag[tid];
-        s_scan[1][tid] = (uint8_t)tid;
-        s_scan[2][tid] = (uint8_t)((tid & 7) * 8 + (tid >> 3));
-        s_lut8[tid] = c_lut8[tid];
-    }
+    init_tables();
     __syncthreads();
     for (;;) {
         if (tid == 0) s_row = atomicAdd(&a.counters[0], 1);
@@ -1348,27 +1465,14 @@ __global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a)
         if (row >= a.mbh) return;
         for (int col = 0; col < a.mbw; ++col) {
             if (tid == 0) {
-                S.row_abort = 0;
-                if (row > 0) {
-                    // Row r-1 must have finished column c+3: the reads of MB (r,c)
-                    // (intra block-copy candidates x in [px-31, px+31], 6-tap
-                    // overshoot -3..+18) reach columns c-3 .. c+3.  Rows below
-                    // then trail by three columns too, so row r+1 has finished at
-                    // most column c-4 and the stale pixels MB (r,c) reads there
-                    // (columns >= c-3) are still unwritten.  The reference waits
-                    // for c+4 (encode.cpp:866-877); c+3 gives the same pixels.
-                    const int need = min(col + 3, a.mbw - 1);
-                    const unsigned long long t0 = globaltimer_ns();
-                    while (ld_acquire(&a.progress[row - 1]) < need) {
-                        if (*(volatile int *)a.error) { S.row_abort = 1; break; }
-                        if ((long long)(globaltimer_ns() - t0) > a.timeout_ns) {
-                            atomicCAS(a.error, 0, EVXG_ERROR_OPERATION_TIMEDOUT);
-                            S.row_abort = 1;
-                            break;
-                        }
-                        __nanosleep(64);
-                    }
-                }
+                // Row r-1 must have finished column c+3: the reads of MB (r,c)
+                // (intra block-copy candidates x in [px-31, px+31], 6-tap
+                // overshoot -3..+18) reach columns c-3 .. c+3.  Rows below
+                // then trail by three columns too, so row r+1 has finished at
+                // most column c-4 and the stale pixels MB (r,c) reads there
+                // (columns >= c-3) are still unwritten.  The reference waits
+                // for c+4 (encode.cpp:866-877); c+3 gives the same pixels.
+                S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 3, a.mbw - 1));
             }
             __syncthreads();
             if (S.row_abort) return;
@@ -1378,6 +1482,270 @@ __global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a)
         }
         __syncthreads();
     }
+}
+
+// ------------------------------------------- cluster form: three CTAs per row
+//
+// A cluster of three CTAs encodes one macroblock row; each search gets a whole
+// CTA (12 warps: a pattern step's eight candidates in one round) instead of a
+// warp group.
+//   rank 0, the leader: waits for the wavefront, runs the intra block-copy
+//     search, takes the other ranks' results, decides, encodes the winner
+//     and writes the MB back.
+//   rank 1: the forward (P: the) inter search.
+//   rank 2: the backward search (B frames), then directional intra; for P
+//     frames also encodes the four intra RDO candidates.
+// The inter searches need only the MV predictor, i.e. the descriptors of the
+// left MB and of row r-1 up to column c+1, so ranks 1 and 2 start MB c as soon
+// as the leader has decided MB c-1 and search while the leader still encodes
+// MB c-1 and runs MB c's intra search.  Directional intra needs MB c-1's
+// reconstruction and row r-1 up to column c.
+//
+// Hand-over is through distributed shared memory: peers store results into
+// the leader's inbox (and the leader its decision into the peers' mail), then
+// a thread releases a sequence number at cluster scope, which the reader
+// acquires.  A writer refills a mail field only after the reader has
+// signalled that it is done with the previous content, so one copy of each
+// suffices.  Every wait is bounded; once any CTA gives up it sets the error
+// word, the others see it in their next wait, and all three reach the final
+// cluster barrier (no CTA exits while a peer may still access its shared
+// memory).
+
+__device__ __forceinline__ unsigned cluster_rank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void cluster_barrier()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+template <class T>
+__device__ __forceinline__ T *peer(T *p, unsigned rank)   // the same shared-memory object in CTA `rank`
+{
+    T *r;
+    asm volatile("mapa.u64 %0, %1, %2;" : "=l"(r) : "l"(p), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void st_release_cl(int *p, int v)
+{
+    asm volatile("st.release.cluster.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_acquire_cl(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.cluster.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+// Thread 0: wait until a mail flag of this CTA reaches v.
+__device__ bool wait_mail(const int *flag, int v, const FrameArgs &a)
+{
+    const unsigned long long t0 = globaltimer_ns();
+    while (ld_acquire_cl(flag) < v) {
+        if (*(volatile int *)a.error) return false;
+        if ((long long)(globaltimer_ns() - t0) > a.timeout_ns) {
+            atomicCAS(a.error, 0, EVXG_ERROR_OPERATION_TIMEDOUT);
+            return false;
+        }
+        __nanosleep(20);
+    }
+    return true;
+}
+__device__ __forceinline__ void copy_block(int16_t *to, const int16_t *from)   // 384 samples, whole CTA
+{
+    for (int c = threadIdx.x; c < MB_N / 8; c += NT) reinterpret_cast<uint4 *>(to)[c] = reinterpret_cast<const uint4 *>(from)[c];
+}
+__device__ void publish_decision(const evxg_block_desc &d, int n)   // leader, one thread
+{
+    MbShared &S = SM();
+    for (unsigned p = 1; p < 3; p++) {
+        int *to = reinterpret_cast<int *>(peer(&S.mail.left, p));
+        for (int i = 0; i < 7; i++) to[i] = reinterpret_cast<const int *>(&d)[i];
+        st_release_cl(peer(&S.mail.dec_seq, p), n);
+    }
+}
+
+// Leader: MB (row, col), the n-th MB of this cluster.
+__device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
+{
+    MbShared &S = SM();
+    const int tid = threadIdx.x;
+    const int px = col * 16, py = row * 16, idx = row * a.mbw + col;
+    if (tid == 0) S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 3, a.mbw - 1));
+    __syncthreads();
+    if (S.row_abort) return false;
+    load_src(a, px, py);
+    if (tid == 0) {
+        setup_mb(a, idx, px, py, false, nullptr);
+        req_window(0, a.planes[a.dpb], px, py - 16, 1);
+    }
+    __syncthreads();
+    load_windows(a.W, a.H);
+    __syncthreads();
+    intra_bc_search(G_ALL, a, px, py);
+    if (tid == 0)
+        S.row_abort = !((a.type == EVXG_FRAME_INTRA || wait_mail(&S.mail.f_seq, n, a)) && wait_mail(&S.mail.d_seq, n, a));
+    __syncthreads();
+    if (S.row_abort) return false;
+    const Inbox &in = S.mail.in;
+    if (a.type != EVXG_FRAME_INTRA) copy_block(S.pred[1], in.f_pred);
+    if (a.type == EVXG_FRAME_BIDIR) copy_block(S.pred[2], in.b_pred);
+    if (a.type != EVXG_FRAME_INTER) copy_block(S.pred[4 + in.dir_best], in.d_pred);
+    if (tid == 0) {
+        S.srch[1].out = in.f_out; S.srch[1].out_sad = in.f_sad;
+        S.srch[2].out = in.b_out; S.srch[2].out_sad = in.b_sad;
+        S.dir_best = in.dir_best; S.dir_sad = in.dir_sad;
+        for (int m = 0; m < 3; m++) S.modes[m] = in.modes[m];
+        if (a.type == EVXG_FRAME_INTER)
+            for (int k = 0; k < 4; k++) { S.cd[k] = in.cd[k]; S.cost[k] = in.cost[k]; S.cpred[k] = k ? 3 + k : -1; }
+    }
+    __syncthreads();
+    if (a.type == EVXG_FRAME_BIDIR) bi_prediction();
+    if (tid == 0) {
+        decide(a);
+        if (a.type != EVXG_FRAME_INTER) publish_decision(S.cd[4].d, n);   // encoding does not change the modes or MVs
+    }
+    __syncthreads();
+    if (S.need_encode) encode_candidates<1>(G_ALL, a, 4, 1);
+    if (tid == 0) {
+        rdo_choose();
+        if (a.type == EVXG_FRAME_INTER) publish_decision(S.cd[S.chosen].d, n);
+    }
+    __syncthreads();
+    const int ch = S.chosen;
+    const bool remote = a.type == EVXG_FRAME_INTER && ch < 4;   // an intra candidate encoded by rank 2
+    write_back(a, px, py, idx, remote ? peer(S.rec[ch], 2) : S.rec[ch], remote ? peer(S.lev[ch], 2) : S.lev[ch]);
+    __syncthreads();
+    if (tid == 0) {
+        st_release(&a.progress[row], col);
+        st_release_cl(peer(&S.mail.wr_seq, 2), n);
+    }
+    return true;
+}
+
+// Ranks 1 and 2: the forward or backward inter search of the n-th MB, handed
+// to the leader's inbox (the caller releases the sequence flag).
+__device__ bool search_mb(const FrameArgs &a, int row, int col, int n, bool bwd)
+{
+    MbShared &S = SM();
+    const int tid = threadIdx.x;
+    const int px = col * 16, py = row * 16, idx = row * a.mbw + col;
+    if (tid == 0)
+        S.row_abort = !(wait_mail(&S.mail.dec_seq, n - 1, a) && (row == 0 || wait_progress(a, row - 1, min(col + 1, a.mbw - 1))));
+    __syncthreads();
+    if (S.row_abort) return false;
+    load_src(a, px, py);
+    const int si = bwd ? 2 : 1, wa = bwd ? 3 : 1;
+    if (tid == 0) {
+        setup_mb(a, idx, px, py, true, col > 0 ? &S.mail.left.d : nullptr);
+        const int16_t *ref = a.planes[bwd ? a.ref_bwd : a.ref_fwd];
+        req_window(wa, ref, px, py, 0);
+        if (S.sep) req_window(wa + 1, ref, S.qx, S.qy, 0);
+    }
+    __syncthreads();
+    load_windows(a.W, a.H);
+    __syncthreads();
+    inter_search(G_ALL, a, si, wa, wa + 1, px, py, S.pred[si]);
+    Inbox *in = peer(&S.mail.in, 0);
+    copy_block(bwd ? in->b_pred : in->f_pred, S.pred[si]);
+    if (tid == 0) {
+        if (bwd) { in->b_out = S.srch[si].out; in->b_sad = S.srch[si].out_sad; }
+        else { in->f_out = S.srch[si].out; in->f_sad = S.srch[si].out_sad; }
+    }
+    return true;
+}
+
+__device__ bool fwd_mb(const FrameArgs &a, int row, int col, int n)   // rank 1
+{
+    if (a.type == EVXG_FRAME_INTRA) return true;
+    if (!search_mb(a, row, col, n, false)) return false;
+    __syncthreads();
+    if (threadIdx.x == 0) st_release_cl(peer(&SM().mail.f_seq, 0), n);
+    return true;
+}
+
+__device__ bool aux_mb(const FrameArgs &a, int row, int col, int n)   // rank 2
+{
+    MbShared &S = SM();
+    const int tid = threadIdx.x;
+    const int px = col * 16, py = row * 16;
+    if (a.type == EVXG_FRAME_BIDIR && !search_mb(a, row, col, n, true)) return false;
+    // Directional intra reads MB (r, c-1), written back by the leader, and
+    // row r-1 up to column c, from the destination slot.
+    if (tid == 0) S.row_abort = !(wait_mail(&S.mail.wr_seq, n - 1, a) && (row == 0 || wait_progress(a, row - 1, col)));
+    __syncthreads();
+    if (S.row_abort) return false;
+    if (a.type != EVXG_FRAME_BIDIR) {
+        load_src(a, px, py);
+        if (tid == 0) setup_mb(a, row * a.mbw + col, px, py, false, nullptr);
+    }
+    const int16_t *dst = a.planes[a.dpb];
+    extract_nbr(px, py, [&](int p, int y, int x) -> int16_t {
+        const int16_t *pl = p == 0 ? dst : dst + (size_t)a.W * a.H + (size_t)(p - 1) * (a.W / 2) * (a.H / 2);
+        return __ldcg(pl + (size_t)y * (p ? a.W / 2 : a.W) + x);
+    });
+    __syncthreads();
+    if (tid == 0) choose_modes();
+    __syncthreads();
+    directional_intra(G_ALL);
+    if (a.type == EVXG_FRAME_INTER) {
+        if (tid == 0) intra_candidates();
+        __syncthreads();
+        encode_candidates<4>(G_ALL, a, 0, 4);
+    }
+    Inbox *in = peer(&S.mail.in, 0);
+    if (a.type != EVXG_FRAME_INTER) copy_block(in->d_pred, S.pred[4 + S.dir_best]);
+    if (tid == 0) {
+        in->dir_best = S.dir_best; in->dir_sad = S.dir_sad;
+        for (int m = 0; m < 3; m++) in->modes[m] = S.modes[m];
+        if (a.type == EVXG_FRAME_INTER)
+            for (int k = 0; k < 4; k++) { in->cd[k] = S.cd[k]; in->cost[k] = S.cost[k]; }
+    }
+    __syncthreads();
+    if (tid == 0) st_release_cl(peer(&S.mail.d_seq, 0), n);
+    return true;
+}
+
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(NT, 1) k_mb_cluster(FrameArgs a)
+{
+    MbShared &S = SM();
+    __shared__ int s_row;
+    const int tid = threadIdx.x;
+    const unsigned rank = cluster_rank();
+    init_tables();
+    if (tid == 0) {
+        S.mail.row_seq = 0; S.mail.dec_seq = 0; S.mail.wr_seq = 0; S.mail.f_seq = 0; S.mail.d_seq = 0;
+        S.row_abort = 0;
+    }
+    cluster_barrier();   // every CTA's mail is initialised before any peer writes to it
+    int n = 0;
+    for (int k = 1;; k++) {
+        if (tid == 0) {
+            if (rank == 0) {   // the leader claims rows and passes them on
+                const int r = atomicAdd(&a.counters[0], 1);
+                s_row = r < a.mbh ? r : -1;
+                for (unsigned p = 1; p < 3; p++) {
+                    *peer(&S.mail.row_val, p) = s_row;
+                    st_release_cl(peer(&S.mail.row_seq, p), k);
+                }
+            } else {
+                s_row = wait_mail(&S.mail.row_seq, k, a) ? S.mail.row_val : -1;
+            }
+        }
+        if (tid < NWIN) S.win[tid].valid = 0;   // windows are reused only along a row
+        __syncthreads();
+        const int row = s_row;
+        if (row < 0) break;
+        bool ok = true;
+        for (int col = 0; col < a.mbw && ok; ++col) {
+            ++n;
+            ok = rank == 0 ? leader_mb(a, row, col, n) : (rank == 1 ? fwd_mb(a, row, col, n) : aux_mb(a, row, col, n));
+            __syncthreads();
+        }
+        if (!ok) break;
+    }
+    cluster_barrier();   // no CTA leaves while a peer may still access its shared memory
 }
 
 size_t mb_shared_bytes() { return sizeof(MbShared); }

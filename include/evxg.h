@@ -144,6 +144,24 @@ int evxg_stream_sync(evxg_stream *s, void *cuda_stream);
 /* Number of kernels launched by the last evxg_encode_frame call. */
 uint32_t evxg_last_launch_count(const evxg_stream *s);
 
+/* Shape of the macroblock pass (no counterpart in the reference, whose WPP
+ * runs one thread per macroblock row):
+ *   EVXG_MB_FORM_CLUSTER  a cluster of three CTAs per macroblock row (intra
+ *                         block-copy search and decision / forward search /
+ *                         backward search and directional intra on separate
+ *                         SMs): the lowest latency per frame; the default
+ *                         when the device can co-schedule such clusters.
+ *   EVXG_MB_FORM_SINGLE   one CTA per row (the searches share it as warp
+ *                         groups): a third of the SMs per row, the higher
+ *                         throughput when many streams share the GPU.
+ * Both give identical output.  evxg_stream_set_mb_form returns
+ * EVXG_ERROR_INVALID_RESOURCE if the cluster form cannot run on this device;
+ * evxg_stream_mb_form reports the current form. */
+#define EVXG_MB_FORM_SINGLE  0
+#define EVXG_MB_FORM_CLUSTER 1
+int evxg_stream_set_mb_form(evxg_stream *s, int form);
+int evxg_stream_mb_form(const evxg_stream *s);
+
 /* Kernel timing (no counterpart in the reference, which has no device work):
  * when enabled, evxg_encode_frame records a CUDA event around each of its
  * kernels; evxg_stream_kernel_ms waits for the last frame and writes up to n

@@ -24,10 +24,14 @@ CASES = [  # (w, h, frames, quality, vmax, intra_at)
 ]
 
 
-def check_stream(oracle, w, h, T, q, vmax, intra_at):
+FORMS = ("cluster", "single")   # three CTAs per macroblock row / one
+
+
+def check_stream(oracle, w, h, T, q, vmax, intra_at, form="cluster"):
     import chicago_b200 as cb
     frames = generate(w, h, T, seed=w * 7 + h, vmax=vmax)
     oc, st = oracle.context(w, h), cb.Stream(w, h)
+    st.mb_form = cb.MB_FORM_CLUSTER if form == "cluster" else cb.MB_FORM_SINGLE
     for k, (ti, f18) in enumerate(plan_gop(T, quality=q, intra_at=intra_at)):
         fr = unpack_frame(f18)
         od = oc.encode_frame(frames[ti], f18)
@@ -41,14 +45,16 @@ def check_stream(oracle, w, h, T, q, vmax, intra_at):
         assert np.array_equal(st.fetch_planes(fr["dpb_slot"]), od.final), f"frame {k}: reconstruction"
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("w,h,T,q,vmax,intra_at", CASES)
-def test_gpu_matches_oracle(oracle, w, h, T, q, vmax, intra_at):
-    check_stream(oracle, w, h, T, q, vmax, intra_at)
+def test_gpu_matches_oracle(oracle, w, h, T, q, vmax, intra_at, form):
+    check_stream(oracle, w, h, T, q, vmax, intra_at, form)
 
 
-def test_gpu_matches_oracle_1080p(oracle):
-    """Full-size frames: I, P and reference-B at 1920x1080 (120x68 MBs)."""
-    check_stream(oracle, 1920, 1080, 3, 8, 24.0, ())
+@pytest.mark.parametrize("form", FORMS)
+def test_gpu_matches_oracle_1080p(oracle, form):
+    """Full-size frames: I, P, reference-B and B at 1920x1080 (120x68 MBs)."""
+    check_stream(oracle, 1920, 1080, 4, 8, 24.0, (), form)
 
 
 def test_evx_bytes_match_stock_reference(ref):
@@ -69,6 +75,17 @@ def test_evx_bytes_match_stock_reference(ref):
     for k, r in enumerate(enc.records):
         sl = ctx.serialize(r["frame18"], r["blocks"], r["prev_blocks"], r["sao"], r["levels"])
         assert r["frame18"] + sl == payloads[k], f"frame {k} bytes differ"
+
+
+def test_cluster_form_is_the_default():
+    """A B200 co-schedules three-CTA clusters: streams start in the cluster form."""
+    import chicago_b200 as cb
+    st = cb.Stream(64, 48)
+    assert st.mb_form == cb.MB_FORM_CLUSTER
+    st.mb_form = cb.MB_FORM_SINGLE
+    assert st.mb_form == cb.MB_FORM_SINGLE
+    with pytest.raises(cb.EvxgError):
+        st.mb_form = 7
 
 
 def test_stream_rejects_bad_frames():
