@@ -149,6 +149,7 @@ struct MbShared {
     int has_pred, sep, qx, qy;
     int modes[3], dsad[3], dir_best, dir_sad;
     int bi_sad, part[NW];
+    unsigned aq[MAXC][4][3];   // adaptive QP: per candidate and luma block, sum / sum of squares / count
     int cpred[MAXC], win_k, need_encode, chosen, rdo;
     WinReq req;
     Desc cd[MAXC];             // 0 intra (no prediction), 1..3 directional modes, 4 SAD winner / final
@@ -448,15 +449,37 @@ __device__ __noinline__ void warp_subpel(const int16_t *src, const Win &w, int x
     if (out4 && lane == 0) { out4[0] = sh; out4[1] = mh; out4[2] = sq; out4[3] = mq; }
 }
 
-// Integer candidate acceptance (motion.cpp:148-177), replayed by one thread;
-// the candidate's cost comes from cand_cost.
+// Integer candidate acceptance test (motion.cpp:148-177) against selection s.
+__device__ __forceinline__ bool takes_int(const Sel &s, int sad, int mad, int ssd, float cost, int thr)
+{
+    if (s.mad < thr) return mad < s.mad || (mad == s.mad && ssd < s.ssd);
+    return (cost < s.cost || ((cost == s.cost && ssd < s.ssd) && sad < SAD_THRESHOLD)) || mad < thr;
+}
+// The same, applied (one thread); the candidate's cost comes from cand_cost.
 __device__ __forceinline__ void accept_int(Sel &s, int x, int y, int sad, int mad, float cost, int px, int py, int thr)
 {
     const int ssd = (x - px) * (x - px) + (y - py) * (y - py);
-    bool take;
-    if (s.mad < thr) take = mad < s.mad || (mad == s.mad && ssd < s.ssd);
-    else take = (cost < s.cost || ((cost == s.cost && ssd < s.ssd) && sad < SAD_THRESHOLD)) || mad < thr;
-    if (take) { s.bx = x; s.by = y; s.sad = sad; s.ssd = ssd; s.mad = mad; s.cost = cost; }
+    if (takes_int(s, sad, mad, ssd, cost, thr)) { s.bx = x; s.by = y; s.sad = sad; s.ssd = ssd; s.mad = mad; s.cost = cost; }
+}
+
+// Replay of an ordered candidate list by one warp: lane k holds candidate k
+// (ok = valid).  Each round every later lane tests the rule against the
+// current selection and the first one that takes it becomes the selection --
+// exactly the sequential loop, whose selection changes only at the
+// candidates it takes -- until no lane takes it (or, with stop_on_copy, the
+// selection's MAD drops below the threshold: the early exit).  take(s) is the
+// lane's test, adopt(s, k) copies candidate k (from its lane) into s.
+template <class Take, class Adopt>
+__device__ __forceinline__ void warp_replay(Sel &s, bool ok, int lane, int thr, bool stop_on_copy, Take take, Adopt adopt)
+{
+    int last = -1;
+    for (;;) {
+        const unsigned b = __ballot_sync(0xffffffffu, ok && lane > last && take(s));
+        if (!b) return;
+        last = __ffs((int)b) - 1;
+        adopt(s, last);
+        if (stop_on_copy && s.mad < thr) return;
+    }
 }
 
 // One pattern step (perform_intra/inter_motion_search, motion.cpp:348-406) on
@@ -490,22 +513,29 @@ __device__ __noinline__ void run_step(const Grp g, int si, int wi, bool intra, i
         }
     }
     gsync(g);
-    if (gt == 0) {
+    if (gw == 0) {   // the reference's loop order, with its early exit
         Sel s = sr.sel;
-        const Sel s0 = s;
-        const int thr = S.thr;
-        for (int k = 0; k < 9; k++) {
-            const int x = bx + l + (k % 3) * st, y = by + t + (k / 3) * st;
-            if (centred && k == 4) {
-                if (intra && y > py - 16 && x > px - 16) continue;   // the intra search's starting point
-                accept_int(s, x, y, s0.sad, s0.mad, s0.cost, px, py, thr);
-            } else {
-                if (!sr.valid[k]) continue;
-                accept_int(s, x, y, sr.m_sad[k], sr.m_mad[k], sr.m_cost[k], px, py, thr);
-            }
-            if (s.mad < thr) break;   // early exit on a copy-quality match
+        const int k = lane < 9 ? lane : 0;
+        const int x = bx + l + (k % 3) * st, y = by + t + (k / 3) * st;
+        const int ssd = (x - px) * (x - px) + (y - py) * (y - py);
+        bool ok;
+        int sad, mad;
+        float cost;
+        if (centred && k == 4) {   // the selection itself; invalid only as the intra search's starting point
+            ok = !(intra && y > py - 16 && x > px - 16);
+            sad = s.sad; mad = s.mad; cost = s.cost;
+        } else {
+            ok = sr.valid[k]; sad = sr.m_sad[k]; mad = sr.m_mad[k]; cost = sr.m_cost[k];
         }
-        sr.sel = s;
+        ok = ok && lane < 9;
+        warp_replay(s, ok, lane, S.thr, true,
+                    [&](const Sel &c) { return takes_int(c, sad, mad, ssd, cost, S.thr); },
+                    [&](Sel &c, int from) {
+                        c.bx = __shfl_sync(0xffffffffu, x, from); c.by = __shfl_sync(0xffffffffu, y, from);
+                        c.sad = __shfl_sync(0xffffffffu, sad, from); c.mad = __shfl_sync(0xffffffffu, mad, from);
+                        c.ssd = __shfl_sync(0xffffffffu, ssd, from); c.cost = __shfl_sync(0xffffffffu, cost, from);
+                    });
+        if (lane == 0) sr.sel = s;
     }
     gsync(g);
 }
@@ -599,23 +629,22 @@ __device__ __noinline__ void run_subpel(const Grp g, int si, int wi, bool intra,
         if (lane == 0) { sr.spm[k][0] = sh; sr.spm[k][1] = mh; sr.spm[k][2] = sq; sr.spm[k][3] = mq; }
     }
     gsync(g);
-    if (gt == 0) {
+    if (gw == 0) {   // 8 directions x (half, quarter), in the reference's order
         Sel s = sr.sel;
         const int thr = S.thr;
         s.sp_index = 0; s.sp_amount = 0; s.sp_enabled = 0;
-        for (int k = 0; k < 8; k++) {
-            if (!sr.valid[k]) continue;
-            const int r = k < 4 ? k : k + 1;
-            for (int q = 0; q < 2; q++) {
-                const int sad = sr.spm[k][q * 2], mad = sr.spm[k][q * 2 + 1];
-                const bool take = s.mad < thr ? (mad < s.mad) : ((sad < s.sad && sad < SAD_THRESHOLD) || mad < thr);
-                if (take) {
-                    s.sp_enabled = 1; s.sp_amount = q; s.sp_index = frac_from_dir(r % 3 - 1, r / 3 - 1);
-                    s.sad = sad; s.mad = mad;
-                }
-            }
-        }
-        sr.sel = s;
+        const int k = (lane >> 1) & 7, q = lane & 1, r = k < 4 ? k : k + 1;
+        const bool ok = lane < 16 && sr.valid[k];
+        const int sad = sr.spm[k][q * 2], mad = sr.spm[k][q * 2 + 1];
+        const int idx = frac_from_dir(r % 3 - 1, r / 3 - 1);
+        warp_replay(s, ok, lane, thr, false,
+                    [&](const Sel &c) { return c.mad < thr ? (mad < c.mad) : ((sad < c.sad && sad < SAD_THRESHOLD) || mad < thr); },
+                    [&](Sel &c, int from) {
+                        c.sp_enabled = 1; c.sp_amount = __shfl_sync(0xffffffffu, q, from);
+                        c.sp_index = __shfl_sync(0xffffffffu, idx, from);
+                        c.sad = __shfl_sync(0xffffffffu, sad, from); c.mad = __shfl_sync(0xffffffffu, mad, from);
+                    });
+        if (lane == 0) sr.sel = s;
     }
     gsync(g);
 }
@@ -823,121 +852,100 @@ __device__ void trellis_warp(int16_t *lev, const int16_t *coef, int b, int qp, b
 
 // encode_block + decode_block for candidates k0 .. k0+nc-1 on a warp group
 // (encode.cpp:481-750, decode.cpp:31-432); with S.rdo set also their RD cost
-// (encode.cpp:39-164).  The transforms give each thread NO outputs of one
-// 8-point line: 8 when the group has few threads per line (several
-// candidates on one group), 1 when it has eight or more (one candidate on
-// the whole CTA), which shortens each transform pass eightfold.
-template <int NO>
+// (encode.cpp:39-164).  One warp runs one 8x8 block through the whole chain
+// -- forward DCT rows and columns, quantisation, trellis, dequantisation,
+// inverse DCT and prediction -- synchronising only with itself, each lane
+// computing two outputs of a line.  The adaptive QP needs the MB's four luma
+// blocks: each block's warp leaves its partial sums, and after one barrier
+// every warp combines the same four (the sums wrap modulo 2^32 like the
+// reference's, so the order does not matter).
 __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, int k0, int nc)
 {
     MbShared &S = SM();
     const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31, nw = g.nt >> 5;
-    constexpr int PER = 8 / NO;   // work items per line
-    for (int j = gt; j < nc * 48 * PER; j += g.nt) {   // forward DCT, rows
-        const int line = j / PER, i0 = (j % PER) * NO;
-        const int k = k0 + line / 48, rem = line % 48, b = rem >> 3, r = rem & 7;
+    const int l4 = lane >> 2, i0 = (lane & 3) * 2;   // line and first of two outputs
+    for (int j = gw; j < nc * 6; j += nw) {   // forward DCT and AQ partial sums
+        const int k = k0 + j / 6, b = j % 6;
         if (S.cd[k].d.block_type & BT_COPY) continue;
         const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
         int in[8];
+        int16_t out[2];
 #pragma unroll
         for (int c = 0; c < 8; c++) {
-            const int e = mb_index(b, r, c);
+            const int e = mb_index(b, l4, c);
             in[c] = (int16_t)(pr ? S.src[e] - pr[e] : S.src[e]);
         }
-        int16_t out[NO];
-        fdct8_part<NO>(in, i0, out);
+        fdct8_part<2>(in, i0, out);
+        S.tmp[k][mb_index(b, l4, i0)] = out[0];
+        S.tmp[k][mb_index(b, l4, i0 + 1)] = out[1];
+        __syncwarp();
 #pragma unroll
-        for (int q = 0; q < NO; q++) S.tmp[k][mb_index(b, r, i0 + q)] = out[q];
-    }
-    gsync(g);
-    for (int j = gt; j < nc * 48 * PER; j += g.nt) {   // columns
-        const int line = j / PER, i0 = (j % PER) * NO;
-        const int k = k0 + line / 48, rem = line % 48, b = rem >> 3, c = rem & 7;
-        if (S.cd[k].d.block_type & BT_COPY) continue;
-        int in[8];
+        for (int r = 0; r < 8; r++) in[r] = S.tmp[k][mb_index(b, r, l4)];
+        fdct8_part<2>(in, i0, out);
+        S.coef[k][mb_index(b, i0, l4)] = out[0];
+        S.coef[k][mb_index(b, i0 + 1, l4)] = out[1];
+        if (b < 4) {   // variance of the nonzero luma AC-and-DC coefficients but the MB's first (quantize.cpp:97-118, analysis.h:251-275)
+            unsigned sum = 0, sq = 0, cnt = 0;
 #pragma unroll
-        for (int r = 0; r < 8; r++) in[r] = S.tmp[k][mb_index(b, r, c)];
-        int16_t out[NO];
-        fdct8_part<NO>(in, i0, out);
+            for (int h = 0; h < 2; h++) {
+                const int e = mb_index(b, i0 + h, l4);
+                const int t = out[h];
+                if (e != 0 && t) { sum += (unsigned)t; sq += (unsigned)wmul(t, t); cnt++; }
+            }
 #pragma unroll
-        for (int q = 0; q < NO; q++) S.coef[k][mb_index(b, i0 + q, c)] = out[q];
-    }
-    gsync(g);
-    // adaptive QP from the luma coefficients' variance (quantize.cpp:97-118, analysis.h:251-275)
-    for (int ci = gw; ci < nc; ci += nw) {
-        const int k = k0 + ci;
-        if (S.cd[k].d.block_type & BT_COPY) continue;
-        unsigned sum = 0, sq = 0, cnt = 0;
-        for (int e = lane; e < 256; e += 32) {
-            if (e == 0) continue;
-            const int t = S.coef[k][e];
-            if (t) { sum += (unsigned)t; sq += (unsigned)wmul(t, t); cnt++; }
-        }
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            sum += __shfl_xor_sync(0xffffffffu, sum, o);
-            sq += __shfl_xor_sync(0xffffffffu, sq, o);
-            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-        }
-        if (lane == 0) {
-            const int var = cnt > 0 ? (int)(sq - (unsigned)rdiv(wmul((int)sum, (int)sum), (int)cnt)) : 0;
-            const int idx = min(max(lg2u((unsigned)var) >> 1, 1), MAXQ);
-            int delta = (int16_t)((int16_t)idx - (int16_t)a.quality) >> 1;
-            delta = min(max(delta, -6), 6);
-            S.cd[k].d.q_index = (uint8_t)min(max(a.quality + delta, 1), MAXQ);
-            S.cd[k].d.variance = (int16_t)var;
+            for (int o = 16; o; o >>= 1) {
+                sum += __shfl_xor_sync(0xffffffffu, sum, o);
+                sq += __shfl_xor_sync(0xffffffffu, sq, o);
+                cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+            }
+            if (lane == 0) { S.aq[k][b][0] = sum; S.aq[k][b][1] = sq; S.aq[k][b][2] = cnt; }
         }
     }
     gsync(g);
-    for (int e = gt; e < nc * MB_N; e += g.nt) {   // quantise
-        const int k = k0 + e / MB_N, p = e % MB_N;
-        const int bt = S.cd[k].d.block_type;
-        if (bt & BT_COPY) continue;
-        const bool chroma = p >= 256;
-        const int qp = chroma ? min(S.cd[k].d.q_index + 2, MAXQ) : S.cd[k].d.q_index;
-        const int o = chroma ? (p & 63) : (((p >> 4) & 7) * 8 + (p & 7));
-        S.lev[k][p] = quant_coeff(S.coef[k][p], qp, o, intra_quant(bt), chroma);
-    }
-    gsync(g);
-    for (int j = gw; j < nc * 6; j += nw) {   // trellis, one warp per 8x8 block
+    for (int j = gw; j < nc * 6; j += nw) {   // quantise, trellis, reconstruct
         const int k = k0 + j / 6, b = j % 6;
         const int bt = S.cd[k].d.block_type;
-        if (bt & BT_COPY) continue;
-        const int qp = b >= 4 ? min(S.cd[k].d.q_index + 2, MAXQ) : S.cd[k].d.q_index;
-        trellis_warp(S.lev[k], S.coef[k], b, qp, intra_quant(bt), S.cd[k].d.intra_mode, a.lambda, lane);
-    }
-    gsync(g);
-    for (int j = gt; j < nc * 48 * PER; j += g.nt) {   // dequantise + inverse DCT, columns
-        const int line = j / PER, i0 = (j % PER) * NO;
-        const int k = k0 + line / 48, rem = line % 48, b = rem >> 3, c = rem & 7;
-        const int bt = S.cd[k].d.block_type;
-        if (bt & BT_COPY) continue;
-        const int qp = b >= 4 ? min(S.cd[k].d.q_index + 2, MAXQ) : S.cd[k].d.q_index;
-        int in[8], out[NO];
-#pragma unroll
-        for (int r = 0; r < 8; r++) in[r] = dequant_coeff(S.lev[k][mb_index(b, r, c)], qp, r * 8 + c, intra_quant(bt), b >= 4);
-        idct8_part<NO>(in, i0, out);
-#pragma unroll
-        for (int q = 0; q < NO; q++) S.tmp[k][mb_index(b, i0 + q, c)] = (int16_t)out[q];
-    }
-    gsync(g);
-    for (int j = gt; j < nc * 48 * PER; j += g.nt) {   // inverse DCT rows + prediction
-        const int line = j / PER, i0 = (j % PER) * NO;
-        const int k = k0 + line / 48, rem = line % 48, b = rem >> 3, r = rem & 7;
         const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
-        if (S.cd[k].d.block_type & BT_COPY) {
+        if (bt & BT_COPY) {
 #pragma unroll
-            for (int q = 0; q < NO; q++) S.rec[k][mb_index(b, r, i0 + q)] = pr ? pr[mb_index(b, r, i0 + q)] : (int16_t)0;
-        } else {
-            int in[8], out[NO];
-#pragma unroll
-            for (int c = 0; c < 8; c++) in[c] = S.tmp[k][mb_index(b, r, c)];
-            idct8_part<NO>(in, i0, out);
-#pragma unroll
-            for (int q = 0; q < NO; q++) {
-                const int e = mb_index(b, r, i0 + q);
-                S.rec[k][e] = (int16_t)(pr ? out[q] + pr[e] : out[q]);
+            for (int h = 0; h < 2; h++) {
+                const int e = mb_index(b, l4, i0 + h);
+                S.rec[k][e] = pr ? pr[e] : (int16_t)0;
             }
+            continue;
+        }
+        unsigned sum = 0, sq = 0, cnt = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) { sum += S.aq[k][q][0]; sq += S.aq[k][q][1]; cnt += S.aq[k][q][2]; }
+        const int var = cnt > 0 ? (int)(sq - (unsigned)rdiv(wmul((int)sum, (int)sum), (int)cnt)) : 0;
+        const int aqi = min(max(lg2u((unsigned)var) >> 1, 1), MAXQ);
+        const int delta = min(max((int)((int16_t)((int16_t)aqi - (int16_t)a.quality) >> 1), -6), 6);
+        const int q_index = min(max(a.quality + delta, 1), MAXQ);
+        if (b == 0 && lane == 0) { S.cd[k].d.q_index = (uint8_t)q_index; S.cd[k].d.variance = (int16_t)var; }
+        const bool chroma = b >= 4, iq = intra_quant(bt);
+        const int qp = chroma ? min(q_index + 2, MAXQ) : q_index;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int o = lane + 32 * h, e = mb_index(b, o >> 3, o & 7);
+            S.lev[k][e] = quant_coeff(S.coef[k][e], qp, o, iq, chroma);
+        }
+        __syncwarp();
+        trellis_warp(S.lev[k], S.coef[k], b, qp, iq, S.cd[k].d.intra_mode, a.lambda, lane);
+        __syncwarp();
+        int in[8], out[2];
+#pragma unroll
+        for (int r = 0; r < 8; r++) in[r] = dequant_coeff(S.lev[k][mb_index(b, r, l4)], qp, r * 8 + l4, iq, chroma);
+        idct8_part<2>(in, i0, out);
+        S.tmp[k][mb_index(b, i0, l4)] = (int16_t)out[0];
+        S.tmp[k][mb_index(b, i0 + 1, l4)] = (int16_t)out[1];
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < 8; c++) in[c] = S.tmp[k][mb_index(b, l4, c)];
+        idct8_part<2>(in, i0, out);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int e = mb_index(b, l4, i0 + h);
+            S.rec[k][e] = (int16_t)(pr ? out[h] + pr[e] : out[h]);
         }
     }
     gsync(g);
@@ -1183,29 +1191,39 @@ __device__ void req_window(int wi, const int16_t *pl, int bx, int by, int coh)  
     q.wi[q.n] = wi; q.pl[q.n] = pl; q.bx[q.n] = bx; q.by[q.n] = by; q.coherent[q.n] = coh; q.n++;
 }
 
-// Neighbours for directional intra (intra_pred.cpp:13-54), threads 0..2 for
-// Y, U, V; sample(p, y, x) returns plane p's sample at plane coordinates.
+// Neighbours for directional intra (intra_pred.cpp:13-54); sample(p, y, x)
+// returns plane p's (Y, U, V) sample at plane coordinates.  Threads 0..63
+// fetch the 64 top / left samples in parallel, the corner and DC follow.
+// Ends with a CTA barrier.
 template <class F>
 __device__ void extract_nbr(int px, int py, F sample)
 {
     MbShared &S = SM();
-    const int p = threadIdx.x;
-    if (p >= 3) return;
-    Nbr &nb = S.nb[p];
-    const int n = p ? 8 : 16, cy = p ? py >> 1 : py, cx = p ? px >> 1 : px;
-    nb.ht = py > 0; nb.hl = px > 0;
-    for (int i = 0; i < n; i++) {
-        nb.top[i] = nb.ht ? sample(p, cy - 1, cx + i) : (int16_t)128;
-        nb.left[i] = nb.hl ? sample(p, cy + i, cx - 1) : (int16_t)128;
+    const int tid = threadIdx.x;
+    const bool ht = py > 0, hl = px > 0;
+    if (tid < 64) {   // luma top 0..15, left 16..31; U top 32..39, left 40..47; V 48..63
+        const int p = tid < 32 ? 0 : (tid < 48 ? 1 : 2);
+        const int k = tid < 32 ? tid : (tid - 32) & 15, n = p ? 8 : 16;
+        const int cy = p ? py >> 1 : py, cx = p ? px >> 1 : px;
+        Nbr &nb = S.nb[p];
+        if (k < n) nb.top[k] = ht ? sample(p, cy - 1, cx + k) : (int16_t)128;
+        else nb.left[k - n] = hl ? sample(p, cy + k - n, cx - 1) : (int16_t)128;
+    } else if (tid < 67) {
+        const int p = tid - 64, cy = p ? py >> 1 : py, cx = p ? px >> 1 : px;
+        S.nb[p].corner = (ht && hl) ? sample(p, cy - 1, cx - 1) : (int16_t)0;
     }
-    if (nb.ht && nb.hl) nb.corner = sample(p, cy - 1, cx - 1);
-    else if (nb.ht) nb.corner = nb.top[0];
-    else if (nb.hl) nb.corner = nb.left[0];
-    else nb.corner = 128;
-    int sum = 0, cnt = 0;
-    if (nb.ht) { for (int i = 0; i < n; i++) sum += nb.top[i]; cnt += n; }
-    if (nb.hl) { for (int i = 0; i < n; i++) sum += nb.left[i]; cnt += n; }
-    nb.dc = cnt > 0 ? (int16_t)((sum + cnt / 2) / cnt) : 128;
+    __syncthreads();
+    if (tid < 3) {
+        Nbr &nb = S.nb[tid];
+        const int n = tid ? 8 : 16;
+        nb.ht = ht; nb.hl = hl;
+        if (!(ht && hl)) nb.corner = ht ? nb.top[0] : (hl ? nb.left[0] : (int16_t)128);
+        int sum = 0, cnt = 0;
+        if (ht) { for (int i = 0; i < n; i++) sum += nb.top[i]; cnt += n; }
+        if (hl) { for (int i = 0; i < n; i++) sum += nb.left[i]; cnt += n; }
+        nb.dc = cnt > 0 ? (int16_t)((sum + cnt / 2) / cnt) : 128;
+    }
+    __syncthreads();
 }
 
 __device__ void choose_modes()   // one thread: gradient-pruned candidates (intra_pred.cpp:225-260)
@@ -1415,7 +1433,6 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
         const Win &w = S.win[0];
         return p == 0 ? w.y[(y - w.oy) * WL + x - w.ox] : (p == 1 ? w.u : w.v)[(y - w.coy) * WC + x - w.cox];
     });
-    __syncthreads();
     if (tid == 0) choose_modes();
     __syncthreads();
 
@@ -1437,14 +1454,14 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
             directional_intra(g);
             if (tid - g.t0 == 0) intra_candidates();
             gsync(g);
-            encode_candidates<8>(g, a, 0, 4);
+            encode_candidates(g, a, 0, 4);
         }
     }
     __syncthreads();
     if (a.type == EVXG_FRAME_BIDIR) bi_prediction();
     if (tid == 0) decide(a);
     __syncthreads();
-    if (S.need_encode) encode_candidates<1>(G_ALL, a, 4, 1);
+    if (S.need_encode) encode_candidates(G_ALL, a, 4, 1);
     if (tid == 0) rdo_choose();
     __syncthreads();
     write_back(a, px, py, idx, S.rec[S.chosen], S.lev[S.chosen]);
@@ -1607,7 +1624,7 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
         if (a.type != EVXG_FRAME_INTER) publish_decision(S.cd[4].d, n);   // encoding does not change the modes or MVs
     }
     __syncthreads();
-    if (S.need_encode) encode_candidates<1>(G_ALL, a, 4, 1);
+    if (S.need_encode) encode_candidates(G_ALL, a, 4, 1);
     if (tid == 0) {
         rdo_choose();
         if (a.type == EVXG_FRAME_INTER) publish_decision(S.cd[S.chosen].d, n);
@@ -1685,14 +1702,13 @@ __device__ bool aux_mb(const FrameArgs &a, int row, int col, int n)   // rank 2
         const int16_t *pl = p == 0 ? dst : dst + (size_t)a.W * a.H + (size_t)(p - 1) * (a.W / 2) * (a.H / 2);
         return __ldcg(pl + (size_t)y * (p ? a.W / 2 : a.W) + x);
     });
-    __syncthreads();
     if (tid == 0) choose_modes();
     __syncthreads();
     directional_intra(G_ALL);
     if (a.type == EVXG_FRAME_INTER) {
         if (tid == 0) intra_candidates();
         __syncthreads();
-        encode_candidates<4>(G_ALL, a, 0, 4);
+        encode_candidates(G_ALL, a, 0, 4);
     }
     Inbox *in = peer(&S.mail.in, 0);
     if (a.type != EVXG_FRAME_INTER) copy_block(in->d_pred, S.pred[4 + S.dir_best]);
