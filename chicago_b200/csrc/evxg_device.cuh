@@ -32,7 +32,7 @@ constexpr int WL_OFF = 34, WC_OFF = 19;
 
 __device__ __forceinline__ int rdiv(int n, int d)   // rounded_div, evx_math.h:228-236
 {
-    return ((n < 0) != (d < 0)) ? (n - d / 2) / d : (n + d / 2) / d;
+    return (((n < 0) != (d < 0)) ? n - d / 2 : n + d / 2) / d;   // one division: select the numerator first
 }
 __device__ __forceinline__ int lg2u(unsigned v) { return v ? 31 - __clz((int)v) : 0; }  // evx_math.h:69-113
 __device__ __forceinline__ int req_bits8(int x) { return lg2u((unsigned)(x & 255)) + 1; }  // required_bits((uint8)x)

@@ -77,11 +77,10 @@ struct alignas(16) Win {
     int valid;                 // 0: contents undefined (start of a row)
 };
 // Windows requested for one MB: window wi[k] around luma (bx[k], by[k]) of
-// plane set pl[k]; coherent[k] selects L2-only loads (the slot being
-// reconstructed); mode[k] is decided by load_windows.
+// plane set pl[k]; mode[k] is decided by load_windows.
 struct WinReq {
     int n;
-    int wi[5], bx[5], by[5], coherent[5], mode[5];
+    int wi[5], bx[5], by[5], mode[5];
     const int16_t *pl[5];
 };
 struct Sel {                   // evx_motion_selection, motion.cpp:53-66
@@ -172,6 +171,8 @@ __device__ __forceinline__ Grp group(int k) { return Grp{1 + k, k * GT, GT}; }
 
 // ---------------------------------------------------------------- helpers
 
+__device__ __forceinline__ int blk_base(int b) { return b < 4 ? (b >> 1) * 128 + (b & 1) * 8 : 256 + (b - 4) * 64; }
+__device__ __forceinline__ int blk_stride(int b) { return b < 4 ? 16 : 8; }
 __device__ __forceinline__ int mb_index(int b, int r, int c)   // element (r,c) of 8x8 block b of an MB buffer
 {
     return b < 4 ? (((b >> 1) * 8 + r) * 16 + (b & 1) * 8 + c) : (256 + (b - 4) * 64 + r * 8 + c);
@@ -197,19 +198,11 @@ __device__ __forceinline__ int frac_from_dir(int i, int j)   // motion.cpp:68-91
     return i + 5;
 }
 
-// Load a clamped search window around luma base (bx, by) from a plane set:
-// aligned 16-byte chunks, all loads of a thread issued before its stores.
-// Rows are clamped to the plane; chunks left/right of the plane are filled
-// with the edge sample, which is the clamping of interp.cpp:8-14.
-template <bool kCoherent>
-__device__ __forceinline__ uint4 ld16(const int16_t *p)
+// 16-byte chunk loads from L2.
+__device__ __forceinline__ uint4 ld16(const int16_t *p) { return __ldcg(reinterpret_cast<const uint4 *>(p)); }
+__device__ __forceinline__ uint4 edge16(const int16_t *p)   // one sample repeated over a chunk
 {
-    return kCoherent ? __ldcg(reinterpret_cast<const uint4 *>(p)) : __ldg(reinterpret_cast<const uint4 *>(p));
-}
-template <bool kCoherent>
-__device__ __forceinline__ uint4 edge16(const int16_t *p)
-{
-    const unsigned v = (unsigned short)(kCoherent ? __ldcg(p) : __ldg(p));
+    const unsigned v = (unsigned short)__ldcg(p);
     const unsigned w2 = v | (v << 16);
     return make_uint4(w2, w2, w2, w2);
 }
@@ -219,13 +212,14 @@ __device__ __forceinline__ int win_cox(int bx) { return (((bx >> 1) - WC_OFF) >>
 
 // One 16-byte chunk of window row r (luma: plane row by-WL_OFF+r, columns
 // x0 .. x0+7; chroma likewise), rows clamped to the plane and columns outside
-// it filled with the edge sample -- the clamping of interp.cpp:8-14.
-__device__ __forceinline__ uint4 win_chunk(const int16_t *plane, int S, int rows, int y, int x0, bool coh)
+// it filled with the edge sample -- the clamping of interp.cpp:8-14.  Loads go
+// to L2 (the slot being reconstructed is written by other SMs during the
+// kernel; a window chunk is read once per MB, so L1 would not help the others).
+__device__ __forceinline__ uint4 win_chunk(const int16_t *plane, int S, int rows, int y, int x0)
 {
     const int16_t *row = plane + (size_t)min(max(y, 0), rows - 1) * S;
-    if (x0 >= 0 && x0 + 8 <= S) return coh ? ld16<true>(row + x0) : ld16<false>(row + x0);
-    const int16_t *e = row + (x0 < 0 ? 0 : S - 1);
-    return coh ? edge16<true>(e) : edge16<false>(e);
+    if (x0 >= 0 && x0 + 8 <= S) return ld16(row + x0);
+    return edge16(row + (x0 < 0 ? 0 : S - 1));
 }
 
 // Fill the requested windows (S.req, built by thread 0).  A window whose
@@ -233,7 +227,7 @@ __device__ __forceinline__ uint4 win_chunk(const int16_t *plane, int S, int rows
 // macroblock (16 luma / 8 chroma columns, same rows) -- the next MB of a row
 // -- is shifted in shared memory and only its new strip is read from memory,
 // one thread per window row; every other window is loaded whole, every thread
-// issuing up to 8 chunk loads before storing them.  A shifted window holds
+// issuing up to 4 chunk loads before storing them.  A shifted window holds
 // what a fresh load would: reference slots do not change during a frame, and
 // for the slot being reconstructed the caller patches each finished MB into
 // window 0, while no other MB writes the retained columns before this MB
@@ -264,7 +258,7 @@ __device__ __noinline__ void load_windows(int W, int H)
         else if (q.mode[k] == 2) shift[ns++] = k;
     }
     const int total = nf * PER;
-    constexpr int B = 8;
+    constexpr int B = 4;
     for (int base = 0; base < total; base += B * NT) {
         uint4 v[B];
 #pragma unroll
@@ -276,11 +270,11 @@ __device__ __noinline__ void load_windows(int W, int H)
                 const int16_t *Y = q.pl[k], *U = Y + (size_t)W * H, *V = U + (size_t)cw * ch;
                 if (c < NL) {
                     const int r = c / NLC, kk = c - r * NLC;
-                    v[i] = win_chunk(Y, W, H, w.oy + r, w.ox + 8 * kk, q.coherent[k]);
+                    v[i] = win_chunk(Y, W, H, w.oy + r, w.ox + 8 * kk);
                 } else {
                     const int cc = c - NL, pl = cc >= WC_ROWS * NCC, qq = cc - pl * WC_ROWS * NCC;
                     const int r = qq / NCC, kk = qq - r * NCC;
-                    v[i] = win_chunk(pl ? V : U, cw, ch, w.coy + r, w.cox + 8 * kk, q.coherent[k]);
+                    v[i] = win_chunk(pl ? V : U, cw, ch, w.coy + r, w.cox + 8 * kk);
                 }
             }
         }
@@ -307,11 +301,10 @@ __device__ __noinline__ void load_windows(int W, int H)
     for (int e = threadIdx.x; e < ns * RT; e += NT) {
         const int k = shift[e / RT], r = e % RT;
         Win &w = S.win[q.wi[k]];
-        const bool coh = q.coherent[k];
         if (r < WL_ROWS) {
             int16_t *row = w.y + r * WL;
-            const uint4 n0 = win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 16, coh);
-            const uint4 n1 = win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 8, coh);
+            const uint4 n0 = win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 16);
+            const uint4 n1 = win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 8);
             uint4 t[NLC - 2];
 #pragma unroll
             for (int j = 0; j < NLC - 2; j++) t[j] = *reinterpret_cast<const uint4 *>(row + 16 + 8 * j);
@@ -323,7 +316,7 @@ __device__ __noinline__ void load_windows(int W, int H)
             const int rr = r - WL_ROWS, pl = rr >= WC_ROWS, cr = rr - pl * WC_ROWS;
             const int16_t *U = q.pl[k] + (size_t)W * H, *V = U + (size_t)cw * ch;
             int16_t *row = (pl ? w.v : w.u) + cr * WC;
-            const uint4 n0 = win_chunk(pl ? V : U, cw, ch, w.coy + cr, w.cox + WC - 8, coh);
+            const uint4 n0 = win_chunk(pl ? V : U, cw, ch, w.coy + cr, w.cox + WC - 8);
             uint4 t[NCC - 1];
 #pragma unroll
             for (int j = 0; j < NCC - 1; j++) t[j] = *reinterpret_cast<const uint4 *>(row + 8 + 8 * j);
@@ -340,7 +333,7 @@ __device__ __noinline__ void load_windows(int W, int H)
 struct Metrics {
     int sad, mad, satd;
 };
-__device__ Metrics warp_metrics(const int16_t *src, const Win &w, int x, int y, int lane)
+__device__ __noinline__ Metrics warp_metrics(const int16_t *src, const Win &w, int x, int y, int lane)
 {
     int sad = 0, mad = 0, satd = 0;
     if (lane < 16) {
@@ -386,67 +379,6 @@ __device__ __forceinline__ float cand_cost(int satd, int x, int y, int px, int p
 {
     const int16_t mx = (int16_t)(x - px), my = (int16_t)(y - py);
     return rd_cost(satd, lambda, (unsigned)(iabs16(mx) + iabs16(my) + 1));
-}
-
-// One column of a 6-tap half-pel block (interp.cpp:52-164) plus its quarter-pel
-// average, accumulating SAD/MAD against the source column.
-template <int N>
-__device__ __forceinline__ void subpel_column(const int16_t *pl, int S, int bx, int by, int c, int dx, int dy,
-                                              const int16_t *scol, int ss, bool luma,
-                                              int &sad_h, int &mad_h, int &sad_q, int &mad_q,
-                                              int16_t *oh, int16_t *oq, int os)
-{
-    const int xo = dx > 0 ? 0 : -1, yo = dy > 0 ? 0 : -1;
-    int16_t hv[N + 5];
-    if (dx && dy) {
-#pragma unroll
-        for (int t = 0; t < N + 5; t++) {
-            const int16_t *rp = pl + (by + yo + t - 2) * S + bx + c + xo;
-            hv[t] = tap6(rp[-2], rp[-1], rp[0], rp[1], rp[2], rp[3]);
-        }
-    }
-#pragma unroll
-    for (int r = 0; r < N; r++) {
-        int16_t half;
-        if (dx && !dy) {
-            const int16_t *rp = pl + (by + r) * S + bx + c + xo;
-            half = tap6(rp[-2], rp[-1], rp[0], rp[1], rp[2], rp[3]);
-        } else if (!dx && dy) {
-            const int16_t *cp = pl + (by + r + yo) * S + bx + c;
-            half = tap6(cp[-2 * S], cp[-S], cp[0], cp[S], cp[2 * S], cp[3 * S]);
-        } else {
-            half = tap6(hv[r], hv[r + 1], hv[r + 2], hv[r + 3], hv[r + 4], hv[r + 5]);
-        }
-        const int full = pl[(by + r) * S + bx + c];
-        const int16_t q = (int16_t)((full + half + 1) >> 1);
-        const int s = scol[r * ss];
-        const int ah = iabs32(s - half), aq = iabs32(s - q);
-        if (luma) { sad_h += ah; sad_q += aq; }
-        mad_h = max(mad_h, ah);
-        mad_q = max(mad_q, aq);
-        if (oh) oh[r * os] = half;
-        if (oq) oq[r * os] = q;
-    }
-}
-
-// Half- and quarter-pel candidate in direction (dx, dy) around integer
-// position (x, y): metrics into out4 = {sad_h, mad_h, sad_q, mad_q}; optionally
-// stores the half (oh) or quarter (oq) block.  One warp, one column per lane.
-__device__ __noinline__ void warp_subpel(const int16_t *src, const Win &w, int x, int y, int dx, int dy, int lane,
-                            int *out4, int16_t *oh, int16_t *oq)
-{
-    int sh = 0, mh = 0, sq = 0, mq = 0;
-    if (lane < 16) {
-        subpel_column<16>(w.y, WL, x - w.ox, y - w.oy, lane, dx, dy, src + lane, 16, true, sh, mh, sq, mq,
-                          oh ? oh + lane : nullptr, oq ? oq + lane : nullptr, 16);
-    } else {
-        const int k = lane - 16, p = k >> 3, c = k & 7;
-        subpel_column<8>(p ? w.v : w.u, WC, (x >> 1) - w.cox, (y >> 1) - w.coy, c, dx, dy, src + 256 + p * 64 + c,
-                         8, false, sh, mh, sq, mq, oh ? oh + 256 + p * 64 + c : nullptr,
-                         oq ? oq + 256 + p * 64 + c : nullptr, 8);
-    }
-    sh = warp_sum(sh); mh = warp_max(mh); sq = warp_sum(sq); mq = warp_max(mq);
-    if (out4 && lane == 0) { out4[0] = sh; out4[1] = mh; out4[2] = sq; out4[3] = mq; }
 }
 
 // Integer candidate acceptance test (motion.cpp:148-177) against selection s.
@@ -590,12 +522,10 @@ __device__ __noinline__ void run_subpel(const Grp g, int si, int wi, bool intra,
     const int bx = sr.sel.bx, by = sr.sel.by;
     const int lx = bx - w.ox, ly = by - w.oy, cx = (bx >> 1) - w.cox, cy = (by >> 1) - w.coy;
     half_planes_a<16>(sr.hy, w.y, WL, lx, ly, gt, g.nt);
-    half_planes_a<8>(sr.hu, w.u, WC, cx, cy, gt, g.nt);
-    half_planes_a<8>(sr.hv, w.v, WC, cx, cy, gt, g.nt);
+    for (int p = 0; p < 2; p++) half_planes_a<8>(p ? sr.hv : sr.hu, p ? w.v : w.u, WC, cx, cy, gt, g.nt);
     gsync(g);
     half_planes_b<16>(sr.hy, gt, g.nt);
-    half_planes_b<8>(sr.hu, gt, g.nt);
-    half_planes_b<8>(sr.hv, gt, g.nt);
+    for (int p = 0; p < 2; p++) half_planes_b<8>(p ? sr.hv : sr.hu, gt, g.nt);
     gsync(g);
     for (int k = gw; k < 8; k += nw) {
         const int r = k < 4 ? k : k + 1, i = r % 3 - 1, j = r / 3 - 1;
@@ -605,6 +535,7 @@ __device__ __noinline__ void run_subpel(const Grp g, int si, int wi, bool intra,
         if (!ok) continue;
         int sh = 0, mh = 0, sq = 0, mq = 0;
         if (lane < 16) {   // luma column
+#pragma unroll 4
             for (int rr = 0; rr < 16; rr++) {
                 const int half = half_at<16>(sr.hy, i, j, rr, lane);
                 const int full = w.y[(ly + rr) * WL + lx + lane];
@@ -617,6 +548,7 @@ __device__ __noinline__ void run_subpel(const Grp g, int si, int wi, bool intra,
             const int kk = lane - 16, pl = kk >> 3, c = kk & 7;
             const HalfPlanes<8> &hp = pl ? sr.hv : sr.hu;
             const int16_t *fp = pl ? w.v : w.u;
+#pragma unroll 4
             for (int rr = 0; rr < 8; rr++) {
                 const int half = half_at<8>(hp, i, j, rr, c);
                 const int full = fp[(cy + rr) * WC + cx + c];
@@ -649,27 +581,31 @@ __device__ __noinline__ void run_subpel(const Grp g, int si, int wi, bool intra,
     gsync(g);
 }
 
-// Prediction block of a search result into out: integer block or half/quarter-pel.
-__device__ void materialize(const Grp g, int wi, int x, int y, int spp, int spa, int spi, int16_t *out)
+// Prediction block of search si's result into out: the integer block at (x, y)
+// of window wi, or its half / quarter-pel block in direction spi, read from
+// the half-pel planes run_subpel built around the same selection
+// (interp.cpp:52-164; quarter = (full + half + 1) >> 1).
+__device__ __noinline__ void materialize(const Grp g, int si, int wi, int x, int y, int spp, int spa, int spi, int16_t *out)
 {
     MbShared &S = SM();
     const Win &w = S.win[wi];
+    const Srch &sr = S.srch[si];
     const int gt = threadIdx.x - g.t0;
-    if (spp) {
-        if ((gt >> 5) == 0) {
-            int dx, dy;
-            dir_from_frac(spi, dx, dy);
-            warp_subpel(S.src, w, x, y, dx, dy, gt & 31, nullptr, spa ? nullptr : out, spa ? out : nullptr);
+    const int lx = x - w.ox, ly = y - w.oy, cx = (x >> 1) - w.cox, cy = (y >> 1) - w.coy;
+    int dx = 0, dy = 0;
+    if (spp) dir_from_frac(spi, dx, dy);
+    for (int e = gt; e < MB_N; e += g.nt) {
+        int full, half = 0;
+        if (e < 256) {
+            const int r = e >> 4, c = e & 15;
+            full = w.y[(ly + r) * WL + lx + c];
+            if (spp) half = half_at<16>(sr.hy, dx, dy, r, c);
+        } else {
+            const int p = (e - 256) >> 6, k = (e - 256) & 63, r = k >> 3, c = k & 7;
+            full = (p ? w.v : w.u)[(cy + r) * WC + cx + c];
+            if (spp) half = half_at<8>(p ? sr.hv : sr.hu, dx, dy, r, c);
         }
-    } else {
-        const int lx = x - w.ox, ly = y - w.oy, cx = (x >> 1) - w.cox, cy = (y >> 1) - w.coy;
-        for (int e = gt; e < MB_N; e += g.nt) {
-            if (e < 256) out[e] = w.y[(ly + (e >> 4)) * WL + lx + (e & 15)];
-            else {
-                const int p = (e - 256) >> 6, k = (e - 256) & 63;
-                out[e] = (p ? w.v : w.u)[(cy + (k >> 3)) * WC + cx + (k & 7)];
-            }
-        }
+        out[e] = !spp ? (int16_t)full : (spa ? (int16_t)((full + half + 1) >> 1) : (int16_t)half);
     }
 }
 
@@ -866,29 +802,30 @@ __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, 
     const int l4 = lane >> 2, i0 = (lane & 3) * 2;   // line and first of two outputs
     for (int j = gw; j < nc * 6; j += nw) {   // forward DCT and AQ partial sums
         const int k = k0 + j / 6, b = j % 6;
+        const int bb = blk_base(b), bs = blk_stride(b);
         if (S.cd[k].d.block_type & BT_COPY) continue;
         const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
         int in[8];
         int16_t out[2];
 #pragma unroll
         for (int c = 0; c < 8; c++) {
-            const int e = mb_index(b, l4, c);
+            const int e = (bb + (l4) * bs + (c));
             in[c] = (int16_t)(pr ? S.src[e] - pr[e] : S.src[e]);
         }
         fdct8_part<2>(in, i0, out);
-        S.tmp[k][mb_index(b, l4, i0)] = out[0];
-        S.tmp[k][mb_index(b, l4, i0 + 1)] = out[1];
+        S.tmp[k][(bb + (l4) * bs + (i0))] = out[0];
+        S.tmp[k][(bb + (l4) * bs + (i0 + 1))] = out[1];
         __syncwarp();
 #pragma unroll
-        for (int r = 0; r < 8; r++) in[r] = S.tmp[k][mb_index(b, r, l4)];
+        for (int r = 0; r < 8; r++) in[r] = S.tmp[k][(bb + (r) * bs + (l4))];
         fdct8_part<2>(in, i0, out);
-        S.coef[k][mb_index(b, i0, l4)] = out[0];
-        S.coef[k][mb_index(b, i0 + 1, l4)] = out[1];
+        S.coef[k][(bb + (i0) * bs + (l4))] = out[0];
+        S.coef[k][(bb + (i0 + 1) * bs + (l4))] = out[1];
         if (b < 4) {   // variance of the nonzero luma AC-and-DC coefficients but the MB's first (quantize.cpp:97-118, analysis.h:251-275)
             unsigned sum = 0, sq = 0, cnt = 0;
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                const int e = mb_index(b, i0 + h, l4);
+                const int e = (bb + (i0 + h) * bs + (l4));
                 const int t = out[h];
                 if (e != 0 && t) { sum += (unsigned)t; sq += (unsigned)wmul(t, t); cnt++; }
             }
@@ -904,12 +841,13 @@ __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, 
     gsync(g);
     for (int j = gw; j < nc * 6; j += nw) {   // quantise, trellis, reconstruct
         const int k = k0 + j / 6, b = j % 6;
+        const int bb = blk_base(b), bs = blk_stride(b);
         const int bt = S.cd[k].d.block_type;
         const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
         if (bt & BT_COPY) {
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                const int e = mb_index(b, l4, i0 + h);
+                const int e = (bb + (l4) * bs + (i0 + h));
                 S.rec[k][e] = pr ? pr[e] : (int16_t)0;
             }
             continue;
@@ -926,7 +864,7 @@ __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, 
         const int qp = chroma ? min(q_index + 2, MAXQ) : q_index;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            const int o = lane + 32 * h, e = mb_index(b, o >> 3, o & 7);
+            const int o = lane + 32 * h, e = (bb + (o >> 3) * bs + (o & 7));
             S.lev[k][e] = quant_coeff(S.coef[k][e], qp, o, iq, chroma);
         }
         __syncwarp();
@@ -934,17 +872,17 @@ __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, 
         __syncwarp();
         int in[8], out[2];
 #pragma unroll
-        for (int r = 0; r < 8; r++) in[r] = dequant_coeff(S.lev[k][mb_index(b, r, l4)], qp, r * 8 + l4, iq, chroma);
+        for (int r = 0; r < 8; r++) in[r] = dequant_coeff(S.lev[k][(bb + (r) * bs + (l4))], qp, r * 8 + l4, iq, chroma);
         idct8_part<2>(in, i0, out);
-        S.tmp[k][mb_index(b, i0, l4)] = (int16_t)out[0];
-        S.tmp[k][mb_index(b, i0 + 1, l4)] = (int16_t)out[1];
+        S.tmp[k][(bb + (i0) * bs + (l4))] = (int16_t)out[0];
+        S.tmp[k][(bb + (i0 + 1) * bs + (l4))] = (int16_t)out[1];
         __syncwarp();
 #pragma unroll
-        for (int c = 0; c < 8; c++) in[c] = S.tmp[k][mb_index(b, l4, c)];
+        for (int c = 0; c < 8; c++) in[c] = S.tmp[k][(bb + (l4) * bs + (c))];
         idct8_part<2>(in, i0, out);
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            const int e = mb_index(b, l4, i0 + h);
+            const int e = (bb + (l4) * bs + (i0 + h));
             S.rec[k][e] = (int16_t)(pr ? out[h] + pr[e] : out[h]);
         }
     }
@@ -1036,7 +974,7 @@ __device__ __noinline__ void intra_bc_search(const Grp g, const FrameArgs &a, in
     }
     gsync(g);
     if (sr.out.d.block_type & BT_MOTION)
-        materialize(g, 0, sr.sel.bx, sr.sel.by, sr.sel.sp_enabled, sr.sel.sp_amount, sr.sel.sp_index, S.pred[0]);
+        materialize(g, 0, 0, sr.sel.bx, sr.sel.by, sr.sel.sp_enabled, sr.sel.sp_amount, sr.sel.sp_index, S.pred[0]);
     gsync(g);
 }
 
@@ -1115,7 +1053,7 @@ __device__ __noinline__ void inter_search(const Grp g, const FrameArgs &a, int s
         }
         run_subpel(g, si, wi, false, px, py, a.W, a.H);
     }
-    materialize(g, wi, sr.sel.bx, sr.sel.by, sr.sel.sp_enabled, sr.sel.sp_amount, sr.sel.sp_index, pred_out);
+    materialize(g, si, wi, sr.sel.bx, sr.sel.by, sr.sel.sp_enabled, sr.sel.sp_amount, sr.sel.sp_index, pred_out);
     if (gt == 0) {
         fill_desc(sr.sel, px, py, false, S.thr, sr.out.d);
         sr.out_sad = sr.sel.sad;
@@ -1169,7 +1107,7 @@ __device__ void load_src(const FrameArgs &a, int px, int py)   // whole CTA
 // One thread: copy threshold (motion.cpp:501), RDO flag and, when searches
 // follow, the MV predictor, which serves every search of the MB.  Clears the
 // window request list.
-__device__ void setup_mb(const FrameArgs &a, int idx, int px, int py, bool need_pred, const evxg_block_desc *left)
+__device__ __noinline__ void setup_mb(const FrameArgs &a, int idx, int px, int py, bool need_pred, const evxg_block_desc *left)
 {
     MbShared &S = SM();
     S.thr = (a.quality >> 2) + 1;
@@ -1185,10 +1123,10 @@ __device__ void setup_mb(const FrameArgs &a, int idx, int px, int py, bool need_
     }
     S.req.n = 0;
 }
-__device__ void req_window(int wi, const int16_t *pl, int bx, int by, int coh)   // one thread
+__device__ void req_window(int wi, const int16_t *pl, int bx, int by)   // one thread
 {
     WinReq &q = SM().req;
-    q.wi[q.n] = wi; q.pl[q.n] = pl; q.bx[q.n] = bx; q.by[q.n] = by; q.coherent[q.n] = coh; q.n++;
+    q.wi[q.n] = wi; q.pl[q.n] = pl; q.bx[q.n] = bx; q.by[q.n] = by; q.n++;
 }
 
 // Neighbours for directional intra (intra_pred.cpp:13-54); sample(p, y, x)
@@ -1277,7 +1215,7 @@ __device__ void bi_prediction()
 // Candidate decision by SAD (encode.cpp:168-277, :374-470); one thread.
 // Sets cd[4]/cpred[4] to the winner and need_encode, or (P frames whose winner
 // is an intra candidate, already encoded) points win_k at that candidate.
-__device__ void decide(const FrameArgs &a)
+__device__ __noinline__ void decide(const FrameArgs &a)
 {
     MbShared &S = SM();
     evxg_block_desc best = S.srch[0].out.d;
@@ -1416,14 +1354,14 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
     load_src(a, px, py);
     if (tid == 0) {
         setup_mb(a, idx, px, py, a.type != EVXG_FRAME_INTRA, nullptr);
-        req_window(0, dst, px, py - 16, 1);   // intra window: the slot being reconstructed
+        req_window(0, dst, px, py - 16);   // intra window: the slot being reconstructed
         if (a.type != EVXG_FRAME_INTRA) {
-            req_window(1, a.planes[a.ref_fwd], px, py, 0);
-            if (S.sep) req_window(2, a.planes[a.ref_fwd], S.qx, S.qy, 0);
+            req_window(1, a.planes[a.ref_fwd], px, py);
+            if (S.sep) req_window(2, a.planes[a.ref_fwd], S.qx, S.qy);
         }
         if (a.type == EVXG_FRAME_BIDIR) {
-            req_window(3, a.planes[a.ref_bwd], px, py, 0);
-            if (S.sep) req_window(4, a.planes[a.ref_bwd], S.qx, S.qy, 0);
+            req_window(3, a.planes[a.ref_bwd], px, py);
+            if (S.sep) req_window(4, a.planes[a.ref_bwd], S.qx, S.qy);
         }
     }
     __syncthreads();
@@ -1595,7 +1533,7 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
     load_src(a, px, py);
     if (tid == 0) {
         setup_mb(a, idx, px, py, false, nullptr);
-        req_window(0, a.planes[a.dpb], px, py - 16, 1);
+        req_window(0, a.planes[a.dpb], px, py - 16);
     }
     __syncthreads();
     load_windows(a.W, a.H);
@@ -1657,8 +1595,8 @@ __device__ bool search_mb(const FrameArgs &a, int row, int col, int n, bool bwd)
     if (tid == 0) {
         setup_mb(a, idx, px, py, true, col > 0 ? &S.mail.left.d : nullptr);
         const int16_t *ref = a.planes[bwd ? a.ref_bwd : a.ref_fwd];
-        req_window(wa, ref, px, py, 0);
-        if (S.sep) req_window(wa + 1, ref, S.qx, S.qy, 0);
+        req_window(wa, ref, px, py);
+        if (S.sep) req_window(wa + 1, ref, S.qx, S.qy);
     }
     __syncthreads();
     load_windows(a.W, a.H);
