@@ -800,32 +800,39 @@ __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, 
     MbShared &S = SM();
     const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31, nw = g.nt >> 5;
     const int l4 = lane >> 2, i0 = (lane & 3) * 2;   // line and first of two outputs
+    // The chain runs once per MB and block, so its code is kept compact (one
+    // loop body per transform direction): the kernel's instruction footprint,
+    // not its arithmetic, bounds these phases.
     for (int j = gw; j < nc * 6; j += nw) {   // forward DCT and AQ partial sums
         const int k = k0 + j / 6, b = j % 6;
         const int bb = blk_base(b), bs = blk_stride(b);
         if (S.cd[k].d.block_type & BT_COPY) continue;
         const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
-        int in[8];
-        int16_t out[2];
-#pragma unroll
-        for (int c = 0; c < 8; c++) {
-            const int e = (bb + (l4) * bs + (c));
-            in[c] = (int16_t)(pr ? S.src[e] - pr[e] : S.src[e]);
+#pragma unroll 1
+        for (int h = 0; h < 2; h++) {   // residual (int16) into coef
+            const int e = bb + l4 * bs + i0 + h;
+            S.coef[k][e] = (int16_t)(pr ? S.src[e] - pr[e] : S.src[e]);
         }
-        fdct8_part<2>(in, i0, out);
-        S.tmp[k][(bb + (l4) * bs + (i0))] = out[0];
-        S.tmp[k][(bb + (l4) * bs + (i0 + 1))] = out[1];
         __syncwarp();
+        int16_t out[2];
+#pragma unroll 1
+        for (int pass = 0; pass < 2; pass++) {   // rows: coef -> tmp, then columns: tmp -> coef
+            const int rs = pass ? 1 : bs, cs = pass ? bs : 1;
+            const int16_t *X = pass ? S.tmp[k] : S.coef[k];
+            int16_t *Y = pass ? S.coef[k] : S.tmp[k];
+            int in[8];
 #pragma unroll
-        for (int r = 0; r < 8; r++) in[r] = S.tmp[k][(bb + (r) * bs + (l4))];
-        fdct8_part<2>(in, i0, out);
-        S.coef[k][(bb + (i0) * bs + (l4))] = out[0];
-        S.coef[k][(bb + (i0 + 1) * bs + (l4))] = out[1];
-        if (b < 4) {   // variance of the nonzero luma AC-and-DC coefficients but the MB's first (quantize.cpp:97-118, analysis.h:251-275)
+            for (int t = 0; t < 8; t++) in[t] = X[bb + l4 * rs + t * cs];
+            fdct8_part<2>(in, i0, out);
+            Y[bb + l4 * rs + i0 * cs] = out[0];
+            Y[bb + l4 * rs + (i0 + 1) * cs] = out[1];
+            __syncwarp();
+        }
+        if (b < 4) {   // variance of the nonzero luma coefficients except the MB's first (quantize.cpp:97-118, analysis.h:251-275)
             unsigned sum = 0, sq = 0, cnt = 0;
-#pragma unroll
+#pragma unroll 1
             for (int h = 0; h < 2; h++) {
-                const int e = (bb + (i0 + h) * bs + (l4));
+                const int e = bb + (i0 + h) * bs + l4;
                 const int t = out[h];
                 if (e != 0 && t) { sum += (unsigned)t; sq += (unsigned)wmul(t, t); cnt++; }
             }
@@ -845,9 +852,9 @@ __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, 
         const int bt = S.cd[k].d.block_type;
         const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
         if (bt & BT_COPY) {
-#pragma unroll
+#pragma unroll 1
             for (int h = 0; h < 2; h++) {
-                const int e = (bb + (l4) * bs + (i0 + h));
+                const int e = bb + l4 * bs + i0 + h;
                 S.rec[k][e] = pr ? pr[e] : (int16_t)0;
             }
             continue;
@@ -862,28 +869,36 @@ __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, 
         if (b == 0 && lane == 0) { S.cd[k].d.q_index = (uint8_t)q_index; S.cd[k].d.variance = (int16_t)var; }
         const bool chroma = b >= 4, iq = intra_quant(bt);
         const int qp = chroma ? min(q_index + 2, MAXQ) : q_index;
-#pragma unroll
+#pragma unroll 1
         for (int h = 0; h < 2; h++) {
-            const int o = lane + 32 * h, e = (bb + (o >> 3) * bs + (o & 7));
+            const int o = lane + 32 * h, e = bb + (o >> 3) * bs + (o & 7);
             S.lev[k][e] = quant_coeff(S.coef[k][e], qp, o, iq, chroma);
         }
         __syncwarp();
         trellis_warp(S.lev[k], S.coef[k], b, qp, iq, S.cd[k].d.intra_mode, a.lambda, lane);
         __syncwarp();
-        int in[8], out[2];
-#pragma unroll
-        for (int r = 0; r < 8; r++) in[r] = dequant_coeff(S.lev[k][(bb + (r) * bs + (l4))], qp, r * 8 + l4, iq, chroma);
-        idct8_part<2>(in, i0, out);
-        S.tmp[k][(bb + (i0) * bs + (l4))] = (int16_t)out[0];
-        S.tmp[k][(bb + (i0 + 1) * bs + (l4))] = (int16_t)out[1];
+#pragma unroll 1
+        for (int h = 0; h < 2; h++) {   // dequantised levels into coef (the trellis no longer needs it)
+            const int o = lane + 32 * h, e = bb + (o >> 3) * bs + (o & 7);
+            S.coef[k][e] = dequant_coeff(S.lev[k][e], qp, o, iq, chroma);
+        }
         __syncwarp();
+#pragma unroll 1
+        for (int pass = 0; pass < 2; pass++) {   // columns: coef -> tmp, then rows + prediction: tmp -> rec
+            const int rs = pass ? bs : 1, cs = pass ? 1 : bs;
+            const int16_t *X = pass ? S.tmp[k] : S.coef[k];
+            int16_t *Y = pass ? S.rec[k] : S.tmp[k];
+            const int16_t *P = pass ? pr : nullptr;
+            int in[8], out2[2];
 #pragma unroll
-        for (int c = 0; c < 8; c++) in[c] = S.tmp[k][(bb + (l4) * bs + (c))];
-        idct8_part<2>(in, i0, out);
+            for (int t = 0; t < 8; t++) in[t] = X[bb + l4 * rs + t * cs];
+            idct8_part<2>(in, i0, out2);
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int e = (bb + (l4) * bs + (i0 + h));
-            S.rec[k][e] = (int16_t)(pr ? out[h] + pr[e] : out[h]);
+            for (int h = 0; h < 2; h++) {
+                const int e = bb + l4 * rs + (i0 + h) * cs;
+                Y[e] = (int16_t)(P ? out2[h] + P[e] : out2[h]);
+            }
+            __syncwarp();
         }
     }
     gsync(g);
