@@ -44,6 +44,9 @@ EXPORTS = [
     "evxg_encoder_clear", "evxg_encoder_insert_intra", "evxg_encoder_set_quality",
     "evxg_encoder_encode", "evxg_encoder_flush", "evxg_encoder_stream", "evxg_mb_pass_noalloc",
     "evxg_stream_set_mb_form", "evxg_stream_mb_form",
+    "evxg_batch_create", "evxg_batch_destroy", "evxg_batch_input", "evxg_batch_encode", "evxg_batch_wait",
+    "evxg_batch_output", "evxg_batch_launch_count", "evxg_batch_set_shape", "evxg_batch_get_shape",
+    "evxg_batch_autotune",
 ]
 MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
 
@@ -85,6 +88,18 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_mb_pass_noalloc.argtypes = [u32, u32, C.c_char_p, vp, C.POINTER(vp), vp, vp, vp, vp]
     L.evxg_stream_set_mb_form.argtypes = [vp, i32]
     L.evxg_stream_mb_form.argtypes = [vp]
+    L.evxg_batch_create.argtypes = [C.POINTER(vp), u32, C.POINTER(vp)]
+    L.evxg_batch_destroy.argtypes = [vp]
+    L.evxg_batch_input.argtypes = [vp, u32, u32]
+    L.evxg_batch_input.restype = C.POINTER(C.c_uint8)
+    L.evxg_batch_encode.argtypes = [vp, C.c_char_p, u32, vp]
+    L.evxg_batch_wait.argtypes = [vp, u32]
+    L.evxg_batch_output.argtypes = [vp, u32, u32] + [C.POINTER(vp)] * 4
+    L.evxg_batch_launch_count.argtypes = [vp]
+    L.evxg_batch_launch_count.restype = u32
+    L.evxg_batch_set_shape.argtypes = [vp, i32, i32, i32]
+    L.evxg_batch_get_shape.argtypes = [vp] + [C.POINTER(i32)] * 3
+    L.evxg_batch_autotune.argtypes = [vp, vp, C.POINTER(C.c_float)]
     return L
 
 
@@ -194,6 +209,75 @@ class Stream:
     @mb_form.setter
     def mb_form(self, form: int):
         _check(lib().evxg_stream_set_mb_form(self.h, int(form)))
+
+
+NO_FRAME = struct.pack("<iIHIBBBB", -1, 0, 0, 0, 0, 0, 0, 0)   # a stream without a frame in a batch tick
+
+
+class Batch:
+    """Batched ticks over several streams (evxg_batch_*): one launch per stage
+    for all streams, the tick replayed as a CUDA graph, two buffer parities.
+
+    Per tick: write frames into input(i, p), encode(frames18, p), wait(p),
+    read output(i, p).  frames18[i] is None for a stream without a frame."""
+
+    def __init__(self, streams):
+        self.streams = list(streams)
+        arr = (C.c_void_p * len(self.streams))(*[s.h.value for s in self.streams])
+        h = C.c_void_p()
+        _check(lib().evxg_batch_create(arr, len(self.streams), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().evxg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def input(self, i: int, parity: int) -> np.ndarray:
+        """Pinned (height, width, 3) uint8 buffer of stream i's next frame of this parity."""
+        s = self.streams[i]
+        p = lib().evxg_batch_input(self.h, i, parity)
+        return np.ctypeslib.as_array(p, shape=(s.height, s.width, 3))
+
+    def encode(self, frames18, parity: int, cuda_stream=None):
+        buf = b"".join(NO_FRAME if f is None else f for f in frames18)
+        _check(lib().evxg_batch_encode(self.h, buf, parity, _ptr(cuda_stream)))
+
+    def wait(self, parity: int):
+        _check(lib().evxg_batch_wait(self.h, parity))
+
+    def output(self, i: int, parity: int) -> dict:
+        """Copies of stream i's tables from the last tick of this parity (as Stream.fetch_tables)."""
+        s = self.streams[i]
+        ptrs = [C.c_void_p() for _ in range(4)]
+        _check(lib().evxg_batch_output(self.h, i, parity, *[C.byref(x) for x in ptrs]))
+        def arr(p, n, dt):
+            return np.ctypeslib.as_array(C.cast(p, C.POINTER(dt)), shape=(n,)).copy()
+        return dict(blocks=arr(ptrs[0], s.nblk * 28, C.c_uint8), prev_blocks=arr(ptrs[1], s.nblk * 28, C.c_uint8),
+                    sao=arr(ptrs[2], s.nblk * 16, C.c_uint8), levels=arr(ptrs[3], s.plane_elems, C.c_int16))
+
+    def launch_count(self) -> int:
+        return lib().evxg_batch_launch_count(self.h)
+
+    @property
+    def shape(self):
+        v = [C.c_int() for _ in range(3)]
+        _check(lib().evxg_batch_get_shape(self.h, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)   # (form, grid, policy)
+
+    def set_shape(self, form: int, grid: int, policy: int):
+        _check(lib().evxg_batch_set_shape(self.h, form, grid, policy))
+
+    def autotune(self, cuda_stream=None) -> float:
+        ms = C.c_float()
+        _check(lib().evxg_batch_autotune(self.h, _ptr(cuda_stream), C.byref(ms)))
+        return ms.value
 
 
 class Encoder:

@@ -10,66 +10,24 @@
 #include <string>
 #include <vector>
 
-#include "evxg.h"
-#include "evxg_device.cuh"
-
-namespace evxg {
-__global__ void k_convert(FrameArgs a);
-__global__ void k_mb_wavefront(FrameArgs a);
-__global__ void k_mb_cluster(FrameArgs a);
-__global__ void k_deblock(FrameArgs a);
-__global__ void k_sao_rdo(FrameArgs a);
-__global__ void k_sao_merge(FrameArgs a);
-__global__ void k_sao_fix(FrameArgs a, int pass);
-__global__ void k_sao_restore(FrameArgs a, int last_pass);
-__global__ void k_sao_apply(FrameArgs a, int last_pass);
-size_t mb_shared_bytes();
-int mb_threads();
-}  // namespace evxg
+#include "evxg_internal.cuh"
 
 using namespace evxg;
 
 static thread_local std::string g_last_error;
-// Fixed-point passes of the SAO application (evxg_filters.cu); the chains they
-// resolve are a few pixels long, the last pass only confirms.
-static const int kSaoPasses = 8;
 
-static int fail(int code, const char *what)
+namespace evxg {
+int fail(int code, const char *what)
 {
     g_last_error = what;
     return code;
 }
-static int cuda_fail(cudaError_t e, const char *where)
+int cuda_fail(cudaError_t e, const char *where)
 {
     g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
     return e == cudaErrorMemoryAllocation ? EVXG_ERROR_OUTOFMEMORY : EVXG_ERROR_EXECUTION_FAILURE;
 }
-#define CK(call)                                              \
-    do {                                                      \
-        cudaError_t e_ = (call);                              \
-        if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
-    } while (0)
-
-struct evxg_stream {
-    uint32_t vw, vh, W, H, mbw, mbh;
-    size_t plane_elems;                 // elements of one plane set
-    int16_t *src, *lev, *dpb[4];
-    evxg_block_desc *bt, *prev, *prev_ser;
-    evxg_sao_info *sao;
-    float *sao_cost;
-    int16_t *sao_orig;                  // pristine copy for the SAO fixed-point passes
-    int *sao_flags;
-    unsigned long long *sao_mail;       // SAO merge hand-over words, epoch-tagged
-    int epoch;
-    uint8_t *rgb;
-    int *sync;                          // 3*mbh progress words, 4 counters, 1 error word
-    int mb_grid, num_sms;
-    int mb_form, mb_clusters;          // macroblock pass shape; clusters launched in the cluster form
-    uint32_t launches;
-    long long timeout_ns;
-    bool profile;
-    cudaEvent_t ev[7];
-};
+}  // namespace evxg
 
 extern "C" {
 
@@ -103,36 +61,10 @@ int evxg_stream_create(uint32_t width, uint32_t height, evxg_stream **out)
     if (e == cudaSuccess) e = cudaMalloc(&s->sao_orig, pb);
     if (e == cudaSuccess) e = cudaMalloc(&s->sao_flags, kSaoPasses * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&s->sao_mail, nblk * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemset(s->sao_mail, 0, nblk * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&s->rgb, (size_t)width * height * 3);
     if (e == cudaSuccess) e = cudaMalloc(&s->sync, (3 * s->mbh + 5) * sizeof(int));
-    // The reference zero-fills every image and table at allocation (image.cpp:89,
-    // common.cpp:167-187); stale-pixel reads of never-written DPB slots see zeros.
-    if (e == cudaSuccess) e = cudaMemset(s->src, 0, pb);
-    if (e == cudaSuccess) e = cudaMemset(s->lev, 0, pb);
-    for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaMemset(s->dpb[i], 0, pb);
-    if (e == cudaSuccess) e = cudaMemset(s->bt, 0, nblk * sizeof(evxg_block_desc));
-    if (e == cudaSuccess) e = cudaMemset(s->prev, 0, nblk * sizeof(evxg_block_desc));
-    if (e == cudaSuccess) e = cudaMemset(s->prev_ser, 0, nblk * sizeof(evxg_block_desc));
-    if (e == cudaSuccess) e = cudaMemset(s->sao, 0, nblk * sizeof(evxg_sao_info));
-    if (e == cudaSuccess) e = cudaMemset(s->sync, 0, (3 * s->mbh + 5) * sizeof(int));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_mb_wavefront, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mb_shared_bytes());
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_mb_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mb_shared_bytes());
-    int max_clusters = 0;
-    if (e == cudaSuccess) {
-        cudaLaunchConfig_t cfg = {};
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = 3; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-        cfg.gridDim = dim3(3); cfg.blockDim = dim3(mb_threads()); cfg.dynamicSmemBytes = mb_shared_bytes();
-        cfg.attrs = at; cfg.numAttrs = 1;
-        if (cudaOccupancyMaxActiveClusters(&max_clusters, (void *)k_mb_cluster, &cfg) != cudaSuccess) {
-            cudaGetLastError();   // the cluster form is optional: fall back to one CTA per row
-            max_clusters = 0;
-        }
-    }
+    if (e == cudaSuccess && reset_stream(s, nullptr)) e = cudaErrorUnknown;
+    const int max_clusters = e == cudaSuccess ? max_active_clusters() : 0;
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         int rc = cuda_fail(e, "evxg_stream_create");
@@ -189,26 +121,77 @@ int evxg_stream_set_mb_form(evxg_stream *s, int form)
 
 int evxg_stream_mb_form(const evxg_stream *s) { return s ? s->mb_form : -EVXG_ERROR_INVALIDARG; }
 
-int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, const evxg_frame *f, void *cuda_stream)
+}  // extern "C"
+
+// The reference zero-fills every image and table at allocation (image.cpp:89,
+// common.cpp:167-187); stale-pixel reads of never-written DPB slots see zeros.
+int evxg::reset_stream(evxg_stream *s, cudaStream_t st)
 {
-    if (!s || !rgb || !f) return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: null argument");
-    if (f->type < EVXG_FRAME_INTRA || f->type > EVXG_FRAME_BIDIR)
-        return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: bad frame type");
-    if (f->dpb_slot > 3 || f->ref_slot_fwd > 3 || f->ref_slot_bwd > 3)
-        return fail(EVXG_ERROR_INVALID_INDEX, "evxg_encode_frame: DPB slot out of range");
-    if (f->quality < 1 || f->quality > 63)
-        return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: quality (QP) must be 1..63");
-    if (f->type != EVXG_FRAME_INTRA && f->ref_slot_fwd == f->dpb_slot)
-        return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: forward reference equals the destination slot");
-    if (f->type == EVXG_FRAME_BIDIR && f->ref_slot_bwd == f->dpb_slot)
-        return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: backward reference equals the destination slot");
-    cudaStream_t st = (cudaStream_t)cuda_stream;
-    const uint8_t *drgb = rgb;
-    if (!rgb_on_device) {
-        CK(cudaMemcpyAsync(s->rgb, rgb, (size_t)s->vw * s->vh * 3, cudaMemcpyHostToDevice, st));
-        drgb = s->rgb;
+    const size_t pb = s->plane_elems * sizeof(int16_t), nblk = (size_t)s->mbw * s->mbh;
+    CK(cudaMemsetAsync(s->src, 0, pb, st));
+    CK(cudaMemsetAsync(s->lev, 0, pb, st));
+    for (int i = 0; i < 4; i++) CK(cudaMemsetAsync(s->dpb[i], 0, pb, st));
+    CK(cudaMemsetAsync(s->bt, 0, nblk * sizeof(evxg_block_desc), st));
+    CK(cudaMemsetAsync(s->prev, 0, nblk * sizeof(evxg_block_desc), st));
+    CK(cudaMemsetAsync(s->prev_ser, 0, nblk * sizeof(evxg_block_desc), st));
+    CK(cudaMemsetAsync(s->sao, 0, nblk * sizeof(evxg_sao_info), st));
+    CK(cudaMemsetAsync(s->sao_mail, 0, nblk * sizeof(unsigned long long), st));
+    CK(cudaMemsetAsync(s->sync, 0, (3 * s->mbh + 5) * sizeof(int), st));
+    s->epoch = 0;
+    return EVXG_SUCCESS;
+}
+
+// Shared-memory limits of the macroblock kernels (once per process and device)
+// and the number of three-CTA clusters the device co-schedules; 0 when the
+// cluster form cannot run.
+int evxg::max_active_clusters()
+{
+    static int cached[64];
+    static bool done[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    if (done[dev]) return cached[dev];
+    const int smem = (int)mb_shared_bytes();
+    cudaFuncSetAttribute(k_mb_wavefront, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_mb_wavefront_b, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int n = 0;
+    if (cudaFuncSetAttribute(k_mb_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
+        cudaFuncSetAttribute(k_mb_cluster_b, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 3; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(3); cfg.blockDim = dim3(mb_threads()); cfg.dynamicSmemBytes = mb_shared_bytes();
+        cfg.attrs = at; cfg.numAttrs = 1;
+        if (cudaOccupancyMaxActiveClusters(&n, (void *)k_mb_cluster, &cfg) != cudaSuccess) n = 0;
     }
-    FrameArgs a{};
+    cudaGetLastError();   // the cluster form is optional: fall back to one CTA per row
+    cached[dev] = n; done[dev] = true;
+    return n;
+}
+
+// Frame descriptor checks shared by the single and the batched path.
+int evxg::check_frame(const evxg_frame *f, const char *who)
+{
+    static thread_local char msg[160];
+    auto bad = [&](int code, const char *what) {
+        snprintf(msg, sizeof msg, "%s: %s", who, what);
+        return fail(code, msg);
+    };
+    if (f->type < EVXG_FRAME_INTRA || f->type > EVXG_FRAME_BIDIR) return bad(EVXG_ERROR_INVALIDARG, "bad frame type");
+    if (f->dpb_slot > 3 || f->ref_slot_fwd > 3 || f->ref_slot_bwd > 3)
+        return bad(EVXG_ERROR_INVALID_INDEX, "DPB slot out of range");
+    if (f->quality < 1 || f->quality > 63) return bad(EVXG_ERROR_INVALIDARG, "quality (QP) must be 1..63");
+    if (f->type != EVXG_FRAME_INTRA && f->ref_slot_fwd == f->dpb_slot)
+        return bad(EVXG_ERROR_INVALIDARG, "forward reference equals the destination slot");
+    if (f->type == EVXG_FRAME_BIDIR && f->ref_slot_bwd == f->dpb_slot)
+        return bad(EVXG_ERROR_INVALIDARG, "backward reference equals the destination slot");
+    return EVXG_SUCCESS;
+}
+
+void evxg::fill_args(evxg_stream *s, const evxg_frame *f, const uint8_t *drgb, FrameArgs &a)
+{
+    a = FrameArgs{};
     a.W = (int)s->W; a.H = (int)s->H; a.mbw = (int)s->mbw; a.mbh = (int)s->mbh;
     a.vis_w = (int)s->vw; a.vis_h = (int)s->vh;
     a.type = f->type; a.quality = f->quality; a.dpb = f->dpb_slot;
@@ -223,6 +206,25 @@ int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, con
     a.epoch = s->epoch;
     a.progress = s->sync; a.counters = s->sync + 3 * s->mbh; a.error = s->sync + 3 * s->mbh + 4;
     a.timeout_ns = s->timeout_ns;
+    a.active = 1;
+    a.prev_tab = s->prev; a.prev_ser = s->prev_ser; a.plane_elems = s->plane_elems;
+}
+
+extern "C" {
+
+int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, const evxg_frame *f, void *cuda_stream)
+{
+    if (!s || !rgb || !f) return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: null argument");
+    int rc = check_frame(f, "evxg_encode_frame");
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    const uint8_t *drgb = rgb;
+    if (!rgb_on_device) {
+        CK(cudaMemcpyAsync(s->rgb, rgb, (size_t)s->vw * s->vh * 3, cudaMemcpyHostToDevice, st));
+        drgb = s->rgb;
+    }
+    FrameArgs a;
+    fill_args(s, f, drgb, a);
     const size_t nblk = (size_t)s->mbw * s->mbh;
     // the serializer of this frame reads the previous table before this frame's update
     CK(cudaMemcpyAsync(s->prev_ser, s->prev, nblk * sizeof(evxg_block_desc), cudaMemcpyDeviceToDevice, st));

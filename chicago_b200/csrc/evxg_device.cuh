@@ -119,6 +119,21 @@ struct FrameArgs {
     int *counters;               // [0] next MB row, [1] next SAO merge row, [2] next SAO apply row
     int *error;                  // device error word (0 = ok)
     long long timeout_ns;        // bound on every spin-wait
+    int active;                  // batched launches: 0 = this stream has no frame in the tick
+    // batched bookkeeping (the single path does these with copies and memsets)
+    evxg_block_desc *prev_tab;   // temporal predictor table (the frame's update target)
+    evxg_block_desc *prev_ser;   // snapshot of it for the serializer
+    size_t plane_elems;          // samples in one plane set
 };
+
+// Batched launches: blockIdx.z selects the stream; its parameters are copied
+// into shared memory once per block.  Returns null for a stream without a
+// frame in this tick (the whole block then returns).
+__device__ __forceinline__ const FrameArgs *batch_args(const FrameArgs *args, FrameArgs &sa)
+{
+    if (threadIdx.x == 0 && threadIdx.y == 0) sa = args[blockIdx.z];
+    __syncthreads();
+    return sa.active ? &sa : nullptr;
+}
 
 }  // namespace evxg

@@ -11,7 +11,7 @@ namespace evxg {
 // ------------------------------------------------------------ conversion
 // One thread per 2x2 pixel quad of the visible (cropped) frame; padding rows
 // and columns of the aligned source stay at their zero initialisation.
-__global__ void k_convert(FrameArgs a)
+__device__ __forceinline__ void convert_body(const FrameArgs &a)
 {
     const int cw = min(a.vis_w, a.W), ch = min(a.vis_h, a.H);
     const int qx = blockIdx.x * blockDim.x + threadIdx.x, qy = blockIdx.y;
@@ -31,6 +31,12 @@ __global__ void k_convert(FrameArgs a)
         }
     U[(size_t)qy * (a.W / 2) + qx] = (int16_t)((u + 2) >> 2);
     V[(size_t)qy * (a.W / 2) + qx] = (int16_t)((v + 2) >> 2);
+}
+__global__ void k_convert(FrameArgs a) { convert_body(a); }
+__global__ void k_convert_b(const FrameArgs *args)
+{
+    __shared__ FrameArgs sa;
+    if (const FrameArgs *a = batch_args(args, sa)) convert_body(*a);
 }
 
 // ------------------------------------------------------------ deblocking
@@ -95,7 +101,7 @@ __device__ __forceinline__ void filter_line(int16_t *e, int step, int qe, int st
 // edge (x, j) only reads columns written by horizontal edges (x-8, j) and
 // (x, j), so running all horizontal edges of the band and then all vertical
 // edges gives the same samples; bands stay in order.
-__global__ void __launch_bounds__(1024) k_deblock(FrameArgs a)
+__device__ __forceinline__ void deblock_body(const FrameArgs &a)
 {
     const int pl = blockIdx.x;
     const bool luma = pl == 0;
@@ -123,6 +129,12 @@ __global__ void __launch_bounds__(1024) k_deblock(FrameArgs a)
         }
         __syncthreads();
     }
+}
+__global__ void __launch_bounds__(1024) k_deblock(FrameArgs a) { deblock_body(a); }
+__global__ void __launch_bounds__(1024) k_deblock_b(const FrameArgs *args)
+{
+    __shared__ FrameArgs sa;
+    if (const FrameArgs *a = batch_args(args, sa)) deblock_body(*a);
 }
 
 // ------------------------------------------------------------------ SAO
@@ -252,7 +264,7 @@ __device__ void sao_rdo_block(const int16_t *s, const int16_t *r, int w, int h, 
 
 // One thread per MB: own luma and chroma (U plane) parameters and the cost of
 // keeping them, the starting point of the merge decision (sao.cpp:414-557).
-__global__ void k_sao_rdo(FrameArgs a)
+__device__ __forceinline__ void sao_rdo_body(const FrameArgs &a)
 {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= a.mbw * a.mbh) return;
@@ -269,6 +281,12 @@ __global__ void k_sao_rdo(FrameArgs a)
                          __fmul_rn(a.lambda, __uint2float_rn(sao_bits(info.luma))));
     a.sao[m] = info;
     a.sao_cost[m] = cur;
+}
+__global__ void k_sao_rdo(FrameArgs a) { sao_rdo_body(a); }
+__global__ void k_sao_rdo_b(const FrameArgs *args)
+{
+    __shared__ FrameArgs sa;
+    if (const FrameArgs *a = batch_args(args, sa)) sao_rdo_body(*a);
 }
 
 __device__ __forceinline__ evxg_sao_params ld_params_cg(const evxg_sao_params *p)
@@ -398,9 +416,8 @@ __device__ __forceinline__ evxg_sao_params unpack_params(unsigned long long v)
     return p;
 }
 
-__global__ void __launch_bounds__(256) k_sao_merge(FrameArgs a)
+__device__ __forceinline__ void sao_merge_body(const FrameArgs &a, MergeTile (&tiles)[8][2])
 {
-    __shared__ MergeTile tiles[8][2];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned long long ep = (unsigned long long)a.epoch;
     for (;;) {
@@ -465,6 +482,17 @@ __global__ void __launch_bounds__(256) k_sao_merge(FrameArgs a)
         }
     }
 }
+__global__ void __launch_bounds__(256) k_sao_merge(FrameArgs a)
+{
+    __shared__ MergeTile tiles[8][2];
+    sao_merge_body(a, tiles);
+}
+__global__ void __launch_bounds__(256) k_sao_merge_b(const FrameArgs *args)
+{
+    __shared__ MergeTile tiles[8][2];
+    __shared__ FrameArgs sa;
+    if (const FrameArgs *a = batch_args(args, sa)) sao_merge_body(*a, tiles);
+}
 
 // ---- application (sao.cpp:99-146) ----
 // The reference applies offsets MB by MB in raster order, in place: a pixel's
@@ -478,7 +506,7 @@ __global__ void __launch_bounds__(256) k_sao_merge(FrameArgs a)
 // flags any change; once a pass changes nothing the frame is exactly x = F(x).
 // Passes after a quiet pass return at once; if the last pass still changed a
 // pixel, k_sao_restore and k_sao_apply redo the frame in raster wavefront order.
-__global__ void __launch_bounds__(256) k_sao_fix(FrameArgs a, int pass)
+__device__ __forceinline__ void sao_fix_body(const FrameArgs &a, int pass)
 {
     if (pass > 0 && __ldcg(&a.sao_flags[pass - 1]) == 0) return;
     const int cw = a.W / 2, ch = a.H / 2;
@@ -519,21 +547,33 @@ __global__ void __launch_bounds__(256) k_sao_fix(FrameArgs a, int pass)
     }
     if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) atomicOr(&a.sao_flags[pass], 1);
 }
+__global__ void __launch_bounds__(256) k_sao_fix(FrameArgs a, int pass) { sao_fix_body(a, pass); }
+__global__ void __launch_bounds__(256) k_sao_fix_b(const FrameArgs *args, int pass)
+{
+    __shared__ FrameArgs sa;
+    if (const FrameArgs *a = batch_args(args, sa)) sao_fix_body(*a, pass);
+}
 
 // Fallback when the fixed point was not reached within the pass budget:
 // restore the unfiltered frame, then the raster wavefront below.
-__global__ void k_sao_restore(FrameArgs a, int last_pass)
+__device__ __forceinline__ void sao_restore_body(const FrameArgs &a, int last_pass)
 {
     if (__ldcg(&a.sao_flags[last_pass]) == 0) return;
     const size_t n = (size_t)a.W * a.H + 2 * (size_t)(a.W / 2) * (a.H / 2);
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         a.planes[a.dpb][i] = a.sao_orig[i];
 }
+__global__ void k_sao_restore(FrameArgs a, int last_pass) { sao_restore_body(a, last_pass); }
+__global__ void k_sao_restore_b(const FrameArgs *args, int last_pass)
+{
+    __shared__ FrameArgs sa;
+    if (const FrameArgs *a = batch_args(args, sa)) sao_restore_body(*a, last_pass);
+}
 
 // In-place application in raster order, one warp per MB row: MB (r, c) runs
 // after (r-1, c+1) and before anything of row r+1 at columns >= c-1.  Runs
 // only when the fixed-point passes did not converge.
-__global__ void k_sao_apply(FrameArgs a, int last_pass)
+__device__ __forceinline__ void sao_apply_body(const FrameArgs &a, int last_pass)
 {
     if (__ldcg(&a.sao_flags[last_pass]) == 0) return;
 
@@ -572,6 +612,57 @@ __global__ void k_sao_apply(FrameArgs a, int last_pass)
             __syncwarp();
         }
     }
+}
+__global__ void k_sao_apply(FrameArgs a, int last_pass) { sao_apply_body(a, last_pass); }
+__global__ void k_sao_apply_b(const FrameArgs *args, int last_pass)
+{
+    __shared__ FrameArgs sa;
+    if (const FrameArgs *a = batch_args(args, sa)) sao_apply_body(*a, last_pass);
+}
+
+// ------------------------------------------- batched-tick bookkeeping
+// In a batched tick these kernels do, for every stream with a frame, what
+// the single path does with copies and memsets around its kernels.
+__device__ __forceinline__ void copy_words(int *to, const int *from, size_t n, size_t t, size_t step)
+{
+    for (size_t i = t; i < n; i += step) to[i] = __ldg(from + i);
+}
+// Before the frame: the serializer's snapshot of the previous table
+// (encode.cpp:985-998 serializes before the update), wavefront progress words
+// to -1, row counters and SAO pass flags to 0.
+__global__ void k_tick_prep_b(const FrameArgs *args, int sao_passes)
+{
+    __shared__ FrameArgs sa;
+    const FrameArgs *a = batch_args(args, sa);
+    if (!a) return;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x, step = (size_t)gridDim.x * blockDim.x;
+    const size_t nblk = (size_t)a->mbw * a->mbh;
+    copy_words(reinterpret_cast<int *>(a->prev_ser), reinterpret_cast<const int *>(a->prev_tab), nblk * 7, t, step);
+    for (size_t i = t; i < 3 * (size_t)a->mbh; i += step) a->progress[i] = -1;
+    if (t < 4) a->counters[t] = 0;
+    if (t < (size_t)sao_passes) a->sao_flags[t] = 0;
+}
+// After deblocking: the pristine copy the SAO fixed-point passes read.
+__global__ void k_sao_copy_b(const FrameArgs *args)
+{
+    __shared__ FrameArgs sa;
+    const FrameArgs *a = batch_args(args, sa);
+    if (!a) return;
+    const uint4 *from = reinterpret_cast<const uint4 *>(a->planes[a->dpb]);
+    uint4 *to = reinterpret_cast<uint4 *>(a->sao_orig);
+    const size_t n = a->plane_elems / 8;   // plane sets are whole 16-byte chunks (16-aligned sizes)
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        to[i] = __ldcg(from + i);
+}
+// After the frame: the temporal predictor table of the next P frame is this
+// frame's table, except after B frames (encode.cpp:990-998).
+__global__ void k_tick_post_b(const FrameArgs *args)
+{
+    __shared__ FrameArgs sa;
+    const FrameArgs *a = batch_args(args, sa);
+    if (!a || a->type == EVXG_FRAME_BIDIR) return;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x, step = (size_t)gridDim.x * blockDim.x;
+    copy_words(reinterpret_cast<int *>(a->prev_tab), reinterpret_cast<const int *>(a->bt), (size_t)a->mbw * a->mbh * 7, t, step);
 }
 
 }  // namespace evxg

@@ -1,0 +1,80 @@
+// evxg_internal.cuh -- host-side internals shared by the C ABI translation
+// units (evxg_api.cu: streams, frames, GOP encoder; evxg_batch.cu: batched
+// ticks): the per-stream device state, the kernels they launch, error helpers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "evxg.h"
+#include "evxg_device.cuh"
+
+namespace evxg {
+__global__ void k_convert(FrameArgs a);
+__global__ void k_mb_wavefront(FrameArgs a);
+__global__ void k_mb_cluster(FrameArgs a);
+__global__ void k_deblock(FrameArgs a);
+__global__ void k_sao_rdo(FrameArgs a);
+__global__ void k_sao_merge(FrameArgs a);
+__global__ void k_sao_fix(FrameArgs a, int pass);
+__global__ void k_sao_restore(FrameArgs a, int last_pass);
+__global__ void k_sao_apply(FrameArgs a, int last_pass);
+// batched forms (blockIdx.z = stream; the MB kernels take the tick's row queue)
+__global__ void k_convert_b(const FrameArgs *args);
+__global__ void k_mb_wavefront_b(const FrameArgs *args, const int2 *queue, const int *qlen, int *qctr);
+__global__ void k_mb_cluster_b(const FrameArgs *args, const int2 *queue, const int *qlen, int *qctr);
+__global__ void k_deblock_b(const FrameArgs *args);
+__global__ void k_sao_rdo_b(const FrameArgs *args);
+__global__ void k_sao_merge_b(const FrameArgs *args);
+__global__ void k_sao_fix_b(const FrameArgs *args, int pass);
+__global__ void k_sao_restore_b(const FrameArgs *args, int last_pass);
+__global__ void k_sao_apply_b(const FrameArgs *args, int last_pass);
+__global__ void k_tick_prep_b(const FrameArgs *args, int sao_passes);
+__global__ void k_sao_copy_b(const FrameArgs *args);
+__global__ void k_tick_post_b(const FrameArgs *args);
+size_t mb_shared_bytes();
+int mb_threads();
+
+// Fixed-point passes of the SAO application (evxg_filters.cu); the chains they
+// resolve are a few pixels long, the last pass only confirms.
+constexpr int kSaoPasses = 8;
+
+int fail(int code, const char *what);
+int cuda_fail(cudaError_t e, const char *where);
+int check_frame(const evxg_frame *f, const char *who);
+int max_active_clusters();
+}  // namespace evxg
+
+#define CK(call)                                                     \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) return evxg::cuda_fail(e_, #call);    \
+    } while (0)
+
+struct evxg_stream {
+    uint32_t vw, vh, W, H, mbw, mbh;
+    size_t plane_elems;                 // elements of one plane set
+    int16_t *src, *lev, *dpb[4];
+    evxg_block_desc *bt, *prev, *prev_ser;
+    evxg_sao_info *sao;
+    float *sao_cost;
+    int16_t *sao_orig;                  // pristine copy for the SAO fixed-point passes
+    int *sao_flags;
+    unsigned long long *sao_mail;       // SAO merge hand-over words, epoch-tagged
+    int epoch;
+    uint8_t *rgb;
+    int *sync;                          // 3*mbh progress words, 4 counters, 1 error word
+    int mb_grid, num_sms;
+    int mb_form, mb_clusters;           // macroblock pass shape; clusters launched in the cluster form
+    uint32_t launches;
+    long long timeout_ns;
+    bool profile;
+    cudaEvent_t ev[7];
+};
+
+namespace evxg {
+// Kernel parameters of stream s for frame f (advances the stream's SAO epoch).
+void fill_args(evxg_stream *s, const evxg_frame *f, const uint8_t *drgb, FrameArgs &a);
+// Return a stream to its state at creation: zero planes and tables, epoch 0.
+int reset_stream(evxg_stream *s, cudaStream_t st);
+}  // namespace evxg

@@ -1420,6 +1420,33 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
     write_back(a, px, py, idx, S.rec[S.chosen], S.lev[S.chosen]);
 }
 
+// One macroblock row, left to right (single-CTA form); false once a wait
+// gave up (the error word is set).
+__device__ bool mb_row(const FrameArgs &a, int row)
+{
+    MbShared &S = SM();
+    const int tid = threadIdx.x;
+    for (int col = 0; col < a.mbw; ++col) {
+        if (tid == 0) {
+            // Row r-1 must have finished column c+3: the reads of MB (r,c)
+            // (intra block-copy candidates x in [px-31, px+31], 6-tap
+            // overshoot -3..+18) reach columns c-3 .. c+3.  Rows below
+            // then trail by three columns too, so row r+1 has finished at
+            // most column c-4 and the stale pixels MB (r,c) reads there
+            // (columns >= c-3) are still unwritten.  The reference waits
+            // for c+4 (encode.cpp:866-877); c+3 gives the same pixels.
+            S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 3, a.mbw - 1));
+        }
+        __syncthreads();
+        if (S.row_abort) return false;
+        process_mb(a, row, col);
+        __syncthreads();
+        if (tid == 0) st_release(&a.progress[row], col);
+    }
+    __syncthreads();
+    return true;
+}
+
 __global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a)
 {
     MbShared &S = SM();
@@ -1432,25 +1459,33 @@ __global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a)
         if (tid < NWIN) S.win[tid].valid = 0;   // windows are reused only along a row
         __syncthreads();
         const int row = s_row;
-        if (row >= a.mbh) return;
-        for (int col = 0; col < a.mbw; ++col) {
-            if (tid == 0) {
-                // Row r-1 must have finished column c+3: the reads of MB (r,c)
-                // (intra block-copy candidates x in [px-31, px+31], 6-tap
-                // overshoot -3..+18) reach columns c-3 .. c+3.  Rows below
-                // then trail by three columns too, so row r+1 has finished at
-                // most column c-4 and the stale pixels MB (r,c) reads there
-                // (columns >= c-3) are still unwritten.  The reference waits
-                // for c+4 (encode.cpp:866-877); c+3 gives the same pixels.
-                S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 3, a.mbw - 1));
-            }
-            __syncthreads();
-            if (S.row_abort) return;
-            process_mb(a, row, col);
-            __syncthreads();
-            if (tid == 0) st_release(&a.progress[row], col);
-        }
+        if (row >= a.mbh || !mb_row(a, row)) return;
+    }
+}
+
+// Batched form: the rows of every stream of a tick form one queue of
+// (stream, row) items, claimed in queue order; within a stream the queue keeps
+// row order, so a row always waits on a row that a running CTA has claimed.
+__global__ void __launch_bounds__(NT, 1) k_mb_wavefront_b(const FrameArgs *args, const int2 *queue, const int *qlen,
+                                                           int *qctr)
+{
+    MbShared &S = SM();
+    __shared__ int s_item;
+    __shared__ FrameArgs sa;
+    const int tid = threadIdx.x;
+    init_tables();
+    __syncthreads();
+    const int nq = __ldg(qlen);
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(qctr, 1);
         __syncthreads();
+        const int item = s_item;
+        if (item >= nq) return;
+        const int2 q = queue[item];
+        if (tid == 0) sa = args[q.x];
+        if (tid < NWIN) S.win[tid].valid = 0;
+        __syncthreads();
+        if (!mb_row(sa, q.y)) return;   // the tick has failed; every wait of it now gives up
     }
 }
 
@@ -1676,36 +1711,53 @@ __device__ bool aux_mb(const FrameArgs &a, int row, int col, int n)   // rank 2
     return true;
 }
 
-__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(NT, 1) k_mb_cluster(FrameArgs a)
+// Rows for a cluster: the leader claims them (single form: the frame's row
+// counter; batched form: the tick's (stream, row) queue) and passes each on
+// to ranks 1 and 2; every CTA then works on the row with that stream's
+// parameters (a copy in its shared memory in the batched form).
+template <bool kBatched>
+__device__ void cluster_main(const FrameArgs &a0, const FrameArgs *args, const int2 *queue, const int *qlen, int *qctr)
 {
     MbShared &S = SM();
-    __shared__ int s_row;
+    __shared__ int s_item;
+    __shared__ FrameArgs sa;
     const int tid = threadIdx.x;
     const unsigned rank = cluster_rank();
     init_tables();
     if (tid == 0) {
         S.mail.row_seq = 0; S.mail.dec_seq = 0; S.mail.wr_seq = 0; S.mail.f_seq = 0; S.mail.d_seq = 0;
         S.row_abort = 0;
+        if (kBatched) sa = args[0];   // every stream of a tick shares the error word and the timeout
     }
+    const int nq = kBatched ? __ldg(qlen) : a0.mbh;
     cluster_barrier();   // every CTA's mail is initialised before any peer writes to it
+    const FrameArgs &w = kBatched ? sa : a0;   // for the waits before a row is known
     int n = 0;
     for (int k = 1;; k++) {
         if (tid == 0) {
-            if (rank == 0) {   // the leader claims rows and passes them on
-                const int r = atomicAdd(&a.counters[0], 1);
-                s_row = r < a.mbh ? r : -1;
+            if (rank == 0) {
+                const int r = atomicAdd(kBatched ? qctr : &a0.counters[0], 1);
+                s_item = r < nq ? r : -1;
                 for (unsigned p = 1; p < 3; p++) {
-                    *peer(&S.mail.row_val, p) = s_row;
+                    *peer(&S.mail.row_val, p) = s_item;
                     st_release_cl(peer(&S.mail.row_seq, p), k);
                 }
             } else {
-                s_row = wait_mail(&S.mail.row_seq, k, a) ? S.mail.row_val : -1;
+                s_item = wait_mail(&S.mail.row_seq, k, w) ? S.mail.row_val : -1;
             }
         }
         if (tid < NWIN) S.win[tid].valid = 0;   // windows are reused only along a row
         __syncthreads();
-        const int row = s_row;
-        if (row < 0) break;
+        const int item = s_item;
+        if (item < 0) break;
+        int row = item;
+        if (kBatched) {
+            const int2 q = queue[item];
+            row = q.y;
+            if (tid == 0) sa = args[q.x];
+            __syncthreads();
+        }
+        const FrameArgs &a = kBatched ? sa : a0;
         bool ok = true;
         for (int col = 0; col < a.mbw && ok; ++col) {
             ++n;
@@ -1715,6 +1767,16 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(NT, 1) k_mb_cluster(
         if (!ok) break;
     }
     cluster_barrier();   // no CTA leaves while a peer may still access its shared memory
+}
+
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(NT, 1) k_mb_cluster(FrameArgs a)
+{
+    cluster_main<false>(a, nullptr, nullptr, nullptr, nullptr);
+}
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(NT, 1) k_mb_cluster_b(const FrameArgs *args, const int2 *queue,
+                                                                                 const int *qlen, int *qctr)
+{
+    cluster_main<true>(args[0], args, queue, qlen, qctr);
 }
 
 size_t mb_shared_bytes() { return sizeof(MbShared); }

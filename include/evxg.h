@@ -170,6 +170,45 @@ int evxg_stream_mb_form(const evxg_stream *s);
 int evxg_stream_profile(evxg_stream *s, int enable);
 int evxg_stream_kernel_ms(evxg_stream *s, float *out_ms, uint32_t n);
 
+/* ---- Batched encoding ----
+ *
+ * No counterpart in the reference, which encodes one stream per evx3_encoder
+ * (evx3enc.cpp:105-414).  A batch holds n streams of any sizes; each tick
+ * advances every stream that has a frame by that one frame, with one kernel
+ * launch per pipeline stage for all of them (the macroblock pass claims
+ * (stream, row) items from one queue), the tick replayed as a CUDA graph.
+ * Every stream's output equals encoding it alone with evxg_encode_frame.
+ *
+ * Host buffers come in two parities (0, 1), so the host prepares tick t+1
+ * while the device runs tick t: write stream i's RGB24 frame into
+ * evxg_batch_input(b, i, p), call evxg_batch_encode(b, frames, p, stream),
+ * and after evxg_batch_wait(b, p) read stream i's tables (the inputs of the
+ * reference serializer, as evxg_fetch_tables returns them) from
+ * evxg_batch_output.  Before rewriting parity p's inputs, wait for parity p.
+ * frames[i].type < 0 means stream i has no frame in this tick.  The streams
+ * stay owned by the caller and must not be used outside the batch while it
+ * exists. */
+typedef struct evxg_batch evxg_batch;
+int evxg_batch_create(evxg_stream *const *streams, uint32_t n, evxg_batch **out);
+int evxg_batch_destroy(evxg_batch *b);
+uint8_t *evxg_batch_input(evxg_batch *b, uint32_t i, uint32_t parity);
+int evxg_batch_encode(evxg_batch *b, const evxg_frame *frames, uint32_t parity, void *cuda_stream);
+int evxg_batch_wait(evxg_batch *b, uint32_t parity);
+int evxg_batch_output(evxg_batch *b, uint32_t i, uint32_t parity, const evxg_block_desc **blocks,
+                      const evxg_block_desc **prev_blocks, const evxg_sao_info **sao, const int16_t **levels);
+/* Kernels one tick launches (the same for any number of streams). */
+uint32_t evxg_batch_launch_count(const evxg_batch *b);
+/* Shape of the tick's macroblock pass: form (EVXG_MB_FORM_*), persistent grid
+ * (CTAs, or clusters in the cluster form; capped at what is co-resident) and
+ * queue order (0: rows interleaved by index; 1: the same, longer remaining
+ * critical path first).  evxg_batch_autotune times the candidates on a short
+ * synthetic I/P/B sequence at the streams' sizes, keeps the fastest, and
+ * returns every stream to its initial state; best_ms (optional) receives the
+ * winner's time for the three timed ticks. */
+int evxg_batch_set_shape(evxg_batch *b, int form, int grid, int policy);
+int evxg_batch_get_shape(const evxg_batch *b, int *form, int *grid, int *policy);
+int evxg_batch_autotune(evxg_batch *b, void *cuda_stream, float *best_ms);
+
 /* lambda = 0.85 * 2^((q-12)/3) in float, as the reference computes it (common.h:264-266). */
 float evxg_lambda(uint16_t quality);
 
