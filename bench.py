@@ -40,9 +40,9 @@ UNIT = "1080p-eq frames/s"
 W, H, FRAMES, QUALITY, VMAX, CUT = 1920, 1080, 120, 8, 24.0, 60
 EQ = (W * H) / (1920 * 1080)
 HBM_PEAK_FALLBACK = 6650.0
-# dram__bytes_read.sum + dram__bytes_write.sum of one k_mb_wavefront launch
-# (a 1080p B frame of this workload), profiles/mb_wavefront_1080p.md
-MB_TRAFFIC_BYTES = 25_676_032 + 488_960
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_mb_cluster launch
+# (a 1080p B frame of this workload), profiles/mb_cluster_1080p.md
+MB_TRAFFIC_BYTES = 25_302_016 + 509_952
 
 
 def peaks():
@@ -218,10 +218,13 @@ def run_gpu(args):
         "p99_frame_ms": round(float(np.percentile(step_ms, 99)), 3),
         "kernel_ms_per_step": {k: round(v / K, 4) for k, v in kernel_tot.items()},
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "roofline": {"kernel": "k_mb_wavefront", "bound": "hbm", "achieved": round(achieved, 3), "peak": peak,
-                     "unit": "GB/s", "frac": round(achieved / peak, 6), "traffic": MB_TRAFFIC_BYTES,
+        "roofline": {"kernel": "k_mb_cluster" if st.mb_form == cb.MB_FORM_CLUSTER else "k_mb_wavefront",
+                     "bound": "hbm", "achieved": round(achieved, 3), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 6),
+                     "traffic": MB_TRAFFIC_BYTES if st.mb_form == cb.MB_FORM_CLUSTER else None,
                      "peak_source": f"{peak_kind} hbm_gbs",
-                     "note": "dependency-latency bound: lag-3 macroblock wavefront (critical path of cols + 3*(rows-1) MB steps)"},
+                     "note": "dependency-latency bound: macroblock wavefront whose critical path is "
+                             "cols + 4*(rows-1) MB steps (388 at 1080p), each one MB's dependent chain"},
         "gpu_launches": st.launch_count() * K,
         "batched": batched,
         "clocks": clk,
