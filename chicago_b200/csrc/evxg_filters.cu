@@ -4,7 +4,7 @@
 //
 // Reference: src/video/convert.cpp:11-160, src/video/deblock.cpp:14-305,
 // src/video/sao.cpp:13-594 (luma-only merge branch, EVX_ENABLE_SAO_CHROMA_MERGE 0).
-#include "evxg_device.cuh"
+#include "evxg_internal.cuh"
 
 namespace evxg {
 
@@ -65,33 +65,40 @@ __device__ __forceinline__ void edge_params(const evxg_block_desc *bt, int li, i
     qe = min(aq + qoff, MAXQ);
 }
 
-// Filter one line across an edge; e points at q0, step is the distance between samples.
-__device__ __forceinline__ void filter_line(int16_t *e, int step, int qe, int st, bool luma)   // deblock.cpp:91-146
+// Filter one line across an edge (deblock.cpp:91-146); tap(k) is the sample
+// k places from q0 (p0 = tap(-1), q0 = tap(0)).
+template <class Tap>
+__device__ __forceinline__ void filter_taps(Tap tap, int qe, int st, bool luma)
 {
-    const int p0 = e[-step], p1 = e[-2 * step], p2 = e[-3 * step], p3 = e[-4 * step];
-    const int q0 = e[0], q1 = e[step], q2 = e[2 * step], q3 = e[3 * step];
+    const int p0 = tap(-1), p1 = tap(-2), p2 = tap(-3), p3 = tap(-4);
+    const int q0 = tap(0), q1 = tap(1), q2 = tap(2), q3 = tap(3);
     int qi = qe;
     if (st == 2 && qe > 0) qi = min(qe + 2, MAXQ);
     if ((int16_t)iabs32(p0 - q0) >= c_alpha[qi] || (int16_t)iabs32(p1 - p0) >= c_beta[qi] ||
         (int16_t)iabs32(q1 - q0) >= c_beta[qi])
         return;
     if (st == 2) {
-        e[-step] = (int16_t)rdiv(p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1, 8);
-        e[-2 * step] = (int16_t)rdiv(p2 + p1 + p0 + q0, 4);
-        e[0] = (int16_t)rdiv(p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2, 8);
-        e[step] = (int16_t)rdiv(p0 + q0 + q1 + q2, 4);
+        tap(-1) = (int16_t)rdiv(p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1, 8);
+        tap(-2) = (int16_t)rdiv(p2 + p1 + p0 + q0, 4);
+        tap(0) = (int16_t)rdiv(p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2, 8);
+        tap(1) = (int16_t)rdiv(p0 + q0 + q1 + q2, 4);
         if (luma) {
-            e[-3 * step] = (int16_t)rdiv(2 * p3 + 3 * p2 + p1 + p0 + q0, 8);
-            e[2 * step] = (int16_t)rdiv(2 * q3 + 3 * q2 + q1 + q0 + p0, 8);
+            tap(-3) = (int16_t)rdiv(2 * p3 + 3 * p2 + p1 + p0 + q0, 8);
+            tap(2) = (int16_t)rdiv(2 * q3 + 3 * q2 + q1 + q0 + p0, 8);
         }
     } else {
-        e[-step] = (int16_t)rdiv(((q0 + p0) * 4) + p1 - q1, 8);
-        e[0] = (int16_t)rdiv(((q0 + p0) * 4) + q1 - p1, 8);
+        tap(-1) = (int16_t)rdiv(((q0 + p0) * 4) + p1 - q1, 8);
+        tap(0) = (int16_t)rdiv(((q0 + p0) * 4) + q1 - p1, 8);
         if (luma) {
-            e[-2 * step] = (int16_t)rdiv((p2 * 4) + (p0 * 2) + (q0 * 2), 8);
-            e[step] = (int16_t)rdiv((q2 * 4) + (q0 * 2) + (p0 * 2), 8);
+            tap(-2) = (int16_t)rdiv((p2 * 4) + (p0 * 2) + (q0 * 2), 8);
+            tap(1) = (int16_t)rdiv((q2 * 4) + (q0 * 2) + (p0 * 2), 8);
         }
     }
+}
+// e points at q0, step is the distance between samples.
+__device__ __forceinline__ void filter_line(int16_t *e, int step, int qe, int st, bool luma)
+{
+    filter_taps([&](int k) -> int16_t & { return e[k * step]; }, qe, st, luma);
 }
 
 // One CTA per plane.  The reference's order (deblock.cpp:233-272) is: row band
@@ -130,11 +137,92 @@ __device__ __forceinline__ void deblock_body(const FrameArgs &a)
         __syncthreads();
     }
 }
-__global__ void __launch_bounds__(1024) k_deblock(FrameArgs a) { deblock_body(a); }
+// The same order on a window of the plane in shared memory: a circular
+// buffer of DB_SLOTS rows.  The next band's rows are read into registers
+// while the current band is filtered; a row goes back to memory once no later
+// edge touches it -- after band j every row up to j+4 is final (later
+// horizontal edges start at row j+8-3, vertical ones at row j+8).  The slots
+// the next band takes held rows that were written back at least a band ago.
+constexpr int DB_SLOTS = 24, DB_PF = 4;   // window rows; chunks of the next band per thread (1024 threads)
+__device__ __forceinline__ int db_slot(int r) { return (r + DB_SLOTS) % DB_SLOTS; }
+__device__ void deblock_smem_body(const FrameArgs &a, int16_t *buf)
+{
+    const int pl = blockIdx.x;
+    const bool luma = pl == 0;
+    const int w = luma ? a.W : a.W / 2, h = luma ? a.H : a.H / 2;
+    const int mbs = luma ? 16 : 8, qoff = luma ? 0 : 2;
+    int16_t *d = a.planes[a.dpb] + (pl == 0 ? 0 : (size_t)a.W * a.H + (pl - 1) * (size_t)(a.W / 2) * (a.H / 2));
+    const int nv = (w / 8 - 1) * 8, cpr = w / 8;   // vertical edge lines per band, 16-byte chunks per row
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int i = tid; i < 8 * cpr; i += nt) {   // band 0
+        const int r = i / cpr, c = i % cpr;
+        *reinterpret_cast<uint4 *>(buf + db_slot(r) * w + 8 * c) = __ldcg(reinterpret_cast<const uint4 *>(d + (size_t)r * w + 8 * c));
+    }
+    __syncthreads();
+    int written = 0;   // rows [0, written) are back in the slot
+    for (int j = 0; j < h; j += 8) {
+        const bool more = j + 8 < h;
+        uint4 pf[DB_PF];
+#pragma unroll
+        for (int k = 0; k < DB_PF; k++) {
+            const int i = tid + k * nt;
+            if (more && i < 8 * cpr)
+                pf[k] = __ldcg(reinterpret_cast<const uint4 *>(d + (size_t)(j + 8 + i / cpr) * w + 8 * (i % cpr)));
+        }
+        if (j > 0) {   // horizontal edges at row j
+            const int brow = (j / mbs) * a.mbw, arow = ((j - 1) / mbs) * a.mbw;
+            int ro[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) ro[k] = db_slot(j - 4 + k) * w;
+            for (int x = tid; x < w; x += nt) {
+                int qe, st;
+                edge_params(a.bt, x / mbs + arow, x / mbs + brow, qoff, qe, st);
+                if (st) filter_taps([&](int k) -> int16_t & { return buf[ro[k + 4] + x]; }, qe, st, luma);
+            }
+            __syncthreads();
+        }
+        const int brow = (j / mbs) * a.mbw;
+        for (int t = tid; t < nv; t += nt) {   // vertical edges of the band
+            const int x = ((t >> 3) + 1) * 8, y = j + (t & 7);
+            int qe, st;
+            edge_params(a.bt, (x - 1) / mbs + brow, x / mbs + brow, qoff, qe, st);
+            if (st) filter_line(buf + db_slot(y) * w + x, 1, qe, st, luma);
+        }
+        __syncthreads();
+        const int upto = more ? j + 5 : h;
+        for (int i = tid; i < (upto - written) * cpr; i += nt) {
+            const int r = written + i / cpr, c = i % cpr;
+            *reinterpret_cast<uint4 *>(d + (size_t)r * w + 8 * c) = *reinterpret_cast<const uint4 *>(buf + db_slot(r) * w + 8 * c);
+        }
+        written = upto;
+#pragma unroll
+        for (int k = 0; k < DB_PF; k++) {
+            const int i = tid + k * nt;
+            if (more && i < 8 * cpr) *reinterpret_cast<uint4 *>(buf + db_slot(j + 8 + i / cpr) * w + 8 * (i % cpr)) = pf[k];
+        }
+        __syncthreads();
+    }
+}
+// Planes up to 4096 samples wide go through shared memory (24 rows, at most
+// 192 KB; the next band is at most 4 chunks per thread); wider ones filter in
+// place in memory.
+__host__ __device__ __forceinline__ bool deblock_fits(int W) { return W <= 4096; }
+size_t deblock_shared_bytes(int W) { return deblock_fits(W) ? (size_t)DB_SLOTS * W * sizeof(int16_t) : 0; }
+__device__ __forceinline__ void deblock_dispatch(const FrameArgs &a, int16_t *buf)
+{
+    if (deblock_fits(a.W)) deblock_smem_body(a, buf);
+    else deblock_body(a);
+}
+__global__ void __launch_bounds__(1024) k_deblock(FrameArgs a)
+{
+    extern __shared__ __align__(16) int16_t db_smem[];
+    deblock_dispatch(a, db_smem);
+}
 __global__ void __launch_bounds__(1024) k_deblock_b(const FrameArgs *args)
 {
+    extern __shared__ __align__(16) int16_t db_smem[];
     __shared__ FrameArgs sa;
-    if (const FrameArgs *a = batch_args(args, sa)) deblock_body(*a);
+    if (const FrameArgs *a = batch_args(args, sa)) deblock_dispatch(*a, db_smem);
 }
 
 // ------------------------------------------------------------------ SAO
@@ -184,109 +272,193 @@ __device__ __forceinline__ int sao_px(const int16_t *img, int w, int h, int x, i
     return v;
 }
 
-// Per-MB RDO of one plane block (sao.cpp:150-343); returns the parameters and
-// the SSD they give.  Band and edge SSDs are assembled from per-band /
-// per-category deltas, which sums the same integers as a full pass.
-__device__ void sao_rdo_block(const int16_t *s, const int16_t *r, int w, int h, int x0, int y0, int n, float lambda,
-                              evxg_sao_params &out, long long &out_ssd)
+// Per-warp scratch of the SAO RDO.
+struct SaoScratch {
+    int bsum[32], bcnt[32], boff[32];
+    unsigned long long bdelta[32];   // signed sums, two's complement
+};
+
+// Per-MB RDO of one N x N plane block (sao.cpp:150-343) on one warp; returns
+// the parameters and the SSD they give.  Lane l holds N*N/32 consecutive
+// pixels of one row and the recon samples around them.  The candidates are
+// costed independently (no SAO, band offsets at positions 0..28, edge
+// offsets of classes 0..3) and the reference's loop -- take a candidate when
+// it is strictly cheaper than the best so far -- picks the first candidate of
+// that order whose cost is the minimum, which a (cost, index) argmin finds.
+// All sums are of integers, so regrouping them changes nothing.
+template <int N>
+__device__ void sao_rdo_warp(const int16_t *s, const int16_t *r, int w, int h, int x0, int y0, float lambda, int lane,
+                             SaoScratch &sc, evxg_sao_params &out, long long &out_ssd)
 {
-    out = evxg_sao_params{};
+    constexpr int P = N * N / 32;   // pixels per lane: 8 (luma) or 2 (chroma)
+    const int y = y0 + lane * P / N, xs = x0 + (lane * P) % N;
+    int pv[P], sv[P], nb[3][P + 2];
+#pragma unroll
+    for (int i = 0; i < P; i++) {
+        pv[i] = __ldg(r + (size_t)y * w + xs + i);
+        sv[i] = __ldg(s + (size_t)y * w + xs + i);
+    }
+#pragma unroll
+    for (int dy = 0; dy < 3; dy++)
+#pragma unroll
+        for (int dx = 0; dx < P + 2; dx++) {
+            const int yy = y - 1 + dy, xx = xs - 1 + dx;
+            nb[dy][dx] = (yy >= 0 && yy < h && xx >= 0 && xx < w) ? __ldg(r + (size_t)yy * w + xx) : 0;
+        }
+    sc.bsum[lane] = 0; sc.bcnt[lane] = 0; sc.bdelta[lane] = 0;
+    __syncwarp();
     long long base = 0;
-    int bsum[32], bcnt[32];
-    for (int k = 0; k < 32; k++) { bsum[k] = 0; bcnt[k] = 0; }
-    for (int y = y0; y < y0 + n; y++)
-        for (int x = x0; x < x0 + n; x++) {
-            const int pv = __ldg(r + (size_t)y * w + x), sv = __ldg(s + (size_t)y * w + x);
-            base += (long long)((sv - pv) * (sv - pv));
-            const int b = sclamp(pv) >> 3;
-            bsum[b] += sv - pv;
-            bcnt[b]++;
-        }
-    float best = rd_cost64(base, lambda, 2u);
-    long long best_ssd = base;
-    // band offsets: the offset of band b does not depend on the band position
-    int boff[32];
-    long long bdelta[32];
-    for (int k = 0; k < 32; k++) { boff[k] = bcnt[k] > 0 ? avg_off(bsum[k], bcnt[k]) : 0; bdelta[k] = 0; }
-    for (int y = y0; y < y0 + n; y++)
-        for (int x = x0; x < x0 + n; x++) {
-            const int pv = __ldg(r + (size_t)y * w + x), sv = __ldg(s + (size_t)y * w + x);
-            const int b = sclamp(pv) >> 3;
-            const int cv = sclamp(pv + boff[b]);
-            bdelta[b] += (long long)((sv - cv) * (sv - cv)) - (long long)((sv - pv) * (sv - pv));
-        }
-    for (int bp = 0; bp <= 28; bp++) {
+#pragma unroll
+    for (int i = 0; i < P; i++) {
+        const int d = sv[i] - pv[i], b = sclamp(pv[i]) >> 3;
+        base += (long long)(d * d);
+        atomicAdd(&sc.bsum[b], d);
+        atomicAdd(&sc.bcnt[b], 1);
+    }
+    base = warp_sum64(base);
+    __syncwarp();
+    // band offsets: lane b owns band b (its offset does not depend on the band position)
+    sc.boff[lane] = sc.bcnt[lane] > 0 ? avg_off(sc.bsum[lane], sc.bcnt[lane]) : 0;
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < P; i++) {
+        const int d = sv[i] - pv[i], b = sclamp(pv[i]) >> 3, cv = sclamp(pv[i] + sc.boff[b]), e = sv[i] - cv;
+        atomicAdd(&sc.bdelta[b], (unsigned long long)((long long)(e * e) - (long long)(d * d)));
+    }
+    __syncwarp();
+    // candidate costs; index 0 = no SAO, 1 + bp = band position bp, 30 + ec = edge class ec
+    float cost = __int_as_float(0x7f800000);   // +inf: not a candidate
+    int idx = 64;
+    long long ssd_c = 0;
+    if (lane <= 28) {
         evxg_sao_params c{};
-        c.type = 2; c.band_position = (uint8_t)bp;
+        c.type = 2; c.band_position = (uint8_t)lane;
         bool nz = false;
         long long ssd = base;
         for (int k = 0; k < 4; k++) {
-            c.offsets[k] = (int8_t)boff[bp + k];
-            nz |= boff[bp + k] != 0;
-            ssd += bdelta[bp + k];
+            c.offsets[k] = (int8_t)sc.boff[lane + k];
+            nz |= sc.boff[lane + k] != 0;
+            ssd += (long long)sc.bdelta[lane + k];
         }
-        if (!nz) continue;
-        const float cost = rd_cost64(ssd, lambda, sao_bits(c));
-        if (cost < best) { best = cost; out = c; best_ssd = ssd; }
+        if (nz) { cost = rd_cost64(ssd, lambda, sao_bits(c)); idx = 1 + lane; ssd_c = ssd; }
     }
+    if (lane == 31) { cost = rd_cost64(base, lambda, 2u); idx = 0; ssd_c = base; }
+    // edge classes: category sums per class, reduced over the warp
+    int cs[4][4], cc[4][4];
+#pragma unroll
+    for (int ec = 0; ec < 4; ec++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) { cs[ec][k] = 0; cc[ec][k] = 0; }
+    int cat[4][P];
+#pragma unroll
+    for (int ec = 0; ec < 4; ec++)
+#pragma unroll
+        for (int i = 0; i < P; i++) {
+            // c_eo as compile-time constants, so the neighbourhood stays in registers
+            constexpr int kEo[4][4] = {{-1, 0, 1, 0}, {0, -1, 0, 1}, {-1, -1, 1, 1}, {1, -1, -1, 1}};
+            const int dxa = kEo[ec][0], dya = kEo[ec][1], dxb = kEo[ec][2], dyb = kEo[ec][3];
+            const int x = xs + i, ax = x + dxa, ay = y + dya, bx = x + dxb, by = y + dyb;
+            int ct = 4;
+            if (!(ax < 0 || ax >= w || ay < 0 || ay >= h || bx < 0 || bx >= w || by < 0 || by >= h))
+                ct = eo_cat(pv[i], nb[1 + dya][1 + i + dxa], nb[1 + dyb][1 + i + dxb]);
+            cat[ec][i] = ct;
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (ct == k) { cs[ec][k] += sv[i] - pv[i]; cc[ec][k]++; }
+        }
+#pragma unroll
+    for (int ec = 0; ec < 4; ec++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) { cs[ec][k] = warp_sum(cs[ec][k]); cc[ec][k] = warp_sum(cc[ec][k]); }
+    long long eo_ssd[4];
+    bool eo_nz[4];
+    int off[4][4];
+#pragma unroll
     for (int ec = 0; ec < 4; ec++) {
-        int cs[4] = {0, 0, 0, 0}, cc[4] = {0, 0, 0, 0};
-        for (int y = y0; y < y0 + n; y++)
-            for (int x = x0; x < x0 + n; x++) {
-                const int ax = x + c_eo[ec][0], ay = y + c_eo[ec][1], bx = x + c_eo[ec][2], by = y + c_eo[ec][3];
-                if (ax < 0 || ax >= w || ay < 0 || ay >= h || bx < 0 || bx >= w || by < 0 || by >= h) continue;
-                const int pv = __ldg(r + (size_t)y * w + x);
-                const int ct = eo_cat(pv, __ldg(r + (size_t)ay * w + ax), __ldg(r + (size_t)by * w + bx));
-                if (ct < 4) { cs[ct] += __ldg(s + (size_t)y * w + x) - pv; cc[ct]++; }
+        eo_nz[ec] = false;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            off[ec][k] = cc[ec][k] > 0 ? avg_off(cs[ec][k], cc[ec][k]) : 0;
+            eo_nz[ec] |= off[ec][k] != 0;
+        }
+        long long dl = 0;
+#pragma unroll
+        for (int i = 0; i < P; i++) {
+            const int ct = cat[ec][i];
+            if (ct < 4) {
+                int o = 0;
+#pragma unroll
+                for (int k = 0; k < 4; k++) o = ct == k ? off[ec][k] : o;
+                const int d = sv[i] - pv[i], e = sv[i] - sclamp(pv[i] + o);
+                dl += (long long)(e * e) - (long long)(d * d);
             }
+        }
+        eo_ssd[ec] = base + warp_sum64(dl);
+    }
+    // argmin over (cost, index): bands / none on their lanes, then the four edge classes
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        const float c2 = __shfl_xor_sync(0xffffffffu, cost, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
+        const long long s2 = __shfl_xor_sync(0xffffffffu, ssd_c, o);
+        if (c2 < cost || (c2 == cost && i2 < idx)) { cost = c2; idx = i2; ssd_c = s2; }
+    }
+#pragma unroll
+    for (int ec = 0; ec < 4; ec++) {   // edge candidates come after every band candidate
+        if (!eo_nz[ec]) continue;
         evxg_sao_params c{};
         c.type = 1; c.eo_class = (uint8_t)ec;
-        bool nz = false;
-        for (int k = 0; k < 4; k++) { c.offsets[k] = (int8_t)(cc[k] > 0 ? avg_off(cs[k], cc[k]) : 0); nz |= c.offsets[k] != 0; }
-        if (!nz) continue;
-        long long ssd = base;
-        for (int y = y0; y < y0 + n; y++)
-            for (int x = x0; x < x0 + n; x++) {
-                const int ax = x + c_eo[ec][0], ay = y + c_eo[ec][1], bx = x + c_eo[ec][2], by = y + c_eo[ec][3];
-                if (ax < 0 || ax >= w || ay < 0 || ay >= h || bx < 0 || bx >= w || by < 0 || by >= h) continue;
-                const int pv = __ldg(r + (size_t)y * w + x);
-                const int ct = eo_cat(pv, __ldg(r + (size_t)ay * w + ax), __ldg(r + (size_t)by * w + bx));
-                if (ct < 4) {
-                    const int sv = __ldg(s + (size_t)y * w + x), cv = sclamp(pv + c.offsets[ct]);
-                    ssd += (long long)((sv - cv) * (sv - cv)) - (long long)((sv - pv) * (sv - pv));
-                }
-            }
-        const float cost = rd_cost64(ssd, lambda, sao_bits(c));
-        if (cost < best) { best = cost; out = c; best_ssd = ssd; }
+        for (int k = 0; k < 4; k++) c.offsets[k] = (int8_t)off[ec][k];
+        const float ce = rd_cost64(eo_ssd[ec], lambda, sao_bits(c));
+        if (ce < cost) { cost = ce; idx = 30 + ec; ssd_c = eo_ssd[ec]; }
     }
-    out_ssd = best_ssd;
+    out = evxg_sao_params{};
+    if (idx >= 30) {
+        out.type = 1; out.eo_class = (uint8_t)(idx - 30);
+        for (int k = 0; k < 4; k++) out.offsets[k] = (int8_t)off[idx - 30][k];
+    } else if (idx >= 1) {
+        out.type = 2; out.band_position = (uint8_t)(idx - 1);
+        for (int k = 0; k < 4; k++) out.offsets[k] = (int8_t)sc.boff[idx - 1 + k];
+    }
+    out_ssd = ssd_c;
+    __syncwarp();
 }
 
-// One thread per MB: own luma and chroma (U plane) parameters and the cost of
+// One warp per MB: own luma and chroma (U plane) parameters and the cost of
 // keeping them, the starting point of the merge decision (sao.cpp:414-557).
-__device__ __forceinline__ void sao_rdo_body(const FrameArgs &a)
+__device__ __forceinline__ void sao_rdo_body(const FrameArgs &a, SaoScratch *scratch)
 {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+    const int m = blockIdx.x * (blockDim.x >> 5) + wi;
     if (m >= a.mbw * a.mbh) return;
     const int bx = m % a.mbw, by = m / a.mbw;
     const int16_t *rec = a.planes[a.dpb];
     const int cw = a.W / 2, ch = a.H / 2;
     evxg_sao_info info{};
     long long lssd, cssd;
-    sao_rdo_block(a.src, rec, a.W, a.H, bx * 16, by * 16, 16, a.lambda, info.luma, lssd);
-    sao_rdo_block(a.src + (size_t)a.W * a.H, rec + (size_t)a.W * a.H, cw, ch, bx * 8, by * 8, 8, a.lambda, info.chroma, cssd);
-    float cur;
-    if (info.luma.type == 0) cur = __fadd_rn(__ll2float_rn(lssd), __fmul_rn(a.lambda, 2.0f));
-    else cur = __fadd_rn(__fsub_rn(__fadd_rn(__ll2float_rn(lssd), __fmul_rn(a.lambda, 1.0f)), __fmul_rn(a.lambda, 1.0f)),
-                         __fmul_rn(a.lambda, __uint2float_rn(sao_bits(info.luma))));
-    a.sao[m] = info;
-    a.sao_cost[m] = cur;
+    sao_rdo_warp<16>(a.src, rec, a.W, a.H, bx * 16, by * 16, a.lambda, lane, scratch[wi], info.luma, lssd);
+    sao_rdo_warp<8>(a.src + (size_t)a.W * a.H, rec + (size_t)a.W * a.H, cw, ch, bx * 8, by * 8, a.lambda, lane, scratch[wi],
+                    info.chroma, cssd);
+    if (lane == 0) {
+        float cur;
+        if (info.luma.type == 0) cur = __fadd_rn(__ll2float_rn(lssd), __fmul_rn(a.lambda, 2.0f));
+        else cur = __fadd_rn(__fsub_rn(__fadd_rn(__ll2float_rn(lssd), __fmul_rn(a.lambda, 1.0f)), __fmul_rn(a.lambda, 1.0f)),
+                             __fmul_rn(a.lambda, __uint2float_rn(sao_bits(info.luma))));
+        a.sao[m] = info;
+        a.sao_cost[m] = cur;
+    }
 }
-__global__ void k_sao_rdo(FrameArgs a) { sao_rdo_body(a); }
-__global__ void k_sao_rdo_b(const FrameArgs *args)
+constexpr int SAO_RDO_WARPS = 8;   // MBs per block of the RDO kernels
+__global__ void __launch_bounds__(32 * SAO_RDO_WARPS) k_sao_rdo(FrameArgs a)
 {
+    __shared__ SaoScratch sc[SAO_RDO_WARPS];
+    sao_rdo_body(a, sc);
+}
+__global__ void __launch_bounds__(32 * SAO_RDO_WARPS) k_sao_rdo_b(const FrameArgs *args)
+{
+    __shared__ SaoScratch sc[SAO_RDO_WARPS];
     __shared__ FrameArgs sa;
-    if (const FrameArgs *a = batch_args(args, sa)) sao_rdo_body(*a);
+    if (const FrameArgs *a = batch_args(args, sa)) sao_rdo_body(*a, sc);
 }
 
 __device__ __forceinline__ evxg_sao_params ld_params_cg(const evxg_sao_params *p)
@@ -416,82 +588,128 @@ __device__ __forceinline__ evxg_sao_params unpack_params(unsigned long long v)
     return p;
 }
 
-__device__ __forceinline__ void sao_merge_body(const FrameArgs &a, MergeTile (&tiles)[8][2])
+// Rows of a merge chunk: one warp per row, a CTA per chunk of MERGE_ROWS
+// consecutive rows.  Within a chunk the final parameters of MB (r-1, c) reach
+// row r through an epoch-tagged word in shared memory (an aligned 64-bit
+// store; no fence, the parameters are the word); the chunk's last row also
+// publishes through a.sao_mail for the first row of the next chunk.  Frames
+// whose words would not fit in shared memory use a.sao_mail for every row.
+constexpr int MERGE_ROWS = kMergeRows;
+constexpr size_t MERGE_SMEM_MAX = 160 * 1024;
+__host__ __device__ __forceinline__ size_t merge_words_bytes(int mbw) { return (size_t)MERGE_ROWS * mbw * 8; }
+__host__ __device__ __forceinline__ bool merge_words_fit(int mbw) { return merge_words_bytes(mbw) <= MERGE_SMEM_MAX; }
+size_t merge_shared_bytes(int mbw)   // dynamic shared memory of the merge kernels
 {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const unsigned long long ep = (unsigned long long)a.epoch;
-    for (;;) {
-        int row = 0;
-        if (lane == 0) row = atomicAdd(&a.counters[1], 1);
-        row = __shfl_sync(0xffffffffu, row, 0);
-        if (row >= a.mbh) return;
-        TileRegs t;
-        tile_load(a, 0, row, lane, t);
-        tile_store(tiles[w][0], lane, t);
-        evxg_sao_info own = ld_info_cg(&a.sao[row * a.mbw]);
-        float own_cost = __ldcg(&a.sao_cost[row * a.mbw]);
-        evxg_sao_info left{};
-        for (int c = 0; c < a.mbw; c++) {
-            const int m = row * a.mbw + c;
-            evxg_sao_info info = own;   // own RDO parameters, prefetched
-            float cur = own_cost;
-            if (c + 1 < a.mbw) {        // next MB's data is in flight while this one waits
-                tile_load(a, c + 1, row, lane, t);
-                own = ld_info_cg(&a.sao[m + 1]);
-                own_cost = __ldcg(&a.sao_cost[m + 1]);
-            }
-            unsigned long long above = 0;
-            if (row > 0) {   // bounded wait for the final parameters of (r-1, c)
-                bool ok = true;
-                if (lane == 0) {
-                    const unsigned long long t0 = globaltimer_ns();
-                    for (;;) {
-                        above = ld_acquire64(&a.sao_mail[m - a.mbw]);
-                        if ((above & 0xFF) == ep) break;
-                        if (*(volatile int *)a.error) { ok = false; break; }
-                        if ((long long)(globaltimer_ns() - t0) > a.timeout_ns) {
-                            atomicCAS(a.error, 0, EVXG_ERROR_OPERATION_TIMEDOUT);
-                            ok = false;
-                            break;
-                        }
-                    }
-                }
-                if (!__shfl_sync(0xffffffffu, ok, 0)) return;
-                above = __shfl_sync(0xffffffffu, above, 0);
-            }
-            __syncwarp();
-            const MergeTile &mt = tiles[w][c & 1];
-            if (c > 0 && left.luma.type != 0) {
-                const float mc = __fadd_rn(__ll2float_rn(tile_sao_ssd(a, mt, c, row, lane, left.luma)), __fmul_rn(a.lambda, 1.0f));
-                if (mc < cur) { info.merge_left = 1; info.luma = left.luma; info.chroma = left.chroma; cur = mc; }
-            }
-            if (!info.merge_left && row > 0) {
-                const evxg_sao_params al = unpack_params(above >> 8), ac = unpack_params(above >> 33);
-                if (al.type != 0) {
-                    const float mc = __fadd_rn(__ll2float_rn(tile_sao_ssd(a, mt, c, row, lane, al)), __fmul_rn(a.lambda, 1.0f));
-                    if (mc < cur) { info.merge_above = 1; info.luma = al; info.chroma = ac; }
-                }
-            }
-            left = info;
-            if (lane == 0) {
-                *reinterpret_cast<uint4 *>(&a.sao[m]) = *reinterpret_cast<const uint4 *>(&info);
-                st_release64(&a.sao_mail[m], ep | (pack_params(info.luma) << 8) | (pack_params(info.chroma) << 33));
-            }
-            __syncwarp();
-            if (c + 1 < a.mbw) tile_store(tiles[w][(c + 1) & 1], lane, t);
+    return MERGE_ROWS * 2 * sizeof(MergeTile) + (merge_words_fit(mbw) ? merge_words_bytes(mbw) : 0);
+}
+
+// Bounded wait of lane 0 for a tagged word; the shared-memory form polls
+// cheaply and looks at the error word and the clock every 256 polls.
+template <bool kShared>
+__device__ __forceinline__ bool wait_word(const FrameArgs &a, const unsigned long long *p, unsigned long long ep,
+                                          unsigned long long &v)
+{
+    const unsigned long long t0 = globaltimer_ns();
+    for (unsigned it = 0;; it++) {
+        v = kShared ? *(const volatile unsigned long long *)p : ld_acquire64(p);
+        if ((v & 0xFF) == ep) return true;
+        if (kShared && (it & 255) != 255) continue;
+        if (*(volatile int *)a.error) return false;
+        if ((long long)(globaltimer_ns() - t0) > a.timeout_ns) {
+            atomicCAS(a.error, 0, EVXG_ERROR_OPERATION_TIMEDOUT);
+            return false;
         }
     }
 }
-__global__ void __launch_bounds__(256) k_sao_merge(FrameArgs a)
+
+// One row of merge decisions (sao.cpp:559-586); false once a wait gave up.
+__device__ bool merge_row(const FrameArgs &a, MergeTile *tiles, unsigned long long *words, int w, int row)
 {
-    __shared__ MergeTile tiles[8][2];
-    sao_merge_body(a, tiles);
+    const int lane = threadIdx.x & 31;
+    const unsigned long long ep = (unsigned long long)a.epoch;
+    TileRegs t;
+    tile_load(a, 0, row, lane, t);
+    tile_store(tiles[0], lane, t);
+    evxg_sao_info own = ld_info_cg(&a.sao[row * a.mbw]);
+    float own_cost = __ldcg(&a.sao_cost[row * a.mbw]);
+    evxg_sao_info left{};
+    const bool from_shared = words && w > 0, to_global = !words || w == MERGE_ROWS - 1;
+    for (int c = 0; c < a.mbw; c++) {
+        const int m = row * a.mbw + c;
+        evxg_sao_info info = own;   // own RDO parameters, prefetched
+        float cur = own_cost;
+        if (c + 1 < a.mbw) {        // next MB's data is in flight while this one waits
+            tile_load(a, c + 1, row, lane, t);
+            own = ld_info_cg(&a.sao[m + 1]);
+            own_cost = __ldcg(&a.sao_cost[m + 1]);
+        }
+        unsigned long long above = 0;
+        if (row > 0) {   // bounded wait for the final parameters of (r-1, c)
+            bool ok = true;
+            if (lane == 0)
+                ok = from_shared ? wait_word<true>(a, &words[(w - 1) * a.mbw + c], ep, above)
+                                 : wait_word<false>(a, &a.sao_mail[m - a.mbw], ep, above);
+            if (!__shfl_sync(0xffffffffu, ok, 0)) return false;
+            above = __shfl_sync(0xffffffffu, above, 0);
+        }
+        __syncwarp();
+        const MergeTile &mt = tiles[c & 1];
+        if (c > 0 && left.luma.type != 0) {
+            const float mc = __fadd_rn(__ll2float_rn(tile_sao_ssd(a, mt, c, row, lane, left.luma)), __fmul_rn(a.lambda, 1.0f));
+            if (mc < cur) { info.merge_left = 1; info.luma = left.luma; info.chroma = left.chroma; cur = mc; }
+        }
+        if (!info.merge_left && row > 0) {
+            const evxg_sao_params al = unpack_params(above >> 8), ac = unpack_params(above >> 33);
+            if (al.type != 0) {
+                const float mc = __fadd_rn(__ll2float_rn(tile_sao_ssd(a, mt, c, row, lane, al)), __fmul_rn(a.lambda, 1.0f));
+                if (mc < cur) { info.merge_above = 1; info.luma = al; info.chroma = ac; }
+            }
+        }
+        left = info;
+        if (lane == 0) {
+            const unsigned long long word = ep | (pack_params(info.luma) << 8) | (pack_params(info.chroma) << 33);
+            *reinterpret_cast<uint4 *>(&a.sao[m]) = *reinterpret_cast<const uint4 *>(&info);
+            if (words) *(volatile unsigned long long *)&words[w * a.mbw + c] = word;
+            if (to_global) st_release64(&a.sao_mail[m], word);
+        }
+        __syncwarp();
+        if (c + 1 < a.mbw) tile_store(tiles[(c + 1) & 1], lane, t);
+    }
+    return true;
 }
-__global__ void __launch_bounds__(256) k_sao_merge_b(const FrameArgs *args)
+
+__device__ __forceinline__ void sao_merge_body(const FrameArgs &a, unsigned char *dsm)
 {
-    __shared__ MergeTile tiles[8][2];
+    __shared__ int s_chunk;
+    MergeTile *tiles = reinterpret_cast<MergeTile *>(dsm);
+    unsigned long long *words =
+        merge_words_fit(a.mbw) ? reinterpret_cast<unsigned long long *>(dsm + MERGE_ROWS * 2 * sizeof(MergeTile)) : nullptr;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    bool alive = true;
+    for (;;) {
+        if (threadIdx.x == 0) s_chunk = atomicAdd(&a.counters[1], 1);
+        if (words)
+            for (int c = lane; c < a.mbw; c += 32) words[w * a.mbw + c] = 0;   // epoch 0 never matches
+        __syncthreads();
+        const int chunk = s_chunk;
+        if (chunk * MERGE_ROWS >= a.mbh) return;
+        const int row = chunk * MERGE_ROWS + w;
+        // after a failed wait the warp only keeps meeting the barriers; the
+        // rows waiting on it give up through the error word
+        if (alive && row < a.mbh) alive = merge_row(a, tiles + 2 * w, words, w, row);
+        __syncthreads();
+    }
+}
+__global__ void __launch_bounds__(32 * MERGE_ROWS) k_sao_merge(FrameArgs a)
+{
+    extern __shared__ __align__(16) unsigned char merge_smem[];
+    sao_merge_body(a, merge_smem);
+}
+__global__ void __launch_bounds__(32 * MERGE_ROWS) k_sao_merge_b(const FrameArgs *args)
+{
+    extern __shared__ __align__(16) unsigned char merge_smem[];
     __shared__ FrameArgs sa;
-    if (const FrameArgs *a = batch_args(args, sa)) sao_merge_body(*a, tiles);
+    if (const FrameArgs *a = batch_args(args, sa)) sao_merge_body(*a, merge_smem);
 }
 
 // ---- application (sao.cpp:99-146) ----

@@ -34,6 +34,9 @@ __global__ void k_sao_copy_b(const FrameArgs *args);
 __global__ void k_tick_post_b(const FrameArgs *args);
 size_t mb_shared_bytes();
 int mb_threads();
+size_t merge_shared_bytes(int mbw);   // dynamic shared memory of k_sao_merge(_b) for a frame mbw MBs wide
+constexpr int kMergeRows = 16;       // MB rows per CTA of the merge kernels (one warp each)
+size_t deblock_shared_bytes(int W);   // dynamic shared memory of k_deblock(_b) for an aligned width W
 
 // Fixed-point passes of the SAO application (evxg_filters.cu); the chains they
 // resolve are a few pixels long, the last pass only confirms.
