@@ -246,13 +246,13 @@ int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, con
     else
         k_mb_wavefront<<<s->mb_grid, mb_threads(), mb_shared_bytes(), st>>>(a);
     mark(2);
-    k_deblock<<<3, 1024, deblock_shared_bytes((int)s->W), st>>>(a);
+    k_deblock<<<kDeblockCtas, kDeblockThreads, deblock_shared_bytes((int)s->W), st>>>(a);
     mark(3);
     CK(cudaMemcpyAsync(s->sao_orig, s->dpb[f->dpb_slot], s->plane_elems * sizeof(int16_t), cudaMemcpyDeviceToDevice, st));
     CK(cudaMemsetAsync(s->sao_flags, 0, kSaoPasses * sizeof(int), st));
     k_sao_rdo<<<(unsigned)((nblk + 7) / 8), 256, 0, st>>>(a);   // one warp per MB
     mark(4);
-    k_sao_merge<<<(s->mbh + kMergeRows - 1) / kMergeRows, 32 * kMergeRows, merge_shared_bytes((int)s->mbw), st>>>(a);
+    k_sao_merge<<<kMergeCtas, kMergeThreads, merge_shared_bytes((int)s->mbw, (int)s->mbh), st>>>(a);
     mark(5);
     for (int p = 0; p < kSaoPasses; p++) k_sao_fix<<<s->num_sms * 8, 256, 0, st>>>(a, p);
     k_sao_restore<<<s->num_sms * 4, 256, 0, st>>>(a, kSaoPasses - 1);

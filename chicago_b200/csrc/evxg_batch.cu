@@ -85,7 +85,7 @@ static int enqueue_tick(evxg_batch *b, int parity, cudaStream_t cs)
 {
     evxg_batch::Side &sd = b->side[parity];
     const unsigned n = (unsigned)b->st.size();
-    unsigned cvx = 1, cvy = 1, rdo = 1, wf = 1, mchunks = 1;
+    unsigned cvx = 1, cvy = 1, rdo = 1, wf = 1;
     size_t msmem = 0, dsmem = 0;
     for (const evxg_stream *s : b->st) {
         const unsigned cw = std::min(s->vw, s->W), ch = std::min(s->vh, s->H);
@@ -93,8 +93,7 @@ static int enqueue_tick(evxg_batch *b, int parity, cudaStream_t cs)
         cvy = std::max(cvy, ch / 2);
         rdo = std::max(rdo, (s->mbw * s->mbh + 7) / 8);   // one warp per MB, 8 per block
         wf = std::max(wf, (s->mbh + 7) / 8);
-        mchunks = std::max(mchunks, (s->mbh + kMergeRows - 1) / kMergeRows);
-        msmem = std::max(msmem, merge_shared_bytes((int)s->mbw));
+        msmem = std::max(msmem, merge_shared_bytes((int)s->mbw, (int)s->mbh));
         dsmem = std::max(dsmem, deblock_shared_bytes((int)s->W));
     }
     const unsigned share = std::max(8u, (unsigned)b->num_sms * 8 / n);
@@ -111,10 +110,10 @@ static int enqueue_tick(evxg_batch *b, int parity, cudaStream_t cs)
         k_mb_cluster_b<<<3 * b->grid, mb_threads(), mb_shared_bytes(), cs>>>(b->d_args, items, qlen, b->d_ctl);
     else
         k_mb_wavefront_b<<<b->grid, mb_threads(), mb_shared_bytes(), cs>>>(b->d_args, items, qlen, b->d_ctl);
-    k_deblock_b<<<dim3(3, 1, n), 1024, dsmem, cs>>>(b->d_args);
+    k_deblock_b<<<dim3(kDeblockCtas, 1, n), kDeblockThreads, dsmem, cs>>>(b->d_args);
     k_sao_copy_b<<<dim3(share / 2, 1, n), 256, 0, cs>>>(b->d_args);
     k_sao_rdo_b<<<dim3(rdo, 1, n), 256, 0, cs>>>(b->d_args);
-    k_sao_merge_b<<<dim3(mchunks, 1, n), 32 * kMergeRows, msmem, cs>>>(b->d_args);
+    k_sao_merge_b<<<dim3(kMergeCtas, 1, n), kMergeThreads, msmem, cs>>>(b->d_args);
     for (int p = 0; p < kSaoPasses; p++) k_sao_fix_b<<<dim3(share, 1, n), 256, 0, cs>>>(b->d_args, p);
     k_sao_restore_b<<<dim3(share / 2, 1, n), 256, 0, cs>>>(b->d_args, kSaoPasses - 1);
     k_sao_apply_b<<<dim3(wf, 1, n), 256, 0, cs>>>(b->d_args, kSaoPasses - 1);

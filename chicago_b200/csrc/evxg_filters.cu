@@ -108,9 +108,8 @@ __device__ __forceinline__ void filter_line(int16_t *e, int step, int qe, int st
 // edge (x, j) only reads columns written by horizontal edges (x-8, j) and
 // (x, j), so running all horizontal edges of the band and then all vertical
 // edges gives the same samples; bands stay in order.
-__device__ __forceinline__ void deblock_body(const FrameArgs &a)
+__device__ __forceinline__ void deblock_body(const FrameArgs &a, int pl)
 {
-    const int pl = blockIdx.x;
     const bool luma = pl == 0;
     const int w = luma ? a.W : a.W / 2, h = luma ? a.H : a.H / 2;
     const int mbs = luma ? 16 : 8, qoff = luma ? 0 : 2;
@@ -137,92 +136,144 @@ __device__ __forceinline__ void deblock_body(const FrameArgs &a)
         __syncthreads();
     }
 }
-// The same order on a window of the plane in shared memory: a circular
-// buffer of DB_SLOTS rows.  The next band's rows are read into registers
-// while the current band is filtered; a row goes back to memory once no later
-// edge touches it -- after band j every row up to j+4 is final (later
-// horizontal edges start at row j+8-3, vertical ones at row j+8).  The slots
-// the next band takes held rows that were written back at least a band ago.
-constexpr int DB_SLOTS = 24, DB_PF = 4;   // window rows; chunks of the next band per thread (1024 threads)
+// The same order on eight column strips per plane, one CTA each, in one
+// cluster.  A strip keeps its columns of the plane in a circular window of
+// DB_SLOTS rows in shared memory; the next band's rows are read into
+// registers while the current band is filtered, and a row goes back to memory
+// once no later edge touches it -- after band j every row up to j+4 is final
+// (later horizontal edges start at row j+8-3, vertical ones at row j+8).  The
+// slots the next band takes held rows written back at least a band ago.
+// Horizontal edges touch only their own columns.  A strip owns the vertical
+// edges at its columns; the first of them reads and writes the four columns
+// left of the strip, which live in the window of the strip that holds them,
+// through distributed shared memory.  Cluster barriers give the band's order:
+// every strip's horizontal edges, then every strip's vertical edges, then the
+// next band.
+constexpr int DB_SLOTS = 24, DB_STRIPS = 8, DB_THREADS = 256;
+constexpr int DB_MAXW = 2048;   // widest strip (columns) that goes through shared memory
 __device__ __forceinline__ int db_slot(int r) { return (r + DB_SLOTS) % DB_SLOTS; }
-__device__ void deblock_smem_body(const FrameArgs &a, int16_t *buf)
+__host__ __device__ __forceinline__ int db_x0(int w, int s) { return ((s * (w / 8)) / DB_STRIPS) * 8; }
+__host__ __device__ __forceinline__ bool deblock_fits(int W) { return db_x0(W, 1) <= DB_MAXW && W - db_x0(W, DB_STRIPS - 1) <= DB_MAXW; }
+size_t deblock_shared_bytes(int W)   // the luma plane has the widest strips
 {
-    const int pl = blockIdx.x;
+    int wmax = 0;
+    for (int s = 0; s < DB_STRIPS; s++) wmax = max(wmax, (s + 1 < DB_STRIPS ? db_x0(W, s + 1) : W) - db_x0(W, s));
+    return deblock_fits(W) ? (size_t)DB_SLOTS * wmax * sizeof(int16_t) : 0;
+}
+__device__ __forceinline__ unsigned db_rank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void db_cluster_barrier()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ int16_t *db_peer(int16_t *p, unsigned rank)
+{
+    int16_t *r;
+    asm volatile("mapa.u64 %0, %1, %2;" : "=l"(r) : "l"(p), "r"(rank));
+    return r;
+}
+__device__ void deblock_strip_body(const FrameArgs &a, int16_t *buf)
+{
+    const int pl = blockIdx.x / DB_STRIPS, sid = (int)db_rank();
     const bool luma = pl == 0;
     const int w = luma ? a.W : a.W / 2, h = luma ? a.H : a.H / 2;
     const int mbs = luma ? 16 : 8, qoff = luma ? 0 : 2;
     int16_t *d = a.planes[a.dpb] + (pl == 0 ? 0 : (size_t)a.W * a.H + (pl - 1) * (size_t)(a.W / 2) * (a.H / 2));
-    const int nv = (w / 8 - 1) * 8, cpr = w / 8;   // vertical edge lines per band, 16-byte chunks per row
+    const int xs = db_x0(w, sid), xe = sid + 1 < DB_STRIPS ? db_x0(w, sid + 1) : w;
+    const int sw = xe - xs, cpr = sw / 8;   // strip width, 16-byte chunks per strip row
+    // the strip holding columns xs-4 .. xs-1 (strips are multiples of 8 wide; empty ones hold nothing)
+    int ls = sid - 1;
+    while (ls >= 0 && db_x0(w, ls) >= xs) ls--;
+    int16_t *lbuf = nullptr;
+    int lw = 0, lx = 0;
+    if (ls >= 0 && sw > 0) {
+        lx = db_x0(w, ls);
+        lw = db_x0(w, ls + 1) - lx;
+        lbuf = db_peer(buf, (unsigned)ls);
+    }
+    const int nvx = sw / 8 - (xs == 0 ? 1 : 0);   // vertical edges owned: x = xs (if > 0), xs + 8, ...
+    const int xv0 = xs == 0 ? 8 : xs;
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int i = tid; i < 8 * cpr; i += nt) {   // band 0
         const int r = i / cpr, c = i % cpr;
-        *reinterpret_cast<uint4 *>(buf + db_slot(r) * w + 8 * c) = __ldcg(reinterpret_cast<const uint4 *>(d + (size_t)r * w + 8 * c));
+        *reinterpret_cast<uint4 *>(buf + db_slot(r) * sw + 8 * c) = __ldcg(reinterpret_cast<const uint4 *>(d + (size_t)r * w + xs + 8 * c));
     }
-    __syncthreads();
-    int written = 0;   // rows [0, written) are back in the slot
+    db_cluster_barrier();
+    int written = 0;   // rows [0, written) of the strip are back in the slot
     for (int j = 0; j < h; j += 8) {
         const bool more = j + 8 < h;
-        uint4 pf[DB_PF];
+        constexpr int PF = DB_MAXW / DB_THREADS;   // next band: at most 8 rows x 256 chunks
+        uint4 pf[PF];
 #pragma unroll
-        for (int k = 0; k < DB_PF; k++) {
+        for (int k = 0; k < PF; k++) {
             const int i = tid + k * nt;
             if (more && i < 8 * cpr)
-                pf[k] = __ldcg(reinterpret_cast<const uint4 *>(d + (size_t)(j + 8 + i / cpr) * w + 8 * (i % cpr)));
+                pf[k] = __ldcg(reinterpret_cast<const uint4 *>(d + (size_t)(j + 8 + i / cpr) * w + xs + 8 * (i % cpr)));
         }
-        if (j > 0) {   // horizontal edges at row j
+        if (j > 0) {   // horizontal edges at row j, own columns
             const int brow = (j / mbs) * a.mbw, arow = ((j - 1) / mbs) * a.mbw;
             int ro[8];
 #pragma unroll
-            for (int k = 0; k < 8; k++) ro[k] = db_slot(j - 4 + k) * w;
-            for (int x = tid; x < w; x += nt) {
+            for (int k = 0; k < 8; k++) ro[k] = db_slot(j - 4 + k) * sw;
+            for (int c = tid; c < sw; c += nt) {
+                const int x = xs + c;
                 int qe, st;
                 edge_params(a.bt, x / mbs + arow, x / mbs + brow, qoff, qe, st);
-                if (st) filter_taps([&](int k) -> int16_t & { return buf[ro[k + 4] + x]; }, qe, st, luma);
+                if (st) filter_taps([&](int k) -> int16_t & { return buf[ro[k + 4] + c]; }, qe, st, luma);
             }
-            __syncthreads();
+            db_cluster_barrier();
         }
         const int brow = (j / mbs) * a.mbw;
-        for (int t = tid; t < nv; t += nt) {   // vertical edges of the band
-            const int x = ((t >> 3) + 1) * 8, y = j + (t & 7);
+        for (int t = tid; t < nvx * 8; t += nt) {   // vertical edges of the band, own
+            const int x = xv0 + (t >> 3) * 8, y = j + (t & 7), c = x - xs;
             int qe, st;
             edge_params(a.bt, (x - 1) / mbs + brow, x / mbs + brow, qoff, qe, st);
-            if (st) filter_line(buf + db_slot(y) * w + x, 1, qe, st, luma);
+            if (!st) continue;
+            int16_t *row = buf + db_slot(y) * sw;
+            if (c >= 4) {
+                filter_line(row + c, 1, qe, st, luma);
+            } else {   // the strip's first edge: its left taps are in the strip holding them
+                int16_t *lrow = lbuf + db_slot(y) * lw + (xs - lx);
+                filter_taps([&](int k) -> int16_t & { return k < 0 ? lrow[k] : row[c + k]; }, qe, st, luma);
+            }
         }
-        __syncthreads();
+        db_cluster_barrier();
         const int upto = more ? j + 5 : h;
         for (int i = tid; i < (upto - written) * cpr; i += nt) {
             const int r = written + i / cpr, c = i % cpr;
-            *reinterpret_cast<uint4 *>(d + (size_t)r * w + 8 * c) = *reinterpret_cast<const uint4 *>(buf + db_slot(r) * w + 8 * c);
+            *reinterpret_cast<uint4 *>(d + (size_t)r * w + xs + 8 * c) = *reinterpret_cast<const uint4 *>(buf + db_slot(r) * sw + 8 * c);
         }
         written = upto;
 #pragma unroll
-        for (int k = 0; k < DB_PF; k++) {
+        for (int k = 0; k < PF; k++) {
             const int i = tid + k * nt;
-            if (more && i < 8 * cpr) *reinterpret_cast<uint4 *>(buf + db_slot(j + 8 + i / cpr) * w + 8 * (i % cpr)) = pf[k];
+            if (more && i < 8 * cpr) *reinterpret_cast<uint4 *>(buf + db_slot(j + 8 + i / cpr) * sw + 8 * (i % cpr)) = pf[k];
         }
         __syncthreads();
     }
+    db_cluster_barrier();   // no strip leaves while a neighbour may still use its window
 }
-// Planes up to 4096 samples wide go through shared memory (24 rows, at most
-// 192 KB; the next band is at most 4 chunks per thread); wider ones filter in
-// place in memory.
-__host__ __device__ __forceinline__ bool deblock_fits(int W) { return W <= 4096; }
-size_t deblock_shared_bytes(int W) { return deblock_fits(W) ? (size_t)DB_SLOTS * W * sizeof(int16_t) : 0; }
-__device__ __forceinline__ void deblock_dispatch(const FrameArgs &a, int16_t *buf)
-{
-    if (deblock_fits(a.W)) deblock_smem_body(a, buf);
-    else deblock_body(a);
-}
-__global__ void __launch_bounds__(1024) k_deblock(FrameArgs a)
+__global__ void __cluster_dims__(DB_STRIPS, 1, 1) __launch_bounds__(DB_THREADS) k_deblock(FrameArgs a)
 {
     extern __shared__ __align__(16) int16_t db_smem[];
-    deblock_dispatch(a, db_smem);
+    if (deblock_fits(a.W)) {
+        deblock_strip_body(a, db_smem);
+    } else if (blockIdx.x % DB_STRIPS == 0) {   // very wide planes: one CTA per plane, in place in memory
+        deblock_body(a, blockIdx.x / DB_STRIPS);
+    }
 }
-__global__ void __launch_bounds__(1024) k_deblock_b(const FrameArgs *args)
+__global__ void __cluster_dims__(DB_STRIPS, 1, 1) __launch_bounds__(DB_THREADS) k_deblock_b(const FrameArgs *args)
 {
     extern __shared__ __align__(16) int16_t db_smem[];
     __shared__ FrameArgs sa;
-    if (const FrameArgs *a = batch_args(args, sa)) deblock_dispatch(*a, db_smem);
+    const FrameArgs *a = batch_args(args, sa);   // a cluster is one stream and plane: active or not for all its CTAs
+    if (!a) return;
+    if (deblock_fits(a->W)) deblock_strip_body(*a, db_smem);
+    else if (blockIdx.x % DB_STRIPS == 0) deblock_body(*a, blockIdx.x / DB_STRIPS);
 }
 
 // ------------------------------------------------------------------ SAO
@@ -536,29 +587,51 @@ __device__ __forceinline__ void tile_store(MergeTile &m, int lane, const TileReg
     for (int i = 0; i < 4; i++) reinterpret_cast<unsigned *>(m.src)[lane + 32 * i] = t.s[i];
 }
 // Luma SSD of the tile's MB under p, one warp (sao.cpp:346-387 without the rate).
-__device__ long long tile_sao_ssd(const FrameArgs &a, const MergeTile &m, int c, int row, int lane, const evxg_sao_params &p)
+// Luma SSD of the tile's MB under p, one warp (sao.cpp:346-387 without the
+// rate).  The parameters are unpacked into registers and the band / edge
+// branch is taken once per call, not per pixel.
+__device__ __forceinline__ int pick4(int k, int o0, int o1, int o2, int o3) { return k == 0 ? o0 : k == 1 ? o1 : k == 2 ? o2 : o3; }
+__device__ __noinline__ long long tile_sao_ssd(const FrameArgs &a, const MergeTile &m, int c, int row, int lane,
+                                               evxg_sao_params p)
 {
     const int ty = lane >> 1, tx0 = (lane & 1) * 8;
-    const int y = row * 16 + ty;
+    const int y = row * 16 + ty, x0 = c * 16 + tx0;
+    const int o0 = p.offsets[0], o1 = p.offsets[1], o2 = p.offsets[2], o3 = p.offsets[3];
+    const int16_t *rr = m.rec + (ty + 1) * MT_W + tx0 + 2;
+    const int16_t *sr = m.src + ty * 16 + tx0;
     long long acc = 0;
+    if (p.type == 2) {
+        const int bp = p.band_position;
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-        const int tx = tx0 + i, x = c * 16 + tx;
-        const int v = m.rec[(ty + 1) * MT_W + tx + 2];
-        int corr = v;
-        if (p.type == 2) {
-            const int idx = (sclamp(v) >> 3) - p.band_position;
-            if (idx >= 0 && idx < 4) corr = sclamp(v + p.offsets[idx]);
-        } else if (p.type == 1) {
-            const int dxa = c_eo[p.eo_class][0], dya = c_eo[p.eo_class][1], dxb = c_eo[p.eo_class][2], dyb = c_eo[p.eo_class][3];
-            const int ax = x + dxa, ay = y + dya, bx = x + dxb, by = y + dyb;
-            if (ax >= 0 && ax < a.W && ay >= 0 && ay < a.H && bx >= 0 && bx < a.W && by >= 0 && by < a.H) {
-                const int ct = eo_cat(v, m.rec[(ty + 1 + dya) * MT_W + tx + 2 + dxa], m.rec[(ty + 1 + dyb) * MT_W + tx + 2 + dxb]);
-                if (ct < 4) corr = sclamp(v + p.offsets[ct]);
-            }
+        for (int i = 0; i < 8; i++) {
+            const int v = rr[i], idx = (sclamp(v) >> 3) - bp;
+            const int corr = (idx >= 0 && idx < 4) ? sclamp(v + pick4(idx, o0, o1, o2, o3)) : v;
+            const int d = sr[i] - corr;
+            acc += (long long)(d * d);
         }
-        const int d = m.src[ty * 16 + tx] - corr;
-        acc += (long long)(d * d);
+    } else if (p.type == 1) {
+        const int ec = p.eo_class;
+        const int dxa = ec == 1 ? 0 : (ec == 3 ? 1 : -1), dya = ec == 0 ? 0 : -1;   // c_eo (sao.cpp:20-25)
+        const int dxb = -dxa, dyb = -dya;
+        const bool rows_ok = y + dya >= 0 && y + dya < a.H && y + dyb >= 0 && y + dyb < a.H;
+        const int da = dya * MT_W + dxa, db = dyb * MT_W + dxb;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int v = rr[i], x = x0 + i;
+            int corr = v;
+            if (rows_ok && x + dxa >= 0 && x + dxa < a.W && x + dxb >= 0 && x + dxb < a.W) {
+                const int ct = eo_cat(v, rr[i + da], rr[i + db]);
+                if (ct < 4) corr = sclamp(v + pick4(ct, o0, o1, o2, o3));
+            }
+            const int d = sr[i] - corr;
+            acc += (long long)(d * d);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int d = sr[i] - rr[i];
+            acc += (long long)(d * d);
+        }
     }
     return warp_sum64(acc);
 }
@@ -588,19 +661,23 @@ __device__ __forceinline__ evxg_sao_params unpack_params(unsigned long long v)
     return p;
 }
 
-// Rows of a merge chunk: one warp per row, a CTA per chunk of MERGE_ROWS
-// consecutive rows.  Within a chunk the final parameters of MB (r-1, c) reach
-// row r through an epoch-tagged word in shared memory (an aligned 64-bit
-// store; no fence, the parameters are the word); the chunk's last row also
-// publishes through a.sao_mail for the first row of the next chunk.  Frames
-// whose words would not fit in shared memory use a.sao_mail for every row.
-constexpr int MERGE_ROWS = kMergeRows;
+// Merge wavefront on one cluster of MERGE_CTAS CTAs per frame: CTA k takes
+// the k-th block of rpc = ceil(rows / MERGE_CTAS) consecutive rows, one warp
+// per row (a warp takes a second row of its block if the block has more rows
+// than warps).  The final parameters of MB (r-1, c) reach row r through an
+// epoch-tagged word in shared memory -- an aligned 64-bit store, with no
+// fence: the parameters are the word -- and at a block boundary the last
+// row stores its words straight into the next CTA's shared memory, so no
+// hand-over goes through global memory.  Frames whose words would not fit
+// use a.sao_mail for every row.
+constexpr int MERGE_CTAS = kMergeCtas, MERGE_WARPS = kMergeThreads / 32;
 constexpr size_t MERGE_SMEM_MAX = 160 * 1024;
-__host__ __device__ __forceinline__ size_t merge_words_bytes(int mbw) { return (size_t)MERGE_ROWS * mbw * 8; }
-__host__ __device__ __forceinline__ bool merge_words_fit(int mbw) { return merge_words_bytes(mbw) <= MERGE_SMEM_MAX; }
-size_t merge_shared_bytes(int mbw)   // dynamic shared memory of the merge kernels
+__host__ __device__ __forceinline__ int merge_rpc(int mbh) { return (mbh + MERGE_CTAS - 1) / MERGE_CTAS; }
+__host__ __device__ __forceinline__ size_t merge_words_bytes(int mbw, int mbh) { return (size_t)(merge_rpc(mbh) + 1) * mbw * 8; }
+__host__ __device__ __forceinline__ bool merge_words_fit(int mbw, int mbh) { return merge_words_bytes(mbw, mbh) <= MERGE_SMEM_MAX; }
+size_t merge_shared_bytes(int mbw, int mbh)   // dynamic shared memory of the merge kernels
 {
-    return MERGE_ROWS * 2 * sizeof(MergeTile) + (merge_words_fit(mbw) ? merge_words_bytes(mbw) : 0);
+    return MERGE_WARPS * 2 * sizeof(MergeTile) + (merge_words_fit(mbw, mbh) ? merge_words_bytes(mbw, mbh) : 0);
 }
 
 // Bounded wait of lane 0 for a tagged word; the shared-memory form polls
@@ -623,7 +700,11 @@ __device__ __forceinline__ bool wait_word(const FrameArgs &a, const unsigned lon
 }
 
 // One row of merge decisions (sao.cpp:559-586); false once a wait gave up.
-__device__ bool merge_row(const FrameArgs &a, MergeTile *tiles, unsigned long long *words, int w, int row)
+// With shared words: above = this CTA's word row i (row i-1 of the block, or
+// for i = 0 the previous block's last row), own = word row i+1, and next (if
+// not null) the next CTA's word row 0.
+__device__ bool merge_row(const FrameArgs &a, MergeTile *tiles, unsigned long long *words, unsigned long long *next,
+                          int i, int row)
 {
     const int lane = threadIdx.x & 31;
     const unsigned long long ep = (unsigned long long)a.epoch;
@@ -633,7 +714,6 @@ __device__ bool merge_row(const FrameArgs &a, MergeTile *tiles, unsigned long lo
     evxg_sao_info own = ld_info_cg(&a.sao[row * a.mbw]);
     float own_cost = __ldcg(&a.sao_cost[row * a.mbw]);
     evxg_sao_info left{};
-    const bool from_shared = words && w > 0, to_global = !words || w == MERGE_ROWS - 1;
     for (int c = 0; c < a.mbw; c++) {
         const int m = row * a.mbw + c;
         evxg_sao_info info = own;   // own RDO parameters, prefetched
@@ -647,8 +727,8 @@ __device__ bool merge_row(const FrameArgs &a, MergeTile *tiles, unsigned long lo
         if (row > 0) {   // bounded wait for the final parameters of (r-1, c)
             bool ok = true;
             if (lane == 0)
-                ok = from_shared ? wait_word<true>(a, &words[(w - 1) * a.mbw + c], ep, above)
-                                 : wait_word<false>(a, &a.sao_mail[m - a.mbw], ep, above);
+                ok = words ? wait_word<true>(a, &words[i * a.mbw + c], ep, above)
+                           : wait_word<false>(a, &a.sao_mail[m - a.mbw], ep, above);
             if (!__shfl_sync(0xffffffffu, ok, 0)) return false;
             above = __shfl_sync(0xffffffffu, above, 0);
         }
@@ -669,8 +749,12 @@ __device__ bool merge_row(const FrameArgs &a, MergeTile *tiles, unsigned long lo
         if (lane == 0) {
             const unsigned long long word = ep | (pack_params(info.luma) << 8) | (pack_params(info.chroma) << 33);
             *reinterpret_cast<uint4 *>(&a.sao[m]) = *reinterpret_cast<const uint4 *>(&info);
-            if (words) *(volatile unsigned long long *)&words[w * a.mbw + c] = word;
-            if (to_global) st_release64(&a.sao_mail[m], word);
+            if (words) {
+                *(volatile unsigned long long *)&words[(i + 1) * a.mbw + c] = word;
+                if (next) *(volatile unsigned long long *)&next[c] = word;
+            } else {
+                st_release64(&a.sao_mail[m], word);
+            }
         }
         __syncwarp();
         if (c + 1 < a.mbw) tile_store(tiles[(c + 1) & 1], lane, t);
@@ -678,38 +762,56 @@ __device__ bool merge_row(const FrameArgs &a, MergeTile *tiles, unsigned long lo
     return true;
 }
 
+__device__ __forceinline__ unsigned merge_rank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void merge_cluster_barrier()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+template <class T>
+__device__ __forceinline__ T *merge_peer(T *p, unsigned rank)
+{
+    T *r;
+    asm volatile("mapa.u64 %0, %1, %2;" : "=l"(r) : "l"(p), "r"(rank));
+    return r;
+}
+
+// Every CTA reaches both cluster barriers: the first makes every CTA's words
+// zero (epoch 0 never matches) before a peer may write into them, the last
+// keeps every CTA alive while a peer may still write into it.
 __device__ __forceinline__ void sao_merge_body(const FrameArgs &a, unsigned char *dsm)
 {
-    __shared__ int s_chunk;
+    const unsigned k = merge_rank();
+    const int w = threadIdx.x >> 5;
+    const int rpc = merge_rpc(a.mbh), r0 = (int)k * rpc, rows = max(0, min(rpc, a.mbh - r0));
     MergeTile *tiles = reinterpret_cast<MergeTile *>(dsm);
     unsigned long long *words =
-        merge_words_fit(a.mbw) ? reinterpret_cast<unsigned long long *>(dsm + MERGE_ROWS * 2 * sizeof(MergeTile)) : nullptr;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        merge_words_fit(a.mbw, a.mbh) ? reinterpret_cast<unsigned long long *>(dsm + MERGE_WARPS * 2 * sizeof(MergeTile)) : nullptr;
+    if (words)
+        for (int e = threadIdx.x; e < (rpc + 1) * a.mbw; e += blockDim.x) words[e] = 0;
+    merge_cluster_barrier();
+    unsigned long long *next = nullptr;
+    if (words && r0 + rpc < a.mbh) next = merge_peer(words, k + 1);   // the next block's word row 0
     bool alive = true;
-    for (;;) {
-        if (threadIdx.x == 0) s_chunk = atomicAdd(&a.counters[1], 1);
-        if (words)
-            for (int c = lane; c < a.mbw; c += 32) words[w * a.mbw + c] = 0;   // epoch 0 never matches
-        __syncthreads();
-        const int chunk = s_chunk;
-        if (chunk * MERGE_ROWS >= a.mbh) return;
-        const int row = chunk * MERGE_ROWS + w;
-        // after a failed wait the warp only keeps meeting the barriers; the
-        // rows waiting on it give up through the error word
-        if (alive && row < a.mbh) alive = merge_row(a, tiles + 2 * w, words, w, row);
-        __syncthreads();
-    }
+    for (int i = w; i < rows && alive; i += MERGE_WARPS)
+        alive = merge_row(a, tiles + 2 * w, words, i == rpc - 1 ? next : nullptr, i, r0 + i);
+    merge_cluster_barrier();
 }
-__global__ void __launch_bounds__(32 * MERGE_ROWS) k_sao_merge(FrameArgs a)
+__global__ void __cluster_dims__(MERGE_CTAS, 1, 1) __launch_bounds__(32 * MERGE_WARPS) k_sao_merge(FrameArgs a)
 {
     extern __shared__ __align__(16) unsigned char merge_smem[];
     sao_merge_body(a, merge_smem);
 }
-__global__ void __launch_bounds__(32 * MERGE_ROWS) k_sao_merge_b(const FrameArgs *args)
+__global__ void __cluster_dims__(MERGE_CTAS, 1, 1) __launch_bounds__(32 * MERGE_WARPS) k_sao_merge_b(const FrameArgs *args)
 {
     extern __shared__ __align__(16) unsigned char merge_smem[];
     __shared__ FrameArgs sa;
-    if (const FrameArgs *a = batch_args(args, sa)) sao_merge_body(*a, merge_smem);
+    const FrameArgs *a = batch_args(args, sa);   // a cluster is one stream: active or not for all its CTAs
+    if (a) sao_merge_body(*a, merge_smem);
 }
 
 // ---- application (sao.cpp:99-146) ----

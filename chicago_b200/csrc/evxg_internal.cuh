@@ -34,9 +34,10 @@ __global__ void k_sao_copy_b(const FrameArgs *args);
 __global__ void k_tick_post_b(const FrameArgs *args);
 size_t mb_shared_bytes();
 int mb_threads();
-size_t merge_shared_bytes(int mbw);   // dynamic shared memory of k_sao_merge(_b) for a frame mbw MBs wide
-constexpr int kMergeRows = 16;       // MB rows per CTA of the merge kernels (one warp each)
+size_t merge_shared_bytes(int mbw, int mbh);   // dynamic shared memory of k_sao_merge(_b) for an mbw x mbh MB frame
+constexpr int kMergeCtas = 8, kMergeThreads = 512;   // the merge kernels: one cluster of 8 CTAs per frame
 size_t deblock_shared_bytes(int W);   // dynamic shared memory of k_deblock(_b) for an aligned width W
+constexpr int kDeblockCtas = 3 * 8, kDeblockThreads = 256;   // 8 column strips (one cluster) per plane
 
 // Fixed-point passes of the SAO application (evxg_filters.cu); the chains they
 // resolve are a few pixels long, the last pass only confirms.
