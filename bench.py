@@ -53,6 +53,21 @@ def peaks():
         return HBM_PEAK_FALLBACK, "fallback"
 
 
+def max_over_ranks(ms: float, world: int, device: str = "cuda") -> float:
+    """The job's time: the slowest rank's (every rank takes part, in the same order)."""
+    if world == 1:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world: int, steps: int, ms: float) -> float:
+    """Whole-job 1080p-eq frames/s: every rank encodes its own stream of `steps` frames."""
+    return world * steps * EQ / (ms / 1e3)
+
+
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
@@ -62,9 +77,14 @@ def plan(seed_offset: int):
     return gop_plan(FRAMES, quality=QUALITY, intra_at=(CUT,))
 
 
+def rank_seed(rank: int) -> int:
+    """Every rank encodes its own stream: the same generator, its own seed."""
+    return 1000 + rank
+
+
 def frames_for(rank: int):
     from chicago_b200.synth import generate
-    return generate(W, H, FRAMES, seed=1000 + rank, vmax=VMAX, n_rects=4, cut_at=CUT)
+    return generate(W, H, FRAMES, seed=rank_seed(rank), vmax=VMAX, n_rects=4, cut_at=CUT)
 
 
 class Clocks:
@@ -166,12 +186,8 @@ def run_gpu(args):
     st.sync(sp)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * K * EQ / (total_ms / 1e3)
+    total_ms = max_over_ranks(sum(step_ms), world)
+    value = job_value(world, K, total_ms)
 
     # end to end through the C ABI: pinned host RGB in, serializer tables out
     nblk = st.mbw * st.mbh
@@ -193,12 +209,8 @@ def run_gpu(args):
         ev1.synchronize()
         if i >= args.warmup:
             e2e_ms.append(ev0.elapsed_time(ev1))
-    e2e_total = sum(e2e_ms)
-    if world > 1:
-        t = torch.tensor([e2e_total], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * K * EQ / (e2e_total / 1e3)
+    e2e_total = max_over_ranks(sum(e2e_ms), world)
+    e2e_value = job_value(world, K, e2e_total)
     h2d = W * H * 3
     d2h = nblk * 28 * 2 + nblk * 16 + st.plane_elems * 2
 
