@@ -47,10 +47,20 @@ EXPORTS = [
     "evxg_batch_create", "evxg_batch_destroy", "evxg_batch_input", "evxg_batch_encode", "evxg_batch_wait",
     "evxg_batch_output", "evxg_batch_launch_count", "evxg_batch_set_shape", "evxg_batch_get_shape",
     "evxg_batch_autotune",
+    "evxg_server_create", "evxg_server_destroy", "evxg_server_open", "evxg_server_submit", "evxg_server_insert_intra",
+    "evxg_server_close", "evxg_server_drain", "evxg_server_stats", "evxg_server_now_ns",
 ]
 MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
 
 FRAME_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
+
+
+class FrameTimes(C.Structure):
+    _fields_ = [("arrival_ns", C.c_uint64), ("ready_ns", C.c_uint64), ("launch_ns", C.c_uint64), ("done_ns", C.c_uint64)]
+
+
+RESULT_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                        C.POINTER(FrameTimes))
 
 
 class EvxgError(RuntimeError):
@@ -100,6 +110,16 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_batch_set_shape.argtypes = [vp, i32, i32, i32]
     L.evxg_batch_get_shape.argtypes = [vp] + [C.POINTER(i32)] * 3
     L.evxg_batch_autotune.argtypes = [vp, vp, C.POINTER(C.c_float)]
+    u64 = C.c_uint64
+    L.evxg_server_create.argtypes = [u64, u32, RESULT_CB, vp, C.POINTER(vp)]
+    L.evxg_server_destroy.argtypes = [vp]
+    L.evxg_server_open.argtypes = [vp, u32, u32, C.c_uint8, C.POINTER(u32)]
+    L.evxg_server_submit.argtypes = [vp, u32, vp, u64]
+    L.evxg_server_insert_intra.argtypes = [vp, u32]
+    L.evxg_server_close.argtypes = [vp, u32]
+    L.evxg_server_drain.argtypes = [vp]
+    L.evxg_server_stats.argtypes = [vp] + [C.POINTER(u64)] * 4
+    L.evxg_server_now_ns.restype = u64
     return L
 
 
@@ -278,6 +298,81 @@ class Batch:
         ms = C.c_float()
         _check(lib().evxg_batch_autotune(self.h, _ptr(cuda_stream), C.byref(ms)))
         return ms.value
+
+
+class Server:
+    """Request loop over live streams (evxg_server_*): admission by device
+    memory budget, batched ticks of whatever frames are ready, results through
+    a callback on the server's worker thread.
+
+    results[stream_id] is that stream's list of records in bitstream order:
+    frame18 and times (arrival, ready, launch, done in ns), plus the
+    serializer's tables when keep_tables is set."""
+
+    def __init__(self, hbm_budget_bytes: int, max_streams: int, keep_tables: bool = True):
+        import threading
+        self.keep_tables = keep_tables
+        self.results = {}
+        self.dims = {}
+        self._lock = threading.Lock()
+        self._cb = RESULT_CB(self._on_result)
+        h = C.c_void_p()
+        _check(lib().evxg_server_create(int(hbm_budget_bytes), int(max_streams), self._cb, None, C.byref(h)))
+        self.h = h
+
+    def _on_result(self, user, sid, frame, bt, pv, sao, lev, times):
+        t = times.contents
+        rec = {"frame18": C.string_at(frame, 18),
+               "times": (t.arrival_ns, t.ready_ns, t.launch_ns, t.done_ns)}
+        if self.keep_tables:
+            nblk, pe = self.dims[sid]
+            def arr(p, n, dt):
+                return np.ctypeslib.as_array(C.cast(p, C.POINTER(dt)), shape=(n,)).copy()
+            rec.update(blocks=arr(bt, nblk * 28, C.c_uint8), prev_blocks=arr(pv, nblk * 28, C.c_uint8),
+                       sao=arr(sao, nblk * 16, C.c_uint8), levels=arr(lev, pe, C.c_int16))
+        with self._lock:
+            self.results.setdefault(sid, []).append(rec)
+
+    def open(self, width: int, height: int, quality: int = 8) -> int:
+        sid = C.c_uint32()
+        aw, ah = (width + 15) & ~15, (height + 15) & ~15
+        _check(lib().evxg_server_open(self.h, width, height, quality, C.byref(sid)))
+        self.dims[sid.value] = ((aw // 16) * (ah // 16), aw * ah + 2 * (aw // 2) * (ah // 2))
+        self.results.setdefault(sid.value, [])
+        return sid.value
+
+    def submit(self, sid: int, rgb, arrival_ns: int = 0):
+        rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+        _check(lib().evxg_server_submit(self.h, sid, rgb.ctypes.data_as(C.c_void_p), int(arrival_ns)))
+
+    def insert_intra(self, sid: int):
+        _check(lib().evxg_server_insert_intra(self.h, sid))
+
+    def close_stream(self, sid: int):
+        _check(lib().evxg_server_close(self.h, sid))
+
+    def drain(self):
+        _check(lib().evxg_server_drain(self.h))
+
+    def stats(self) -> dict:
+        v = [C.c_uint64() for _ in range(4)]
+        _check(lib().evxg_server_stats(self.h, *[C.byref(x) for x in v]))
+        return dict(zip(("frames", "ticks", "rebuilds", "bytes_in_use"), (x.value for x in v)))
+
+    @staticmethod
+    def now_ns() -> int:
+        return lib().evxg_server_now_ns()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().evxg_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Encoder:

@@ -353,7 +353,14 @@ struct evxg_encoder {
     std::vector<evxg_block_desc> h_bt, h_prev;
     std::vector<evxg_sao_info> h_sao;
     std::vector<int16_t> h_lev;
+    // Where a frame goes once its place in encode order is known: encoded at
+    // once on the encoder's own stream, or handed to a sink (the server queues
+    // it for a batched tick; the encoder then has no stream of its own).
+    evxg::FrameSink sink = nullptr;
+    void *sink_ctx = nullptr;
 };
+
+void evxg::encoder_set_sink(evxg_encoder *e, FrameSink sink, void *ctx) { e->sink = sink; e->sink_ctx = ctx; }
 
 static const uint32_t kBFrames = 3, kIntraRate = 3600;
 static uint8_t ip_slot(uint32_t ip) { return (uint8_t)(ip % 2); }
@@ -375,6 +382,11 @@ static int encode_one(evxg_encoder *e, const uint8_t *px, const evxg_frame &f)
     return EVXG_SUCCESS;
 }
 
+static int emit(evxg_encoder *e, const uint8_t *px, const evxg_frame &f)
+{
+    return e->sink ? e->sink(e->sink_ctx, px, e->width, e->height, &f) : encode_one(e, px, f);
+}
+
 static int encode_gop(evxg_encoder *e)   // evx3enc.cpp:279-383
 {
     const uint32_t p_idx = e->reorder_count - 1;
@@ -385,7 +397,7 @@ static int encode_gop(evxg_encoder *e)   // evx3enc.cpp:279-383
     p.is_reference = 1;
     p.ref_slot_fwd = ip_slot(e->ip_index - 1);
     p.ref_slot_bwd = 0;
-    int rc = encode_one(e, e->reorder[p_idx].px.data(), p);
+    int rc = emit(e, e->reorder[p_idx].px.data(), p);
     if (rc) return rc;
     e->frame.index++;
     const uint32_t b_count = e->reorder_count - 1;
@@ -399,7 +411,7 @@ static int encode_gop(evxg_encoder *e)   // evx3enc.cpp:279-383
         b.ref_slot_fwd = ip_slot(e->ip_index - 1);
         b.ref_slot_bwd = ip_slot(e->ip_index);
         b.quality = (uint16_t)std::min<int>(e->frame.quality + 1, 31);
-        if ((rc = encode_one(e, e->reorder[ref_b].px.data(), b))) return rc;
+        if ((rc = emit(e, e->reorder[ref_b].px.data(), b))) return rc;
         e->frame.index++;
         for (uint32_t bi = 0; bi < b_count; bi++) {
             if (bi == ref_b) continue;
@@ -411,7 +423,7 @@ static int encode_gop(evxg_encoder *e)   // evx3enc.cpp:279-383
             nb.quality = (uint16_t)std::min<int>(e->frame.quality + 2, 31);
             if (bi < ref_b) { nb.ref_slot_fwd = ip_slot(e->ip_index - 1); nb.ref_slot_bwd = 2; }
             else { nb.ref_slot_fwd = 2; nb.ref_slot_bwd = ip_slot(e->ip_index); }
-            if ((rc = encode_one(e, e->reorder[bi].px.data(), nb))) return rc;
+            if ((rc = emit(e, e->reorder[bi].px.data(), nb))) return rc;
             e->frame.index++;
         }
     }
@@ -473,7 +485,11 @@ int evxg_encoder_encode(evxg_encoder *e, const uint8_t *rgb, uint32_t width, uin
 {
     if (!e || !rgb || !width || !height) return fail(EVXG_ERROR_INVALIDARG, "evxg_encoder_encode: bad argument");
     int rc;
-    if (!e->stream) {
+    if (e->sink && !e->width) {   // frames go to the sink: no stream of its own
+        e->width = width; e->height = height;
+        e->reorder_count = 0; e->display_counter = 0; e->ip_index = 0; e->first = true;
+    }
+    if (!e->stream && !e->sink) {
         if ((rc = evxg_stream_create(width, height, &e->stream))) return rc;
         e->width = width; e->height = height;
         const size_t nblk = (size_t)e->stream->mbw * e->stream->mbh;
@@ -507,7 +523,7 @@ int evxg_encoder_encode(evxg_encoder *e, const uint8_t *rgb, uint32_t width, uin
         i.is_reference = 1;
         i.ref_slot_fwd = 0;
         i.ref_slot_bwd = 0;
-        if ((rc = encode_one(e, e->reorder[0].px.data(), i))) return rc;
+        if ((rc = emit(e, e->reorder[0].px.data(), i))) return rc;
         e->ip_index++;
         e->frame.type = EVXG_FRAME_INTER;
         e->frame.index++;
@@ -531,7 +547,7 @@ int evxg_encoder_flush(evxg_encoder *e)   // evx3enc.cpp:385-414
         p.is_reference = 1;
         p.ref_slot_fwd = ip_slot(e->ip_index - 1);
         p.ref_slot_bwd = 0;
-        if ((rc = encode_one(e, e->reorder[0].px.data(), p))) return rc;
+        if ((rc = emit(e, e->reorder[0].px.data(), p))) return rc;
         e->frame.index++;
         e->ip_index++;
     } else if ((rc = encode_gop(e))) {

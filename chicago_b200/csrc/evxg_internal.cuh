@@ -81,4 +81,8 @@ namespace evxg {
 void fill_args(evxg_stream *s, const evxg_frame *f, const uint8_t *drgb, FrameArgs &a);
 // Return a stream to its state at creation: zero planes and tables, epoch 0.
 int reset_stream(evxg_stream *s, cudaStream_t st);
+// A GOP-level encoder whose frames, once their encode order is known, go to
+// sink(ctx, rgb, width, height, frame) instead of its own stream.
+typedef int (*FrameSink)(void *ctx, const uint8_t *rgb, uint32_t width, uint32_t height, const evxg_frame *f);
+void encoder_set_sink(evxg_encoder *e, FrameSink sink, void *ctx);
 }  // namespace evxg

@@ -1,0 +1,397 @@
+// evxg_serve.cu -- serving: a request loop over many live streams.
+//
+// No counterpart in the reference, which encodes one stream per
+// evx3_encoder.  Streams are admitted by a device-memory budget and keep all
+// their state (DPB slots, tables, levels, SAO state) on the device while they
+// live.  Callers submit RGB frames as they arrive; each stream's GOP logic is
+// the reference encoder's (evx3enc.cpp:105-414, the same planner evxg_encoder
+// runs), so a frame becomes ready to encode once the frames it depends on
+// have arrived.  A worker thread batches whatever is ready -- at most one
+// frame per stream per tick -- into batched ticks (evxg_batch.cu), building
+// tick t+1 while tick t runs on the device, and delivers every frame's
+// serializer inputs, with its arrival / ready / launch / done times, through a
+// callback.  Streams that join or leave change the batch at the next tick
+// boundary; the others' device state is untouched.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "evxg_internal.cuh"
+
+using namespace evxg;
+
+namespace {
+
+uint64_t now_ns()
+{
+    return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+               std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Device memory a stream holds (evxg_stream_create's allocations).
+size_t stream_bytes(uint32_t w, uint32_t h)
+{
+    const size_t W = (w + 15) & ~15u, H = (h + 15) & ~15u, nblk = (W / 16) * (H / 16);
+    const size_t planeset = (W * H + 2 * (W / 2) * (H / 2)) * sizeof(int16_t);
+    return 7 * planeset + (size_t)w * h * 3 + nblk * (3 * sizeof(evxg_block_desc) + sizeof(evxg_sao_info) + 12) +
+           (3 * (H / 16) + 5) * sizeof(int) + kSaoPasses * sizeof(int);
+}
+
+struct Ready {
+    std::vector<uint8_t> px;
+    evxg_frame f;
+    evxg_frame_times t;
+};
+
+struct Slot {
+    uint32_t id = 0, w = 0, h = 0;
+    size_t bytes = 0;
+    evxg_stream *st = nullptr;
+    evxg_encoder *planner = nullptr;
+    std::deque<Ready> ready;                   // frames whose encode order is known, oldest first
+    std::map<uint32_t, uint64_t> arrival;      // arrival stamp by display order, until the frame is ready
+    uint32_t next_order = 0;
+    bool closing = false;                      // no more input; removed once drained
+    int in_flight = 0;                         // frames in ticks not yet delivered
+};
+
+}  // namespace
+
+struct evxg_server {
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::map<uint32_t, Slot *> slots;
+    uint32_t next_id = 1, max_streams = 0;
+    uint64_t budget = 0, used = 0;
+    evxg_result_callback cb = nullptr;
+    void *user = nullptr;
+    std::thread worker;
+    bool stop = false, set_dirty = true;
+    int error = 0;
+    uint64_t frames_done = 0, ticks = 0, rebuilds = 0;
+    // worker-owned
+    evxg_batch *batch = nullptr;
+    std::vector<Slot *> bslots;                // batch order
+    struct Pending {
+        bool used = false;
+        std::vector<Ready> frames;             // per batch index; f.type < 0 = none
+    } pend[2];
+    cudaStream_t cs = nullptr;
+    int device = 0;
+};
+
+namespace {
+
+// Planner sink: the frame's encode order is known (called under the lock).
+int sink(void *ctx, const uint8_t *rgb, uint32_t w, uint32_t h, const evxg_frame *f)
+{
+    Slot *s = static_cast<Slot *>(ctx);
+    Ready r;
+    r.px.assign(rgb, rgb + (size_t)w * h * 3);
+    r.f = *f;
+    auto it = s->arrival.find(f->display_order);
+    r.t.arrival_ns = it != s->arrival.end() ? it->second : 0;
+    if (it != s->arrival.end()) s->arrival.erase(it);
+    r.t.ready_ns = now_ns();
+    r.t.launch_ns = r.t.done_ns = 0;
+    s->ready.push_back(std::move(r));
+    return EVXG_SUCCESS;
+}
+
+bool drained(const Slot *s) { return s->ready.empty() && s->in_flight == 0; }
+
+// Deliver tick q's results (worker thread, without the lock).
+int complete(evxg_server *v, int q)
+{
+    evxg_server::Pending &pd = v->pend[q];
+    if (!pd.used) return EVXG_SUCCESS;
+    pd.used = false;
+    int rc = evxg_batch_wait(v->batch, (uint32_t)q);
+    const uint64_t done = now_ns();
+    for (size_t i = 0; i < pd.frames.size() && !rc; i++) {
+        Ready &r = pd.frames[i];
+        if (r.f.type < 0) continue;
+        r.t.done_ns = done;
+        const evxg_block_desc *bt, *pv;
+        const evxg_sao_info *sao;
+        const int16_t *lev;
+        rc = evxg_batch_output(v->batch, (uint32_t)i, (uint32_t)q, &bt, &pv, &sao, &lev);
+        if (!rc && v->cb) v->cb(v->user, v->bslots[i]->id, &r.f, bt, pv, sao, lev, &r.t);
+    }
+    std::lock_guard<std::mutex> lk(v->mu);
+    for (size_t i = 0; i < pd.frames.size(); i++)
+        if (pd.frames[i].f.type >= 0) { v->bslots[i]->in_flight--; v->frames_done++; }
+    if (rc && !v->error) v->error = rc;
+    pd.frames.clear();
+    v->cv_done.notify_all();
+    return rc;
+}
+
+// MB-pass shape for a stream set: three-CTA clusters while the rows the
+// wavefronts keep busy fit the co-resident clusters (lowest latency), one CTA
+// per row beyond that (a third of the SMs per row).
+void choose_shape(evxg_server *v)
+{
+    int busy = 0;
+    for (Slot *s : v->bslots) busy += (int)std::min<uint32_t>(s->st->mbh, s->st->mbw / 4 + 4);
+    const int clusters = max_active_clusters();
+    if (clusters > 0 && busy <= clusters) evxg_batch_set_shape(v->batch, EVXG_MB_FORM_CLUSTER, busy, 1);
+    // else: the batch's default, one CTA per row on every SM
+}
+
+}  // namespace
+
+namespace {
+
+// Worker: rebuild the batch when the stream set changed (with no tick in
+// flight), launch a tick of whatever is ready, then deliver the tick before it.
+void work(evxg_server *v)
+{
+    cudaSetDevice(v->device);   // the caller's device
+    int p = 0;
+    for (;;) {
+        std::unique_lock<std::mutex> lk(v->mu);
+        auto any_ready = [&] {
+            for (auto &kv : v->slots)
+                if (!kv.second->ready.empty()) return true;
+            return false;
+        };
+        auto removable = [&] {
+            for (auto &kv : v->slots)
+                if (kv.second->closing && drained(kv.second)) return true;
+            return false;
+        };
+        v->cv_work.wait(lk, [&] {
+            return v->stop || v->set_dirty || any_ready() || removable() || v->pend[0].used || v->pend[1].used;
+        });
+        if (v->error) {   // a tick failed: deliver nothing more, let callers see the error
+            v->cv_done.notify_all();
+            if (v->stop) break;
+            v->cv_work.wait(lk, [&] { return v->stop; });
+            break;
+        }
+        if (v->stop && !any_ready() && !v->pend[0].used && !v->pend[1].used) break;
+        bool dirty = v->set_dirty || removable();
+        if (dirty) {
+            if (v->pend[0].used || v->pend[1].used) {   // finish the batch's ticks first, oldest first
+                lk.unlock();
+                complete(v, p ^ 1);
+                complete(v, p);
+                continue;
+            }
+            for (auto it = v->slots.begin(); it != v->slots.end();) {
+                Slot *s = it->second;
+                if (s->closing && drained(s)) {
+                    evxg_encoder_destroy(s->planner);
+                    evxg_stream_destroy(s->st);
+                    v->used -= s->bytes;
+                    delete s;
+                    it = v->slots.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+            if (v->batch) { evxg_batch_destroy(v->batch); v->batch = nullptr; }
+            v->bslots.clear();
+            std::vector<evxg_stream *> sts;
+            for (auto &kv : v->slots) { v->bslots.push_back(kv.second); sts.push_back(kv.second->st); }
+            if (!sts.empty()) {
+                const int rc = evxg_batch_create(sts.data(), (uint32_t)sts.size(), &v->batch);
+                if (rc) { v->error = rc; continue; }
+                choose_shape(v);
+            }
+            v->set_dirty = false;
+            v->rebuilds++;
+            p = 0;
+            v->cv_done.notify_all();
+            continue;
+        }
+        // a tick of whatever is ready: at most one frame per stream, its oldest
+        std::vector<Ready> frames(v->bslots.size());
+        bool any = false;
+        for (size_t i = 0; i < v->bslots.size(); i++) {
+            Slot *s = v->bslots[i];
+            if (s->ready.empty()) { frames[i].f.type = -1; continue; }
+            frames[i] = std::move(s->ready.front());
+            s->ready.pop_front();
+            s->in_flight++;
+            any = true;
+        }
+        lk.unlock();
+        if (!any) {   // nothing new: deliver what is in flight
+            complete(v, p ^ 1);
+            complete(v, p);
+            continue;
+        }
+        if (complete(v, p)) continue;   // this parity's buffers are free again
+        std::vector<evxg_frame> fr(frames.size());
+        const uint64_t launch = now_ns();
+        for (size_t i = 0; i < frames.size(); i++) {
+            fr[i] = frames[i].f;
+            if (frames[i].f.type < 0) continue;
+            memcpy(evxg_batch_input(v->batch, (uint32_t)i, (uint32_t)p), frames[i].px.data(), frames[i].px.size());
+            frames[i].t.launch_ns = launch;
+            frames[i].px.clear();
+            frames[i].px.shrink_to_fit();
+        }
+        int rc = evxg_batch_encode(v->batch, fr.data(), (uint32_t)p, v->cs);
+        {
+            std::lock_guard<std::mutex> g(v->mu);
+            if (rc && !v->error) v->error = rc;
+            v->ticks++;
+        }
+        if (rc) continue;
+        v->pend[p].used = true;
+        v->pend[p].frames = std::move(frames);
+        complete(v, p ^ 1);   // the tick before runs ahead of this one; deliver it while this one runs
+        p ^= 1;
+    }
+    complete(v, p ^ 1);
+    complete(v, p);
+}
+
+}  // namespace
+
+extern "C" {
+
+uint64_t evxg_server_now_ns(void) { return now_ns(); }
+
+int evxg_server_create(uint64_t hbm_budget_bytes, uint32_t max_streams, evxg_result_callback cb, void *user,
+                       evxg_server **out)
+{
+    if (!out || !max_streams || !hbm_budget_bytes) return fail(EVXG_ERROR_INVALIDARG, "evxg_server_create: bad argument");
+    evxg_server *v = new evxg_server();
+    v->budget = hbm_budget_bytes;
+    v->max_streams = max_streams;
+    v->cb = cb;
+    v->user = user;
+    if (cudaGetDevice(&v->device) != cudaSuccess || cudaStreamCreateWithFlags(&v->cs, cudaStreamNonBlocking) != cudaSuccess) {
+        delete v;
+        return fail(EVXG_ERROR_EXECUTION_FAILURE, "evxg_server_create: stream creation failed");
+    }
+    v->worker = std::thread(work, v);
+    *out = v;
+    return EVXG_SUCCESS;
+}
+
+int evxg_server_open(evxg_server *v, uint32_t width, uint32_t height, uint8_t quality, uint32_t *stream_id)
+{
+    if (!v || !stream_id) return fail(EVXG_ERROR_INVALIDARG, "evxg_server_open: bad argument");
+    const size_t bytes = stream_bytes(width, height);
+    {
+        std::lock_guard<std::mutex> lk(v->mu);
+        if (v->error) return fail(v->error, "evxg_server_open: the server has failed");
+        if (v->slots.size() >= v->max_streams) return fail(EVXG_ERROR_CAPACITY_LIMIT, "evxg_server_open: every stream slot is taken");
+        if (v->used + bytes > v->budget) return fail(EVXG_ERROR_CAPACITY_LIMIT, "evxg_server_open: the device memory budget is spent");
+        v->used += bytes;   // reserved while the stream is created
+    }
+    Slot *s = new Slot();
+    s->w = width; s->h = height; s->bytes = bytes;
+    int rc = evxg_stream_create(width, height, &s->st);
+    if (!rc) rc = evxg_encoder_create(nullptr, nullptr, &s->planner);
+    if (!rc) { encoder_set_sink(s->planner, sink, s); rc = evxg_encoder_set_quality(s->planner, quality); }
+    std::lock_guard<std::mutex> lk(v->mu);
+    if (rc) {
+        if (s->planner) evxg_encoder_destroy(s->planner);
+        if (s->st) evxg_stream_destroy(s->st);
+        delete s;
+        v->used -= bytes;
+        return rc;
+    }
+    s->id = v->next_id++;
+    v->slots[s->id] = s;
+    v->set_dirty = true;
+    *stream_id = s->id;
+    v->cv_work.notify_all();
+    return EVXG_SUCCESS;
+}
+
+int evxg_server_submit(evxg_server *v, uint32_t stream_id, const uint8_t *rgb, uint64_t arrival_ns)
+{
+    if (!v || !rgb) return fail(EVXG_ERROR_INVALIDARG, "evxg_server_submit: bad argument");
+    std::lock_guard<std::mutex> lk(v->mu);
+    if (v->error) return fail(v->error, "evxg_server_submit: the server has failed");
+    auto it = v->slots.find(stream_id);
+    if (it == v->slots.end() || it->second->closing) return fail(EVXG_ERROR_INVALID_INDEX, "evxg_server_submit: no such open stream");
+    Slot *s = it->second;
+    s->arrival[s->next_order++] = arrival_ns ? arrival_ns : now_ns();
+    const int rc = evxg_encoder_encode(s->planner, rgb, s->w, s->h);
+    v->cv_work.notify_all();
+    return rc;
+}
+
+int evxg_server_insert_intra(evxg_server *v, uint32_t stream_id)
+{
+    if (!v) return EVXG_ERROR_INVALIDARG;
+    std::lock_guard<std::mutex> lk(v->mu);
+    auto it = v->slots.find(stream_id);
+    if (it == v->slots.end() || it->second->closing) return fail(EVXG_ERROR_INVALID_INDEX, "evxg_server_insert_intra: no such open stream");
+    return evxg_encoder_insert_intra(it->second->planner);
+}
+
+int evxg_server_close(evxg_server *v, uint32_t stream_id)
+{
+    if (!v) return EVXG_ERROR_INVALIDARG;
+    std::lock_guard<std::mutex> lk(v->mu);
+    auto it = v->slots.find(stream_id);
+    if (it == v->slots.end() || it->second->closing) return fail(EVXG_ERROR_INVALID_INDEX, "evxg_server_close: no such open stream");
+    const int rc = evxg_encoder_flush(it->second->planner);   // the frames still waiting for their anchor
+    it->second->closing = true;
+    v->cv_work.notify_all();
+    return rc;
+}
+
+int evxg_server_drain(evxg_server *v)
+{
+    if (!v) return EVXG_ERROR_INVALIDARG;
+    std::unique_lock<std::mutex> lk(v->mu);
+    v->cv_done.wait(lk, [&] {
+        if (v->error) return true;
+        if (v->pend[0].used || v->pend[1].used) return false;
+        for (auto &kv : v->slots)
+            if (!kv.second->ready.empty() || kv.second->in_flight || (kv.second->closing)) return false;
+        return !v->set_dirty;
+    });
+    return v->error ? fail(v->error, "evxg_server_drain: a tick failed") : EVXG_SUCCESS;
+}
+
+int evxg_server_stats(evxg_server *v, uint64_t *frames, uint64_t *ticks, uint64_t *rebuilds, uint64_t *bytes_in_use)
+{
+    if (!v) return EVXG_ERROR_INVALIDARG;
+    std::lock_guard<std::mutex> lk(v->mu);
+    if (frames) *frames = v->frames_done;
+    if (ticks) *ticks = v->ticks;
+    if (rebuilds) *rebuilds = v->rebuilds;
+    if (bytes_in_use) *bytes_in_use = v->used;
+    return EVXG_SUCCESS;
+}
+
+int evxg_server_destroy(evxg_server *v)
+{
+    if (!v) return EVXG_ERROR_INVALIDARG;
+    {
+        std::lock_guard<std::mutex> lk(v->mu);
+        for (auto &kv : v->slots)
+            if (!kv.second->closing) { evxg_encoder_flush(kv.second->planner); kv.second->closing = true; }
+        v->stop = true;
+        v->cv_work.notify_all();
+    }
+    v->worker.join();
+    if (v->batch) evxg_batch_destroy(v->batch);
+    for (auto &kv : v->slots) {
+        evxg_encoder_destroy(kv.second->planner);
+        evxg_stream_destroy(kv.second->st);
+        delete kv.second;
+    }
+    cudaStreamDestroy(v->cs);
+    delete v;
+    return EVXG_SUCCESS;
+}
+
+}  // extern "C"

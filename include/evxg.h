@@ -209,6 +209,44 @@ int evxg_batch_set_shape(evxg_batch *b, int form, int grid, int policy);
 int evxg_batch_get_shape(const evxg_batch *b, int *form, int *grid, int *policy);
 int evxg_batch_autotune(evxg_batch *b, void *cuda_stream, float *best_ms);
 
+/* ---- Serving ----
+ *
+ * No counterpart in the reference.  A request loop over many live streams:
+ * evxg_server_open admits a stream if a slot is free and its device memory
+ * fits what is left of the budget (else EVXG_ERROR_CAPACITY_LIMIT: retry once
+ * a stream has closed); its state stays on the device until it closes.
+ * evxg_server_submit copies one RGB24 frame in (arrival_ns on the
+ * evxg_server_now_ns clock; 0 = now).  Each stream follows the reference
+ * encoder's GOP (evx3enc.cpp:105-414), so a frame is ready to encode once the
+ * frames it depends on have arrived; a worker thread batches whatever is ready
+ * (at most one frame per stream per tick, see Batched encoding) while the
+ * previous tick runs, and calls cb on that thread, in each stream's bitstream
+ * order, with the frame's serializer inputs (valid during the call) and its
+ * times.  evxg_server_close flushes a stream (its last frames are encoded)
+ * and frees it once delivered; evxg_server_drain waits until every frame that
+ * can be encoded has been delivered.  Every stream's results equal encoding
+ * it alone with evxg_encoder_*. */
+typedef struct evxg_server evxg_server;
+typedef struct {
+    uint64_t arrival_ns;   /* submitted */
+    uint64_t ready_ns;     /* its place in encode order known */
+    uint64_t launch_ns;    /* its tick launched */
+    uint64_t done_ns;      /* its tick's results seen by the host */
+} evxg_frame_times;
+typedef void (*evxg_result_callback)(void *user, uint32_t stream_id, const evxg_frame *frame,
+                                     const evxg_block_desc *blocks, const evxg_block_desc *prev_blocks,
+                                     const evxg_sao_info *sao, const int16_t *levels, const evxg_frame_times *times);
+int evxg_server_create(uint64_t hbm_budget_bytes, uint32_t max_streams, evxg_result_callback cb, void *user,
+                       evxg_server **out);
+int evxg_server_destroy(evxg_server *srv);
+int evxg_server_open(evxg_server *srv, uint32_t width, uint32_t height, uint8_t quality, uint32_t *stream_id);
+int evxg_server_submit(evxg_server *srv, uint32_t stream_id, const uint8_t *rgb, uint64_t arrival_ns);
+int evxg_server_insert_intra(evxg_server *srv, uint32_t stream_id);
+int evxg_server_close(evxg_server *srv, uint32_t stream_id);
+int evxg_server_drain(evxg_server *srv);
+int evxg_server_stats(evxg_server *srv, uint64_t *frames, uint64_t *ticks, uint64_t *rebuilds, uint64_t *bytes_in_use);
+uint64_t evxg_server_now_ns(void);
+
 /* lambda = 0.85 * 2^((q-12)/3) in float, as the reference computes it (common.h:264-266). */
 float evxg_lambda(uint16_t quality);
 

@@ -1,0 +1,89 @@
+"""Serving (evxg_server_*): continuous batching over live streams.
+
+Streams of different sizes and qualities join while others are on the GPU,
+submit frames interleaved with the others', insert intra frames and close at
+different times; each stream's results (frame descriptor and the
+serializer's tables, in bitstream order) must equal the same stream encoded
+alone by the GOP-level encoder (evxg_encoder_*), bit for bit -- the tolerance
+of every parity test here.  Admission by the device memory budget refuses a
+stream that does not fit and admits it once another has closed."""
+import time
+
+import numpy as np
+import pytest
+
+from chicago_b200.synth import generate
+
+pytestmark = pytest.mark.gpu
+
+# (width, height, quality, frames, intra insertions, round it joins)
+SPEC = [(64, 48, 8, 9, (), 0), (176, 144, 4, 11, (5,), 0), (96, 64, 16, 7, (), 3), (34, 18, 12, 10, (3,), 5)]
+
+
+def alone(w, h, q, frames, intra_at):
+    import chicago_b200 as cb
+    enc = cb.Encoder(quality=q)
+    for t, f in enumerate(frames):
+        if t in intra_at:
+            enc.insert_intra()
+        enc.encode(f)
+    enc.flush()
+    return enc.records
+
+
+@pytest.mark.timeout(300)
+def test_server_results_equal_streams_alone():
+    import chicago_b200 as cb
+    srv = cb.Server(hbm_budget_bytes=1 << 34, max_streams=8)
+    seqs = [generate(w, h, n, seed=300 + k, vmax=3.0 + k) for k, (w, h, q, n, ia, j) in enumerate(SPEC)]
+    ids, pos = [None] * len(SPEC), [0] * len(SPEC)
+    for rnd in range(100):
+        for k, (w, h, q, n, ia, join) in enumerate(SPEC):
+            if ids[k] is None and rnd >= join:
+                ids[k] = srv.open(w, h, q)
+            if ids[k] is None or pos[k] >= n:
+                continue
+            if pos[k] in ia:
+                srv.insert_intra(ids[k])
+            srv.submit(ids[k], seqs[k][pos[k]])
+            pos[k] += 1
+            if pos[k] == n:
+                srv.close_stream(ids[k])
+        if all(p >= s[3] for p, s in zip(pos, SPEC)):
+            break
+        time.sleep(0.003)   # frames keep arriving while ticks run
+    srv.drain()
+    for k, (w, h, q, n, ia, join) in enumerate(SPEC):
+        got, want = srv.results[ids[k]], alone(w, h, q, seqs[k], ia)
+        assert len(got) == len(want) == n
+        for i, (g, e) in enumerate(zip(got, want)):
+            assert g["frame18"] == e["frame18"], f"stream {k} record {i}: frame"
+            for key in ("blocks", "prev_blocks", "sao", "levels"):
+                assert np.array_equal(g[key], e[key]), f"stream {k} record {i}: {key}"
+            a, r, l, d = g["times"]
+            assert 0 < a <= r <= l <= d
+    st = srv.stats()
+    assert st["frames"] == sum(s[3] for s in SPEC) and st["rebuilds"] >= 2 and st["bytes_in_use"] == 0
+    srv.close()
+
+
+@pytest.mark.timeout(300)
+def test_server_admission_by_memory_budget():
+    import chicago_b200 as cb
+    srv = cb.Server(hbm_budget_bytes=1_500_000, max_streams=8)   # room for two 176x144 streams (about 0.62 MB each)
+    a, b = srv.open(176, 144), srv.open(176, 144)
+    with pytest.raises(cb.EvxgError) as e:
+        srv.open(176, 144)
+    assert e.value.code == 7   # EVXG_ERROR_CAPACITY_LIMIT
+    frames = generate(176, 144, 2, seed=7, vmax=2.0)
+    srv.submit(a, frames[0])
+    srv.close_stream(a)
+    srv.drain()                # the closed stream's memory is back in the budget
+    c = srv.open(176, 144)
+    srv.submit(c, frames[1])
+    srv.close_stream(b)
+    srv.close_stream(c)
+    srv.drain()
+    assert len(srv.results[a]) == 1 and len(srv.results[c]) == 1 and len(srv.results[b]) == 0
+    assert srv.stats()["bytes_in_use"] == 0
+    srv.close()
