@@ -215,6 +215,9 @@ def run_gpu(args):
     d2h = nblk * 28 * 2 + nblk * 16 + st.plane_elems * 2
 
     batched = run_batched(args, stream) if args.batch > 1 and world == 1 else None
+    served = run_served(args) if args.serve_streams > 0 and world == 1 else None
+    served_light = (run_served(args, n=8, per=12, sizes_from=[(640, 360), (1280, 720)], seed=11)
+                    if args.serve_streams > 0 and world == 1 else None)
 
     peak, peak_kind = peaks()
     achieved = mb_bytes / (sum(mb_ms) / 1e3) / 1e9
@@ -239,6 +242,8 @@ def run_gpu(args):
                              "cols + 4*(rows-1) MB steps (388 at 1080p), each one MB's dependent chain"},
         "gpu_launches": st.launch_count() * K,
         "batched": batched,
+        "served": served,
+        "served_light": served_light,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -329,6 +334,72 @@ def run_batched(args, stream):
     return res
 
 
+# The serving configuration: 64 streams at 60 fps, sizes drawn uniformly from
+# 640x360 / 1280x720 / 1920x1080 / 3840x2160, arrivals every 1/60 s with
+# +-2 ms jitter from a random phase, quality 8.
+SERVE_SIZES = [(640, 360), (1280, 720), (1920, 1080), (3840, 2160)]
+
+
+def run_served(args, n=None, per=None, sizes_from=None, seed=7):
+    """The request loop (evxg_server_*): all streams admitted by the device
+    memory budget, frames submitted at their arrival times by this thread, the
+    server's worker batching whatever is ready.  A frame's latency is its done
+    time (results seen by the host) minus its arrival time, so it includes the
+    reference GOP's reorder wait (a B frame waits for its anchor) and queueing;
+    each stream sends `serve_frames` frames and then closes (flushing)."""
+    import chicago_b200 as cb
+    from chicago_b200.synth import generate
+    rng = np.random.default_rng(seed)
+    n = args.serve_streams if n is None else n
+    per = args.serve_frames if per is None else per
+    choices = SERVE_SIZES if sizes_from is None else sizes_from
+    sizes = [choices[i] for i in rng.integers(0, len(choices), n)]
+    pool = {sz: generate(sz[0], sz[1], per + 3, seed=3000 + k, vmax=max(4.0, 24.0 * sz[0] / 1920))
+            for k, sz in enumerate(SERVE_SIZES) if sz in sizes}
+    srv = cb.Server(hbm_budget_bytes=96 << 30, max_streams=n, keep_tables=False)
+    ids = [srv.open(w, h, QUALITY) for w, h in sizes]
+    srv.drain()   # the batch over every admitted stream exists before the first arrival
+    phase = rng.uniform(0, 1 / 60, n)
+    events = sorted((phase[k] + t / 60 + rng.uniform(-0.002, 0.002), k, t) for k in range(n) for t in range(per))
+    t0 = cb.Server.now_ns()
+    sent = [0] * n
+    for at, k, t in events:
+        due = t0 + int(max(at, 0.0) * 1e9)
+        while cb.Server.now_ns() < due:
+            time.sleep(min(0.0005, (due - cb.Server.now_ns()) / 1e9))
+        off = k % 3   # streams of a size class start at different frames of its pool
+        srv.submit(ids[k], pool[sizes[k]][off + t], arrival_ns=cb.Server.now_ns())
+        sent[k] += 1
+        if sent[k] == per:
+            srv.close_stream(ids[k])
+    srv.drain()
+    lat, work, eq, first, last = [], [], 0.0, None, 0
+    for k, sid in enumerate(ids):
+        w, h = sizes[k]
+        for r in srv.results[sid]:
+            a, rd, _, d = r["times"]
+            lat.append((d - a) / 1e6)
+            work.append((d - rd) / 1e6)
+            eq += w * h / (1920 * 1080)
+            first = a if first is None else min(first, a)
+            last = max(last, d)
+    st = srv.stats()
+    srv.close()
+    offered = sum(w * h for w, h in sizes) / (1920 * 1080) * 60
+    counts = {f"{w}x{h}": sizes.count((w, h)) for w, h in SERVE_SIZES if (w, h) in sizes}
+    return {"streams": n, "sizes": counts, "frames": len(lat), "frames_per_stream": per,
+            "value": round(eq / ((last - first) / 1e9), 3), "unit": UNIT,
+            "offered_1080p_eq_fps": round(offered, 1),
+            "p50_frame_ms": round(float(np.percentile(lat, 50)), 3),
+            "p99_frame_ms": round(float(np.percentile(lat, 99)), 3),
+            "p999_frame_ms": round(float(np.percentile(lat, 99.9)), 3),
+            "ready_to_done_ms": {q: round(float(np.percentile(work, v)), 3) for q, v in (("p50", 50), ("p99", 99), ("p999", 99.9))},
+            "ticks": st["ticks"], "batch_rebuilds": st["rebuilds"],
+            "note": "latency = results seen by the host minus arrival: includes the reference GOP's reorder wait "
+                    "(a B frame waits for its anchor, 3 frames later) and any queueing; ready_to_done starts when "
+                    "the frame's encode order is known"}
+
+
 def cpu_baseline(n_frames: int = 8):
     """The unmodified reference encoder (built here from its sources) with its
     WPP threads on all host cores, on the first n_frames of the same workload."""
@@ -395,6 +466,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=16, help="streams of the batched measurement (1 = skip)")
     ap.add_argument("--batch-ticks", type=int, default=12, help="timed ticks of the batched measurement")
+    ap.add_argument("--serve-streams", type=int, default=64, help="streams of the serving measurement (0 = skip)")
+    ap.add_argument("--serve-frames", type=int, default=4, help="frames each served stream sends")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

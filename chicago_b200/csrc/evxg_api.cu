@@ -63,9 +63,14 @@ int evxg_stream_create(uint32_t width, uint32_t height, evxg_stream **out)
     if (e == cudaSuccess) e = cudaMalloc(&s->sao_mail, nblk * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&s->rgb, (size_t)width * height * 3);
     if (e == cudaSuccess) e = cudaMalloc(&s->sync, (3 * s->mbh + 5) * sizeof(int));
-    if (e == cudaSuccess && reset_stream(s, nullptr)) e = cudaErrorUnknown;
+    // Zeroing on a private stream, synchronised alone: no device-wide
+    // synchronisation, which another thread capturing a graph would forbid.
+    cudaStream_t zs = nullptr;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&zs, cudaStreamNonBlocking);
+    if (e == cudaSuccess && reset_stream(s, zs)) e = cudaErrorUnknown;
     const int max_clusters = e == cudaSuccess ? max_active_clusters() : 0;
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(zs);
+    if (zs) cudaStreamDestroy(zs);
     if (e != cudaSuccess) {
         int rc = cuda_fail(e, "evxg_stream_create");
         evxg_stream_destroy(s);

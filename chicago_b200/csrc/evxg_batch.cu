@@ -50,6 +50,34 @@ struct evxg_batch {
 
 static const int kTickKernels = 10 + kSaoPasses;   // kernels per tick, whatever the number of streams
 
+// Shape of the macroblock pass from a model of the tick: a tick lasts at least
+// its longest wavefront's critical path (cols + 4 x (rows - 1) MB steps) and at
+// least the MBs of all streams over the units working on them (SMs in the
+// single form, three-SM clusters in the cluster form), each MB step costing
+// about kSingleVsCluster times as long in the single form (clock64 probes of
+// both forms on 1080p frames).
+static const double kSingleVsCluster = 2.2;
+static void model_shape(evxg_batch *b)
+{
+    double path = 0, mbs = 0;
+    int busy = 0;
+    for (const evxg_stream *s : b->st) {
+        path = std::max(path, (double)(s->mbw + 4 * (s->mbh - 1)));
+        mbs += (double)s->mbw * s->mbh;
+        busy += (int)std::min<uint32_t>(s->mbh, s->mbw / 4 + 4);
+    }
+    const double t_single = kSingleVsCluster * std::max(path, mbs / b->num_sms);
+    const double t_cluster = b->max_clusters > 0 ? std::max(path, mbs / b->max_clusters) : 1e30;
+    if (t_cluster < t_single) {
+        b->form = EVXG_MB_FORM_CLUSTER;
+        b->grid = std::max(1, std::min(busy, b->max_clusters));
+    } else {
+        b->form = EVXG_MB_FORM_SINGLE;
+        b->grid = std::max(1, std::min((int)b->qcap, b->num_sms));
+    }
+    b->policy = 0;
+}
+
 static size_t out_bytes(const evxg_stream *s)
 {
     const size_t nblk = (size_t)s->mbw * s->mbh;
@@ -140,7 +168,7 @@ static int build_graph(evxg_batch *b, int parity)
     cudaStream_t cs;
     CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);   // other threads may allocate meanwhile
     int rc = e == cudaSuccess ? enqueue_tick(b, parity, cs) : cuda_fail(e, "cudaStreamBeginCapture");
     if (e == cudaSuccess) {
         const cudaError_t e2 = cudaStreamEndCapture(cs, &g);
@@ -193,7 +221,7 @@ int evxg_batch_create(evxg_stream *const *streams, uint32_t n, evxg_batch **out)
     for (evxg_stream *s : b->st) b->qcap += s->mbh;
     b->num_sms = b->st[0]->num_sms;
     b->max_clusters = max_active_clusters();
-    b->grid = std::min<int>(b->num_sms, (int)b->qcap);
+    model_shape(b);   // the default shape; evxg_batch_autotune measures instead
     cudaError_t e = cudaMalloc(&b->d_args, n * sizeof(FrameArgs));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, (2 + 2 * (size_t)b->qcap) * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_ctl, 2 * sizeof(int));

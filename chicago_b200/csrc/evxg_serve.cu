@@ -73,6 +73,7 @@ struct evxg_server {
     void *user = nullptr;
     std::thread worker;
     bool stop = false, set_dirty = true;
+    int drainers = 0;                          // threads waiting in evxg_server_drain
     int error = 0;
     uint64_t frames_done = 0, ticks = 0, rebuilds = 0;
     // worker-owned
@@ -105,6 +106,16 @@ int sink(void *ctx, const uint8_t *rgb, uint32_t w, uint32_t h, const evxg_frame
 }
 
 bool drained(const Slot *s) { return s->ready.empty() && s->in_flight == 0; }
+// Closed streams that have delivered everything stay in the batch (without
+// frames) until the next rebuild, which a new stream's admission brings; until
+// then their memory counts as free for admissions.
+size_t dead_bytes(const evxg_server *v)
+{
+    size_t b = 0;
+    for (auto &kv : v->slots)
+        if (kv.second->closing && drained(kv.second)) b += kv.second->bytes;
+    return b;
+}
 
 // Deliver tick q's results (worker thread, without the lock).
 int complete(evxg_server *v, int q)
@@ -133,18 +144,6 @@ int complete(evxg_server *v, int q)
     return rc;
 }
 
-// MB-pass shape for a stream set: three-CTA clusters while the rows the
-// wavefronts keep busy fit the co-resident clusters (lowest latency), one CTA
-// per row beyond that (a third of the SMs per row).
-void choose_shape(evxg_server *v)
-{
-    int busy = 0;
-    for (Slot *s : v->bslots) busy += (int)std::min<uint32_t>(s->st->mbh, s->st->mbw / 4 + 4);
-    const int clusters = max_active_clusters();
-    if (clusters > 0 && busy <= clusters) evxg_batch_set_shape(v->batch, EVXG_MB_FORM_CLUSTER, busy, 1);
-    // else: the batch's default, one CTA per row on every SM
-}
-
 }  // namespace
 
 namespace {
@@ -162,13 +161,10 @@ void work(evxg_server *v)
                 if (!kv.second->ready.empty()) return true;
             return false;
         };
-        auto removable = [&] {
-            for (auto &kv : v->slots)
-                if (kv.second->closing && drained(kv.second)) return true;
-            return false;
-        };
         v->cv_work.wait(lk, [&] {
-            return v->stop || v->set_dirty || any_ready() || removable() || v->pend[0].used || v->pend[1].used;
+            // a changed stream set is rebuilt when there is work for it or a drain waits on it, so a
+            // burst of admissions costs one rebuild
+            return v->stop || (v->set_dirty && v->drainers > 0) || any_ready() || v->pend[0].used || v->pend[1].used;
         });
         if (v->error) {   // a tick failed: deliver nothing more, let callers see the error
             v->cv_done.notify_all();
@@ -177,8 +173,7 @@ void work(evxg_server *v)
             break;
         }
         if (v->stop && !any_ready() && !v->pend[0].used && !v->pend[1].used) break;
-        bool dirty = v->set_dirty || removable();
-        if (dirty) {
+        if (v->set_dirty) {
             if (v->pend[0].used || v->pend[1].used) {   // finish the batch's ticks first, oldest first
                 lk.unlock();
                 complete(v, p ^ 1);
@@ -203,8 +198,7 @@ void work(evxg_server *v)
             for (auto &kv : v->slots) { v->bslots.push_back(kv.second); sts.push_back(kv.second->st); }
             if (!sts.empty()) {
                 const int rc = evxg_batch_create(sts.data(), (uint32_t)sts.size(), &v->batch);
-                if (rc) { v->error = rc; continue; }
-                choose_shape(v);
+                if (rc) { v->error = rc; continue; }   // the batch's default shape: its tick model (evxg_batch.cu)
             }
             v->set_dirty = false;
             v->rebuilds++;
@@ -287,8 +281,12 @@ int evxg_server_open(evxg_server *v, uint32_t width, uint32_t height, uint8_t qu
     {
         std::lock_guard<std::mutex> lk(v->mu);
         if (v->error) return fail(v->error, "evxg_server_open: the server has failed");
-        if (v->slots.size() >= v->max_streams) return fail(EVXG_ERROR_CAPACITY_LIMIT, "evxg_server_open: every stream slot is taken");
-        if (v->used + bytes > v->budget) return fail(EVXG_ERROR_CAPACITY_LIMIT, "evxg_server_open: the device memory budget is spent");
+        size_t dead_slots = 0;
+        for (auto &kv : v->slots) dead_slots += kv.second->closing && drained(kv.second);
+        if (v->slots.size() - dead_slots >= v->max_streams)
+            return fail(EVXG_ERROR_CAPACITY_LIMIT, "evxg_server_open: every stream slot is taken");
+        if (v->used - dead_bytes(v) + bytes > v->budget)
+            return fail(EVXG_ERROR_CAPACITY_LIMIT, "evxg_server_open: the device memory budget is spent");
         v->used += bytes;   // reserved while the stream is created
     }
     Slot *s = new Slot();
@@ -351,13 +349,16 @@ int evxg_server_drain(evxg_server *v)
 {
     if (!v) return EVXG_ERROR_INVALIDARG;
     std::unique_lock<std::mutex> lk(v->mu);
+    v->drainers++;
+    v->cv_work.notify_all();
     v->cv_done.wait(lk, [&] {
         if (v->error) return true;
         if (v->pend[0].used || v->pend[1].used) return false;
         for (auto &kv : v->slots)
-            if (!kv.second->ready.empty() || kv.second->in_flight || (kv.second->closing)) return false;
+            if (!kv.second->ready.empty() || kv.second->in_flight) return false;
         return !v->set_dirty;
     });
+    v->drainers--;
     return v->error ? fail(v->error, "evxg_server_drain: a tick failed") : EVXG_SUCCESS;
 }
 
@@ -368,7 +369,7 @@ int evxg_server_stats(evxg_server *v, uint64_t *frames, uint64_t *ticks, uint64_
     if (frames) *frames = v->frames_done;
     if (ticks) *ticks = v->ticks;
     if (rebuilds) *rebuilds = v->rebuilds;
-    if (bytes_in_use) *bytes_in_use = v->used;
+    if (bytes_in_use) *bytes_in_use = v->used - dead_bytes(v);   // streams not yet closed and delivered
     return EVXG_SUCCESS;
 }
 

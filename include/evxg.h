@@ -201,7 +201,9 @@ uint32_t evxg_batch_launch_count(const evxg_batch *b);
 /* Shape of the tick's macroblock pass: form (EVXG_MB_FORM_*), persistent grid
  * (CTAs, or clusters in the cluster form; capped at what is co-resident) and
  * queue order (0: rows interleaved by index; 1: the same, longer remaining
- * critical path first).  evxg_batch_autotune times the candidates on a short
+ * critical path first).  A new batch takes the shape a model of the tick
+ * favours (the longer of the longest critical path and all MBs over the
+ * working units, per form).  evxg_batch_autotune times the candidates on a short
  * synthetic I/P/B sequence at the streams' sizes, keeps the fastest, and
  * returns every stream to its initial state; best_ms (optional) receives the
  * winner's time for the three timed ticks. */
@@ -222,9 +224,12 @@ int evxg_batch_autotune(evxg_batch *b, void *cuda_stream, float *best_ms);
  * (at most one frame per stream per tick, see Batched encoding) while the
  * previous tick runs, and calls cb on that thread, in each stream's bitstream
  * order, with the frame's serializer inputs (valid during the call) and its
- * times.  evxg_server_close flushes a stream (its last frames are encoded)
- * and frees it once delivered; evxg_server_drain waits until every frame that
- * can be encoded has been delivered.  Every stream's results equal encoding
+ * times.  evxg_server_close flushes a stream (its last frames are encoded);
+ * once they are delivered its memory counts as free for admissions and is
+ * released when the next admission rebuilds the batch.  evxg_server_drain
+ * waits until every frame that can be encoded has been delivered (and the
+ * batch covers every admitted stream).  evxg_server_stats' bytes_in_use counts
+ * the streams not yet closed and delivered.  Every stream's results equal encoding
  * it alone with evxg_encoder_*. */
 typedef struct evxg_server evxg_server;
 typedef struct {
