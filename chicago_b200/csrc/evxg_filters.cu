@@ -591,8 +591,8 @@ __device__ __forceinline__ void tile_store(MergeTile &m, int lane, const TileReg
 // rate).  The parameters are unpacked into registers and the band / edge
 // branch is taken once per call, not per pixel.
 __device__ __forceinline__ int pick4(int k, int o0, int o1, int o2, int o3) { return k == 0 ? o0 : k == 1 ? o1 : k == 2 ? o2 : o3; }
-__device__ __noinline__ long long tile_sao_ssd(const FrameArgs &a, const MergeTile &m, int c, int row, int lane,
-                                               evxg_sao_params p)
+__device__ __forceinline__ long long tile_sao_ssd(int W, int H, const MergeTile &m, int c, int row, int lane,
+                                                  evxg_sao_params p)
 {
     const int ty = lane >> 1, tx0 = (lane & 1) * 8;
     const int y = row * 16 + ty, x0 = c * 16 + tx0;
@@ -613,13 +613,13 @@ __device__ __noinline__ long long tile_sao_ssd(const FrameArgs &a, const MergeTi
         const int ec = p.eo_class;
         const int dxa = ec == 1 ? 0 : (ec == 3 ? 1 : -1), dya = ec == 0 ? 0 : -1;   // c_eo (sao.cpp:20-25)
         const int dxb = -dxa, dyb = -dya;
-        const bool rows_ok = y + dya >= 0 && y + dya < a.H && y + dyb >= 0 && y + dyb < a.H;
+        const bool rows_ok = y + dya >= 0 && y + dya < H && y + dyb >= 0 && y + dyb < H;
         const int da = dya * MT_W + dxa, db = dyb * MT_W + dxb;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             const int v = rr[i], x = x0 + i;
             int corr = v;
-            if (rows_ok && x + dxa >= 0 && x + dxa < a.W && x + dxb >= 0 && x + dxb < a.W) {
+            if (rows_ok && x + dxa >= 0 && x + dxa < W && x + dxb >= 0 && x + dxb < W) {
                 const int ct = eo_cat(v, rr[i + da], rr[i + db]);
                 if (ct < 4) corr = sclamp(v + pick4(ct, o0, o1, o2, o3));
             }
@@ -723,6 +723,13 @@ __device__ bool merge_row(const FrameArgs &a, MergeTile *tiles, unsigned long lo
             own = ld_info_cg(&a.sao[m + 1]);
             own_cost = __ldcg(&a.sao_cost[m + 1]);
         }
+        // The merge-left cost needs only this row's previous MB: it is computed
+        // before the wait for the row above, off the wavefront's critical path.
+        __syncwarp();
+        const MergeTile &mt = tiles[c & 1];
+        const bool try_left = c > 0 && left.luma.type != 0;
+        float mc_left = 0.0f;
+        if (try_left) mc_left = __fadd_rn(__ll2float_rn(tile_sao_ssd(a.W, a.H, mt, c, row, lane, left.luma)), __fmul_rn(a.lambda, 1.0f));
         unsigned long long above = 0;
         if (row > 0) {   // bounded wait for the final parameters of (r-1, c)
             bool ok = true;
@@ -732,16 +739,11 @@ __device__ bool merge_row(const FrameArgs &a, MergeTile *tiles, unsigned long lo
             if (!__shfl_sync(0xffffffffu, ok, 0)) return false;
             above = __shfl_sync(0xffffffffu, above, 0);
         }
-        __syncwarp();
-        const MergeTile &mt = tiles[c & 1];
-        if (c > 0 && left.luma.type != 0) {
-            const float mc = __fadd_rn(__ll2float_rn(tile_sao_ssd(a, mt, c, row, lane, left.luma)), __fmul_rn(a.lambda, 1.0f));
-            if (mc < cur) { info.merge_left = 1; info.luma = left.luma; info.chroma = left.chroma; cur = mc; }
-        }
+        if (try_left && mc_left < cur) { info.merge_left = 1; info.luma = left.luma; info.chroma = left.chroma; cur = mc_left; }
         if (!info.merge_left && row > 0) {
             const evxg_sao_params al = unpack_params(above >> 8), ac = unpack_params(above >> 33);
             if (al.type != 0) {
-                const float mc = __fadd_rn(__ll2float_rn(tile_sao_ssd(a, mt, c, row, lane, al)), __fmul_rn(a.lambda, 1.0f));
+                const float mc = __fadd_rn(__ll2float_rn(tile_sao_ssd(a.W, a.H, mt, c, row, lane, al)), __fmul_rn(a.lambda, 1.0f));
                 if (mc < cur) { info.merge_above = 1; info.luma = al; info.chroma = ac; }
             }
         }
@@ -826,42 +828,55 @@ __global__ void __cluster_dims__(MERGE_CTAS, 1, 1) __launch_bounds__(32 * MERGE_
 // flags any change; once a pass changes nothing the frame is exactly x = F(x).
 // Passes after a quiet pass return at once; if the last pass still changed a
 // pixel, k_sao_restore and k_sao_apply redo the frame in raster wavefront order.
+// One work item is 8 consecutive samples of a row (always inside one MB:
+// MBs are 16 luma / 8 chroma samples wide), read and written as 16-byte
+// chunks; the item's row and column come from one 32-bit division.
 __device__ __forceinline__ void sao_fix_body(const FrameArgs &a, int pass)
 {
     if (pass > 0 && __ldcg(&a.sao_flags[pass - 1]) == 0) return;
     const int cw = a.W / 2, ch = a.H / 2;
+    const int ly = a.H * (a.W / 8), lc = ch * (cw / 8);   // items per plane
     const size_t ny = (size_t)a.W * a.H, nc = (size_t)cw * ch;
     bool changed = false;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < ny + 2 * nc; i += (size_t)gridDim.x * blockDim.x) {
-        const int pl = i < ny ? 0 : (i < ny + nc ? 1 : 2);
-        const size_t k = pl == 0 ? i : (pl == 1 ? i - ny : i - ny - nc);
-        const int w = pl ? cw : a.W, h = pl ? ch : a.H, n = pl ? 8 : 16;
-        const int y = (int)(k / w), x = (int)(k % w);
-        const int m = (y / n) * a.mbw + x / n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ly + 2 * lc; i += gridDim.x * blockDim.x) {
+        const int pl = i < ly ? 0 : (i < ly + lc ? 1 : 2);
+        const int j = pl == 0 ? i : (pl == 1 ? i - ly : i - ly - lc);
+        const int w = pl ? cw : a.W, h = pl ? ch : a.H, sh = pl ? 3 : 4;   // MB size 8 / 16 = 1 << sh
+        const int cpr = w / 8, y = j / cpr, x0 = (j - y * cpr) * 8;
+        const int m = (y >> sh) * a.mbw + (x0 >> sh);
         const evxg_sao_params p = pl ? a.sao[m].chroma : a.sao[m].luma;
         if (p.type == 0) continue;
         const size_t off = pl == 0 ? 0 : (pl == 1 ? ny : ny + nc);
         const int16_t *orig = a.sao_orig + off;
         int16_t *img = a.planes[a.dpb] + off;
-        const int v = orig[k];
-        int corr = v;
-        if (p.type == 2) {
-            const int idx = (sclamp(v) >> 3) - p.band_position;
-            if (idx >= 0 && idx < 4) corr = sclamp(v + p.offsets[idx]);
-        } else {
-            const int ax = x + c_eo[p.eo_class][0], ay = y + c_eo[p.eo_class][1];
-            const int bx = x + c_eo[p.eo_class][2], by = y + c_eo[p.eo_class][3];
-            if (ax >= 0 && ax < w && ay >= 0 && ay < h && bx >= 0 && bx < w && by >= 0 && by < h) {
-                const int ma = (ay / n) * a.mbw + ax / n, mb = (by / n) * a.mbw + bx / n;
-                const size_t ka = (size_t)ay * w + ax, kb = (size_t)by * w + bx;
-                const int va = ma < m ? __ldcg(img + ka) : orig[ka];
-                const int vb = mb < m ? __ldcg(img + kb) : orig[kb];
-                const int ct = eo_cat(v, va, vb);
-                if (ct < 4) corr = sclamp(v + p.offsets[ct]);
+        const size_t k0 = (size_t)y * w + x0;
+        uint4 ov = *reinterpret_cast<const uint4 *>(orig + k0), iv = __ldcg(reinterpret_cast<const uint4 *>(img + k0));
+        const int16_t *o8 = reinterpret_cast<const int16_t *>(&ov);
+        int16_t *i8 = reinterpret_cast<int16_t *>(&iv);
+        bool any = false;
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const int x = x0 + e, v = o8[e];
+            int corr = v;
+            if (p.type == 2) {
+                const int idx = (sclamp(v) >> 3) - p.band_position;
+                if (idx >= 0 && idx < 4) corr = sclamp(v + p.offsets[idx]);
+            } else {
+                const int ax = x + c_eo[p.eo_class][0], ay = y + c_eo[p.eo_class][1];
+                const int bx = x + c_eo[p.eo_class][2], by = y + c_eo[p.eo_class][3];
+                if (ax >= 0 && ax < w && ay >= 0 && ay < h && bx >= 0 && bx < w && by >= 0 && by < h) {
+                    const int ma = (ay >> sh) * a.mbw + (ax >> sh), mb = (by >> sh) * a.mbw + (bx >> sh);
+                    const size_t ka = (size_t)ay * w + ax, kb = (size_t)by * w + bx;
+                    const int va = ma < m ? __ldcg(img + ka) : orig[ka];
+                    const int vb = mb < m ? __ldcg(img + kb) : orig[kb];
+                    const int ct = eo_cat(v, va, vb);
+                    if (ct < 4) corr = sclamp(v + p.offsets[ct]);
+                }
             }
+            if (i8[e] != corr) { i8[e] = (int16_t)corr; any = true; }
         }
-        if (__ldcg(img + k) != corr) {
-            img[k] = (int16_t)corr;
+        if (any) {   // the item's samples are this thread's alone
+            *reinterpret_cast<uint4 *>(img + k0) = iv;
             changed = true;
         }
     }
