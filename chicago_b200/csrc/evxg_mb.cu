@@ -7,11 +7,15 @@
 // src/video/transform.cpp, src/video/quantize.cpp, src/video/interp.cpp.
 //
 // Schedule.  A persistent grid of CTAs claims macroblock rows in order from an
-// atomic counter; a CTA processes its row left to right and, before MB (r,c),
-// waits until row r-1 has finished column min(c+4, cols-1): the reference's
-// WPP lag (encode.cpp:866-877).  With that lag every MB sees exactly the
-// reconstruction the sequential raster encoder sees: all raster-earlier MBs in
-// its search window are finished and no raster-later MB has been written, so
+// atomic counter; a CTA processes its row left to right and starts MB (r,c)
+// once row r-1 has finished column min(c+2, cols-1) (the reference's WPP waits
+// for c+4, encode.cpp:866-877).  MB (r,c) reads the destination slot at columns
+// c-3 .. c+3; the reads of column c+3 above row r (half-pel planes around a
+// selection at the right edge of the search range) wait for row r-1 to finish
+// c+3 first, and MB (r,c) writes back only after MB (r-1, c+3), whose reads
+// reach its stale pixels, has finished.  Every MB therefore sees exactly the
+// reconstruction the sequential raster encoder sees -- all raster-earlier MBs
+// it reads are finished and no raster-later MB it reads has been written -- so
 // the stale pixels the intra block-copy search and the 6-tap overshoot read in
 // the destination DPB slot are the same.  Waits are bounded by a timeout that
 // sets the device error word.
@@ -82,6 +86,10 @@ struct WinReq {
     int n;
     int wi[5], bx[5], by[5], mode[5];
     const int16_t *pl[5];
+    // window 0 only: rows [fy0, fy1) (luma) and [fcy0, fcy1) (chroma) of the
+    // columns just behind the new strip are read from memory again when the
+    // window shifts (they were loaded before the row above finished them)
+    int fy0, fy1, fcy0, fcy1;
 };
 struct Sel {                   // evx_motion_selection, motion.cpp:53-66
     int bx, by, sad, mad, ssd;
@@ -301,13 +309,21 @@ __device__ __noinline__ void load_windows(int W, int H)
     for (int e = threadIdx.x; e < ns * RT; e += NT) {
         const int k = shift[e / RT], r = e % RT;
         Win &w = S.win[q.wi[k]];
+        const bool fresh = q.wi[k] == 0;
         if (r < WL_ROWS) {
             int16_t *row = w.y + r * WL;
             const uint4 n0 = win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 16);
             const uint4 n1 = win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 8);
+            const bool again = fresh && r >= q.fy0 && r < q.fy1;
+            uint4 f0, f1;
+            if (again) {
+                f0 = win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 32);
+                f1 = win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 24);
+            }
             uint4 t[NLC - 2];
 #pragma unroll
             for (int j = 0; j < NLC - 2; j++) t[j] = *reinterpret_cast<const uint4 *>(row + 16 + 8 * j);
+            if (again) { t[NLC - 4] = f0; t[NLC - 3] = f1; }
 #pragma unroll
             for (int j = 0; j < NLC - 2; j++) *reinterpret_cast<uint4 *>(row + 8 * j) = t[j];
             *reinterpret_cast<uint4 *>(row + WL - 16) = n0;
@@ -317,12 +333,45 @@ __device__ __noinline__ void load_windows(int W, int H)
             const int16_t *U = q.pl[k] + (size_t)W * H, *V = U + (size_t)cw * ch;
             int16_t *row = (pl ? w.v : w.u) + cr * WC;
             const uint4 n0 = win_chunk(pl ? V : U, cw, ch, w.coy + cr, w.cox + WC - 8);
+            const bool again = fresh && cr >= q.fcy0 && cr < q.fcy1;
+            uint4 f0;
+            if (again) f0 = win_chunk(pl ? V : U, cw, ch, w.coy + cr, w.cox + WC - 16);
             uint4 t[NCC - 1];
 #pragma unroll
             for (int j = 0; j < NCC - 1; j++) t[j] = *reinterpret_cast<const uint4 *>(row + 8 + 8 * j);
+            if (again) t[NCC - 2] = f0;
 #pragma unroll
             for (int j = 0; j < NCC - 1; j++) *reinterpret_cast<uint4 *>(row + 8 * j) = t[j];
             *reinterpret_cast<uint4 *>(row + WC - 8) = n0;
+        }
+    }
+}
+
+// Rows of window 0 (loaded around (px, py-16)) that show MB row r-1 of the
+// destination slot: window rows [y0, y1) luma and [cy0, cy1) chroma.  For
+// r = 1 the rows clamped to plane row 0 (above the frame) show it too.
+__device__ __forceinline__ void rows_above(int py, int &y0, int &y1, int &cy0, int &cy1)
+{
+    y0 = y1 = cy0 = cy1 = 0;
+    if (py < 16) return;
+    y1 = WL_OFF + 16; cy1 = WC_OFF + 8;                          // plane rows py-16 .. py-1
+    y0 = py == 16 ? 0 : WL_OFF; cy0 = py == 16 ? 0 : WC_OFF;
+}
+// Read window 0's newest strip (luma columns WL-16.., chroma WC-8..: MB
+// column c+3) again for rows [y0, y1) / [cy0, cy1); threads of group g.
+__device__ void refresh_newest(const Grp g, Win &w, const int16_t *plane, int W, int H, int y0, int y1, int cy0, int cy1)
+{
+    const int gt = threadIdx.x - g.t0, cw = W / 2, ch = H / 2;
+    const int16_t *U = plane + (size_t)W * H, *V = U + (size_t)cw * ch;
+    const int nl = (y1 - y0) * 2, nc = (cy1 - cy0) * 2;
+    for (int e = gt; e < nl + nc; e += g.nt) {
+        if (e < nl) {
+            const int r = y0 + e / 2, j = e % 2;
+            *reinterpret_cast<uint4 *>(w.y + r * WL + WL - 16 + 8 * j) = win_chunk(plane, W, H, w.oy + r, w.ox + WL - 16 + 8 * j);
+        } else {
+            const int f = e - nl, p = f & 1, r = cy0 + f / 2;
+            *reinterpret_cast<uint4 *>((p ? w.v : w.u) + r * WC + WC - 8) =
+                win_chunk(p ? V : U, cw, ch, w.coy + r, w.cox + WC - 8);
         }
     }
 }
@@ -960,6 +1009,8 @@ __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, 
 
 // ------------------------------------------------------------- searches
 
+__device__ bool wait_progress(const FrameArgs &a, int r, int need);
+
 // Intra block-copy search in the current frame (motion.cpp:485-565), window 0.
 __device__ __noinline__ void intra_bc_search(const Grp g, const FrameArgs &a, int px, int py)
 {
@@ -982,6 +1033,23 @@ __device__ __noinline__ void intra_bc_search(const Grp g, const FrameArgs &a, in
             run_step(g, 0, 0, true, -st, -st, st, px, py, a.W, a.H, a.lambda);
             if (sr.sel.mad < S.thr) break;
         }
+    {
+        // The wavefront starts MB (r, c) once row r-1 has finished column c+2.
+        // The half-pel planes around a selection at x >= px+28 reach column
+        // c+3 (chroma from px+28, luma from px+30); if they reach it above row
+        // r, wait for row r-1 to finish c+3 and read that strip of window 0
+        // again.  (Integer candidates end at px+46, inside column c+2.)  A
+        // wait that gives up leaves the error word set; the frame has failed.
+        const int row = py / 16, col = px / 16;
+        if (row > 0 && col + 3 < a.mbw && sr.sel.bx >= px + 28 && sr.sel.by <= py + 5) {
+            if (gt == 0) wait_progress(a, row - 1, col + 3);
+            gsync(g);
+            int y0, y1, cy0, cy1;
+            rows_above(py, y0, y1, cy0, cy1);
+            refresh_newest(g, S.win[0], a.planes[a.dpb], a.W, a.H, y0, y1, cy0, cy1);
+            gsync(g);
+        }
+    }
     run_subpel(g, 0, 0, true, px, py, a.W, a.H);
     if (gt == 0) {
         fill_desc(sr.sel, px, py, true, S.thr, sr.out.d);
@@ -1137,11 +1205,21 @@ __device__ __noinline__ void setup_mb(const FrameArgs &a, int idx, int px, int p
         S.sep = S.has_pred && (S.qx != px || S.qy != py);
     }
     S.req.n = 0;
+    S.req.fy0 = S.req.fy1 = S.req.fcy0 = S.req.fcy1 = 0;
 }
+// Window 0's request: the slot being reconstructed around (px, py-16), with
+// the rows that show MB row r-1 read again behind the new strip.
+__device__ void req_window0(const FrameArgs &a, int px, int py);
 __device__ void req_window(int wi, const int16_t *pl, int bx, int by)   // one thread
 {
     WinReq &q = SM().req;
     q.wi[q.n] = wi; q.pl[q.n] = pl; q.bx[q.n] = bx; q.by[q.n] = by; q.n++;
+}
+__device__ void req_window0(const FrameArgs &a, int px, int py)   // one thread
+{
+    req_window(0, a.planes[a.dpb], px, py - 16);
+    WinReq &q = SM().req;
+    rows_above(py, q.fy0, q.fy1, q.fcy0, q.fcy1);
 }
 
 // Neighbours for directional intra (intra_pred.cpp:13-54); sample(p, y, x)
@@ -1325,7 +1403,8 @@ __device__ void write_back(const FrameArgs &a, int px, int py, int idx, const in
     // an MB on the top, bottom or left edge the next MB loads window 0 afresh.
     if (tid == 0 && (px == 0 || py == 0 || py + 16 == a.H)) w0.valid = 0;
     if (tid < 7) reinterpret_cast<int *>(a.bt + idx)[tid] = reinterpret_cast<const int *>(&S.cd[ch].d)[tid];
-    __threadfence();   // every writer orders its stores before the row's progress release
+    // the caller publishes after a CTA barrier with one fence by the releasing
+    // thread (the barrier orders every writer's stores before that fence)
 }
 
 // Thread 0: wait until row r has finished column need (the wavefront's
@@ -1364,12 +1443,11 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
     MbShared &S = SM();
     const int tid = threadIdx.x;
     const int px = col * 16, py = row * 16, idx = row * a.mbw + col;
-    int16_t *dst = a.planes[a.dpb];
 
     load_src(a, px, py);
     if (tid == 0) {
         setup_mb(a, idx, px, py, a.type != EVXG_FRAME_INTRA, nullptr);
-        req_window(0, dst, px, py - 16);   // intra window: the slot being reconstructed
+        req_window0(a, px, py);   // intra window: the slot being reconstructed
         if (a.type != EVXG_FRAME_INTRA) {
             req_window(1, a.planes[a.ref_fwd], px, py);
             if (S.sep) req_window(2, a.planes[a.ref_fwd], S.qx, S.qy);
@@ -1415,7 +1493,12 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
     if (tid == 0) decide(a);
     __syncthreads();
     if (S.need_encode) encode_candidates(G_ALL, a, 4, 1);
-    if (tid == 0) rdo_choose();
+    if (tid == 0) {
+        rdo_choose();
+        // MB (r-1, c+3), started before this one, may read this MB's stale
+        // pixels (its 6-tap reach ends at column c): write back after it.
+        if (row > 0) wait_progress(a, row - 1, min(col + 3, a.mbw - 1));
+    }
     __syncthreads();
     write_back(a, px, py, idx, S.rec[S.chosen], S.lev[S.chosen]);
 }
@@ -1428,20 +1511,25 @@ __device__ bool mb_row(const FrameArgs &a, int row)
     const int tid = threadIdx.x;
     for (int col = 0; col < a.mbw; ++col) {
         if (tid == 0) {
-            // Row r-1 must have finished column c+3: the reads of MB (r,c)
-            // (intra block-copy candidates x in [px-31, px+31], 6-tap
-            // overshoot -3..+18) reach columns c-3 .. c+3.  Rows below
-            // then trail by three columns too, so row r+1 has finished at
-            // most column c-4 and the stale pixels MB (r,c) reads there
-            // (columns >= c-3) are still unwritten.  The reference waits
-            // for c+4 (encode.cpp:866-877); c+3 gives the same pixels.
-            S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 3, a.mbw - 1));
+            // MB (r,c) reads the destination slot at columns c-3 .. c+3 (intra
+            // block-copy candidates x in [px-31, px+31], 6-tap overshoot
+            // -3..+18).  It starts once row r-1 has finished column c+2,
+            // which covers every read but the half-pel planes that reach
+            // column c+3 (intra_bc_search waits for those), and it writes
+            // back only after MB (r-1, c+3), whose reads reach this MB's
+            // stale pixels, has finished.  Every MB then reads what the
+            // sequential raster encoder reads.  The reference waits for
+            // c+4 (encode.cpp:866-877).
+            S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 2, a.mbw - 1));
         }
         __syncthreads();
         if (S.row_abort) return false;
         process_mb(a, row, col);
         __syncthreads();
-        if (tid == 0) st_release(&a.progress[row], col);
+        if (tid == 0) {
+            __threadfence();
+            st_release(&a.progress[row], col);
+        }
     }
     __syncthreads();
     return true;
@@ -1577,13 +1665,13 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
     MbShared &S = SM();
     const int tid = threadIdx.x;
     const int px = col * 16, py = row * 16, idx = row * a.mbw + col;
-    if (tid == 0) S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 3, a.mbw - 1));
+    if (tid == 0) S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 2, a.mbw - 1));   // see mb_row
     __syncthreads();
     if (S.row_abort) return false;
     load_src(a, px, py);
     if (tid == 0) {
         setup_mb(a, idx, px, py, false, nullptr);
-        req_window(0, a.planes[a.dpb], px, py - 16);
+        req_window0(a, px, py);
     }
     __syncthreads();
     load_windows(a.W, a.H);
@@ -1618,11 +1706,14 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
         if (a.type == EVXG_FRAME_INTER) publish_decision(S.cd[S.chosen].d, n);
     }
     __syncthreads();
+    if (tid == 0 && row > 0) wait_progress(a, row - 1, min(col + 3, a.mbw - 1));   // write back after MB (r-1, c+3)
+    __syncthreads();
     const int ch = S.chosen;
     const bool remote = a.type == EVXG_FRAME_INTER && ch < 4;   // an intra candidate encoded by rank 2
     write_back(a, px, py, idx, remote ? peer(S.rec[ch], 2) : S.rec[ch], remote ? peer(S.lev[ch], 2) : S.lev[ch]);
     __syncthreads();
     if (tid == 0) {
+        __threadfence();
         st_release(&a.progress[row], col);
         st_release_cl(peer(&S.mail.wr_seq, 2), n);
     }
