@@ -1495,9 +1495,7 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
     if (S.need_encode) encode_candidates(G_ALL, a, 4, 1);
     if (tid == 0) {
         rdo_choose();
-        // MB (r-1, c+3), started before this one, may read this MB's stale
-        // pixels (its 6-tap reach ends at column c): write back after it.
-        if (row > 0) wait_progress(a, row - 1, min(col + 3, a.mbw - 1));
+        if (row == 1) wait_progress(a, 0, min(col + 3, a.mbw - 1));   // see mb_row
     }
     __syncthreads();
     write_back(a, px, py, idx, S.rec[S.chosen], S.lev[S.chosen]);
@@ -1514,12 +1512,16 @@ __device__ bool mb_row(const FrameArgs &a, int row)
             // MB (r,c) reads the destination slot at columns c-3 .. c+3 (intra
             // block-copy candidates x in [px-31, px+31], 6-tap overshoot
             // -3..+18).  It starts once row r-1 has finished column c+2,
-            // which covers every read but the half-pel planes that reach
-            // column c+3 (intra_bc_search waits for those), and it writes
-            // back only after MB (r-1, c+3), whose reads reach this MB's
-            // stale pixels, has finished.  Every MB then reads what the
-            // sequential raster encoder reads.  The reference waits for
-            // c+4 (encode.cpp:866-877).
+            // which covers every read above it but the half-pel planes that
+            // reach column c+3 (intra_bc_search waits for those).  Its reads of
+            // stale pixels below (rows r+1, r+2) come from window 0, whose
+            // strips were read from memory when they came into view, at
+            // MB (r, c-3) or earlier -- before row r+1 can have written them --
+            // except in row 0, whose every MB reads its window afresh (the top
+            // edge); so MBs of row 1 write back only after MB (0, c+3) has
+            // finished (row 2 then follows through row 1's schedule).  Every
+            // MB reads what the sequential raster encoder reads.  The
+            // reference waits for c+4 (encode.cpp:866-877).
             S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 2, a.mbw - 1));
         }
         __syncthreads();
@@ -1706,7 +1708,7 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
         if (a.type == EVXG_FRAME_INTER) publish_decision(S.cd[S.chosen].d, n);
     }
     __syncthreads();
-    if (tid == 0 && row > 0) wait_progress(a, row - 1, min(col + 3, a.mbw - 1));   // write back after MB (r-1, c+3)
+    if (tid == 0 && row == 1) wait_progress(a, 0, min(col + 3, a.mbw - 1));   // see mb_row
     __syncthreads();
     const int ch = S.chosen;
     const bool remote = a.type == EVXG_FRAME_INTER && ch < 4;   // an intra candidate encoded by rank 2
