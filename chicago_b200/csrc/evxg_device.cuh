@@ -50,18 +50,9 @@ __device__ __forceinline__ float rd_cost(int a, float lambda, unsigned b)
     return __fadd_rn(__int2float_rn(a), __fmul_rn(lambda, __uint2float_rn(b)));
 }
 
-__device__ __forceinline__ int warp_sum(int v)
-{
-#pragma unroll
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-__device__ __forceinline__ int warp_max(int v)
-{
-#pragma unroll
-    for (int o = 16; o; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
+// Whole-warp integer sum / max (wrapping sum: the order does not matter).
+__device__ __forceinline__ int warp_sum(int v) { return __reduce_add_sync(0xffffffffu, v); }
+__device__ __forceinline__ int warp_max(int v) { return __reduce_max_sync(0xffffffffu, v); }
 __device__ __forceinline__ long long warp_sum64(long long v)
 {
 #pragma unroll

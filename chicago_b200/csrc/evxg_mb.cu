@@ -118,8 +118,8 @@ struct HalfPlanes {
 struct Srch {
     HalfPlanes<16> hy;
     HalfPlanes<8> hu, hv;
-    int m_sad[9], m_mad[9], valid[9];
-    float m_cost[9];           // RD cost of each pattern slot
+    int m_sad[2][9], m_mad[2][9], valid[8];   // pattern slot metrics, by step parity; sub-pel validity
+    float m_cost[2][9];        // RD cost of each pattern slot
     int spm[8][4];
     Sel sel;
     int cur;                   // window the search runs in
@@ -376,51 +376,87 @@ __device__ void refresh_newest(const Grp g, Win &w, const int16_t *plane, int W,
     }
 }
 
-// SAD (luma), MAD (Y, U, V) and SATD (luma) of the 16x16 block at plane
-// position (x, y) against the source; one warp, every lane gets the sums.
-// analysis.h:89-202.
-struct Metrics {
-    int sad, mad, satd;
+// Candidate metrics (analysis.h:89-202): SAD (luma), MAD (Y, U, V) and SATD
+// (luma) of the 16x16 block at plane position (x, y) against the source.  A
+// warp evaluates two candidates, one per half: lane & 15 of a half owns luma
+// 4x4 block lane & 15 (rows 4*(b>>2).., columns 4*(b&3)..) and chroma row
+// lane & 7 of plane (lane >> 3) & 1, so every lane runs the same 16 luma and
+// 8 chroma samples.  SrcLane holds that lane's source samples.
+struct SrcLane {
+    int y[16], c[8];
 };
-__device__ __noinline__ Metrics warp_metrics(const int16_t *src, const Win &w, int x, int y, int lane)
+__device__ __forceinline__ void unpack2(unsigned w, int &lo, int &hi) { lo = (int)(int16_t)(w & 0xffffu); hi = (int)w >> 16; }
+__device__ __forceinline__ SrcLane src_lane(const int16_t *src, int lane)   // src: 16-byte aligned MB buffer
 {
-    int sad = 0, mad = 0, satd = 0;
-    if (lane < 16) {
-        const int lx = x - w.ox, ly = y - w.oy;
-        const int rr = (lane >> 2) * 4, cc = (lane & 3) * 4;
-        int d[16];
+    SrcLane o;
+    const int b = lane & 15, r0 = (b >> 2) * 4, c0 = (b & 3) * 4;
 #pragma unroll
-        for (int r = 0; r < 4; r++)
+    for (int r = 0; r < 4; r++) {
+        const uint2 w = *reinterpret_cast<const uint2 *>(src + (r0 + r) * 16 + c0);
+        unpack2(w.x, o.y[r * 4], o.y[r * 4 + 1]);
+        unpack2(w.y, o.y[r * 4 + 2], o.y[r * 4 + 3]);
+    }
+    const uint4 w = *reinterpret_cast<const uint4 *>(src + 256 + ((lane >> 3) & 1) * 64 + (lane & 7) * 8);
+    unpack2(w.x, o.c[0], o.c[1]); unpack2(w.y, o.c[2], o.c[3]);
+    unpack2(w.z, o.c[4], o.c[5]); unpack2(w.w, o.c[6], o.c[7]);
+    return o;
+}
+// Samples x0 .. x0+3 of a 4-byte aligned row, any x0 >= 0: three words, two
+// byte permutes picking the aligned pairs (the third word is read also when
+// x0 is even; every window row has room for it).
+__device__ __forceinline__ void ld4(const int16_t *row, int x0, int v[4])
+{
+    const unsigned *w = reinterpret_cast<const unsigned *>(row) + (x0 >> 1);
+    const unsigned a = w[0], b = w[1], c = w[2], sel = (x0 & 1) ? 0x5432u : 0x3210u;
+    unpack2(__byte_perm(a, b, sel), v[0], v[1]);
+    unpack2(__byte_perm(b, c, sel), v[2], v[3]);
+}
+// This lane's share of the metrics of the candidate at (x, y) in window w.
+__device__ __forceinline__ void half_metrics(const SrcLane &sl, const Win &w, int x, int y, int lane, int &sad, int &mad, int &satd)
+{
+    const int b = lane & 15, r0 = (b >> 2) * 4, c0 = (b & 3) * 4;
+    const int lx = x - w.ox, ly = y - w.oy;
+    sad = 0; mad = 0; satd = 0;
+    int t[16];
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
-                int df = src[(rr + r) * 16 + cc + c] - w.y[(ly + rr + r) * WL + lx + cc + c];
-                int a = iabs32(df);
-                sad += a;
-                mad = max(mad, a);
-                d[r * 4 + c] = (int16_t)df;   // analysis.h:97 stores the difference as int16
-            }
-        int t[16];
-#pragma unroll
-        for (int r = 0; r < 4; r++) {     // hadamard_4x4, analysis.h:44-85
-            int a = d[r * 4], b = d[r * 4 + 1], c = d[r * 4 + 2], e = d[r * 4 + 3];
-            t[r * 4 + 0] = (a + b) + (c + e); t[r * 4 + 1] = (a - b) + (c - e);
-            t[r * 4 + 2] = (a + b) - (c + e); t[r * 4 + 3] = (a - b) - (c - e);
-        }
+    for (int r = 0; r < 4; r++) {
+        int v[4], d[4];
+        ld4(w.y + (ly + r0 + r) * WL, lx + c0, v);
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-            int a = t[c], b = t[4 + c], cc2 = t[8 + c], e = t[12 + c];
-            satd += iabs32((a + b) + (cc2 + e)) + iabs32((a - b) + (cc2 - e)) +
-                    iabs32((a + b) - (cc2 + e)) + iabs32((a - b) - (cc2 - e));
+            const int df = sl.y[r * 4 + c] - v[c], a = iabs32(df);
+            sad += a;
+            mad = max(mad, a);
+            d[c] = (int16_t)df;   // analysis.h:97 stores the difference as int16
         }
-    } else {
-        const int k = lane - 16, pl = k >> 3, row = k & 7;
-        const int cx = (x >> 1) - w.cox, cy = (y >> 1) - w.coy;
-        const int16_t *pp = (pl ? w.v : w.u) + (cy + row) * WC + cx;
-        const int16_t *sp = src + 256 + pl * 64 + row * 8;
-#pragma unroll
-        for (int c = 0; c < 8; c++) mad = max(mad, iabs32(sp[c] - pp[c]));
+        // hadamard_4x4 (analysis.h:44-85): the row pass, then the column pass below
+        t[r * 4 + 0] = (d[0] + d[1]) + (d[2] + d[3]); t[r * 4 + 1] = (d[0] - d[1]) + (d[2] - d[3]);
+        t[r * 4 + 2] = (d[0] + d[1]) - (d[2] + d[3]); t[r * 4 + 3] = (d[0] - d[1]) - (d[2] - d[3]);
     }
-    return Metrics{warp_sum(sad), warp_max(mad), (warp_sum(satd) + 1) >> 1};
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int a = t[c], bb = t[4 + c], cc = t[8 + c], e = t[12 + c];
+        satd += iabs32((a + bb) + (cc + e)) + iabs32((a - bb) + (cc - e)) +
+                iabs32((a + bb) - (cc + e)) + iabs32((a - bb) - (cc - e));
+    }
+    const int cx = (x >> 1) - w.cox, cy = (y >> 1) - w.coy;
+    const int16_t *pp = (((lane >> 3) & 1) ? w.v : w.u) + (cy + (lane & 7)) * WC;
+    int v[8];
+    ld4(pp, cx, v);
+    ld4(pp, cx + 4, v + 4);
+#pragma unroll
+    for (int c = 0; c < 8; c++) mad = max(mad, iabs32(sl.c[c] - v[c]));
+}
+// Sum / max over each half of the warp (every lane gets its half's value).
+__device__ __forceinline__ int half_sum(int v, int lane)
+{
+    const int lo = __reduce_add_sync(0xffffffffu, lane < 16 ? v : 0), hi = __reduce_add_sync(0xffffffffu, lane < 16 ? 0 : v);
+    return lane < 16 ? lo : hi;
+}
+__device__ __forceinline__ int half_max(int v, int lane)   // v >= 0
+{
+    const int lo = __reduce_max_sync(0xffffffffu, lane < 16 ? v : 0), hi = __reduce_max_sync(0xffffffffu, lane < 16 ? 0 : v);
+    return lane < 16 ? lo : hi;
 }
 // RD cost of an integer candidate: (float)satd + lambda * (|mvx| + |mvy| + 1)
 // with the motion vector taken as int16 (motion.cpp:136-146).
@@ -464,61 +500,69 @@ __device__ __forceinline__ void warp_replay(Sel &s, bool ok, int lane, int thr, 
 }
 
 // One pattern step (perform_intra/inter_motion_search, motion.cpp:348-406) on
-// a warp group: every warp evaluates slots of the 3x3 pattern (validity is
-// decided identically by all lanes), then the group leader replays the
-// reference's loop order in registers, with its early exit.
+// a warp group, from selection s: every warp evaluates two slots of the 3x3
+// pattern (validity is decided identically by all lanes) into the metrics
+// buffer of step parity par, then every warp replays the reference's loop
+// order in registers, with its early exit, and returns the new selection --
+// the same in every warp, so no second barrier is needed (a buffer is
+// rewritten two steps later, after the next step's barrier).
 //
 // When the pattern is centred on the selection (l = t = -st) its centre slot
-// is the selection itself, whose SAD, MAD and cost are already in sr.sel:
-// every selection but the intra search's starting point was accepted from a
+// is the selection itself, whose SAD, MAD and cost are already in s: every
+// selection but the intra search's starting point was accepted from a
 // candidate evaluation (its stored sad/mad/cost are that candidate's), and
 // that starting point lies in the excluded region, so it is never valid.
-// The eight remaining slots take two rounds on four warps instead of three.
-__device__ __noinline__ void run_step(const Grp g, int si, int wi, bool intra, int l, int t, int st, int px, int py,
-                                      int W, int H, float lambda)
+// The eight remaining slots take one round of four warps.
+__device__ __noinline__ Sel run_step(const Grp g, int si, int wi, bool intra, int l, int t, int st, int px, int py,
+                                     int W, int H, float lambda, Sel s, int par)
 {
     MbShared &S = SM();
     Srch &sr = S.srch[si];
     const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31, nw = g.nt >> 5;
-    const int bx = sr.sel.bx, by = sr.sel.by;
+    const int bx = s.bx, by = s.by;
     const bool centred = l == -st && t == -st;
     const int n = centred ? 8 : 9;
-    for (int j = gw; j < n; j += nw) {
-        const int k = centred && j >= 4 ? j + 1 : j;
-        const int x = bx + l + (k % 3) * st, y = by + t + (k / 3) * st;
-        const bool ok = !(intra && y > py - 16 && x > px - 16) && !(x < 0 || x > W - 16 || y < 0 || y > H - 16);
-        if (lane == 0) sr.valid[k] = ok;
-        if (ok) {
-            const Metrics m = warp_metrics(S.src, S.win[wi], x, y, lane);
-            if (lane == 0) { sr.m_sad[k] = m.sad; sr.m_mad[k] = m.mad; sr.m_cost[k] = cand_cost(m.satd, x, y, px, py, lambda); }
+    auto valid = [&](int x, int y) {
+        return !(intra && y > py - 16 && x > px - 16) && !(x < 0 || x > W - 16 || y < 0 || y > H - 16);
+    };
+    if (2 * gw < n) {
+        const SrcLane sl = src_lane(S.src, lane);
+        for (int j0 = 2 * gw; j0 < n; j0 += 2 * nw) {
+            const int j = j0 + (lane >> 4);
+            const int k = centred && j >= 4 ? j + 1 : j;
+            const int x = bx + l + (k % 3) * st, y = by + t + (k / 3) * st;
+            const bool ok = j < n && valid(x, y);
+            int sad = 0, mad = 0, satd = 0;
+            if (ok) half_metrics(sl, S.win[wi], x, y, lane, sad, mad, satd);
+            sad = half_sum(sad, lane); mad = half_max(mad, lane); satd = (half_sum(satd, lane) + 1) >> 1;
+            if ((lane & 15) == 0 && ok) {
+                sr.m_sad[par][k] = sad; sr.m_mad[par][k] = mad; sr.m_cost[par][k] = cand_cost(satd, x, y, px, py, lambda);
+            }
         }
     }
     gsync(g);
-    if (gw == 0) {   // the reference's loop order, with its early exit
-        Sel s = sr.sel;
-        const int k = lane < 9 ? lane : 0;
-        const int x = bx + l + (k % 3) * st, y = by + t + (k / 3) * st;
-        const int ssd = (x - px) * (x - px) + (y - py) * (y - py);
-        bool ok;
-        int sad, mad;
-        float cost;
-        if (centred && k == 4) {   // the selection itself; invalid only as the intra search's starting point
-            ok = !(intra && y > py - 16 && x > px - 16);
-            sad = s.sad; mad = s.mad; cost = s.cost;
-        } else {
-            ok = sr.valid[k]; sad = sr.m_sad[k]; mad = sr.m_mad[k]; cost = sr.m_cost[k];
-        }
-        ok = ok && lane < 9;
-        warp_replay(s, ok, lane, S.thr, true,
-                    [&](const Sel &c) { return takes_int(c, sad, mad, ssd, cost, S.thr); },
-                    [&](Sel &c, int from) {
-                        c.bx = __shfl_sync(0xffffffffu, x, from); c.by = __shfl_sync(0xffffffffu, y, from);
-                        c.sad = __shfl_sync(0xffffffffu, sad, from); c.mad = __shfl_sync(0xffffffffu, mad, from);
-                        c.ssd = __shfl_sync(0xffffffffu, ssd, from); c.cost = __shfl_sync(0xffffffffu, cost, from);
-                    });
-        if (lane == 0) sr.sel = s;
+    // the reference's loop order, with its early exit (every warp)
+    const int k = lane < 9 ? lane : 0;
+    const int x = bx + l + (k % 3) * st, y = by + t + (k / 3) * st;
+    const int ssd = (x - px) * (x - px) + (y - py) * (y - py);
+    bool ok;
+    int sad, mad;
+    float cost;
+    if (centred && k == 4) {   // the selection itself; invalid only as the intra search's starting point
+        ok = !(intra && y > py - 16 && x > px - 16);
+        sad = s.sad; mad = s.mad; cost = s.cost;
+    } else {
+        ok = valid(x, y); sad = sr.m_sad[par][k]; mad = sr.m_mad[par][k]; cost = sr.m_cost[par][k];
     }
-    gsync(g);
+    ok = ok && lane < 9;
+    warp_replay(s, ok, lane, S.thr, true,
+                [&](const Sel &c) { return takes_int(c, sad, mad, ssd, cost, S.thr); },
+                [&](Sel &c, int from) {
+                    c.bx = __shfl_sync(0xffffffffu, x, from); c.by = __shfl_sync(0xffffffffu, y, from);
+                    c.sad = __shfl_sync(0xffffffffu, sad, from); c.mad = __shfl_sync(0xffffffffu, mad, from);
+                    c.ssd = __shfl_sync(0xffffffffu, ssd, from); c.cost = __shfl_sync(0xffffffffu, cost, from);
+                });
+    return s;
 }
 
 // Half-pel planes for one plane block (window plane pl, stride S, selection at
@@ -558,17 +602,21 @@ __device__ __forceinline__ int half_at(const HalfPlanes<N> &hp, int dx, int dy, 
     return hp.dd[ry * (N + 1) + cx];
 }
 
-// Sub-pel refinement around the selection (motion.cpp:180-261, :408-483).
-// The interpolation reads only the selection, which the refinement does not
-// move, so the three half-pel planes are built once and each direction's
-// half and quarter blocks (quarter = (full + half + 1) >> 1) are read from them.
-__device__ __noinline__ void run_subpel(const Grp g, int si, int wi, bool intra, int px, int py, int W, int H)
+// Sub-pel refinement around selection s (motion.cpp:180-261, :408-483); the
+// result goes to sr.sel (every thread of the group reads it after the final
+// barrier).  The interpolation reads only the selection, which the
+// refinement does not move, so the three half-pel planes are built once and
+// each direction's half and quarter blocks (quarter = (full + half + 1) >> 1)
+// are read from them.  One warp per direction, every lane the same share:
+// luma column lane & 15, rows 8*(lane >> 4) .. +7, and chroma plane lane >> 4,
+// column lane & 7, rows 4*((lane >> 3) & 1) .. +3.
+__device__ __noinline__ void run_subpel(const Grp g, int si, int wi, bool intra, int px, int py, int W, int H, Sel s)
 {
     MbShared &S = SM();
     Srch &sr = S.srch[si];
     const Win &w = S.win[wi];
     const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31, nw = g.nt >> 5;
-    const int bx = sr.sel.bx, by = sr.sel.by;
+    const int bx = s.bx, by = s.by;
     const int lx = bx - w.ox, ly = by - w.oy, cx = (bx >> 1) - w.cox, cy = (by >> 1) - w.coy;
     half_planes_a<16>(sr.hy, w.y, WL, lx, ly, gt, g.nt);
     for (int p = 0; p < 2; p++) half_planes_a<8>(p ? sr.hv : sr.hu, p ? w.v : w.u, WC, cx, cy, gt, g.nt);
@@ -576,42 +624,49 @@ __device__ __noinline__ void run_subpel(const Grp g, int si, int wi, bool intra,
     half_planes_b<16>(sr.hy, gt, g.nt);
     for (int p = 0; p < 2; p++) half_planes_b<8>(p ? sr.hv : sr.hu, gt, g.nt);
     gsync(g);
-    for (int k = gw; k < 8; k += nw) {
-        const int r = k < 4 ? k : k + 1, i = r % 3 - 1, j = r / 3 - 1;
-        const int x = bx + i, y = by + j;
-        const bool ok = !(intra && y > py - 16 && x > px - 16) && !(x < 0 || x > W - 16 || y < 0 || y > H - 16);
-        if (lane == 0) sr.valid[k] = ok;
-        if (!ok) continue;
-        int sh = 0, mh = 0, sq = 0, mq = 0;
-        if (lane < 16) {   // luma column
-#pragma unroll 4
-            for (int rr = 0; rr < 16; rr++) {
-                const int half = half_at<16>(sr.hy, i, j, rr, lane);
-                const int full = w.y[(ly + rr) * WL + lx + lane];
+    if (gw < 8) {
+        const int lc = lane & 15, r0 = (lane >> 4) * 8;
+        const int pl = lane >> 4, cc = lane & 7, cr0 = ((lane >> 3) & 1) * 4;
+        const HalfPlanes<8> &hc = pl ? sr.hv : sr.hu;
+        const int16_t *fy = w.y + (ly + r0) * WL + lx + lc, *fc = (pl ? w.v : w.u) + (cy + cr0) * WC + cx + cc;
+        int sy[8], sc[4];
+#pragma unroll
+        for (int r = 0; r < 8; r++) sy[r] = S.src[(r0 + r) * 16 + lc];
+#pragma unroll
+        for (int r = 0; r < 4; r++) sc[r] = S.src[256 + pl * 64 + (cr0 + r) * 8 + cc];
+        for (int k = gw; k < 8; k += nw) {
+            const int r = k < 4 ? k : k + 1, i = r % 3 - 1, j = r / 3 - 1;
+            const int x = bx + i, y = by + j;
+            const bool ok = !(intra && y > py - 16 && x > px - 16) && !(x < 0 || x > W - 16 || y < 0 || y > H - 16);
+            if (lane == 0) sr.valid[k] = ok;
+            if (!ok) continue;
+            // direction (i, j)'s half-pel block inside a plane (half_at)
+            const int16_t *hy, *hcp;
+            int ys, cs;
+            if (i && !j) { hy = sr.hy.hh + 3 * 17 + (i > 0); ys = 17; hcp = hc.hh + 3 * 9 + (i > 0); cs = 9; }
+            else if (!i && j) { hy = sr.hy.vv + (j > 0) * 16; ys = 16; hcp = hc.vv + (j > 0) * 8; cs = 8; }
+            else { hy = sr.hy.dd + (j > 0) * 17 + (i > 0); ys = 17; hcp = hc.dd + (j > 0) * 9 + (i > 0); cs = 9; }
+            hy += r0 * ys + lc; hcp += cr0 * cs + cc;
+            int sh = 0, mh = 0, sq = 0, mq = 0;
+#pragma unroll
+            for (int rr = 0; rr < 8; rr++) {
+                const int half = hy[rr * ys], full = fy[rr * WL];
                 const int q = (int16_t)((full + half + 1) >> 1);
-                const int s0 = S.src[rr * 16 + lane];
-                const int ah = iabs32(s0 - half), aq = iabs32(s0 - q);
+                const int ah = iabs32(sy[rr] - half), aq = iabs32(sy[rr] - q);
                 sh += ah; sq += aq; mh = max(mh, ah); mq = max(mq, aq);
             }
-        } else {           // chroma column
-            const int kk = lane - 16, pl = kk >> 3, c = kk & 7;
-            const HalfPlanes<8> &hp = pl ? sr.hv : sr.hu;
-            const int16_t *fp = pl ? w.v : w.u;
-#pragma unroll 4
-            for (int rr = 0; rr < 8; rr++) {
-                const int half = half_at<8>(hp, i, j, rr, c);
-                const int full = fp[(cy + rr) * WC + cx + c];
+#pragma unroll
+            for (int rr = 0; rr < 4; rr++) {
+                const int half = hcp[rr * cs], full = fc[rr * WC];
                 const int q = (int16_t)((full + half + 1) >> 1);
-                const int s0 = S.src[256 + pl * 64 + rr * 8 + c];
-                mh = max(mh, iabs32(s0 - half)); mq = max(mq, iabs32(s0 - q));
+                mh = max(mh, iabs32(sc[rr] - half)); mq = max(mq, iabs32(sc[rr] - q));
             }
+            sh = warp_sum(sh); mh = warp_max(mh); sq = warp_sum(sq); mq = warp_max(mq);
+            if (lane == 0) { sr.spm[k][0] = sh; sr.spm[k][1] = mh; sr.spm[k][2] = sq; sr.spm[k][3] = mq; }
         }
-        sh = warp_sum(sh); mh = warp_max(mh); sq = warp_sum(sq); mq = warp_max(mq);
-        if (lane == 0) { sr.spm[k][0] = sh; sr.spm[k][1] = mh; sr.spm[k][2] = sq; sr.spm[k][3] = mq; }
     }
     gsync(g);
     if (gw == 0) {   // 8 directions x (half, quarter), in the reference's order
-        Sel s = sr.sel;
         const int thr = S.thr;
         s.sp_index = 0; s.sp_amount = 0; s.sp_enabled = 0;
         const int k = (lane >> 1) & 7, q = lane & 1, r = k < 4 ? k : k + 1;
@@ -1027,12 +1082,14 @@ __device__ __noinline__ void intra_bc_search(const Grp g, const FrameArgs &a, in
         }
     }
     gsync(g);
-    run_step(g, 0, 0, true, -SEARCH_RADIUS, -(SEARCH_RADIUS << 1), SEARCH_RADIUS, px, py, a.W, a.H, a.lambda);
-    if (sr.sel.mad >= S.thr)
-        for (int st = SEARCH_RADIUS >> 1; st > 0; st >>= 1) {
-            run_step(g, 0, 0, true, -st, -st, st, px, py, a.W, a.H, a.lambda);
-            if (sr.sel.mad < S.thr) break;
+    Sel s = run_step(g, 0, 0, true, -SEARCH_RADIUS, -(SEARCH_RADIUS << 1), SEARCH_RADIUS, px, py, a.W, a.H, a.lambda, sr.sel, 0);
+    if (s.mad >= S.thr) {
+        int par = 1;
+        for (int st = SEARCH_RADIUS >> 1; st > 0; st >>= 1, par ^= 1) {
+            s = run_step(g, 0, 0, true, -st, -st, st, px, py, a.W, a.H, a.lambda, s, par);
+            if (s.mad < S.thr) break;
         }
+    }
     {
         // The wavefront starts MB (r, c) once row r-1 has finished column c+2.
         // The half-pel planes around a selection at x >= px+28 reach column
@@ -1041,7 +1098,7 @@ __device__ __noinline__ void intra_bc_search(const Grp g, const FrameArgs &a, in
         // again.  (Integer candidates end at px+46, inside column c+2.)  A
         // wait that gives up leaves the error word set; the frame has failed.
         const int row = py / 16, col = px / 16;
-        if (row > 0 && col + 3 < a.mbw && sr.sel.bx >= px + 28 && sr.sel.by <= py + 5) {
+        if (row > 0 && col + 3 < a.mbw && s.bx >= px + 28 && s.by <= py + 5) {
             if (gt == 0) wait_progress(a, row - 1, col + 3);
             gsync(g);
             int y0, y1, cy0, cy1;
@@ -1050,7 +1107,7 @@ __device__ __noinline__ void intra_bc_search(const Grp g, const FrameArgs &a, in
             gsync(g);
         }
     }
-    run_subpel(g, 0, 0, true, px, py, a.W, a.H);
+    run_subpel(g, 0, 0, true, px, py, a.W, a.H, s);
     if (gt == 0) {
         fill_desc(sr.sel, px, py, true, S.thr, sr.out.d);
         sr.out_sad = sr.sel.sad;
@@ -1106,35 +1163,38 @@ __device__ __noinline__ void inter_search(const Grp g, const FrameArgs &a, int s
     MbShared &S = SM();
     Srch &sr = S.srch[si];
     const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31;
-    if (gw == 0) {
-        const Metrics m = warp_metrics(S.src, S.win[wa], px, py, lane);
-        if (lane == 0) { sr.m_sad[0] = m.sad; sr.m_mad[0] = m.mad; sr.m_cost[0] = rd_cost(m.satd, a.lambda, 1u); }
-    }
-    if (gw == 1 && S.has_pred) {
-        const Metrics m = warp_metrics(S.src, S.win[S.sep ? wb : wa], S.qx, S.qy, lane);
-        if (lane == 0) { sr.m_sad[1] = m.sad; sr.m_mad[1] = m.mad; sr.m_cost[1] = cand_cost(m.satd, S.qx, S.qy, px, py, a.lambda); }
+    if (gw == 0) {   // the MB position (half 0) and the predictor (half 1)
+        const SrcLane sl = src_lane(S.src, lane);
+        const bool hp = lane >= 16, ok = !hp || S.has_pred;
+        int sad = 0, mad = 0, satd = 0;
+        if (ok) half_metrics(sl, S.win[hp && S.sep ? wb : wa], hp ? S.qx : px, hp ? S.qy : py, lane, sad, mad, satd);
+        sad = half_sum(sad, lane); mad = half_max(mad, lane); satd = (half_sum(satd, lane) + 1) >> 1;
+        if (lane == 0) { sr.m_sad[0][0] = sad; sr.m_mad[0][0] = mad; sr.m_cost[0][0] = rd_cost(satd, a.lambda, 1u); }
+        if (lane == 16 && ok) { sr.m_sad[0][1] = sad; sr.m_mad[0][1] = mad; sr.m_cost[0][1] = cand_cost(satd, S.qx, S.qy, px, py, a.lambda); }
     }
     gsync(g);
     if (gt == 0) {
         Sel s;
-        s.bx = px; s.by = py; s.sad = sr.m_sad[0]; s.mad = sr.m_mad[0]; s.ssd = INT_MAX;
-        s.cost = sr.m_cost[0];
+        s.bx = px; s.by = py; s.sad = sr.m_sad[0][0]; s.mad = sr.m_mad[0][0]; s.ssd = INT_MAX;
+        s.cost = sr.m_cost[0][0];
         s.sp_index = 0; s.sp_amount = 0; s.sp_enabled = 0;
-        if (S.has_pred) accept_int(s, S.qx, S.qy, sr.m_sad[1], sr.m_mad[1], sr.m_cost[1], px, py, S.thr);
+        if (S.has_pred) accept_int(s, S.qx, S.qy, sr.m_sad[0][1], sr.m_mad[0][1], sr.m_cost[0][1], px, py, S.thr);
         sr.sel = s;
         sr.cur = (S.sep && s.bx == S.qx && s.by == S.qy) ? wb : wa;
     }
     gsync(g);
     const int wi = sr.cur;
-    if (sr.sel.mad >= S.thr) {
+    Sel s = sr.sel;
+    if (s.mad >= S.thr) {
         int r = SEARCH_RADIUS;   // adaptive radius, motion.cpp:640-646
-        if (sr.sel.sad < SAD_THRESHOLD / 4) r = SEARCH_RADIUS / 4;
-        else if (sr.sel.sad < SAD_THRESHOLD / 2) r = SEARCH_RADIUS / 2;
-        for (int st = r; st > 0; st >>= 1) {
-            run_step(g, si, wi, false, -st, -st, st, px, py, a.W, a.H, a.lambda);
-            if (sr.sel.mad < S.thr) break;
+        if (s.sad < SAD_THRESHOLD / 4) r = SEARCH_RADIUS / 4;
+        else if (s.sad < SAD_THRESHOLD / 2) r = SEARCH_RADIUS / 2;
+        int par = 0;
+        for (int st = r; st > 0; st >>= 1, par ^= 1) {
+            s = run_step(g, si, wi, false, -st, -st, st, px, py, a.W, a.H, a.lambda, s, par);
+            if (s.mad < S.thr) break;
         }
-        run_subpel(g, si, wi, false, px, py, a.W, a.H);
+        run_subpel(g, si, wi, false, px, py, a.W, a.H, s);
     }
     materialize(g, si, wi, sr.sel.bx, sr.sel.by, sr.sel.sp_enabled, sr.sel.sp_amount, sr.sel.sp_index, pred_out);
     if (gt == 0) {
