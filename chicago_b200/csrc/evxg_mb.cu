@@ -101,6 +101,9 @@ struct Nbr {                   // intra_pred.cpp:13-54
     int16_t corner;
     int ht, hl, dc;
 };
+struct PredIn {                // MV predictor inputs but the left neighbour (see pred_gather)
+    int has[3], mx[3], my[3];  // above, above-right / above-left, temporal
+};
 struct alignas(4) Desc { evxg_block_desc d; };   // 4-aligned so it can be copied as 7 words
 
 // State of one motion search, owned by one warp group.
@@ -154,6 +157,8 @@ struct MbShared {
     Srch srch[3];              // 0 intra block copy, 1 forward / P inter, 2 backward
     int thr, row_abort;
     int has_pred, sep, qx, qy;
+    PredIn pin;                // cluster ranks 1, 2: predictor inputs gathered before the left neighbour is known
+    int w0_early;              // cluster leader: window 0 shifts before the wavefront wait
     int modes[3], dsad[3], dir_best, dir_sad;
     int bi_sad, part[NW];
     unsigned aq[MAXC][4][3];   // adaptive QP: per candidate and luma block, sum / sum of squares / count
@@ -357,9 +362,10 @@ __device__ __forceinline__ void rows_above(int py, int &y0, int &y1, int &cy0, i
     y1 = WL_OFF + 16; cy1 = WC_OFF + 8;                          // plane rows py-16 .. py-1
     y0 = py == 16 ? 0 : WL_OFF; cy0 = py == 16 ? 0 : WC_OFF;
 }
-// Read window 0's newest strip (luma columns WL-16.., chroma WC-8..: MB
-// column c+3) again for rows [y0, y1) / [cy0, cy1); threads of group g.
-__device__ void refresh_newest(const Grp g, Win &w, const int16_t *plane, int W, int H, int y0, int y1, int cy0, int cy1)
+// Read a 16-column strip of window 0 (luma columns lc.., chroma cc..) again
+// for rows [y0, y1) / [cy0, cy1); threads of group g.
+__device__ void refresh_strip(const Grp g, Win &w, const int16_t *plane, int W, int H, int y0, int y1, int cy0, int cy1,
+                              int lc, int cc)
 {
     const int gt = threadIdx.x - g.t0, cw = W / 2, ch = H / 2;
     const int16_t *U = plane + (size_t)W * H, *V = U + (size_t)cw * ch;
@@ -367,13 +373,17 @@ __device__ void refresh_newest(const Grp g, Win &w, const int16_t *plane, int W,
     for (int e = gt; e < nl + nc; e += g.nt) {
         if (e < nl) {
             const int r = y0 + e / 2, j = e % 2;
-            *reinterpret_cast<uint4 *>(w.y + r * WL + WL - 16 + 8 * j) = win_chunk(plane, W, H, w.oy + r, w.ox + WL - 16 + 8 * j);
+            *reinterpret_cast<uint4 *>(w.y + r * WL + lc + 8 * j) = win_chunk(plane, W, H, w.oy + r, w.ox + lc + 8 * j);
         } else {
             const int f = e - nl, p = f & 1, r = cy0 + f / 2;
-            *reinterpret_cast<uint4 *>((p ? w.v : w.u) + r * WC + WC - 8) =
-                win_chunk(p ? V : U, cw, ch, w.coy + r, w.cox + WC - 8);
+            *reinterpret_cast<uint4 *>((p ? w.v : w.u) + r * WC + cc) = win_chunk(p ? V : U, cw, ch, w.coy + r, w.cox + cc);
         }
     }
+}
+// The newest strip (MB column c+3).
+__device__ void refresh_newest(const Grp g, Win &w, const int16_t *plane, int W, int H, int y0, int y1, int cy0, int cy1)
+{
+    refresh_strip(g, w, plane, W, H, y0, y1, cy0, cy1, WL - 16, WC - 8);
 }
 
 // Candidate metrics (analysis.h:89-202): SAD (luma), MAD (Y, U, V) and SATD
@@ -1119,59 +1129,93 @@ __device__ __noinline__ void intra_bc_search(const Grp g, const FrameArgs &a, in
 }
 
 // MV predictor (motion.cpp:271-346) from the live block table and, for P
-// frames, the previous frame's table.  left, when given, replaces the table
-// entry of the left neighbour (the cluster form hands it over in shared
-// memory before the leader writes the table).
-__device__ void mv_predictor(const FrameArgs &a, int idx, bool temporal, const evxg_block_desc *left, int &ox, int &oy)
+// frames, the previous frame's table.  Its inputs other than the left
+// neighbour -- the MB above, above-right (else above-left) and the temporal
+// entry -- are gathered first (pred_gather: row r-1 must have finished column
+// c+1), then combined with the left neighbour (pred_combine).  left, when
+// given, replaces the table entry of the left neighbour (the cluster form
+// hands it over in shared memory before the leader writes the table).
+__device__ void pred_gather(const FrameArgs &a, int idx, bool temporal, PredIn &o)
 {
     const int mbw = a.mbw, bx = idx % mbw, by = idx / mbw;
-    int mx[3], my[3], n = 0;
     auto motion = [&](int i) { return (__ldcg(&a.bt[i].block_type) & BT_MOTION) != 0; };
-    auto take = [&](int i) { mx[n] = __ldcg(&a.bt[i].motion_x); my[n] = __ldcg(&a.bt[i].motion_y); n++; };
+    auto take = [&](int k, int i) { o.has[k] = 1; o.mx[k] = __ldcg(&a.bt[i].motion_x); o.my[k] = __ldcg(&a.bt[i].motion_y); };
+    o.has[0] = o.has[1] = o.has[2] = 0;
+    if (by > 0 && motion(idx - mbw)) take(0, idx - mbw);
+    if (by > 0 && bx + 1 < mbw && motion(idx - mbw + 1)) take(1, idx - mbw + 1);
+    else if (by > 0 && bx > 0 && motion(idx - mbw - 1)) take(1, idx - mbw - 1);
+    if (temporal && (a.prev[idx].block_type & BT_MOTION)) { o.has[2] = 1; o.mx[2] = a.prev[idx].motion_x; o.my[2] = a.prev[idx].motion_y; }
+}
+__device__ void pred_combine(const FrameArgs &a, int idx, const PredIn &p, const evxg_block_desc *left, int &ox, int &oy)
+{
+    const int bx = idx % a.mbw;
+    int mx[3], my[3], n = 0;
     if (bx > 0) {
         if (left) {
             if (left->block_type & BT_MOTION) { mx[n] = left->motion_x; my[n] = left->motion_y; n++; }
-        } else if (motion(idx - 1)) {
-            take(idx - 1);
+        } else if (__ldcg(&a.bt[idx - 1].block_type) & BT_MOTION) {
+            mx[n] = __ldcg(&a.bt[idx - 1].motion_x); my[n] = __ldcg(&a.bt[idx - 1].motion_y); n++;
         }
     }
-    if (by > 0 && motion(idx - mbw)) take(idx - mbw);
-    if (by > 0 && bx + 1 < mbw && motion(idx - mbw + 1)) take(idx - mbw + 1);
-    else if (by > 0 && bx > 0 && motion(idx - mbw - 1)) take(idx - mbw - 1);
-    if (n < 3 && temporal && (a.prev[idx].block_type & BT_MOTION)) { mx[n] = a.prev[idx].motion_x; my[n] = a.prev[idx].motion_y; n++; }
+    for (int k = 0; k < 2; k++)
+        if (p.has[k]) { mx[n] = p.mx[k]; my[n] = p.my[k]; n++; }
+    if (n < 3 && p.has[2]) { mx[n] = p.mx[2]; my[n] = p.my[2]; n++; }
     if (n == 0) { ox = 0; oy = 0; }
     else if (n == 1) { ox = mx[0]; oy = my[0]; }
     else if (n == 2) { ox = (int16_t)((mx[0] + mx[1]) / 2); oy = (int16_t)((my[0] + my[1]) / 2); }
     else {
         int v[2];
         for (int k = 0; k < 2; k++) {
-            int p = k ? my[0] : mx[0], q = k ? my[1] : mx[1], r = k ? my[2] : mx[2], t;
-            if (p > q) { t = p; p = q; q = t; }
+            int p0 = k ? my[0] : mx[0], q = k ? my[1] : mx[1], r = k ? my[2] : mx[2], t;
+            if (p0 > q) { t = p0; p0 = q; q = t; }
             if (q > r) q = r;
-            if (p > q) q = p;
+            if (p0 > q) q = p0;
             v[k] = q;
         }
         ox = v[0]; oy = v[1];
     }
 }
+// One thread: the MB's search predictor (has_pred, sep, qx, qy) from its inputs.
+__device__ void set_predictor(const FrameArgs &a, int idx, int px, int py, const PredIn &p, const evxg_block_desc *left)
+{
+    MbShared &S = SM();
+    int pmx, pmy;
+    pred_combine(a, idx, p, left, pmx, pmy);
+    S.has_pred = (pmx || pmy);
+    S.qx = min(max(px + pmx, 0), a.W - 16);
+    S.qy = min(max(py + pmy, 0), a.H - 16);
+    S.sep = S.has_pred && (S.qx != px || S.qy != py);
+}
 
-// Inter search (motion.cpp:567-679) on one warp group: window wa holds the
-// reference around the MB, wb around the predictor when that differs.
-__device__ __noinline__ void inter_search(const Grp g, const FrameArgs &a, int si, int wa, int wb, int px, int py,
-                                          int16_t *pred_out)
+// The inter search's first candidates on warp 0 of g: the MB position in
+// window wa (half 0, unless done) and the predictor (half 1, when pred), in
+// wb when that differs.
+__device__ __noinline__ void first_candidates(const Grp g, const FrameArgs &a, int si, int wa, int wb, int px, int py,
+                                              bool mb, bool pred)
 {
     MbShared &S = SM();
     Srch &sr = S.srch[si];
     const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31;
-    if (gw == 0) {   // the MB position (half 0) and the predictor (half 1)
-        const SrcLane sl = src_lane(S.src, lane);
-        const bool hp = lane >= 16, ok = !hp || S.has_pred;
-        int sad = 0, mad = 0, satd = 0;
-        if (ok) half_metrics(sl, S.win[hp && S.sep ? wb : wa], hp ? S.qx : px, hp ? S.qy : py, lane, sad, mad, satd);
-        sad = half_sum(sad, lane); mad = half_max(mad, lane); satd = (half_sum(satd, lane) + 1) >> 1;
-        if (lane == 0) { sr.m_sad[0][0] = sad; sr.m_mad[0][0] = mad; sr.m_cost[0][0] = rd_cost(satd, a.lambda, 1u); }
-        if (lane == 16 && ok) { sr.m_sad[0][1] = sad; sr.m_mad[0][1] = mad; sr.m_cost[0][1] = cand_cost(satd, S.qx, S.qy, px, py, a.lambda); }
-    }
+    if (gw != 0) return;
+    const SrcLane sl = src_lane(S.src, lane);
+    const bool hp = lane >= 16, ok = hp ? pred : mb;
+    int sad = 0, mad = 0, satd = 0;
+    if (ok) half_metrics(sl, S.win[hp && S.sep ? wb : wa], hp ? S.qx : px, hp ? S.qy : py, lane, sad, mad, satd);
+    sad = half_sum(sad, lane); mad = half_max(mad, lane); satd = (half_sum(satd, lane) + 1) >> 1;
+    if (lane == 0 && ok) { sr.m_sad[0][0] = sad; sr.m_mad[0][0] = mad; sr.m_cost[0][0] = rd_cost(satd, a.lambda, 1u); }
+    if (lane == 16 && ok) { sr.m_sad[0][1] = sad; sr.m_mad[0][1] = mad; sr.m_cost[0][1] = cand_cost(satd, S.qx, S.qy, px, py, a.lambda); }
+}
+
+// Inter search (motion.cpp:567-679) on one warp group: window wa holds the
+// reference around the MB, wb around the predictor when that differs.  With
+// first_done the MB position's metrics are in place already (first_candidates).
+__device__ __noinline__ void inter_search(const Grp g, const FrameArgs &a, int si, int wa, int wb, int px, int py,
+                                          int16_t *pred_out, bool first_done)
+{
+    MbShared &S = SM();
+    Srch &sr = S.srch[si];
+    const int gt = threadIdx.x - g.t0;
+    first_candidates(g, a, si, wa, wb, px, py, !first_done, S.has_pred);
     gsync(g);
     if (gt == 0) {
         Sel s;
@@ -1257,12 +1301,9 @@ __device__ __noinline__ void setup_mb(const FrameArgs &a, int idx, int px, int p
     S.rdo = a.type == EVXG_FRAME_INTER;
     S.has_pred = 0; S.sep = 0; S.qx = px; S.qy = py;
     if (need_pred) {
-        int pmx, pmy;
-        mv_predictor(a, idx, a.type == EVXG_FRAME_INTER, left, pmx, pmy);
-        S.has_pred = (pmx || pmy);
-        S.qx = min(max(px + pmx, 0), a.W - 16);
-        S.qy = min(max(py + pmy, 0), a.H - 16);
-        S.sep = S.has_pred && (S.qx != px || S.qy != py);
+        PredIn p;
+        pred_gather(a, idx, a.type == EVXG_FRAME_INTER, p);
+        set_predictor(a, idx, px, py, p, left);
     }
     S.req.n = 0;
     S.req.fy0 = S.req.fy1 = S.req.fcy0 = S.req.fcy1 = 0;
@@ -1463,8 +1504,9 @@ __device__ void write_back(const FrameArgs &a, int px, int py, int idx, const in
     // an MB on the top, bottom or left edge the next MB loads window 0 afresh.
     if (tid == 0 && (px == 0 || py == 0 || py + 16 == a.H)) w0.valid = 0;
     if (tid < 7) reinterpret_cast<int *>(a.bt + idx)[tid] = reinterpret_cast<const int *>(&S.cd[ch].d)[tid];
-    // the caller publishes after a CTA barrier with one fence by the releasing
-    // thread (the barrier orders every writer's stores before that fence)
+    // the caller publishes with a release store by one thread after a CTA
+    // barrier: the barrier orders every writer's stores before the release,
+    // whose ordering is cumulative
 }
 
 // Thread 0: wait until row r has finished column need (the wavefront's
@@ -1535,10 +1577,10 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
         if (a.type == EVXG_FRAME_BIDIR) directional_intra(g);
     } else if (gi == 1) {
         if (a.type == EVXG_FRAME_INTRA) directional_intra(g);
-        else inter_search(g, a, 1, 1, 2, px, py, S.pred[1]);
+        else inter_search(g, a, 1, 1, 2, px, py, S.pred[1], false);
     } else {
         if (a.type == EVXG_FRAME_BIDIR) {
-            inter_search(g, a, 2, 3, 4, px, py, S.pred[2]);
+            inter_search(g, a, 2, 3, 4, px, py, S.pred[2], false);
         } else if (a.type == EVXG_FRAME_INTER) {
             // The intra RDO candidates do not depend on the searches
             // (encode.cpp:295-336): encode them while the searches run.
@@ -1588,10 +1630,7 @@ __device__ bool mb_row(const FrameArgs &a, int row)
         if (S.row_abort) return false;
         process_mb(a, row, col);
         __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            st_release(&a.progress[row], col);
-        }
+        if (tid == 0) st_release(&a.progress[row], col);   // release: ordered after the barrier, so after every thread's stores
     }
     __syncthreads();
     return true;
@@ -1727,16 +1766,31 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
     MbShared &S = SM();
     const int tid = threadIdx.x;
     const int px = col * 16, py = row * 16, idx = row * a.mbw + col;
-    if (tid == 0) S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 2, a.mbw - 1));   // see mb_row
-    __syncthreads();
-    if (S.row_abort) return false;
+    // Before the wavefront wait: the source and, when window 0 moves on by
+    // one MB, its shift and new strip (column c+3, whose rows above are read
+    // again on demand); the rows above of column c+2 are read after the wait.
+    // A window loaded whole is loaded after the wait.
     load_src(a, px, py);
     if (tid == 0) {
         setup_mb(a, idx, px, py, false, nullptr);
-        req_window0(a, px, py);
+        req_window(0, a.planes[a.dpb], px, py - 16);
+        const Win &w = S.win[0];
+        S.w0_early = w.valid && w.pl == a.planes[a.dpb] && w.oy == py - 16 - WL_OFF && w.coy == ((py - 16) >> 1) - WC_OFF &&
+                     w.ox + 16 == win_ox(px) && w.cox + 8 == win_cox(px);
     }
     __syncthreads();
-    load_windows(a.W, a.H);
+    const bool early = S.w0_early;
+    if (early) load_windows(a.W, a.H);
+    if (tid == 0) S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 2, a.mbw - 1));   // see mb_row
+    __syncthreads();
+    if (S.row_abort) return false;
+    if (!early) {
+        load_windows(a.W, a.H);
+    } else if (row > 0) {
+        int y0, y1, cy0, cy1;
+        rows_above(py, y0, y1, cy0, cy1);
+        refresh_strip(G_ALL, S.win[0], a.planes[a.dpb], a.W, a.H, y0, y1, cy0, cy1, WL - 32, WC - 16);
+    }
     __syncthreads();
     intra_bc_search(G_ALL, a, px, py);
     if (tid == 0)
@@ -1774,8 +1828,7 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
     const bool remote = a.type == EVXG_FRAME_INTER && ch < 4;   // an intra candidate encoded by rank 2
     write_back(a, px, py, idx, remote ? peer(S.rec[ch], 2) : S.rec[ch], remote ? peer(S.lev[ch], 2) : S.lev[ch]);
     __syncthreads();
-    if (tid == 0) {
-        __threadfence();
+    if (tid == 0) {   // releases: ordered after the barrier, so after every thread's stores
         st_release(&a.progress[row], col);
         st_release_cl(peer(&S.mail.wr_seq, 2), n);
     }
@@ -1783,28 +1836,46 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
 }
 
 // Ranks 1 and 2: the forward or backward inter search of the n-th MB, handed
-// to the leader's inbox (the caller releases the sequence flag).
+// to the leader's inbox (the caller releases the sequence flag).  What does
+// not depend on the left neighbour's decision -- the source, the predictor's
+// other inputs (row r-1 has finished column c+1), the window around the MB
+// and its metrics -- comes before the wait for the leader's decision of the
+// previous MB.
 __device__ bool search_mb(const FrameArgs &a, int row, int col, int n, bool bwd)
 {
     MbShared &S = SM();
     const int tid = threadIdx.x;
     const int px = col * 16, py = row * 16, idx = row * a.mbw + col;
-    if (tid == 0)
-        S.row_abort = !(wait_mail(&S.mail.dec_seq, n - 1, a) && (row == 0 || wait_progress(a, row - 1, min(col + 1, a.mbw - 1))));
+    const int si = bwd ? 2 : 1, wa = bwd ? 3 : 1;
+    const int16_t *ref = a.planes[bwd ? a.ref_bwd : a.ref_fwd];
+    if (tid == 0) S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 1, a.mbw - 1));
     __syncthreads();
     if (S.row_abort) return false;
     load_src(a, px, py);
-    const int si = bwd ? 2 : 1, wa = bwd ? 3 : 1;
     if (tid == 0) {
-        setup_mb(a, idx, px, py, true, col > 0 ? &S.mail.left.d : nullptr);
-        const int16_t *ref = a.planes[bwd ? a.ref_bwd : a.ref_fwd];
+        setup_mb(a, idx, px, py, false, nullptr);
+        pred_gather(a, idx, a.type == EVXG_FRAME_INTER, S.pin);
         req_window(wa, ref, px, py);
-        if (S.sep) req_window(wa + 1, ref, S.qx, S.qy);
     }
     __syncthreads();
     load_windows(a.W, a.H);
     __syncthreads();
-    inter_search(G_ALL, a, si, wa, wa + 1, px, py, S.pred[si]);
+    first_candidates(G_ALL, a, si, wa, wa + 1, px, py, true, false);
+    if (tid == 0) {
+        S.row_abort = !wait_mail(&S.mail.dec_seq, n - 1, a);
+        if (!S.row_abort) {
+            set_predictor(a, idx, px, py, S.pin, col > 0 ? &S.mail.left.d : nullptr);
+            S.req.n = 0;
+            if (S.sep) req_window(wa + 1, ref, S.qx, S.qy);
+        }
+    }
+    __syncthreads();
+    if (S.row_abort) return false;
+    if (S.req.n) {
+        load_windows(a.W, a.H);
+        __syncthreads();
+    }
+    inter_search(G_ALL, a, si, wa, wa + 1, px, py, S.pred[si], true);
     Inbox *in = peer(&S.mail.in, 0);
     copy_block(bwd ? in->b_pred : in->f_pred, S.pred[si]);
     if (tid == 0) {
