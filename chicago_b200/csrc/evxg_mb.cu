@@ -140,7 +140,7 @@ struct alignas(16) Inbox {
     float cost[4];             // P: RD costs of the intra candidates cd[0..3]
 };
 struct Mail {
-    Inbox in;                  // leader: results for the current MB
+    Inbox in[2];               // leader: results for MB n in in[n & 1] (the ranks write MB n+1's while it reads MB n's)
     Desc left;                 // ranks 1, 2: the leader's final descriptor of the previous MB
     int row_val;               // ranks 1, 2: row of the latest assignment (-1: no rows left)
     int row_seq;               // ranks 1, 2: number of row assignments made
@@ -153,6 +153,7 @@ struct MbShared {
     int16_t src[MB_N];
     Win win[NWIN];
     int16_t pred[7][MB_N];     // 0 intra-BC, 1 inter/fwd, 2 bwd, 3 bi, 4..6 directional candidates
+    const int16_t *predp[7];   // where prediction k is (pred[k], or the cluster leader's inbox)
     Nbr nb[3];
     Srch srch[3];              // 0 intra block copy, 1 forward / P inter, 2 backward
     int thr, row_abort;
@@ -921,7 +922,7 @@ __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, 
         const int k = k0 + j / 6, b = j % 6;
         const int bb = blk_base(b), bs = blk_stride(b);
         if (S.cd[k].d.block_type & BT_COPY) continue;
-        const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
+        const int16_t *pr = S.cpred[k] >= 0 ? S.predp[S.cpred[k]] : nullptr;
 #pragma unroll 1
         for (int h = 0; h < 2; h++) {   // residual (int16) into coef
             const int e = bb + l4 * bs + i0 + h;
@@ -964,7 +965,7 @@ __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, 
         const int k = k0 + j / 6, b = j % 6;
         const int bb = blk_base(b), bs = blk_stride(b);
         const int bt = S.cd[k].d.block_type;
-        const int16_t *pr = S.cpred[k] >= 0 ? S.pred[S.cpred[k]] : nullptr;
+        const int16_t *pr = S.cpred[k] >= 0 ? S.predp[S.cpred[k]] : nullptr;
         if (bt & BT_COPY) {
 #pragma unroll 1
             for (int h = 0; h < 2; h++) {
@@ -1392,7 +1393,7 @@ __device__ void bi_prediction()
     const int tid = threadIdx.x;
     int s = 0;
     for (int e = tid; e < MB_N; e += NT) {
-        const int av = (S.pred[1][e] + S.pred[2][e] + 1) >> 1;
+        const int av = (S.predp[1][e] + S.predp[2][e] + 1) >> 1;
         S.pred[3][e] = (int16_t)av;
         s += iabs32(S.src[e] - av);
     }
@@ -1528,6 +1529,7 @@ __device__ bool wait_progress(const FrameArgs &a, int r, int need)
 __device__ void init_tables()
 {
     const int tid = threadIdx.x;
+    if (tid < 7) SM().predp[tid] = SM().pred[tid];
     if (tid < 64) {
         s_qm[0][tid] = c_qm_intra[tid]; s_qm[1][tid] = c_qm_inter[tid];
         s_dz[0][tid] = c_dz_intra[tid]; s_dz[1][tid] = c_dz_inter[tid];
@@ -1726,6 +1728,11 @@ __device__ __forceinline__ void st_release_cl(int *p, int v)
 {
     asm volatile("st.release.cluster.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ void fence_cl() { asm volatile("fence.acq_rel.cluster;" ::: "memory"); }
+__device__ __forceinline__ void st_relaxed_cl(int *p, int v)   // after fence_cl: a release
+{
+    asm volatile("st.relaxed.cluster.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 __device__ __forceinline__ int ld_acquire_cl(const int *p)
 {
     int v;
@@ -1756,8 +1763,10 @@ __device__ void publish_decision(const evxg_block_desc &d, int n)   // leader, o
     for (unsigned p = 1; p < 3; p++) {
         int *to = reinterpret_cast<int *>(peer(&S.mail.left, p));
         for (int i = 0; i < 7; i++) to[i] = reinterpret_cast<const int *>(&d)[i];
-        st_release_cl(peer(&S.mail.dec_seq, p), n);
     }
+    fence_cl();   // one fence releases both descriptors
+    st_relaxed_cl(peer(&S.mail.dec_seq, 1), n);
+    st_relaxed_cl(peer(&S.mail.dec_seq, 2), n);
 }
 
 // Leader: MB (row, col), the n-th MB of this cluster.
@@ -1797,11 +1806,9 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
         S.row_abort = !((a.type == EVXG_FRAME_INTRA || wait_mail(&S.mail.f_seq, n, a)) && wait_mail(&S.mail.d_seq, n, a));
     __syncthreads();
     if (S.row_abort) return false;
-    const Inbox &in = S.mail.in;
-    if (a.type != EVXG_FRAME_INTRA) copy_block(S.pred[1], in.f_pred);
-    if (a.type == EVXG_FRAME_BIDIR) copy_block(S.pred[2], in.b_pred);
-    if (a.type != EVXG_FRAME_INTER) copy_block(S.pred[4 + in.dir_best], in.d_pred);
-    if (tid == 0) {
+    const Inbox &in = S.mail.in[n & 1];
+    if (tid == 0) {   // the predictions are read where the ranks left them
+        S.predp[1] = in.f_pred; S.predp[2] = in.b_pred; S.predp[4 + in.dir_best] = in.d_pred;
         S.srch[1].out = in.f_out; S.srch[1].out_sad = in.f_sad;
         S.srch[2].out = in.b_out; S.srch[2].out_sad = in.b_sad;
         S.dir_best = in.dir_best; S.dir_sad = in.dir_sad;
@@ -1828,8 +1835,8 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
     const bool remote = a.type == EVXG_FRAME_INTER && ch < 4;   // an intra candidate encoded by rank 2
     write_back(a, px, py, idx, remote ? peer(S.rec[ch], 2) : S.rec[ch], remote ? peer(S.lev[ch], 2) : S.lev[ch]);
     __syncthreads();
-    if (tid == 0) {   // releases: ordered after the barrier, so after every thread's stores
-        st_release(&a.progress[row], col);
+    if (tid == NT - 32) {   // releases, ordered after the barrier (so after every thread's stores), by
+        st_release(&a.progress[row], col);     // the last warp: thread 0 goes on to the next MB's waits
         st_release_cl(peer(&S.mail.wr_seq, 2), n);
     }
     return true;
@@ -1876,7 +1883,7 @@ __device__ bool search_mb(const FrameArgs &a, int row, int col, int n, bool bwd)
         __syncthreads();
     }
     inter_search(G_ALL, a, si, wa, wa + 1, px, py, S.pred[si], true);
-    Inbox *in = peer(&S.mail.in, 0);
+    Inbox *in = peer(&S.mail.in[n & 1], 0);
     copy_block(bwd ? in->b_pred : in->f_pred, S.pred[si]);
     if (tid == 0) {
         if (bwd) { in->b_out = S.srch[si].out; in->b_sad = S.srch[si].out_sad; }
@@ -1922,7 +1929,7 @@ __device__ bool aux_mb(const FrameArgs &a, int row, int col, int n)   // rank 2
         __syncthreads();
         encode_candidates(G_ALL, a, 0, 4);
     }
-    Inbox *in = peer(&S.mail.in, 0);
+    Inbox *in = peer(&S.mail.in[n & 1], 0);
     if (a.type != EVXG_FRAME_INTER) copy_block(in->d_pred, S.pred[4 + S.dir_best]);
     if (tid == 0) {
         in->dir_best = S.dir_best; in->dir_sad = S.dir_sad;
@@ -1986,7 +1993,9 @@ __device__ void cluster_main(const FrameArgs &a0, const FrameArgs *args, const i
         for (int col = 0; col < a.mbw && ok; ++col) {
             ++n;
             ok = rank == 0 ? leader_mb(a, row, col, n) : (rank == 1 ? fwd_mb(a, row, col, n) : aux_mb(a, row, col, n));
-            __syncthreads();
+            // The leader's MB ends with a barrier before its releases, which the
+            // last warp makes while the others start the next MB.
+            if (rank != 0) __syncthreads();
         }
         if (!ok) break;
     }
