@@ -90,6 +90,7 @@ struct WinReq {
     // columns just behind the new strip are read from memory again when the
     // window shifts (they were loaded before the row above finished them)
     int fy0, fy1, fcy0, fcy1;
+    int staged;                // window 0 only: its new strip is in MbShared::nstrip (prefetched)
 };
 struct Sel {                   // evx_motion_selection, motion.cpp:53-66
     int bx, by, sad, mad, ssd;
@@ -147,6 +148,7 @@ struct Mail {
     int dec_seq;               // ranks 1, 2: MBs whose descriptor the leader has published
     int wr_seq;                // rank 2: MBs the leader has written back to the slot
     int f_seq, d_seq;          // leader: MBs whose rank-1 / rank-2 results are in the inbox
+    int16_t lcol[32];          // rank 2: the right column (Y 16, U 8, V 8) of the MB the leader wrote back last
 };
 
 struct MbShared {
@@ -161,7 +163,7 @@ struct MbShared {
     PredIn pin;                // cluster ranks 1, 2: predictor inputs gathered before the left neighbour is known
     int w0_early;              // cluster leader: window 0 shifts before the wavefront wait
     int modes[3], dsad[3], dir_best, dir_sad;
-    int bi_sad, part[NW];
+    int bi_sad, part[NW], dpart[3][NW];
     unsigned aq[MAXC][4][3];   // adaptive QP: per candidate and luma block, sum / sum of squares / count
     int cpred[MAXC], win_k, need_encode, chosen, rdo;
     WinReq req;
@@ -169,6 +171,11 @@ struct MbShared {
     float cost[MAXC];
     int16_t coef[MAXC][MB_N], lev[MAXC][MB_N], rec[MAXC][MB_N], tmp[MAXC][MB_N];
     Mail mail;
+    // cluster leader: the next MB's source and window 0's new strip, copied
+    // in asynchronously during the current MB (prefetch_next)
+    alignas(16) int16_t nsrc[MB_N];
+    uint4 nstrip[2 * WL_ROWS + 2 * WC_ROWS];   // luma rows x 2 chunks, then U and V rows x 1 chunk
+    int pf_px, pf_py, pf_strip;
 };
 
 extern __shared__ __align__(16) unsigned char g_smem[];
@@ -316,10 +323,11 @@ __device__ __noinline__ void load_windows(int W, int H)
         const int k = shift[e / RT], r = e % RT;
         Win &w = S.win[q.wi[k]];
         const bool fresh = q.wi[k] == 0;
+        const bool staged = fresh && q.staged;
         if (r < WL_ROWS) {
             int16_t *row = w.y + r * WL;
-            const uint4 n0 = win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 16);
-            const uint4 n1 = win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 8);
+            const uint4 n0 = staged ? S.nstrip[2 * r] : win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 16);
+            const uint4 n1 = staged ? S.nstrip[2 * r + 1] : win_chunk(q.pl[k], W, H, w.oy + r, w.ox + WL - 8);
             const bool again = fresh && r >= q.fy0 && r < q.fy1;
             uint4 f0, f1;
             if (again) {
@@ -338,7 +346,7 @@ __device__ __noinline__ void load_windows(int W, int H)
             const int rr = r - WL_ROWS, pl = rr >= WC_ROWS, cr = rr - pl * WC_ROWS;
             const int16_t *U = q.pl[k] + (size_t)W * H, *V = U + (size_t)cw * ch;
             int16_t *row = (pl ? w.v : w.u) + cr * WC;
-            const uint4 n0 = win_chunk(pl ? V : U, cw, ch, w.coy + cr, w.cox + WC - 8);
+            const uint4 n0 = staged ? S.nstrip[2 * WL_ROWS + rr] : win_chunk(pl ? V : U, cw, ch, w.coy + cr, w.cox + WC - 8);
             const bool again = fresh && cr >= q.fcy0 && cr < q.fcy1;
             uint4 f0;
             if (again) f0 = win_chunk(pl ? V : U, cw, ch, w.coy + cr, w.cox + WC - 16);
@@ -1253,25 +1261,34 @@ __device__ __noinline__ void inter_search(const Grp g, const FrameArgs &a, int s
 __device__ __noinline__ void directional_intra(const Grp g)
 {
     MbShared &S = SM();
-    const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31;
-    for (int e = gt; e < 3 * MB_N; e += g.nt) {
-        const int m = e / MB_N, p = e % MB_N;
-        int16_t v;
-        if (p < 256) v = intra_px(S.modes[m], S.nb[0], 16, p & 15, p >> 4);
-        else { const int q = p - 256, pl = q >> 6, k = q & 63; v = intra_px(S.modes[m], S.nb[1 + pl], 8, k & 7, k >> 3); }
-        S.pred[4 + m][p] = v;
+    const int gt = threadIdx.x - g.t0, gw = gt >> 5, lane = gt & 31, nw = g.nt >> 5;
+    const int m0 = S.modes[0], m1 = S.modes[1], m2 = S.modes[2];
+    int s0 = 0, s1 = 0, s2 = 0;   // luma SADs, accumulated where the predictions are made
+    for (int e = gt; e < MB_N; e += g.nt) {
+        int16_t v0, v1, v2;
+        if (e < 256) {
+            const int x = e & 15, y = e >> 4;
+            v0 = intra_px(m0, S.nb[0], 16, x, y); v1 = intra_px(m1, S.nb[0], 16, x, y); v2 = intra_px(m2, S.nb[0], 16, x, y);
+            const int sv = S.src[e];
+            s0 += iabs32(sv - v0); s1 += iabs32(sv - v1); s2 += iabs32(sv - v2);
+        } else {
+            const int q = e - 256, pl = q >> 6, k = q & 63;
+            const Nbr &nb = S.nb[1 + pl];
+            v0 = intra_px(m0, nb, 8, k & 7, k >> 3); v1 = intra_px(m1, nb, 8, k & 7, k >> 3); v2 = intra_px(m2, nb, 8, k & 7, k >> 3);
+        }
+        S.pred[4][e] = v0; S.pred[5][e] = v1; S.pred[6][e] = v2;
     }
-    gsync(g);
-    if (gw < 3) {
-        int s = 0;
-        for (int e = lane; e < 256; e += 32) s += iabs32(S.src[e] - S.pred[4 + gw][e]);
-        s = warp_sum(s);
-        if (lane == 0) S.dsad[gw] = s;
-    }
+    s0 = warp_sum(s0); s1 = warp_sum(s1); s2 = warp_sum(s2);
+    if (lane == 0) { S.dpart[0][gw] = s0; S.dpart[1][gw] = s1; S.dpart[2][gw] = s2; }
     gsync(g);
     if (gt == 0) {
         int best = INT_MAX, bm = 0;
-        for (int m = 0; m < 3; m++) if (S.dsad[m] < best) { best = S.dsad[m]; bm = m; }
+        for (int m = 0; m < 3; m++) {
+            int t = 0;
+            for (int w = 0; w < nw; w++) t += S.dpart[m][w];
+            S.dsad[m] = t;
+            if (t < best) { best = t; bm = m; }
+        }
         S.dir_best = bm; S.dir_sad = best;
     }
     gsync(g);
@@ -1279,11 +1296,11 @@ __device__ __noinline__ void directional_intra(const Grp g)
 
 // ------------------------------------------------------------- per-MB steps
 
-__device__ void load_src(const FrameArgs &a, int px, int py)   // whole CTA
+__device__ void load_src_n(const FrameArgs &a, int px, int py, int nt)   // threads 0 .. nt-1
 {
     MbShared &S = SM();
     const int16_t *srcY = a.src, *srcU = a.src + (size_t)a.W * a.H, *srcV = srcU + (size_t)(a.W / 2) * (a.H / 2);
-    for (int e = threadIdx.x; e < MB_N; e += NT) {
+    for (int e = threadIdx.x; e < MB_N; e += nt) {
         if (e < 256) S.src[e] = __ldg(srcY + (size_t)(py + (e >> 4)) * a.W + px + (e & 15));
         else {
             const int pl = (e - 256) >> 6, k = (e - 256) & 63;
@@ -1291,6 +1308,7 @@ __device__ void load_src(const FrameArgs &a, int px, int py)   // whole CTA
         }
     }
 }
+__device__ void load_src(const FrameArgs &a, int px, int py) { load_src_n(a, px, py, NT); }   // whole CTA
 
 // One thread: copy threshold (motion.cpp:501), RDO flag and, when searches
 // follow, the MV predictor, which serves every search of the MB.  Clears the
@@ -1308,6 +1326,7 @@ __device__ __noinline__ void setup_mb(const FrameArgs &a, int idx, int px, int p
     }
     S.req.n = 0;
     S.req.fy0 = S.req.fy1 = S.req.fcy0 = S.req.fcy1 = 0;
+    S.req.staged = 0;
 }
 // Window 0's request: the slot being reconstructed around (px, py-16), with
 // the rows that show MB row r-1 read again behind the new strip.
@@ -1370,6 +1389,66 @@ __device__ void choose_modes()   // one thread: gradient-pruned candidates (intr
     if (gv > gh * 3 / 2) { S.modes[1] = 2; S.modes[2] = 6; }
     else if (gh > gv * 3 / 2) { S.modes[1] = 1; S.modes[2] = 5; }
     else { S.modes[1] = 3; S.modes[2] = 4; }
+}
+
+// Cluster rank 2: the directional neighbours in two parts.  nbr_top (threads
+// 0..34, before the left neighbour is final): the top rows and corners from
+// the destination slot.  nbr_left_modes (warp 0, ends with a CTA barrier):
+// the left columns from the mail, then what extract_nbr and choose_modes
+// derive -- corner fallbacks, DC, the gradient-pruned modes.
+__device__ void nbr_top(const FrameArgs &a, int px, int py)
+{
+    MbShared &S = SM();
+    const int tid = threadIdx.x, cw = a.W / 2, ch = a.H / 2;
+    const bool ht = py > 0, hl = px > 0;
+    const int16_t *D = a.planes[a.dpb];
+    auto plane = [&](int p) { return p == 0 ? D : D + (size_t)a.W * a.H + (size_t)(p - 1) * cw * ch; };
+    if (tid < 32) {   // luma top 0..15, U 16..23, V 24..31
+        const int p = tid < 16 ? 0 : (tid < 24 ? 1 : 2), k = p ? (tid - 16) & 7 : tid;
+        const int cy = p ? py >> 1 : py, cx = p ? px >> 1 : px;
+        S.nb[p].top[k] = ht ? __ldcg(plane(p) + (size_t)(cy - 1) * (p ? cw : a.W) + cx + k) : (int16_t)128;
+    } else if (tid < 35) {
+        const int p = tid - 32, cy = p ? py >> 1 : py, cx = p ? px >> 1 : px;
+        S.nb[p].corner = (ht && hl) ? __ldcg(plane(p) + (size_t)(cy - 1) * (p ? cw : a.W) + cx - 1) : (int16_t)0;
+    }
+}
+__device__ void nbr_left_modes(int px, int py)
+{
+    MbShared &S = SM();
+    const int tid = threadIdx.x;
+    const bool ht = py > 0, hl = px > 0;
+    if (tid < 32) {
+        const int lane = tid, p = lane < 16 ? 0 : (lane < 24 ? 1 : 2), k = p ? (lane - 16) & 7 : lane, n = p ? 8 : 16;
+        Nbr &nb = S.nb[p];
+        const int16_t left = hl ? S.mail.lcol[lane] : (int16_t)128;
+        nb.left[k] = left;
+        const int top = nb.top[k];
+        __syncwarp();
+        // DC of each plane: top (if any) and left (if any) samples (intra_pred.cpp:13-54)
+        const int v = (ht ? top : 0) + (hl ? left : 0);
+        const int sy = __reduce_add_sync(0xffffffffu, p == 0 ? v : 0), su = __reduce_add_sync(0xffffffffu, p == 1 ? v : 0),
+                  sv = __reduce_add_sync(0xffffffffu, p == 2 ? v : 0);
+        // luma gradients along the top row and the left column (intra_pred.cpp:225-260)
+        const int tprev = __shfl_up_sync(0xffffffffu, top, 1), lprev = __shfl_up_sync(0xffffffffu, (int)left, 1);
+        const bool gl = p == 0 && k >= 1;
+        const int gh = __reduce_add_sync(0xffffffffu, gl && ht ? iabs32(top - tprev) : 0);
+        const int gv = __reduce_add_sync(0xffffffffu, gl && hl ? iabs32(left - lprev) : 0);
+        if (lane < 3) {
+            Nbr &q = S.nb[lane];
+            const int nn = lane ? 8 : 16, cnt = (ht ? nn : 0) + (hl ? nn : 0), sum = lane == 0 ? sy : (lane == 1 ? su : sv);
+            q.ht = ht; q.hl = hl;
+            if (!(ht && hl)) q.corner = ht ? q.top[0] : (hl ? q.left[0] : (int16_t)128);
+            q.dc = cnt > 0 ? (int16_t)((sum + cnt / 2) / cnt) : 128;
+        }
+        if (lane == 0) {
+            S.modes[0] = 0;
+            if (gv > gh * 3 / 2) { S.modes[1] = 2; S.modes[2] = 6; }
+            else if (gh > gv * 3 / 2) { S.modes[1] = 1; S.modes[2] = 5; }
+            else { S.modes[1] = 3; S.modes[2] = 4; }
+        }
+        (void)n;
+    }
+    __syncthreads();
 }
 
 // P frames: the intra RDO candidates -- intra without prediction and the
@@ -1638,12 +1717,14 @@ __device__ bool mb_row(const FrameArgs &a, int row)
     return true;
 }
 
-__global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a)
+__global__ void __launch_bounds__(NT, 1) k_mb_wavefront(FrameArgs a0)
 {
     MbShared &S = SM();
     __shared__ int s_row;
+    __shared__ FrameArgs a;   // the parameters in shared memory (a kernel parameter read by reference lives in local memory)
     const int tid = threadIdx.x;
     init_tables();
+    if (tid == 0) a = a0;
     __syncthreads();
     for (;;) {
         if (tid == 0) s_row = atomicAdd(&a.counters[0], 1);
@@ -1769,6 +1850,102 @@ __device__ void publish_decision(const evxg_block_desc &d, int n)   // leader, o
     st_relaxed_cl(peer(&S.mail.dec_seq, 2), n);
 }
 
+__device__ __forceinline__ void bar_sync(int id, int nt) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nt) : "memory"); }
+
+// Window 0 moved on by one MB (new origin nox / ncox): every row shifts left
+// in shared memory and takes its new strip, from nstrip (prefetched) or from
+// memory; one thread per row, threads 0 .. WL_ROWS + 2*WC_ROWS - 1.  The
+// origin fields are left to the caller.
+__device__ void shift_window0(const FrameArgs &a, int nox, int ncox, bool staged)
+{
+    MbShared &S = SM();
+    Win &w = S.win[0];
+    const int r = threadIdx.x, cw = a.W / 2, ch = a.H / 2;
+    const int16_t *D = a.planes[a.dpb];
+    constexpr int NLC = WL / 8, NCC = WC / 8;
+    if (r < WL_ROWS) {
+        int16_t *rowp = w.y + r * WL;
+        const uint4 n0 = staged ? S.nstrip[2 * r] : win_chunk(D, a.W, a.H, w.oy + r, nox + WL - 16);
+        const uint4 n1 = staged ? S.nstrip[2 * r + 1] : win_chunk(D, a.W, a.H, w.oy + r, nox + WL - 8);
+        uint4 t[NLC - 2];
+#pragma unroll
+        for (int j = 0; j < NLC - 2; j++) t[j] = *reinterpret_cast<const uint4 *>(rowp + 16 + 8 * j);
+#pragma unroll
+        for (int j = 0; j < NLC - 2; j++) *reinterpret_cast<uint4 *>(rowp + 8 * j) = t[j];
+        *reinterpret_cast<uint4 *>(rowp + WL - 16) = n0;
+        *reinterpret_cast<uint4 *>(rowp + WL - 8) = n1;
+    } else if (r < WL_ROWS + 2 * WC_ROWS) {
+        const int rr = r - WL_ROWS, pl = rr >= WC_ROWS, cr = rr - pl * WC_ROWS;
+        const int16_t *P = D + (size_t)a.W * a.H + (pl ? (size_t)cw * ch : 0);
+        int16_t *rowp = (pl ? w.v : w.u) + cr * WC;
+        const uint4 n0 = staged ? S.nstrip[2 * WL_ROWS + rr] : win_chunk(P, cw, ch, w.coy + cr, ncox + WC - 8);
+        uint4 t[NCC - 1];
+#pragma unroll
+        for (int j = 0; j < NCC - 1; j++) t[j] = *reinterpret_cast<const uint4 *>(rowp + 8 + 8 * j);
+#pragma unroll
+        for (int j = 0; j < NCC - 1; j++) *reinterpret_cast<uint4 *>(rowp + 8 * j) = t[j];
+        *reinterpret_cast<uint4 *>(rowp + WC - 8) = n0;
+    }
+}
+
+// 16-byte asynchronous copies global -> shared (the caller's thread waits
+// for its own with cp_async_wait_all).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Leader, whole CTA, after the wavefront wait of MB (row, col): start copying
+// the next MB's source and window 0's new strip for it (MB column c+4) into
+// nsrc / nstrip.  Row r-2 has finished column c+4 (row r-1 finished c+2 after
+// it), rows r and below have not reached it, and row r-1's pixels there are
+// read again on demand, as for any newest strip; so the strip holds what the
+// next MB would read itself.  Strips beyond the right edge (edge-filled
+// chunks) are left to the next MB.
+__device__ void prefetch_next(const FrameArgs &a, int row, int col, int nt)
+{
+    MbShared &S = SM();
+    const int tid = threadIdx.x;
+    const int ncol = col + 1;
+    if (ncol >= a.mbw) {
+        if (tid == 0) S.pf_px = -1;
+        return;
+    }
+    const int npx = ncol * 16, npy = row * 16, cw = a.W / 2, ch = a.H / 2;
+    const int16_t *Y = a.src, *U = Y + (size_t)a.W * a.H, *V = U + (size_t)cw * ch;
+    if (tid < 48) {   // source: 16 luma rows x 2 chunks, 8 + 8 chroma rows
+        const int16_t *from;
+        int16_t *to;
+        if (tid < 32) { from = Y + (size_t)(npy + (tid >> 1)) * a.W + npx + (tid & 1) * 8; to = S.nsrc + (tid >> 1) * 16 + (tid & 1) * 8; }
+        else {
+            const int k = tid - 32, pl = k >> 3, r = k & 7;
+            from = (pl ? V : U) + (size_t)((npy >> 1) + r) * cw + (npx >> 1);
+            to = S.nsrc + 256 + pl * 64 + r * 8;
+        }
+        cp_async16(to, from);
+    }
+    const Win &w = S.win[0];
+    const int nox = win_ox(npx), ncox = win_cox(npx);
+    const bool strip = w.valid && nox + WL <= a.W && ncox + WC <= cw;
+    if (strip) {
+        const int16_t *D = a.planes[a.dpb], *DU = D + (size_t)a.W * a.H, *DV = DU + (size_t)cw * ch;
+        for (int e = tid; e < 2 * WL_ROWS + 2 * WC_ROWS; e += nt) {
+            const int16_t *from;
+            if (e < 2 * WL_ROWS) {
+                const int r = e >> 1, y = min(max(w.oy + r, 0), a.H - 1);
+                from = D + (size_t)y * a.W + nox + WL - 16 + (e & 1) * 8;
+            } else {
+                const int rr = e - 2 * WL_ROWS, pl = rr >= WC_ROWS, cr = rr - pl * WC_ROWS;
+                const int y = min(max(w.coy + cr, 0), ch - 1);
+                from = (pl ? DV : DU) + (size_t)y * cw + ncox + WC - 8;
+            }
+            cp_async16(&S.nstrip[e], from);
+        }
+    }
+    if (tid == 0) { S.pf_px = npx; S.pf_py = npy; S.pf_strip = strip; }
+}
+
 // Leader: MB (row, col), the n-th MB of this cluster.
 __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
 {
@@ -1777,30 +1954,50 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
     const int px = col * 16, py = row * 16, idx = row * a.mbw + col;
     // Before the wavefront wait: the source and, when window 0 moves on by
     // one MB, its shift and new strip (column c+3, whose rows above are read
-    // again on demand); the rows above of column c+2 are read after the wait.
-    // A window loaded whole is loaded after the wait.
-    load_src(a, px, py);
-    if (tid == 0) {
-        setup_mb(a, idx, px, py, false, nullptr);
-        req_window(0, a.planes[a.dpb], px, py - 16);
-        const Win &w = S.win[0];
-        S.w0_early = w.valid && w.pl == a.planes[a.dpb] && w.oy == py - 16 - WL_OFF && w.coy == ((py - 16) >> 1) - WC_OFF &&
-                     w.ox + 16 == win_ox(px) && w.cox + 8 == win_cox(px);
+    // again on demand) -- both prefetched during the previous MB when it was
+    // in this row; the rows above of column c+2 are read after the wait.  A
+    // window loaded whole is loaded after the wait.  Warps 0..10 do this
+    // part (named barrier 1) while the last warp may still be making the
+    // previous MB's releases; it joins at the CTA barrier before the search.
+    constexpr int NP = NT - 32;
+    if (tid < NP) {
+        // (window 0's fields are as the previous MB, which ended with a CTA barrier, left them)
+        Win &w = S.win[0];
+        const int nox = win_ox(px), ncox = win_cox(px);
+        const int16_t *dst = a.planes[a.dpb];
+        const bool early = w.valid && w.pl == dst && w.oy == py - 16 - WL_OFF && w.coy == ((py - 16) >> 1) - WC_OFF &&
+                           w.ox + 16 == nox && w.cox + 8 == ncox;
+        cp_async_wait_all();
+        bar_sync(1, NP);   // every prefetch copy has landed; every thread has compared window 0's origin
+        const bool pf = S.pf_px == px && S.pf_py == py;
+        if (pf) { if (tid < MB_N / 8) reinterpret_cast<uint4 *>(S.src)[tid] = reinterpret_cast<const uint4 *>(S.nsrc)[tid]; }
+        else load_src_n(a, px, py, NP);
+        if (early) shift_window0(a, nox, ncox, pf && S.pf_strip);
+        if (tid == 0) {
+            setup_mb(a, idx, px, py, false, nullptr);
+            S.w0_early = early;
+            if (early) { w.ox = nox; w.cox = ncox; }
+            else req_window(0, dst, px, py - 16);
+            S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 2, a.mbw - 1));   // see mb_row
+        }
+        bar_sync(1, NP);
+        if (!S.row_abort) {
+            if (early) {
+                if (row > 0) {
+                    int y0, y1, cy0, cy1;
+                    rows_above(py, y0, y1, cy0, cy1);
+                    refresh_strip(Grp{1, 0, NP}, S.win[0], dst, a.W, a.H, y0, y1, cy0, cy1, WL - 32, WC - 16);
+                }
+            }
+            prefetch_next(a, row, col, NP);
+        }
     }
-    __syncthreads();
-    const bool early = S.w0_early;
-    if (early) load_windows(a.W, a.H);
-    if (tid == 0) S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 2, a.mbw - 1));   // see mb_row
     __syncthreads();
     if (S.row_abort) return false;
-    if (!early) {
+    if (!S.w0_early) {
         load_windows(a.W, a.H);
-    } else if (row > 0) {
-        int y0, y1, cy0, cy1;
-        rows_above(py, y0, y1, cy0, cy1);
-        refresh_strip(G_ALL, S.win[0], a.planes[a.dpb], a.W, a.H, y0, y1, cy0, cy1, WL - 32, WC - 16);
+        __syncthreads();
     }
-    __syncthreads();
     intra_bc_search(G_ALL, a, px, py);
     if (tid == 0)
         S.row_abort = !((a.type == EVXG_FRAME_INTRA || wait_mail(&S.mail.f_seq, n, a)) && wait_mail(&S.mail.d_seq, n, a));
@@ -1833,7 +2030,10 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
     __syncthreads();
     const int ch = S.chosen;
     const bool remote = a.type == EVXG_FRAME_INTER && ch < 4;   // an intra candidate encoded by rank 2
-    write_back(a, px, py, idx, remote ? peer(S.rec[ch], 2) : S.rec[ch], remote ? peer(S.lev[ch], 2) : S.lev[ch]);
+    const int16_t *rec = remote ? peer(S.rec[ch], 2) : S.rec[ch];
+    write_back(a, px, py, idx, rec, remote ? peer(S.lev[ch], 2) : S.lev[ch]);
+    if (tid < 32)   // the right column, rank 2's left neighbour for the next MB (released with wr_seq)
+        peer(S.mail.lcol, 2)[tid] = rec[tid < 16 ? tid * 16 + 15 : 256 + ((tid - 16) >> 3) * 64 + ((tid - 16) & 7) * 8 + 7];
     __syncthreads();
     if (tid == NT - 32) {   // releases, ordered after the barrier (so after every thread's stores), by
         st_release(&a.progress[row], col);     // the last warp: thread 0 goes on to the next MB's waits
@@ -1907,22 +2107,21 @@ __device__ bool aux_mb(const FrameArgs &a, int row, int col, int n)   // rank 2
     const int tid = threadIdx.x;
     const int px = col * 16, py = row * 16;
     if (a.type == EVXG_FRAME_BIDIR && !search_mb(a, row, col, n, true)) return false;
-    // Directional intra reads MB (r, c-1), written back by the leader, and
-    // row r-1 up to column c, from the destination slot.
-    if (tid == 0) S.row_abort = !(wait_mail(&S.mail.wr_seq, n - 1, a) && (row == 0 || wait_progress(a, row - 1, col)));
+    // Directional intra reads row r-1 up to column c from the destination
+    // slot (the search has waited for column c+1) and the right column of
+    // MB (r, c-1), which the leader hands over in lcol with wr_seq.
+    if (tid == 0) S.row_abort = a.type != EVXG_FRAME_BIDIR && row > 0 && !wait_progress(a, row - 1, col);
     __syncthreads();
     if (S.row_abort) return false;
     if (a.type != EVXG_FRAME_BIDIR) {
         load_src(a, px, py);
         if (tid == 0) setup_mb(a, row * a.mbw + col, px, py, false, nullptr);
     }
-    const int16_t *dst = a.planes[a.dpb];
-    extract_nbr(px, py, [&](int p, int y, int x) -> int16_t {
-        const int16_t *pl = p == 0 ? dst : dst + (size_t)a.W * a.H + (size_t)(p - 1) * (a.W / 2) * (a.H / 2);
-        return __ldcg(pl + (size_t)y * (p ? a.W / 2 : a.W) + x);
-    });
-    if (tid == 0) choose_modes();
+    nbr_top(a, px, py);
+    if (tid == 0) S.row_abort = !wait_mail(&S.mail.wr_seq, n - 1, a);
     __syncthreads();
+    if (S.row_abort) return false;
+    nbr_left_modes(px, py);
     directional_intra(G_ALL);
     if (a.type == EVXG_FRAME_INTER) {
         if (tid == 0) intra_candidates();
@@ -1957,12 +2156,12 @@ __device__ void cluster_main(const FrameArgs &a0, const FrameArgs *args, const i
     init_tables();
     if (tid == 0) {
         S.mail.row_seq = 0; S.mail.dec_seq = 0; S.mail.wr_seq = 0; S.mail.f_seq = 0; S.mail.d_seq = 0;
-        S.row_abort = 0;
-        if (kBatched) sa = args[0];   // every stream of a tick shares the error word and the timeout
+        S.row_abort = 0; S.pf_px = -1;
+        sa = kBatched ? args[0] : a0;   // batched: every stream of a tick shares the error word and the timeout
     }
     const int nq = kBatched ? __ldg(qlen) : a0.mbh;
     cluster_barrier();   // every CTA's mail is initialised before any peer writes to it
-    const FrameArgs &w = kBatched ? sa : a0;   // for the waits before a row is known
+    const FrameArgs &w = sa;   // for the waits before a row is known
     int n = 0;
     for (int k = 1;; k++) {
         if (tid == 0) {
@@ -1988,7 +2187,7 @@ __device__ void cluster_main(const FrameArgs &a0, const FrameArgs *args, const i
             if (tid == 0) sa = args[q.x];
             __syncthreads();
         }
-        const FrameArgs &a = kBatched ? sa : a0;
+        const FrameArgs &a = sa;   // shared memory: read much faster than the kernel parameter by reference
         bool ok = true;
         for (int col = 0; col < a.mbw && ok; ++col) {
             ++n;
@@ -1999,6 +2198,7 @@ __device__ void cluster_main(const FrameArgs &a0, const FrameArgs *args, const i
         }
         if (!ok) break;
     }
+    cp_async_wait_all();
     cluster_barrier();   // no CTA leaves while a peer may still access its shared memory
 }
 
