@@ -361,6 +361,16 @@ __device__ __noinline__ void load_windows(int W, int H)
     }
 }
 
+// 16-byte asynchronous copies global -> shared, in commit groups.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Rows of window 0 (loaded around (px, py-16)) that show MB row r-1 of the
 // destination slot: window rows [y0, y1) luma and [cy0, cy1) chroma.  For
 // r = 1 the rows clamped to plane row 0 (above the frame) show it too.
@@ -388,6 +398,27 @@ __device__ void refresh_strip(const Grp g, Win &w, const int16_t *plane, int W, 
             *reinterpret_cast<uint4 *>((p ? w.v : w.u) + r * WC + cc) = win_chunk(p ? V : U, cw, ch, w.coy + r, w.cox + cc);
         }
     }
+}
+// refresh_strip for luma columns lc.. / chroma cc.. with asynchronous copies
+// (the caller commits and waits); false, copying nothing, when the strip is
+// not inside the plane (edge-filled chunks).
+__device__ bool refresh_strip_async(const Grp g, Win &w, const int16_t *plane, int W, int H, int y0, int y1, int cy0, int cy1,
+                                    int lc, int cc)
+{
+    const int gt = threadIdx.x - g.t0, cw = W / 2, ch = H / 2;
+    if (w.ox + lc < 0 || w.ox + lc + 16 > W || w.cox + cc < 0 || w.cox + cc + 8 > cw) return false;
+    const int16_t *U = plane + (size_t)W * H, *V = U + (size_t)cw * ch;
+    const int nl = (y1 - y0) * 2, nc = (cy1 - cy0) * 2;
+    for (int e = gt; e < nl + nc; e += g.nt) {
+        if (e < nl) {
+            const int r = y0 + e / 2, j = e % 2;
+            cp_async16(w.y + r * WL + lc + 8 * j, plane + (size_t)min(max(w.oy + r, 0), H - 1) * W + w.ox + lc + 8 * j);
+        } else {
+            const int f = e - nl, p = f & 1, r = cy0 + f / 2;
+            cp_async16((p ? w.v : w.u) + r * WC + cc, (p ? V : U) + (size_t)min(max(w.coy + r, 0), ch - 1) * cw + w.cox + cc);
+        }
+    }
+    return true;
 }
 // The newest strip (MB column c+3).
 __device__ void refresh_newest(const Grp g, Win &w, const int16_t *plane, int W, int H, int y0, int y1, int cy0, int cy1)
@@ -1086,7 +1117,10 @@ __device__ __noinline__ void encode_candidates(const Grp g, const FrameArgs &a, 
 __device__ bool wait_progress(const FrameArgs &a, int r, int need);
 
 // Intra block-copy search in the current frame (motion.cpp:485-565), window 0.
-__device__ __noinline__ void intra_bc_search(const Grp g, const FrameArgs &a, int px, int py)
+// With strip_pending, column c+2's rows above are still being copied into
+// window 0 (the callers' older commit group): the first step does not read
+// them (its candidates end at column c+1), the others wait for them.
+__device__ __noinline__ void intra_bc_search(const Grp g, const FrameArgs &a, int px, int py, bool strip_pending)
 {
     MbShared &S = SM();
     Srch &sr = S.srch[0];
@@ -1102,6 +1136,10 @@ __device__ __noinline__ void intra_bc_search(const Grp g, const FrameArgs &a, in
     }
     gsync(g);
     Sel s = run_step(g, 0, 0, true, -SEARCH_RADIUS, -(SEARCH_RADIUS << 1), SEARCH_RADIUS, px, py, a.W, a.H, a.lambda, sr.sel, 0);
+    if (strip_pending) {
+        cp_async_wait_group<1>();   // this thread's strip copies; the prefetch group may go on
+        gsync(g);
+    }
     if (s.mad >= S.thr) {
         int par = 1;
         for (int st = SEARCH_RADIUS >> 1; st > 0; st >>= 1, par ^= 1) {
@@ -1654,7 +1692,7 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
     const int gi = tid / GT;
     const Grp g = group(gi);
     if (gi == 0) {
-        intra_bc_search(g, a, px, py);
+        intra_bc_search(g, a, px, py, false);
         if (a.type == EVXG_FRAME_BIDIR) directional_intra(g);
     } else if (gi == 1) {
         if (a.type == EVXG_FRAME_INTRA) directional_intra(g);
@@ -1888,14 +1926,6 @@ __device__ void shift_window0(const FrameArgs &a, int nox, int ncox, bool staged
     }
 }
 
-// 16-byte asynchronous copies global -> shared (the caller's thread waits
-// for its own with cp_async_wait_all).
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
 // Leader, whole CTA, after the wavefront wait of MB (row, col): start copying
 // the next MB's source and window 0's new strip for it (MB column c+4) into
 // nsrc / nstrip.  Row r-2 has finished column c+4 (row r-1 finished c+2 after
@@ -1982,14 +2012,16 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
         }
         bar_sync(1, NP);
         if (!S.row_abort) {
-            if (early) {
-                if (row > 0) {
-                    int y0, y1, cy0, cy1;
-                    rows_above(py, y0, y1, cy0, cy1);
-                    refresh_strip(Grp{1, 0, NP}, S.win[0], dst, a.W, a.H, y0, y1, cy0, cy1, WL - 32, WC - 16);
-                }
+            if (early && row > 0) {   // column c+2's rows above: copied while the search's first step runs
+                int y0, y1, cy0, cy1;
+                rows_above(py, y0, y1, cy0, cy1);
+                const Grp gp{1, 0, NP};
+                if (!refresh_strip_async(gp, S.win[0], dst, a.W, a.H, y0, y1, cy0, cy1, WL - 32, WC - 16))
+                    refresh_strip(gp, S.win[0], dst, a.W, a.H, y0, y1, cy0, cy1, WL - 32, WC - 16);
             }
+            cp_async_commit();
             prefetch_next(a, row, col, NP);
+            cp_async_commit();
         }
     }
     __syncthreads();
@@ -1998,7 +2030,7 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
         load_windows(a.W, a.H);
         __syncthreads();
     }
-    intra_bc_search(G_ALL, a, px, py);
+    intra_bc_search(G_ALL, a, px, py, true);
     if (tid == 0)
         S.row_abort = !((a.type == EVXG_FRAME_INTRA || wait_mail(&S.mail.f_seq, n, a)) && wait_mail(&S.mail.d_seq, n, a));
     __syncthreads();
