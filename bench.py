@@ -42,7 +42,7 @@ EQ = (W * H) / (1920 * 1080)
 HBM_PEAK_FALLBACK = 6650.0
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_mb_cluster launch
 # (a 1080p B frame of this workload), profiles/mb_cluster_1080p.md
-MB_TRAFFIC_BYTES = 25_302_016 + 509_952
+MB_TRAFFIC_BYTES = 25_386_496 + 257_792
 
 
 def peaks():
@@ -239,7 +239,7 @@ def run_gpu(args):
                      "traffic": MB_TRAFFIC_BYTES if st.mb_form == cb.MB_FORM_CLUSTER else None,
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "note": "dependency-latency bound: macroblock wavefront whose critical path is "
-                             "cols + 4*(rows-1) MB steps (388 at 1080p), each one MB's dependent chain"},
+                             "cols + 3*(rows-1) MB steps (321 at 1080p), each one MB's dependent chain"},
         "gpu_launches": st.launch_count() * K,
         "batched": batched,
         "served": served,
