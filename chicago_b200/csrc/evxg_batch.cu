@@ -51,20 +51,20 @@ struct evxg_batch {
 static const int kTickKernels = 10 + kSaoPasses;   // kernels per tick, whatever the number of streams
 
 // Shape of the macroblock pass from a model of the tick: a tick lasts at least
-// its longest wavefront's critical path (cols + 4 x (rows - 1) MB steps) and at
+// its longest wavefront's critical path (cols + 3 x (rows - 1) MB steps) and at
 // least the MBs of all streams over the units working on them (SMs in the
 // single form, three-SM clusters in the cluster form), each MB step costing
-// about kSingleVsCluster times as long in the single form (clock64 probes of
-// both forms on 1080p frames).
-static const double kSingleVsCluster = 2.2;
+// about kSingleVsCluster times as long in the single form (both forms timed on
+// one 1080p, 720p and 360p stream: 1.53 at every size).
+static const double kSingleVsCluster = 1.5;
 static void model_shape(evxg_batch *b)
 {
     double path = 0, mbs = 0;
     int busy = 0;
     for (const evxg_stream *s : b->st) {
-        path = std::max(path, (double)(s->mbw + 4 * (s->mbh - 1)));
+        path = std::max(path, (double)(s->mbw + 3 * (s->mbh - 1)));
         mbs += (double)s->mbw * s->mbh;
-        busy += (int)std::min<uint32_t>(s->mbh, s->mbw / 4 + 4);
+        busy += (int)std::min<uint32_t>(s->mbh, s->mbw / 3 + 3);
     }
     const double t_single = kSingleVsCluster * std::max(path, mbs / b->num_sms);
     const double t_cluster = b->max_clusters > 0 ? std::max(path, mbs / b->max_clusters) : 1e30;
@@ -86,9 +86,9 @@ static size_t out_bytes(const evxg_stream *s)
 
 // Row queue of a tick.  Policy 0 interleaves the streams row by row (rows
 // that can start at about the same time are claimed together: row r of any
-// stream starts about 4r macroblock steps into the tick); policy 1 also puts,
+// stream starts about 3r macroblock steps into the tick); policy 1 also puts,
 // among rows of the same index, the streams with the longer remaining
-// critical path (columns + 4 x rows left) first.  Both keep every stream's
+// critical path (columns + 3 x rows left) first.  Both keep every stream's
 // rows in order, which the wavefront's deadlock freedom needs.
 static int build_queue(const evxg_batch *b, const std::vector<char> &active, int *q)
 {
@@ -98,7 +98,7 @@ static int build_queue(const evxg_batch *b, const std::vector<char> &active, int
         if (!active[i]) continue;
         const evxg_stream *s = b->st[i];
         for (uint32_t r = 0; r < s->mbh; r++)
-            v.push_back({(int)i, (int)r, (long)r, b->policy == 1 ? -(long)(s->mbw + 4 * (s->mbh - 1 - r)) : (long)i});
+            v.push_back({(int)i, (int)r, (long)r, b->policy == 1 ? -(long)(s->mbw + 3 * (s->mbh - 1 - r)) : (long)i});
     }
     std::stable_sort(v.begin(), v.end(), [](const Item &x, const Item &y) {
         return x.key != y.key ? x.key < y.key : x.tie < y.tie;

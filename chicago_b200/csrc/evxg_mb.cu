@@ -1184,14 +1184,26 @@ __device__ __noinline__ void intra_bc_search(const Grp g, const FrameArgs &a, in
 // hands it over in shared memory before the leader writes the table).
 __device__ void pred_gather(const FrameArgs &a, int idx, bool temporal, PredIn &o)
 {
+    // Every candidate entry's first three words are read at once (one round
+    // trip), then the reference's order picks among them.
     const int mbw = a.mbw, bx = idx % mbw, by = idx / mbw;
-    auto motion = [&](int i) { return (__ldcg(&a.bt[i].block_type) & BT_MOTION) != 0; };
-    auto take = [&](int k, int i) { o.has[k] = 1; o.mx[k] = __ldcg(&a.bt[i].motion_x); o.my[k] = __ldcg(&a.bt[i].motion_y); };
+    auto words = [&](const evxg_block_desc *t, int i, int4 &w) {
+        const int *p = reinterpret_cast<const int *>(t + i);
+        w.x = __ldcg(p); w.y = __ldcg(p + 1); w.z = __ldcg(p + 2);
+    };
+    int4 wt = {0, 0, 0, 0}, wr = {0, 0, 0, 0}, wl = {0, 0, 0, 0}, wp = {0, 0, 0, 0};
+    if (by > 0) words(a.bt, idx - mbw, wt);
+    if (by > 0 && bx + 1 < mbw) words(a.bt, idx - mbw + 1, wr);
+    if (by > 0 && bx > 0) words(a.bt, idx - mbw - 1, wl);
+    if (temporal) words(a.prev, idx, wp);
+    // word 0 block_type; word 1 bytes 2..3 motion_x; word 2 bytes 0..1 motion_y
+    static_assert(offsetof(evxg_block_desc, motion_x) == 6 && offsetof(evxg_block_desc, motion_y) == 8, "descriptor layout");
+    auto take = [&](int k, const int4 &w) { o.has[k] = 1; o.mx[k] = (int16_t)(w.y >> 16); o.my[k] = (int16_t)(w.z & 0xffff); };
     o.has[0] = o.has[1] = o.has[2] = 0;
-    if (by > 0 && motion(idx - mbw)) take(0, idx - mbw);
-    if (by > 0 && bx + 1 < mbw && motion(idx - mbw + 1)) take(1, idx - mbw + 1);
-    else if (by > 0 && bx > 0 && motion(idx - mbw - 1)) take(1, idx - mbw - 1);
-    if (temporal && (a.prev[idx].block_type & BT_MOTION)) { o.has[2] = 1; o.mx[2] = a.prev[idx].motion_x; o.my[2] = a.prev[idx].motion_y; }
+    if (by > 0 && (wt.x & BT_MOTION)) take(0, wt);
+    if (by > 0 && bx + 1 < mbw && (wr.x & BT_MOTION)) take(1, wr);
+    else if (by > 0 && bx > 0 && (wl.x & BT_MOTION)) take(1, wl);
+    if (temporal && (wp.x & BT_MOTION)) take(2, wp);
 }
 __device__ void pred_combine(const FrameArgs &a, int idx, const PredIn &p, const evxg_block_desc *left, int &ox, int &oy)
 {
