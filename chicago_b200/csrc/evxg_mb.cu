@@ -1393,59 +1393,10 @@ __device__ void req_window0(const FrameArgs &a, int px, int py)   // one thread
     rows_above(py, q.fy0, q.fy1, q.fcy0, q.fcy1);
 }
 
-// Neighbours for directional intra (intra_pred.cpp:13-54); sample(p, y, x)
-// returns plane p's (Y, U, V) sample at plane coordinates.  Threads 0..63
-// fetch the 64 top / left samples in parallel, the corner and DC follow.
-// Ends with a CTA barrier.
-template <class F>
-__device__ void extract_nbr(int px, int py, F sample)
-{
-    MbShared &S = SM();
-    const int tid = threadIdx.x;
-    const bool ht = py > 0, hl = px > 0;
-    if (tid < 64) {   // luma top 0..15, left 16..31; U top 32..39, left 40..47; V 48..63
-        const int p = tid < 32 ? 0 : (tid < 48 ? 1 : 2);
-        const int k = tid < 32 ? tid : (tid - 32) & 15, n = p ? 8 : 16;
-        const int cy = p ? py >> 1 : py, cx = p ? px >> 1 : px;
-        Nbr &nb = S.nb[p];
-        if (k < n) nb.top[k] = ht ? sample(p, cy - 1, cx + k) : (int16_t)128;
-        else nb.left[k - n] = hl ? sample(p, cy + k - n, cx - 1) : (int16_t)128;
-    } else if (tid < 67) {
-        const int p = tid - 64, cy = p ? py >> 1 : py, cx = p ? px >> 1 : px;
-        S.nb[p].corner = (ht && hl) ? sample(p, cy - 1, cx - 1) : (int16_t)0;
-    }
-    __syncthreads();
-    if (tid < 3) {
-        Nbr &nb = S.nb[tid];
-        const int n = tid ? 8 : 16;
-        nb.ht = ht; nb.hl = hl;
-        if (!(ht && hl)) nb.corner = ht ? nb.top[0] : (hl ? nb.left[0] : (int16_t)128);
-        int sum = 0, cnt = 0;
-        if (ht) { for (int i = 0; i < n; i++) sum += nb.top[i]; cnt += n; }
-        if (hl) { for (int i = 0; i < n; i++) sum += nb.left[i]; cnt += n; }
-        nb.dc = cnt > 0 ? (int16_t)((sum + cnt / 2) / cnt) : 128;
-    }
-    __syncthreads();
-}
-
-__device__ void choose_modes()   // one thread: gradient-pruned candidates (intra_pred.cpp:225-260)
-{
-    MbShared &S = SM();
-    const Nbr &nb = S.nb[0];
-    int gh = 0, gv = 0;
-    if (nb.ht) for (int i = 1; i < 16; i++) gh += iabs32(nb.top[i] - nb.top[i - 1]);
-    if (nb.hl) for (int i = 1; i < 16; i++) gv += iabs32(nb.left[i] - nb.left[i - 1]);
-    S.modes[0] = 0;
-    if (gv > gh * 3 / 2) { S.modes[1] = 2; S.modes[2] = 6; }
-    else if (gh > gv * 3 / 2) { S.modes[1] = 1; S.modes[2] = 5; }
-    else { S.modes[1] = 3; S.modes[2] = 4; }
-}
-
 // Cluster rank 2: the directional neighbours in two parts.  nbr_top (threads
 // 0..34, before the left neighbour is final): the top rows and corners from
 // the destination slot.  nbr_left_modes (warp 0, ends with a CTA barrier):
-// the left columns from the mail, then what extract_nbr and choose_modes
-// derive -- corner fallbacks, DC, the gradient-pruned modes.
+// the left columns from the mail, then nbr_derive.
 __device__ void nbr_top(const FrameArgs &a, int px, int py)
 {
     MbShared &S = SM();
@@ -1462,32 +1413,36 @@ __device__ void nbr_top(const FrameArgs &a, int px, int py)
         S.nb[p].corner = (ht && hl) ? __ldcg(plane(p) + (size_t)(cy - 1) * (p ? cw : a.W) + cx - 1) : (int16_t)0;
     }
 }
-__device__ void nbr_left_modes(int px, int py)
+// Warp 0 of the CTA (ends with a CTA barrier): the directional neighbours
+// from top(p, k), left(p, k) and corner(p) (plane p, sample k; samples
+// outside the frame are 128), the corner fallbacks, each plane's DC and the
+// gradient-pruned candidate modes (intra_pred.cpp:13-54, :225-260).
+template <class Top, class Left, class Corner>
+__device__ void nbr_derive(int px, int py, Top top_of, Left left_of, Corner corner_of)
 {
     MbShared &S = SM();
     const int tid = threadIdx.x;
     const bool ht = py > 0, hl = px > 0;
     if (tid < 32) {
-        const int lane = tid, p = lane < 16 ? 0 : (lane < 24 ? 1 : 2), k = p ? (lane - 16) & 7 : lane, n = p ? 8 : 16;
+        const int lane = tid, p = lane < 16 ? 0 : (lane < 24 ? 1 : 2), k = p ? (lane - 16) & 7 : lane;
         Nbr &nb = S.nb[p];
-        const int16_t left = hl ? S.mail.lcol[lane] : (int16_t)128;
-        nb.left[k] = left;
-        const int top = nb.top[k];
-        __syncwarp();
-        // DC of each plane: top (if any) and left (if any) samples (intra_pred.cpp:13-54)
+        const int top = ht ? (int)top_of(p, k) : 128, left = hl ? (int)left_of(p, k) : 128;
+        nb.top[k] = (int16_t)top; nb.left[k] = (int16_t)left;
+        // DC of each plane: top (if any) and left (if any) samples
         const int v = (ht ? top : 0) + (hl ? left : 0);
         const int sy = __reduce_add_sync(0xffffffffu, p == 0 ? v : 0), su = __reduce_add_sync(0xffffffffu, p == 1 ? v : 0),
                   sv = __reduce_add_sync(0xffffffffu, p == 2 ? v : 0);
-        // luma gradients along the top row and the left column (intra_pred.cpp:225-260)
-        const int tprev = __shfl_up_sync(0xffffffffu, top, 1), lprev = __shfl_up_sync(0xffffffffu, (int)left, 1);
+        // luma gradients along the top row and the left column
+        const int tprev = __shfl_up_sync(0xffffffffu, top, 1), lprev = __shfl_up_sync(0xffffffffu, left, 1);
         const bool gl = p == 0 && k >= 1;
         const int gh = __reduce_add_sync(0xffffffffu, gl && ht ? iabs32(top - tprev) : 0);
         const int gv = __reduce_add_sync(0xffffffffu, gl && hl ? iabs32(left - lprev) : 0);
+        __syncwarp();
         if (lane < 3) {
             Nbr &q = S.nb[lane];
             const int nn = lane ? 8 : 16, cnt = (ht ? nn : 0) + (hl ? nn : 0), sum = lane == 0 ? sy : (lane == 1 ? su : sv);
             q.ht = ht; q.hl = hl;
-            if (!(ht && hl)) q.corner = ht ? q.top[0] : (hl ? q.left[0] : (int16_t)128);
+            q.corner = (ht && hl) ? (int16_t)corner_of(lane) : (ht ? q.top[0] : (hl ? q.left[0] : (int16_t)128));
             q.dc = cnt > 0 ? (int16_t)((sum + cnt / 2) / cnt) : 128;
         }
         if (lane == 0) {
@@ -1496,9 +1451,15 @@ __device__ void nbr_left_modes(int px, int py)
             else if (gh > gv * 3 / 2) { S.modes[1] = 1; S.modes[2] = 5; }
             else { S.modes[1] = 3; S.modes[2] = 4; }
         }
-        (void)n;
     }
     __syncthreads();
+}
+// Rank 2, after nbr_top and the write-back wait: left columns from the mail.
+__device__ void nbr_left_modes(int px, int py)
+{
+    MbShared &S = SM();
+    nbr_derive(px, py, [&](int p, int k) { return S.nb[p].top[k]; },
+               [&](int p, int k) { return S.mail.lcol[p == 0 ? k : 8 + 8 * p + k]; }, [&](int p) { return S.nb[p].corner; });
 }
 
 // P frames: the intra RDO candidates -- intra without prediction and the
@@ -1693,12 +1654,16 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
     __syncthreads();
     load_windows(a.W, a.H);
     __syncthreads();
-    extract_nbr(px, py, [&](int p, int y, int x) -> int16_t {   // from window 0
+    {   // directional neighbours from window 0
         const Win &w = S.win[0];
-        return p == 0 ? w.y[(y - w.oy) * WL + x - w.ox] : (p == 1 ? w.u : w.v)[(y - w.coy) * WC + x - w.cox];
-    });
-    if (tid == 0) choose_modes();
-    __syncthreads();
+        auto at = [&](int p, int y, int x) -> int16_t {
+            return p == 0 ? w.y[(y - w.oy) * WL + x - w.ox] : (p == 1 ? w.u : w.v)[(y - w.coy) * WC + x - w.cox];
+        };
+        auto cy = [&](int p) { return p ? py >> 1 : py; };
+        auto cx = [&](int p) { return p ? px >> 1 : px; };
+        nbr_derive(px, py, [&](int p, int k) { return at(p, cy(p) - 1, cx(p) + k); },
+                   [&](int p, int k) { return at(p, cy(p) + k, cx(p) - 1); }, [&](int p) { return at(p, cy(p) - 1, cx(p) - 1); });
+    }
 
     // Independent work runs concurrently on three warp groups.
     const int gi = tid / GT;
@@ -1714,18 +1679,21 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
             inter_search(g, a, 2, 3, 4, px, py, S.pred[2], false);
         } else if (a.type == EVXG_FRAME_INTER) {
             // The intra RDO candidates do not depend on the searches
-            // (encode.cpp:295-336): encode them while the searches run.
+            // (encode.cpp:295-336): two of them are encoded while the
+            // searches run, the other two with the SAD winner afterwards
+            // (candidates 2..4 on the whole CTA), which balances the groups.
             directional_intra(g);
             if (tid - g.t0 == 0) intra_candidates();
             gsync(g);
-            encode_candidates(g, a, 0, 4);
+            encode_candidates(g, a, 0, 2);
         }
     }
     __syncthreads();
     if (a.type == EVXG_FRAME_BIDIR) bi_prediction();
     if (tid == 0) decide(a);
     __syncthreads();
-    if (S.need_encode) encode_candidates(G_ALL, a, 4, 1);
+    if (a.type == EVXG_FRAME_INTER) encode_candidates(G_ALL, a, 2, S.need_encode ? 3 : 2);
+    else if (S.need_encode) encode_candidates(G_ALL, a, 4, 1);
     if (tid == 0) {
         rdo_choose();
         if (row == 1) wait_progress(a, 0, min(col + 3, a.mbw - 1));   // see mb_row
