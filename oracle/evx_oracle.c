@@ -62,7 +62,8 @@ enum { INTRA_DEFAULT = 1, INTRA_MOTION_COPY = 7, INTRA_MOTION_DELTA = 3, INTER_C
 enum { F_INTRA = 0, F_INTER = 1, F_BIDIR = 2 };
 #define MODE_NONE 7
 #define SAD_THRESHOLD 8192   /* motion.cpp:24 */
-#define SEARCH_RADIUS 16     /* motion.cpp:29 */
+/* EVX_MOTION_SEARCH_RADIUS (motion.cpp:29) is 16 in the default build; the
+ * context carries it (orc_set_config) so that build variants can be restated. */
 #define MAXQ 63              /* quantize.h:42 (levels - 1) */
 
 /* ---------- integer helpers (evx_math.h) ---------- */
@@ -581,6 +582,10 @@ static void trellis_mb(u8 qp, i32 bt, mbv tc, u8 mode, float lambda, mbv lv) /* 
 /* ---------- encoder context ---------- */
 struct orc_ctx {
     i32 w, h, mbw, mbh;
+    /* compile-time switches of the reference build being restated:
+     * EVX_ENABLE_B_FRAMES (config.h:120), EVX_REFERENCE_FRAME_COUNT (:39),
+     * EVX_MOTION_SEARCH_RADIUS (motion.cpp:29) */
+    int b_frames, ref_count, radius;
     i16 *src_mem, *lev_mem, *dpb_mem[4];
     pset src, lev, dpb[4];
     blk *bt, *prev;
@@ -592,6 +597,7 @@ orc_ctx *orc_create(u32 aw, u32 ah)
     orc_ctx *c = (orc_ctx *)calloc(1, sizeof(orc_ctx));
     size_t n = (size_t)aw * ah + 2 * (size_t)(aw / 2) * (ah / 2);
     c->w = (i32)aw; c->h = (i32)ah; c->mbw = (i32)aw / 16; c->mbh = (i32)ah / 16;
+    c->b_frames = 1; c->ref_count = 4; c->radius = 16;
     c->src_mem = (i16 *)calloc(n, 2); c->lev_mem = (i16 *)calloc(n, 2);
     c->src = pset_wrap(c->src_mem, c->w, c->h); c->lev = pset_wrap(c->lev_mem, c->w, c->h);
     for (int i = 0; i < 4; i++) { c->dpb_mem[i] = (i16 *)calloc(n, 2); c->dpb[i] = pset_wrap(c->dpb_mem[i], c->w, c->h); }
@@ -606,6 +612,19 @@ void orc_destroy(orc_ctx *c)
     free(c->src_mem); free(c->lev_mem);
     for (int i = 0; i < 4; i++) free(c->dpb_mem[i]);
     free(c->bt); free(c->prev); free(c->sao); free(c);
+}
+int orc_set_config(orc_ctx *c, int b_frames, int ref_count, int radius)
+{
+    if (b_frames ? ref_count != 4 : (ref_count != 2 && ref_count != 4)) return 1;
+    if (radius != 16 && radius != 32) return 1;
+    c->b_frames = b_frames; c->ref_count = ref_count; c->radius = radius;
+    return 0;
+}
+/* Without B frames every slot follows from the frame index:
+ * query_prediction_index_by_offset (common.cpp:256-259). */
+static u32 slot_by_offset(const orc_ctx *c, const frm *f, u32 offset)
+{
+    return (f->index + (u32)c->ref_count - offset) % (u32)c->ref_count;
 }
 static size_t pset_n(const orc_ctx *c) { return (size_t)c->w * c->h + 2 * (size_t)(c->w / 2) * (c->h / 2); }
 int orc_get_slot(orc_ctx *c, u32 slot, i16 *out) { if (slot > 3) return 1; memcpy(out, c->dpb_mem[slot], pset_n(c) * 2); return 0; }
@@ -703,9 +722,10 @@ static i32 intra_bc_search(const frm *f, orc_ctx *c, mbv src, i32 px, i32 py, bl
     sel s = {px, py, sad_self(src), INT32_MAX, INT32_MAX, 0.0f, 0, 0, 0};
     s.cost = (float)s.sad;
     sparams pp = {&c->dpb[f->dpb_slot], (i16)((f->quality >> 2) + 1), px, py, orc_lambda(f->quality)};
-    step_search(1, -SEARCH_RADIUS, -(SEARCH_RADIUS << 1), SEARCH_RADIUS, 0, SEARCH_RADIUS, &pp, src, &s);
+    const i16 R = (i16)c->radius;
+    step_search(1, -R, -(R << 1), R, 0, R, &pp, src, &s);
     if (s.mad >= pp.thr)
-        for (i16 st = SEARCH_RADIUS >> 1; st > 0; st >>= 1) {
+        for (i16 st = R >> 1; st > 0; st >>= 1) {
             step_search(1, -st, -st, st, st, st, &pp, src, &s);
             if (s.mad < pp.thr) break;
         }
@@ -758,9 +778,9 @@ static i32 inter_search(const frm *f, orc_ctx *c, mbv src, i32 px, i32 py, u32 s
         eval_cand(x, y, &pp, src, &s);
     }
     if (s.mad >= pp.thr) {
-        i16 r = SEARCH_RADIUS;
-        if (s.sad < SAD_THRESHOLD / 4) r = SEARCH_RADIUS / 4;
-        else if (s.sad < SAD_THRESHOLD / 2) r = SEARCH_RADIUS / 2;
+        i16 r = (i16)c->radius;
+        if (s.sad < SAD_THRESHOLD / 4) r = (i16)(c->radius / 4);
+        else if (s.sad < SAD_THRESHOLD / 2) r = (i16)(c->radius / 2);
         for (i16 st = r; st > 0; st >>= 1) {
             step_search(0, -st, -st, st, st, st, &pp, src, &s);
             if (s.mad < pp.thr) break;
@@ -816,8 +836,11 @@ static int build_pred(const frm *f, orc_ctx *c, const blk *d, i32 i, i32 j, mbbu
         bi_average(fw, bw, mb_buf(b2));
         *out = mb_buf(b2); return 1;
     }
-    if (IS_MOTION(bt)) motion_pred(&c->dpb[d->prediction_target], i + d->motion_x, j + d->motion_y, d->sp_pred, d->sp_amount, d->sp_index, b0, out);
-    else *out = mb_at(&c->dpb[d->prediction_target], i, j);
+    /* with B frames the target is a DPB slot, without them an offset from the
+     * frame index (encode.cpp:597-608, decode.cpp:196-203) */
+    const u32 ref = c->b_frames ? d->prediction_target : slot_by_offset(c, f, d->prediction_target);
+    if (IS_MOTION(bt)) motion_pred(&c->dpb[ref], i + d->motion_x, j + d->motion_y, d->sp_pred, d->sp_amount, d->sp_index, b0, out);
+    else *out = mb_at(&c->dpb[ref], i, j);
     return 1;
 }
 
@@ -937,12 +960,24 @@ static void classify(const frm *f, orc_ctx *c, mbv src, i32 i, i32 j, u32 idx, b
         *out = best;
         return;
     }
-    if (f->type == F_INTER) {
+    if (f->type == F_INTER && c->b_frames) {   /* one reference, the frame's forward slot (encode.cpp:182-209) */
         blk in; i32 is = inter_search(f, c, src, i, j, f->ref_slot_fwd, idx, c->prev, &in);
         in.prediction_target = f->ref_slot_fwd;
         if (IS_COPY(in.block_type) ^ IS_COPY(best.block_type)) {
             if (IS_COPY(in.block_type)) { best = in; best_sad = is; }
         } else if (is < best_sad) { best = in; best_sad = is; }
+    } else if (f->type == F_INTER) {
+        /* without B frames: every offset 1 .. EVX_REFERENCE_FRAME_COUNT-1, the
+         * nearer references favoured by a distance bias (encode.cpp:211-247,
+         * calculate_inter_prediction motion.cpp:681-698) */
+        for (u32 off = 1; off < (u32)c->ref_count; off++) {
+            blk in; i32 is = inter_search(f, c, src, i, j, slot_by_offset(c, f, off), idx, c->prev, &in);
+            in.prediction_target = (u8)off;
+            const i32 bias = (i32)(lambda * (float)(off * 2));
+            if (IS_COPY(in.block_type) ^ IS_COPY(best.block_type)) {
+                if (IS_COPY(in.block_type)) { best = in; best_sad = is; }
+            } else if (is + bias < best_sad) { best = in; best_sad = is; }
+        }
     }
     i32 ds; u8 m = best_intra_mode(src, &c->dpb[f->dpb_slot], i, j, &ds);
     if (ds < best_sad) { clear_blk(&best); best.intra_mode = m; best_sad = ds; }
@@ -1169,6 +1204,12 @@ int orc_encode_frame(orc_ctx *c, const u8 *rgb, u32 w, u32 h, const u8 *frame18,
 {
     frm f; memcpy(&f, frame18, sizeof f);
     if ((w | h) & 1) return 1;
+    if (!c->b_frames) {   /* the destination follows from the index (encode.cpp:952-956) */
+        if (f.type == F_BIDIR) return 1;
+        f.dpb_slot = (u8)slot_by_offset(c, &f, 0);
+        f.ref_slot_fwd = (u8)slot_by_offset(c, &f, 1);
+        f.ref_slot_bwd = 0;
+    }
     if (f.dpb_slot > 3 || f.ref_slot_fwd > 3 || f.ref_slot_bwd > 3) return 1;
     orc_convert(rgb, w, h, c->src_mem, (u32)c->w, (u32)c->h);
     dump_pset(c, c->src_mem, dump_src);
@@ -1192,6 +1233,6 @@ int orc_encode_frame(orc_ctx *c, const u8 *rgb, u32 w, u32 h, const u8 *frame18,
     sao_frame(c, dst, orc_lambda(f.quality));
     if (dump_sao) memcpy(dump_sao, c->sao, (size_t)c->mbw * c->mbh * 16);
     dump_pset(c, dst->y, dump_final);
-    if (f.type != F_BIDIR) memcpy(c->prev, c->bt, (size_t)c->mbw * c->mbh * sizeof(blk));
+    if (f.type != F_BIDIR) memcpy(c->prev, c->bt, (size_t)c->mbw * c->mbh * sizeof(blk));   /* encode.cpp:988-998 */
     return 0;
 }

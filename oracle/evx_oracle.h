@@ -25,6 +25,14 @@ typedef struct orc_ctx orc_ctx;
 orc_ctx *orc_create(uint32_t aligned_w, uint32_t aligned_h);
 void orc_destroy(orc_ctx *c);
 
+/* The reference build being restated (compile-time switches there):
+ * b_frames = EVX_ENABLE_B_FRAMES (1 default; 0 = I/P GOP whose P frames search
+ * the slots at offsets 1 .. ref_count-1 from the frame index), ref_count =
+ * EVX_REFERENCE_FRAME_COUNT (4 default; 2 or 4 without B frames), radius =
+ * EVX_MOTION_SEARCH_RADIUS (16 default, or 32).  Non-zero for an unsupported
+ * combination.  Call before the first frame. */
+int orc_set_config(orc_ctx *c, int b_frames, int ref_count, int radius);
+
 /* One frame of engine_encode_frame minus serialization (encode.cpp:945-998).
  * frame18: 18-byte packed evx_frame.  Dumps may be NULL; same layouts as the
  * reference harness (blocks: 28 B per MB, sao: 16 B per MB). */

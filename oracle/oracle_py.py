@@ -8,6 +8,13 @@
 * ``plan_gop`` -- the frame-type / DPB-slot schedule of the reference encoder's
                   GOP logic (src/video/evx3enc.cpp:105-414), restated in Python,
                   used to drive the staged engines frame by frame.
+* ``plan_ip``  -- the same for the I/P builds (EVX_ENABLE_B_FRAMES 0,
+                  evx3enc.cpp:137-160): one frame out per frame in.
+
+Build variants of the reference (oracle/variants/, ``REF_VARIANTS``): "ip1"
+(I/P GOP, one reference), "ip3" (I/P GOP, three references), "seq" (default
+GOP, one thread).  ``Ref(variant=...)`` loads one; ``Oracle.context(...,
+config=...)`` restates the same switches.
 """
 from __future__ import annotations
 
@@ -19,6 +26,12 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libevxref.so")
+# variant -> (library, EVX_ENABLE_B_FRAMES, EVX_REFERENCE_FRAME_COUNT)
+REF_VARIANTS = {
+    "ip1": (os.path.join(HERE, "_ref", "libevxref_ip1.so"), 0, 2),
+    "ip3": (os.path.join(HERE, "_ref", "libevxref_ip3.so"), 0, 4),
+    "seq": (os.path.join(HERE, "_ref", "libevxref_seq.so"), 1, 4),
+}
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 
 BLOCK_DTYPE = np.dtype([
@@ -129,6 +142,33 @@ def plan_gop(n_frames: int, quality: int = 8, intra_at=(), b_frames: int = 3):
     return out
 
 
+def plan_ip(n_frames: int, quality: int = 8, intra_at=(), ref_count: int = 2):
+    """Yield (input_frame_index, frame18) for the I/P builds
+    (EVX_ENABLE_B_FRAMES 0): every frame is encoded as it arrives
+    (evx3enc.cpp:137-160), an I frame first and after each insert_intra(),
+    else a P frame; the index grows by one per frame and selects the DPB slots
+    (query_prediction_index_by_offset, common.cpp:256-259).  Only the first 10
+    bytes (type, index, quality) exist in those builds; the rest of the 18-byte
+    record carries the slots the index selects: dpb_slot = offset 0,
+    ref_fwd = offset 1."""
+    qp = quality_to_qp(quality)
+    out, ftype = [], FRAME_INTRA
+    for t in range(n_frames):
+        if t in intra_at:
+            ftype = FRAME_INTRA
+        out.append((t, pack_frame(ftype, t, qp, t, 1, t % ref_count, (t + ref_count - 1) % ref_count, 0)))
+        ftype = FRAME_INTER
+        if (t + 1) % 3600 == 0:   # EVX_PERIODIC_INTRA_RATE
+            ftype = FRAME_INTRA
+    return out
+
+
+def join_ip_stream(header: bytes, frames) -> bytes:
+    """An I/P build's stream: the 14-byte header, then per frame its 10-byte
+    evx_frame and the slice bytes, with no size prefix (evx3enc.cpp:141-147)."""
+    return header + b"".join(bytes(f18[:10]) + sl for f18, sl in frames)
+
+
 def split_stream(data: bytes):
     """Split a stock .evx stream into (header, [frame payloads]); each payload
     is frame18 + slice bytes (evx3enc.cpp:249-277)."""
@@ -168,10 +208,16 @@ class StageDump:
 class Ref:
     """The unmodified reference library (built here from its own sources)."""
 
-    def __init__(self, path: str = REF_SO):
+    def __init__(self, path: str = REF_SO, variant: str | None = None):
+        if variant is not None:
+            path = REF_VARIANTS[variant][0]
         if not os.path.exists(path):
-            raise FileNotFoundError(f"reference library not built: {path} (make -C oracle ref)")
+            raise FileNotFoundError(f"reference library not built: {path} (make -C oracle ref variants)")
         L = self.lib = C.CDLL(path)
+        L.evxref_config.argtypes = [C.POINTER(C.c_int)] * 5
+        v = [C.c_int(0) for _ in range(5)]
+        L.evxref_config(*[C.byref(x) for x in v])
+        self.b_frames, self.ref_count, self.wpp, self.frame_bytes, self.block_bytes = [x.value for x in v]
         L.evxref_enc_create.restype = C.c_void_p
         L.evxref_enc_create.argtypes = [C.c_uint32]
         L.evxref_enc_destroy.argtypes = [C.c_void_p]
@@ -275,6 +321,7 @@ class Oracle:
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.c_uint32, C.c_uint32]
         L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_set_config.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
         L.orc_encode_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_char_p] + \
                                       [C.c_void_p] * 7
         for nm in ("orc_get_slot",):
@@ -298,14 +345,18 @@ class Oracle:
         L.orc_deblock_strength.argtypes = [C.c_int32, C.c_void_p, C.c_void_p]
         L.orc_convert.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32]
 
-    def context(self, width: int, height: int):
-        return OracleContext(self, align16(width), align16(height))
+    def context(self, width: int, height: int, b_frames: int = 1, ref_count: int = 4, radius: int = 16):
+        """A stream context restating the reference build with these switches
+        (EVX_ENABLE_B_FRAMES, EVX_REFERENCE_FRAME_COUNT, EVX_MOTION_SEARCH_RADIUS)."""
+        return OracleContext(self, align16(width), align16(height), b_frames, ref_count, radius)
 
 
 class OracleContext:
-    def __init__(self, orc: Oracle, aw: int, ah: int):
+    def __init__(self, orc: Oracle, aw: int, ah: int, b_frames: int = 1, ref_count: int = 4, radius: int = 16):
         self.orc, self.aw, self.ah = orc, aw, ah
         self.h = orc.lib.orc_create(aw, ah)
+        if orc.lib.orc_set_config(self.h, b_frames, ref_count, radius):
+            raise ValueError(f"unsupported oracle configuration b_frames={b_frames} ref_count={ref_count} radius={radius}")
 
     def __del__(self):
         if getattr(self, "h", None):

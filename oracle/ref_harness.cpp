@@ -40,9 +40,49 @@ evx_status encode_slice(const evx_frame &frame, evx_context *context);
 evx_status encode_slice_wpp(const evx_frame &frame, evx_context *context);
 }
 
+/*
+ * Every table crosses this harness in the layouts of the default build
+ * (evx_block_desc 28 B, evx_frame 18 B, pack(2)).  The I/P variants
+ * (EVX_ENABLE_B_FRAMES 0, see oracle/variants/) drop the B-frame fields at
+ * the end of both structs (common.h:75-81, :105-113): their descriptor is the
+ * first 18 bytes of the wide one and their frame the first 10, so the harness
+ * converts by truncation and zero extension.
+ */
+static const size_t WIDE_BLOCK = 28, WIDE_FRAME = 18;
+#if EVX_ENABLE_B_FRAMES
 static_assert(sizeof(evx_block_desc) == 28, "block desc wire size");
-static_assert(sizeof(evx_sao_info) == 16, "sao info wire size");
 static_assert(sizeof(evx_frame) == 18, "frame header wire size");
+#else
+static_assert(sizeof(evx_block_desc) == 18, "block desc wire size (no B frames)");
+static_assert(sizeof(evx_frame) == 10, "frame header wire size (no B frames)");
+#endif
+static_assert(sizeof(evx_sao_info) == 16, "sao info wire size");
+
+static evx_frame frame_from_wide(const uint8_t *wide)
+{
+    evx_frame f;
+    memcpy(&f, wide, sizeof(evx_frame));   /* the native struct is a prefix of the wide one */
+    return f;
+}
+static uint32_t dest_slot(const evx_frame &f)
+{
+#if EVX_ENABLE_B_FRAMES
+    return f.dpb_slot;
+#else
+    return query_prediction_index_by_offset(f, 0);   /* encode.cpp:952-956 */
+#endif
+}
+static void blocks_to_wide(const evx_block_desc *t, uint32_t n, uint8_t *wide)
+{
+    for (uint32_t i = 0; i < n; i++) {
+        memset(wide + i * WIDE_BLOCK, 0, WIDE_BLOCK);
+        memcpy(wide + i * WIDE_BLOCK, t + i, sizeof(evx_block_desc));
+    }
+}
+static void blocks_from_wide(const uint8_t *wide, uint32_t n, evx_block_desc *t)
+{
+    for (uint32_t i = 0; i < n; i++) memcpy(t + i, wide + i * WIDE_BLOCK, sizeof(evx_block_desc));
+}
 
 extern "C" {
 
@@ -91,7 +131,11 @@ int evxref_enc_flush(void *p, uint8_t *out, uint32_t cap, uint32_t *out_len)
 {
     evxref_enc *e = (evxref_enc *)p;
     e->out.empty();
+#if EVX_ENABLE_B_FRAMES
     evx_status s = e->enc->flush(&e->out);
+#else
+    evx_status s = EVX_SUCCESS;   /* no reorder buffer, nothing pending (evx3.h:92-95) */
+#endif
     uint32_t n = e->out.query_byte_occupancy();
     *out_len = n;
     if (s != EVX_SUCCESS) return s;
@@ -144,8 +188,12 @@ static void load_set(image_set *s, const int16_t *src, uint32_t w, uint32_t h)
 
 /*
  * Plane-set buffers are laid out Y (w*h) then U then V ((w/2)*(h/2) each), int16.
- * Any dump pointer may be NULL.  frame18 is the 18-byte packed evx_frame.
- * use_wpp selects encode_slice_wpp (the stock schedule) instead of encode_slice.
+ * Any dump pointer may be NULL.  frame18 is the 18-byte packed evx_frame of the
+ * default build (variants read its prefix); dump_blocks receives 28-byte
+ * descriptors.  use_wpp selects encode_slice_wpp (the stock schedule) instead
+ * of encode_slice where the build has it.  The destination slot is the
+ * frame's dpb_slot, or, without B frames, the one its index selects
+ * (query_prediction_index_by_offset(frame, 0), common.cpp:256-259).
  */
 int evxref_ctx_encode_frame(void *p, const uint8_t *rgb, uint32_t w, uint32_t h,
                             const uint8_t *frame18, int use_wpp,
@@ -155,8 +203,7 @@ int evxref_ctx_encode_frame(void *p, const uint8_t *rgb, uint32_t w, uint32_t h,
                             uint8_t *bytes, uint32_t cap, uint32_t *nbytes)
 {
     evxref_ctx *c = (evxref_ctx *)p;
-    evx_frame frame;
-    memcpy(&frame, frame18, sizeof(evx_frame));
+    evx_frame frame = frame_from_wide(frame18);
     uint32_t nblk = c->ctx.width_in_blocks * c->ctx.height_in_blocks;
 
     image input;
@@ -164,10 +211,15 @@ int evxref_ctx_encode_frame(void *p, const uint8_t *rgb, uint32_t w, uint32_t h,
     if (convert_image(input, &c->ctx.cache_bank.input_cache) != EVX_SUCCESS) return 101;
     copy_set(c->ctx.cache_bank.input_cache, dump_src, c->w, c->h);
 
+#if EVX_ENABLE_WPP
     evx_status s = use_wpp ? encode_slice_wpp(frame, &c->ctx) : encode_slice(frame, &c->ctx);
+#else
+    (void)use_wpp;
+    evx_status s = encode_slice(frame, &c->ctx);
+#endif
     if (s != EVX_SUCCESS) return 102;
-    image_set &dest = c->ctx.cache_bank.prediction_cache[frame.dpb_slot];
-    if (dump_blocks) memcpy(dump_blocks, c->ctx.block_table, (size_t)nblk * 28);
+    image_set &dest = c->ctx.cache_bank.prediction_cache[dest_slot(frame)];
+    if (dump_blocks) blocks_to_wide(c->ctx.block_table, nblk, dump_blocks);
     copy_set(c->ctx.cache_bank.output_cache, dump_levels, c->w, c->h);
     copy_set(dest, dump_recon, c->w, c->h);
 
@@ -189,7 +241,9 @@ int evxref_ctx_encode_frame(void *p, const uint8_t *rgb, uint32_t w, uint32_t h,
         memcpy(bytes, c->stream.query_data(), n);
     }
 
-    if (frame.type != EVX_FRAME_BIDIR)
+#if EVX_ENABLE_B_FRAMES
+    if (frame.type != EVX_FRAME_BIDIR)   /* encode.cpp:990-998 */
+#endif
         memcpy(c->ctx.prev_block_table, c->ctx.block_table, (size_t)nblk * sizeof(evx_block_desc));
     return 0;
 }
@@ -205,11 +259,10 @@ int evxref_ctx_serialize(void *p, const uint8_t *frame18, const uint8_t *blocks,
                          const int16_t *levels, uint8_t *bytes, uint32_t cap, uint32_t *nbytes)
 {
     evxref_ctx *c = (evxref_ctx *)p;
-    evx_frame frame;
-    memcpy(&frame, frame18, sizeof(evx_frame));
+    evx_frame frame = frame_from_wide(frame18);
     uint32_t nblk = c->ctx.width_in_blocks * c->ctx.height_in_blocks;
-    memcpy(c->ctx.block_table, blocks, (size_t)nblk * 28);
-    memcpy(c->ctx.prev_block_table, prev_blocks, (size_t)nblk * 28);
+    blocks_from_wide(blocks, nblk, c->ctx.block_table);
+    blocks_from_wide(prev_blocks, nblk, c->ctx.prev_block_table);
     memcpy(c->ctx.sao_table, sao, (size_t)nblk * 16);
     load_set(&c->ctx.cache_bank.output_cache, levels, c->w, c->h);
     c->stream.empty();
@@ -231,6 +284,18 @@ int evxref_ctx_get_slot(void *p, uint32_t slot, int16_t *out)
 }
 
 float evxref_lambda(uint16_t q) { return compute_lambda(q); }
+
+/* The compile-time configuration of this build: B frames on/off
+ * (EVX_ENABLE_B_FRAMES), DPB slots (EVX_REFERENCE_FRAME_COUNT), WPP threads
+ * on/off (EVX_ENABLE_WPP) and the native sizes of evx_frame / evx_block_desc. */
+void evxref_config(int *b_frames, int *ref_count, int *wpp, int *frame_bytes, int *block_bytes)
+{
+    *b_frames = EVX_ENABLE_B_FRAMES;
+    *ref_count = EVX_REFERENCE_FRAME_COUNT;
+    *wpp = EVX_ENABLE_WPP;
+    *frame_bytes = (int)sizeof(evx_frame);
+    *block_bytes = (int)sizeof(evx_block_desc);
+}
 
 uint32_t evxref_sizeof_block_desc(void) { return sizeof(evx_block_desc); }
 

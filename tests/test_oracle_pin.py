@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from chicago_b200.synth import generate
-from oracle_py import compare_blocks, plan_gop, split_stream, unpack_frame
+from oracle_py import REF_VARIANTS, Ref, compare_blocks, join_ip_stream, plan_gop, plan_ip, split_stream, unpack_frame
 
 CASES = [  # (w, h, frames, quality, vmax, intra_at)
     (64, 48, 6, 8, 6.0, ()),
@@ -43,3 +43,58 @@ def test_wpp_schedule_equals_raster(ref):
         da, sa = a.encode_frame(frames[ti], f18, wpp=False)
         db, sb = b.encode_frame(frames[ti], f18, wpp=True)
         assert sa == sb and np.array_equal(da.final, db.final)
+
+
+IP_CASES = [  # (variant, w, h, frames, quality, vmax, intra_at); the last two ip3 cases must use all three references
+    ("ip1", 64, 48, 6, 8, 6.0, ()),
+    ("ip1", 100, 60, 8, 16, 14.0, (5,)),
+    ("ip3", 64, 48, 7, 8, 6.0, ()),
+    ("ip3", 96, 64, 9, 1, 20.0, (6,)),
+    ("ip3", 48, 32, 6, 31, 3.0, ()),
+    ("ip3", 176, 144, 6, 4, 8.0, ()),
+    ("ip3", 176, 144, 8, 8, 3.0, (7,)),
+]
+COVER = {("ip3", 176, 144)}
+
+
+def variant_ref(variant):
+    if not __import__("os").path.exists(REF_VARIANTS[variant][0]):
+        pytest.skip(f"reference variant {variant} not built (make -C oracle variants)")
+    return Ref(variant=variant)
+
+
+@pytest.mark.parametrize("variant,w,h,T,q,vmax,intra_at", IP_CASES)
+def test_oracle_matches_reference_ip_variants(oracle, variant, w, h, T, q, vmax, intra_at):
+    """The I/P builds (EVX_ENABLE_B_FRAMES 0; one or three references): the
+    planner-driven staged reference reproduces the stock stream, and the
+    restatement with the same switches matches it at every stage."""
+    ref = variant_ref(variant)
+    _, b_frames, ref_count = REF_VARIANTS[variant]
+    assert (ref.b_frames, ref.ref_count, ref.frame_bytes, ref.block_bytes) == (0, ref_count, 10, 18)
+    frames = generate(w, h, T, seed=w * 5 + h + ref_count, vmax=vmax)
+    stock = ref.encode_stream(frames, quality=q, intra_at=intra_at)
+    plan = plan_ip(T, quality=q, intra_at=intra_at, ref_count=ref_count)
+    rc, oc = ref.context(w, h), oracle.context(w, h, b_frames=0, ref_count=ref_count)
+    staged = []
+    targets = set()
+    for k, (ti, f18) in enumerate(plan):
+        d, sl = rc.encode_frame(frames[ti], f18)
+        staged.append((f18, sl))
+        od = oc.encode_frame(frames[ti], f18)
+        assert not compare_blocks(d.blocks, od.blocks), f"block table differs at frame {k} {unpack_frame(f18)}"
+        for nm in ("src", "levels", "recon", "deblock", "sao", "final"):
+            assert np.array_equal(getattr(d, nm), getattr(od, nm)), f"{nm} differs at frame {k}"
+        bt = d.block_table()
+        targets |= set(bt["prediction_target"][(bt["block_type"] & 1) == 0].tolist())
+    assert join_ip_stream(stock[:14], staged) == stock, "staged reference != stock I/P encoder"
+    if (variant, w, h) in COVER:
+        assert targets == {1, 2, 3}, f"expected blocks predicted from all three references, saw {targets}"
+
+
+def test_sequential_build_equals_wpp_build(ref):
+    """The single-thread reference build (EVX_ENABLE_WPP 0) encodes the same
+    stream as the default WPP build."""
+    seq = variant_ref("seq")
+    assert seq.wpp == 0 and ref.wpp == 1
+    frames = generate(96, 64, 6, seed=3, vmax=8.0)
+    assert seq.encode_stream(frames, quality=8) == ref.encode_stream(frames, quality=8)
