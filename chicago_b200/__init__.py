@@ -10,6 +10,10 @@ importing this package without it raises: there is no CPU fallback.
 * :class:`Encoder` -- the reference's evx3_encoder (src/video/evx3.h:67-100:
   set_quality / insert_intra / encode / flush / clear) with its GOP logic,
   emitting one record per encoded frame in bitstream order.
+* :class:`Config` -- the reference build a stream reproduces (EVX_ENABLE_B_FRAMES,
+  EVX_REFERENCE_FRAME_COUNT, EVX_MOTION_SEARCH_RADIUS); ``CONFIGS`` names the
+  supported ones: "default" (hierarchical P/B GOP), "ip1" / "ip3" (I/P GOP with
+  one / three references).
 """
 from __future__ import annotations
 
@@ -49,8 +53,28 @@ EXPORTS = [
     "evxg_batch_autotune",
     "evxg_server_create", "evxg_server_destroy", "evxg_server_open", "evxg_server_submit", "evxg_server_insert_intra",
     "evxg_server_close", "evxg_server_drain", "evxg_server_stats", "evxg_server_now_ns",
+    "evxg_config_default", "evxg_stream_create_config", "evxg_stream_config", "evxg_encoder_create_config",
+    "evxg_server_open_config",
 ]
 MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
+
+
+class Config(C.Structure):
+    """evxg_config: the compile-time switches of the reference build a stream
+    reproduces (include/evxg.h)."""
+    _fields_ = [("b_frames", C.c_uint8), ("ref_count", C.c_uint8), ("search_radius", C.c_uint8),
+                ("reserved", C.c_uint8)]
+
+
+CONFIGS = {"default": (1, 4, 16), "ip1": (0, 2, 16), "ip3": (0, 4, 16)}
+
+
+def config(name_or_tuple="default") -> Config:
+    """A Config from a name in CONFIGS or a (b_frames, ref_count, search_radius) tuple."""
+    if isinstance(name_or_tuple, Config):
+        return name_or_tuple
+    v = CONFIGS[name_or_tuple] if isinstance(name_or_tuple, str) else tuple(name_or_tuple)
+    return Config(v[0], v[1], v[2], 0)
 
 FRAME_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
 
@@ -75,6 +99,10 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L = C.CDLL(path)
     vp, u32, i32 = C.c_void_p, C.c_uint32, C.c_int
     L.evxg_stream_create.argtypes = [u32, u32, C.POINTER(vp)]
+    L.evxg_stream_create_config.argtypes = [u32, u32, C.POINTER(Config), C.POINTER(vp)]
+    L.evxg_stream_config.argtypes = [vp, C.POINTER(Config)]
+    L.evxg_config_default.argtypes = [C.POINTER(Config)]
+    L.evxg_config_default.restype = None
     L.evxg_stream_destroy.argtypes = [vp]
     L.evxg_stream_dims.argtypes = [vp] + [C.POINTER(u32)] * 4
     L.evxg_encode_frame.argtypes = [vp, vp, i32, C.c_char_p, vp]
@@ -89,6 +117,7 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_lambda.restype = C.c_float
     L.evxg_last_error.restype = C.c_char_p
     L.evxg_encoder_create.argtypes = [FRAME_CB, vp, C.POINTER(vp)]
+    L.evxg_encoder_create_config.argtypes = [FRAME_CB, vp, C.POINTER(Config), C.POINTER(vp)]
     for n in ("evxg_encoder_destroy", "evxg_encoder_clear", "evxg_encoder_insert_intra", "evxg_encoder_flush"):
         getattr(L, n).argtypes = [vp]
     L.evxg_encoder_set_quality.argtypes = [vp, C.c_uint8]
@@ -114,6 +143,7 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_server_create.argtypes = [u64, u32, RESULT_CB, vp, C.POINTER(vp)]
     L.evxg_server_destroy.argtypes = [vp]
     L.evxg_server_open.argtypes = [vp, u32, u32, C.c_uint8, C.POINTER(u32)]
+    L.evxg_server_open_config.argtypes = [vp, u32, u32, C.c_uint8, C.POINTER(Config), C.POINTER(u32)]
     L.evxg_server_submit.argtypes = [vp, u32, vp, u64]
     L.evxg_server_insert_intra.argtypes = [vp, u32]
     L.evxg_server_close.argtypes = [vp, u32]
@@ -158,12 +188,14 @@ def pack_frame(ftype, index, quality, display_order, is_reference, dpb_slot, ref
 
 
 class Stream:
-    """One device encoding context (evx_context on the GPU)."""
+    """One device encoding context (evx_context on the GPU) of the reference
+    build ``cfg`` names (see :func:`config`)."""
 
-    def __init__(self, width: int, height: int):
+    def __init__(self, width: int, height: int, cfg="default"):
         self.width, self.height = int(width), int(height)
+        self.cfg = config(cfg)
         h = C.c_void_p()
-        _check(lib().evxg_stream_create(self.width, self.height, C.byref(h)))
+        _check(lib().evxg_stream_create_config(self.width, self.height, C.byref(self.cfg), C.byref(h)))
         self.h = h
         d = [C.c_uint32() for _ in range(4)]
         _check(lib().evxg_stream_dims(self.h, *[C.byref(x) for x in d]))
@@ -333,10 +365,11 @@ class Server:
         with self._lock:
             self.results.setdefault(sid, []).append(rec)
 
-    def open(self, width: int, height: int, quality: int = 8) -> int:
+    def open(self, width: int, height: int, quality: int = 8, cfg="default") -> int:
         sid = C.c_uint32()
         aw, ah = (width + 15) & ~15, (height + 15) & ~15
-        _check(lib().evxg_server_open(self.h, width, height, quality, C.byref(sid)))
+        c = config(cfg)
+        _check(lib().evxg_server_open_config(self.h, width, height, quality, C.byref(c), C.byref(sid)))
         self.dims[sid.value] = ((aw // 16) * (ah // 16), aw * ah + 2 * (aw // 2) * (ah // 2))
         self.results.setdefault(sid.value, [])
         return sid.value
@@ -378,11 +411,12 @@ class Server:
 class Encoder:
     """evx3_encoder mirror: frames in, per-frame table records out (bitstream order)."""
 
-    def __init__(self, quality: int | None = None):
+    def __init__(self, quality: int | None = None, cfg="default"):
         self.records = []
+        self.cfg = config(cfg)
         self._cb = FRAME_CB(self._on_frame)
         h = C.c_void_p()
-        _check(lib().evxg_encoder_create(self._cb, None, C.byref(h)))
+        _check(lib().evxg_encoder_create_config(self._cb, None, C.byref(self.cfg), C.byref(h)))
         self.h = h
         if quality is not None:
             self.set_quality(quality)

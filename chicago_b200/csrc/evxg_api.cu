@@ -35,12 +35,55 @@ float evxg_lambda(uint16_t q) { return 0.85f * powf(2.0f, ((float)q - 12.0f) / 3
 
 const char *evxg_last_error(void) { return g_last_error.c_str(); }
 
+void evxg_config_default(evxg_config *cfg)
+{
+    if (!cfg) return;
+    *cfg = evxg_config{};
+    cfg->b_frames = 1; cfg->ref_count = 4; cfg->search_radius = 16;
+}
+
+static int check_config(const evxg_config *c, const char *who)
+{
+    static thread_local char msg[200];
+    const bool ok = (c->b_frames == 1 && c->ref_count == 4) || (c->b_frames == 0 && (c->ref_count == 2 || c->ref_count == 4));
+    if (!ok) {
+        snprintf(msg, sizeof msg, "%s: unsupported configuration (b_frames %u, ref_count %u): B frames need 4 DPB slots, "
+                 "I/P streams 2 or 4", who, c->b_frames, c->ref_count);
+        return fail(EVXG_ERROR_INVALIDARG, msg);
+    }
+    if (c->search_radius != 16 || c->reserved) {
+        snprintf(msg, sizeof msg, "%s: unsupported search radius %u (16)", who, c->search_radius);
+        return fail(EVXG_ERROR_INVALIDARG, msg);
+    }
+    return EVXG_SUCCESS;
+}
+
 int evxg_stream_create(uint32_t width, uint32_t height, evxg_stream **out)
+{
+    return evxg_stream_create_config(width, height, nullptr, out);
+}
+
+int evxg_stream_config(const evxg_stream *s, evxg_config *out)
+{
+    if (!s || !out) return fail(EVXG_ERROR_INVALIDARG, "evxg_stream_config: null argument");
+    *out = s->cfg;
+    return EVXG_SUCCESS;
+}
+
+int evxg_stream_create_config(uint32_t width, uint32_t height, const evxg_config *cfg, evxg_stream **out)
 {
     if (!out || !width || !height || width > 65535 || height > 65535 || (width & 1) || (height & 1))
         return fail(EVXG_ERROR_INVALIDARG, "evxg_stream_create: width/height must be even and in 2..65534");
     *out = nullptr;
+    evxg_config c;
+    evxg_config_default(&c);
+    if (cfg) {
+        int rc = check_config(cfg, "evxg_stream_create");
+        if (rc) return rc;
+        c = *cfg;
+    }
     evxg_stream *s = new evxg_stream();
+    s->cfg = c;
     s->vw = width; s->vh = height;
     s->W = (width + 15) & ~15u; s->H = (height + 15) & ~15u;
     s->mbw = s->W / 16; s->mbh = s->H / 16;
@@ -179,15 +222,27 @@ int evxg::max_active_clusters()
     return n;
 }
 
-// Frame descriptor checks shared by the single and the batched path.
-int evxg::check_frame(const evxg_frame *f, const char *who)
+// Frame descriptor checks shared by the single and the batched path.  Without
+// B frames the reference's evx_frame has no slot fields: the destination and
+// the references follow from the index (query_prediction_index_by_offset,
+// common.cpp:256-259), and are written into the copy.
+int evxg::check_frame(const evxg_stream *s, const evxg_frame *fin, const char *who, evxg_frame *out)
 {
     static thread_local char msg[160];
     auto bad = [&](int code, const char *what) {
         snprintf(msg, sizeof msg, "%s: %s", who, what);
         return fail(code, msg);
     };
+    evxg_frame g = *fin;
+    const evxg_frame *f = &g;
     if (f->type < EVXG_FRAME_INTRA || f->type > EVXG_FRAME_BIDIR) return bad(EVXG_ERROR_INVALIDARG, "bad frame type");
+    if (!s->cfg.b_frames) {
+        if (f->type == EVXG_FRAME_BIDIR) return bad(EVXG_ERROR_INVALIDARG, "B frame in a stream without B frames");
+        const uint32_t R = s->cfg.ref_count;
+        g.dpb_slot = (uint8_t)(f->index % R);
+        g.ref_slot_fwd = (uint8_t)((f->index + R - 1) % R);
+        g.ref_slot_bwd = 0;
+    }
     if (f->dpb_slot > 3 || f->ref_slot_fwd > 3 || f->ref_slot_bwd > 3)
         return bad(EVXG_ERROR_INVALID_INDEX, "DPB slot out of range");
     if (f->quality < 1 || f->quality > 63) return bad(EVXG_ERROR_INVALIDARG, "quality (QP) must be 1..63");
@@ -195,6 +250,7 @@ int evxg::check_frame(const evxg_frame *f, const char *who)
         return bad(EVXG_ERROR_INVALIDARG, "forward reference equals the destination slot");
     if (f->type == EVXG_FRAME_BIDIR && f->ref_slot_bwd == f->dpb_slot)
         return bad(EVXG_ERROR_INVALIDARG, "backward reference equals the destination slot");
+    if (out) *out = g;
     return EVXG_SUCCESS;
 }
 
@@ -205,6 +261,13 @@ void evxg::fill_args(evxg_stream *s, const evxg_frame *f, const uint8_t *drgb, F
     a.vis_w = (int)s->vw; a.vis_h = (int)s->vh;
     a.type = f->type; a.quality = f->quality; a.dpb = f->dpb_slot;
     a.ref_fwd = f->ref_slot_fwd; a.ref_bwd = f->ref_slot_bwd;
+    if (s->cfg.b_frames) {
+        a.nref = 1; a.ref_slot[0] = f->ref_slot_fwd; a.ip_mode = 0;
+    } else {   // offsets 1 .. ref_count-1 from the index (encode.cpp:211-247); f's slots come from check_frame
+        const uint32_t R = s->cfg.ref_count;
+        a.nref = (int)R - 1; a.ip_mode = 1;
+        for (uint32_t k = 0; k + 1 < R; k++) a.ref_slot[k] = (int)((f->index + R - (k + 1)) % R);
+    }
     a.lambda = evxg_lambda(f->quality);
     for (int i = 0; i < 4; i++) a.planes[i] = s->dpb[i];
     a.src = s->src; a.lev = s->lev; a.bt = s->bt;
@@ -221,11 +284,13 @@ void evxg::fill_args(evxg_stream *s, const evxg_frame *f, const uint8_t *drgb, F
 
 extern "C" {
 
-int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, const evxg_frame *f, void *cuda_stream)
+int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, const evxg_frame *fin, void *cuda_stream)
 {
-    if (!s || !rgb || !f) return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: null argument");
-    int rc = check_frame(f, "evxg_encode_frame");
+    if (!s || !rgb || !fin) return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: null argument");
+    evxg_frame fr;
+    int rc = check_frame(s, fin, "evxg_encode_frame", &fr);
     if (rc) return rc;
+    const evxg_frame *f = &fr;
     cudaStream_t st = (cudaStream_t)cuda_stream;
     const uint8_t *drgb = rgb;
     if (!rgb_on_device) {
@@ -344,10 +409,12 @@ int evxg_fetch_planes(evxg_stream *s, uint32_t slot, int16_t *out, int to_device
 // Mirrors evx3_encoder_impl with EVX_ENABLE_B_FRAMES 1, EVX_B_FRAME_COUNT 3 and
 // EVX_PERIODIC_INTRA_RATE 3600 (config.h:41, :120-121): frame types, display
 // order, DPB slot assignment (common.cpp:256-283) and the hierarchical
-// P / reference-B / B reorder (evx3enc.cpp:279-383).
+// P / reference-B / B reorder (evx3enc.cpp:279-383); or, configured without
+// B frames, its I/P path (evx3enc.cpp:137-160).
 struct evxg_encoder {
     evxg_frame_callback cb = nullptr;
     void *user = nullptr;
+    evxg_config cfg{};
     evxg_stream *stream = nullptr;
     evxg_frame frame{};                 // the running frame state (clear_frame, common.cpp:48-66)
     uint32_t width = 0, height = 0;
@@ -442,9 +509,21 @@ extern "C" {
 
 int evxg_encoder_create(evxg_frame_callback cb, void *user, evxg_encoder **out)
 {
+    return evxg_encoder_create_config(cb, user, nullptr, out);
+}
+
+int evxg_encoder_create_config(evxg_frame_callback cb, void *user, const evxg_config *cfg, evxg_encoder **out)
+{
     if (!out) return EVXG_ERROR_INVALIDARG;
+    evxg_config c;
+    evxg_config_default(&c);
+    if (cfg) {
+        const int rc = check_config(cfg, "evxg_encoder_create_config");
+        if (rc) return rc;
+        c = *cfg;
+    }
     evxg_encoder *e = new evxg_encoder();
-    e->cb = cb; e->user = user;
+    e->cb = cb; e->user = user; e->cfg = c;
     clear_frame(e->frame);
     *out = e;
     return EVXG_SUCCESS;
@@ -495,7 +574,7 @@ int evxg_encoder_encode(evxg_encoder *e, const uint8_t *rgb, uint32_t width, uin
         e->reorder_count = 0; e->display_counter = 0; e->ip_index = 0; e->first = true;
     }
     if (!e->stream && !e->sink) {
-        if ((rc = evxg_stream_create(width, height, &e->stream))) return rc;
+        if ((rc = evxg_stream_create_config(width, height, &e->cfg, &e->stream))) return rc;
         e->width = width; e->height = height;
         const size_t nblk = (size_t)e->stream->mbw * e->stream->mbh;
         e->h_bt.resize(nblk); e->h_prev.resize(nblk); e->h_sao.resize(nblk);
@@ -504,6 +583,20 @@ int evxg_encoder_encode(evxg_encoder *e, const uint8_t *rgb, uint32_t width, uin
     }
     if (width != e->width || height != e->height)
         return fail(EVXG_ERROR_INVALID_RESOURCE, "evxg_encoder_encode: frame size changed within a stream");
+    if (!e->cfg.b_frames) {   // I/P: every frame as it arrives (evx3enc.cpp:137-160)
+        const uint32_t R = e->cfg.ref_count;
+        evxg_frame f = e->frame;
+        f.display_order = e->display_counter++;
+        f.is_reference = 1;
+        f.dpb_slot = (uint8_t)(f.index % R);
+        f.ref_slot_fwd = (uint8_t)((f.index + R - 1) % R);
+        f.ref_slot_bwd = 0;
+        if ((rc = emit(e, rgb, f))) return rc;
+        e->frame.type = EVXG_FRAME_INTER;
+        if ((e->frame.index + 1) % kIntraRate == 0) e->frame.type = EVXG_FRAME_INTRA;   // periodic intra
+        e->frame.index++;
+        return EVXG_SUCCESS;
+    }
     if (e->display_counter > 0 && e->display_counter % kIntraRate == 0) {   // periodic intra
         if (e->reorder_count > 0 && (rc = encode_gop(e))) return rc;
         e->frame.type = EVXG_FRAME_INTRA;

@@ -307,16 +307,17 @@ int evxg_batch_encode(evxg_batch *b, const evxg_frame *frames, uint32_t parity, 
     }
     const size_t n = b->st.size();
     std::vector<char> active(n, 0);
+    std::vector<evxg_frame> fr(n);
     for (size_t i = 0; i < n; i++) {
         if (frames[i].type < 0) continue;   // no frame for this stream in this tick
-        const int rc = check_frame(&frames[i], "evxg_batch_encode");
+        const int rc = check_frame(b->st[i], &frames[i], "evxg_batch_encode", &fr[i]);
         if (rc) return rc;
         active[i] = 1;
     }
     for (size_t i = 0; i < n; i++) {
         FrameArgs &a = sd.args[i];
         if (active[i]) {
-            fill_args(b->st[i], &frames[i], b->st[i]->rgb, a);
+            fill_args(b->st[i], &fr[i], b->st[i]->rgb, a);
         } else {
             a = FrameArgs{};
             a.active = 0;
@@ -361,8 +362,8 @@ int evxg_batch_get_shape(const evxg_batch *b, int *form, int *grid, int *policy)
 }
 
 // Autotuner: times each candidate shape of the macroblock pass on a short
-// synthetic sequence (an I, a P and two B frames per stream, at the streams'
-// own sizes), keeps the fastest and returns every stream to its initial
+// synthetic sequence (an I, a P and two B frames per stream -- I/P streams: an
+// I and three P frames -- at the streams' own sizes), keeps the fastest and returns every stream to its initial
 // state.  Candidates: one CTA per row or three-CTA clusters, the persistent
 // grid at full and at two-thirds width, and both queue orders.
 int evxg_batch_autotune(evxg_batch *b, void *cuda_stream, float *best_ms)
@@ -404,7 +405,9 @@ int evxg_batch_autotune(evxg_batch *b, void *cuda_stream, float *best_ms)
             const uint32_t par = (uint32_t)(t & 1);
             for (size_t i = 0; i < n; i++) {
                 fr[i] = evxg_frame{};
-                fr[i].type = types[t]; fr[i].index = (uint32_t)t; fr[i].quality = 8; fr[i].display_order = (uint32_t)t;
+                // I/P streams: I then P frames (their slots follow from the index)
+                fr[i].type = b->st[i]->cfg.b_frames ? types[t] : (t ? EVXG_FRAME_INTER : EVXG_FRAME_INTRA);
+                fr[i].index = (uint32_t)t; fr[i].quality = 8; fr[i].display_order = (uint32_t)t;
                 fr[i].is_reference = t < 3; fr[i].dpb_slot = (uint8_t)dpb[t];
                 fr[i].ref_slot_fwd = (uint8_t)fwd[t]; fr[i].ref_slot_bwd = (uint8_t)bwd[t];
             }

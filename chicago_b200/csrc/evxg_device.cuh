@@ -93,6 +93,12 @@ struct FrameArgs {
     int W, H, mbw, mbh;          // aligned context size and MB grid
     int vis_w, vis_h;            // visible RGB size
     int type, quality, dpb, ref_fwd, ref_bwd;
+    // P frames: the references searched, nearest first.  With B frames one,
+    // the frame's forward slot; without them (EVX_ENABLE_B_FRAMES 0) the slots
+    // at offsets 1 .. EVX_REFERENCE_FRAME_COUNT-1 from the frame index
+    // (encode.cpp:211-247), whose descriptors name the offset and which pay a
+    // distance bias (ip_mode).
+    int nref, ref_slot[3], ip_mode;
     float lambda;
     int16_t *planes[4];          // DPB plane sets
     int16_t *src;                // converted source plane set

@@ -45,7 +45,10 @@ constexpr int kSaoPasses = 8;
 
 int fail(int code, const char *what);
 int cuda_fail(cudaError_t e, const char *where);
-int check_frame(const evxg_frame *f, const char *who);
+// Checks a frame descriptor against the stream's configuration and, for
+// streams without B frames, derives its DPB slots from the index (out may be
+// the same as f).
+int check_frame(const evxg_stream *s, const evxg_frame *f, const char *who, evxg_frame *out);
 int max_active_clusters();
 }  // namespace evxg
 
@@ -72,6 +75,7 @@ struct evxg_stream {
     int mb_form, mb_clusters;           // macroblock pass shape; clusters launched in the cluster form
     uint32_t launches;
     long long timeout_ns;
+    evxg_config cfg;                    // reference build configuration the stream reproduces
     bool profile;
     cudaEvent_t ev[7];
 };

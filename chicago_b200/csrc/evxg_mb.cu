@@ -21,8 +21,10 @@
 // sets the device error word.
 //
 // Inside an MB, three groups of four warps run the independent work at the
-// same time: the intra block-copy search, the forward (P: the only) inter
-// search, and the backward search (B) or the intra RDO candidates (P).  In a
+// same time: the intra block-copy search, the forward (P: the nearest
+// reference's) inter search, and the backward search (B), the second
+// reference's search (P frames of an I/P stream with several references) or
+// the intra RDO candidates (P).  In a
 // search step every warp evaluates candidates of the 3x3 pattern (16 lanes do
 // 4x4 luma Hadamard/SAD/MAD, 16 lanes chroma MAD) and the group leader
 // replays the reference's order-dependent acceptance rule; sub-pel refinement
@@ -135,9 +137,11 @@ struct Srch {
 // leader for one MB, and the sequence flags the CTAs exchange.  Every field
 // of Mail is written by exactly one other CTA of the cluster.
 struct alignas(16) Inbox {
-    int16_t f_pred[MB_N], b_pred[MB_N], d_pred[MB_N];   // forward, backward, best directional prediction
-    Desc f_out, b_out, cd[4];
-    int f_sad, b_sad, dir_best, dir_sad, modes[3];
+    // forward (P: nearest reference), backward (P: second reference), third
+    // reference (P), best directional prediction
+    int16_t f_pred[MB_N], b_pred[MB_N], x_pred[MB_N], d_pred[MB_N];
+    Desc f_out, b_out, x_out, cd[4];
+    int f_sad, b_sad, x_sad, dir_best, dir_sad, modes[3];
     float cost[4];             // P: RD costs of the intra candidates cd[0..3]
 };
 struct Mail {
@@ -164,6 +168,8 @@ struct MbShared {
     int w0_early;              // cluster leader: window 0 shifts before the wavefront wait
     int modes[3], dsad[3], dir_best, dir_sad;
     int bi_sad, part[NW], dpart[3][NW];
+    Desc rout[3];              // P: each reference's search result (nearest first), its SAD and prediction index
+    int rsad[3], rpred[3];
     unsigned aq[MAXC][4][3];   // adaptive QP: per candidate and luma block, sum / sum of squares / count
     int cpred[MAXC], win_k, need_encode, chosen, rdo;
     WinReq req;
@@ -1506,11 +1512,18 @@ __device__ __noinline__ void decide(const FrameArgs &a)
     evxg_block_desc best = S.srch[0].out.d;
     int bsad = S.srch[0].out_sad, bpred = (best.block_type & BT_MOTION) ? 0 : -1;
     if (a.type == EVXG_FRAME_INTER) {
-        evxg_block_desc in = S.srch[1].out.d;
-        in.prediction_target = (uint8_t)a.ref_fwd;
-        const bool ci = in.block_type & BT_COPY, cb = best.block_type & BT_COPY;
-        if (ci != cb) { if (ci) { best = in; bsad = S.srch[1].out_sad; bpred = 1; } }
-        else if (S.srch[1].out_sad < bsad) { best = in; bsad = S.srch[1].out_sad; bpred = 1; }
+        // Each reference in turn, nearest first: a copy block wins over a
+        // non-copy one either way, else the smaller SAD -- without B frames
+        // after a distance bias (int)(lambda * 2 * offset) on the farther
+        // references, and the descriptor names the offset (encode.cpp:182-247).
+        for (int k = 0; k < a.nref; k++) {
+            evxg_block_desc in = S.rout[k].d;
+            in.prediction_target = (uint8_t)(a.ip_mode ? k + 1 : a.ref_fwd);
+            const int bias = a.ip_mode ? __float2int_rz(__fmul_rn(a.lambda, __int2float_rn(2 * (k + 1)))) : 0;
+            const bool ci = in.block_type & BT_COPY, cb = best.block_type & BT_COPY;
+            if (ci != cb) { if (ci) { best = in; bsad = S.rsad[k]; bpred = S.rpred[k]; } }
+            else if (S.rsad[k] + bias < bsad) { best = in; bsad = S.rsad[k]; bpred = S.rpred[k]; }
+        }
     } else if (a.type == EVXG_FRAME_BIDIR) {
         evxg_block_desc f = S.srch[1].out.d, b = S.srch[2].out.d;
         f.prediction_mode = 0; f.prediction_target = (uint8_t)a.ref_fwd;
@@ -1643,12 +1656,14 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
         setup_mb(a, idx, px, py, a.type != EVXG_FRAME_INTRA, nullptr);
         req_window0(a, px, py);   // intra window: the slot being reconstructed
         if (a.type != EVXG_FRAME_INTRA) {
-            req_window(1, a.planes[a.ref_fwd], px, py);
-            if (S.sep) req_window(2, a.planes[a.ref_fwd], S.qx, S.qy);
+            const int16_t *r1 = a.planes[a.type == EVXG_FRAME_INTER ? a.ref_slot[0] : a.ref_fwd];
+            req_window(1, r1, px, py);
+            if (S.sep) req_window(2, r1, S.qx, S.qy);
         }
-        if (a.type == EVXG_FRAME_BIDIR) {
-            req_window(3, a.planes[a.ref_bwd], px, py);
-            if (S.sep) req_window(4, a.planes[a.ref_bwd], S.qx, S.qy);
+        if (a.type == EVXG_FRAME_BIDIR || (a.type == EVXG_FRAME_INTER && a.nref >= 2)) {
+            const int16_t *r2 = a.planes[a.type == EVXG_FRAME_BIDIR ? a.ref_bwd : a.ref_slot[1]];
+            req_window(3, r2, px, py);
+            if (S.sep) req_window(4, r2, S.qx, S.qy);
         }
     }
     __syncthreads();
@@ -1665,17 +1680,21 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
                    [&](int p, int k) { return at(p, cy(p) + k, cx(p) - 1); }, [&](int p) { return at(p, cy(p) - 1, cx(p) - 1); });
     }
 
-    // Independent work runs concurrently on three warp groups.
+    // Independent work runs concurrently on three warp groups.  P frames
+    // with several references (no B frames) search the second one where B
+    // frames search backwards, and the third one afterwards on the whole CTA
+    // in the first reference's windows.
+    const bool multi = a.type == EVXG_FRAME_INTER && a.nref >= 2;
     const int gi = tid / GT;
     const Grp g = group(gi);
     if (gi == 0) {
         intra_bc_search(g, a, px, py, false);
-        if (a.type == EVXG_FRAME_BIDIR) directional_intra(g);
+        if (a.type == EVXG_FRAME_BIDIR || multi) directional_intra(g);
     } else if (gi == 1) {
         if (a.type == EVXG_FRAME_INTRA) directional_intra(g);
         else inter_search(g, a, 1, 1, 2, px, py, S.pred[1], false);
     } else {
-        if (a.type == EVXG_FRAME_BIDIR) {
+        if (a.type == EVXG_FRAME_BIDIR || multi) {
             inter_search(g, a, 2, 3, 4, px, py, S.pred[2], false);
         } else if (a.type == EVXG_FRAME_INTER) {
             // The intra RDO candidates do not depend on the searches
@@ -1689,10 +1708,29 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
         }
     }
     __syncthreads();
+    if (a.type == EVXG_FRAME_INTER && tid == 0) {
+        for (int k = 0; k < 2 && k < a.nref; k++) { S.rout[k] = S.srch[1 + k].out; S.rsad[k] = S.srch[1 + k].out_sad; S.rpred[k] = 1 + k; }
+        if (a.nref >= 3) {   // the third reference: windows 1 / 2 again, prediction into pred[3]
+            S.req.n = 0; S.req.fy0 = S.req.fy1 = S.req.fcy0 = S.req.fcy1 = 0; S.req.staged = 0;
+            req_window(1, a.planes[a.ref_slot[2]], px, py);
+            if (S.sep) req_window(2, a.planes[a.ref_slot[2]], S.qx, S.qy);
+        }
+    }
+    if (a.type == EVXG_FRAME_INTER && a.nref >= 3) {
+        __syncthreads();
+        load_windows(a.W, a.H);
+        __syncthreads();
+        inter_search(G_ALL, a, 1, 1, 2, px, py, S.pred[3], false);
+        if (tid == 0) { S.rout[2] = S.srch[1].out; S.rsad[2] = S.srch[1].out_sad; S.rpred[2] = 3; }
+    }
     if (a.type == EVXG_FRAME_BIDIR) bi_prediction();
-    if (tid == 0) decide(a);
+    if (tid == 0) {
+        if (multi) intra_candidates();
+        decide(a);
+    }
     __syncthreads();
-    if (a.type == EVXG_FRAME_INTER) encode_candidates(G_ALL, a, 2, S.need_encode ? 3 : 2);
+    if (multi) encode_candidates(G_ALL, a, 0, S.need_encode ? 5 : 4);
+    else if (a.type == EVXG_FRAME_INTER) encode_candidates(G_ALL, a, 2, S.need_encode ? 3 : 2);
     else if (S.need_encode) encode_candidates(G_ALL, a, 4, 1);
     if (tid == 0) {
         rdo_choose();
@@ -2018,8 +2056,14 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
     const Inbox &in = S.mail.in[n & 1];
     if (tid == 0) {   // the predictions are read where the ranks left them
         S.predp[1] = in.f_pred; S.predp[2] = in.b_pred; S.predp[4 + in.dir_best] = in.d_pred;
+        S.predp[3] = a.type == EVXG_FRAME_INTER ? in.x_pred : S.pred[3];   // third reference, or the bi-prediction
         S.srch[1].out = in.f_out; S.srch[1].out_sad = in.f_sad;
         S.srch[2].out = in.b_out; S.srch[2].out_sad = in.b_sad;
+        if (a.type == EVXG_FRAME_INTER) {
+            S.rout[0] = in.f_out; S.rsad[0] = in.f_sad; S.rpred[0] = 1;
+            S.rout[1] = in.b_out; S.rsad[1] = in.b_sad; S.rpred[1] = 2;
+            S.rout[2] = in.x_out; S.rsad[2] = in.x_sad; S.rpred[2] = 3;
+        }
         S.dir_best = in.dir_best; S.dir_sad = in.dir_sad;
         for (int m = 0; m < 3; m++) S.modes[m] = in.modes[m];
         if (a.type == EVXG_FRAME_INTER)
@@ -2054,19 +2098,21 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
     return true;
 }
 
-// Ranks 1 and 2: the forward or backward inter search of the n-th MB, handed
-// to the leader's inbox (the caller releases the sequence flag).  What does
-// not depend on the left neighbour's decision -- the source, the predictor's
-// other inputs (row r-1 has finished column c+1), the window around the MB
-// and its metrics -- comes before the wait for the leader's decision of the
-// previous MB.
-__device__ bool search_mb(const FrameArgs &a, int row, int col, int n, bool bwd)
+// Ranks 1 and 2: one or two inter searches of the n-th MB, handed to the
+// leader's inbox (the caller releases the sequence flag).  Search k runs in
+// srch[1 + k] over windows 1 + 2k (at the MB) and 2 + 2k (at the predictor)
+// of reference plane set ref[k] and goes to the inbox's result slot out[k]
+// (0 forward, 1 backward, 2 third reference); two searches run side by side
+// on two six-warp groups.  What does not depend on the left neighbour's
+// decision -- the source, the predictor's other inputs (row r-1 has finished
+// column c+1), the windows around the MB and their metrics -- comes before
+// the wait for the leader's decision of the previous MB.
+__device__ bool search_mb(const FrameArgs &a, int row, int col, int n, int ns, const int16_t *const ref[2],
+                          const int out[2])
 {
     MbShared &S = SM();
     const int tid = threadIdx.x;
     const int px = col * 16, py = row * 16, idx = row * a.mbw + col;
-    const int si = bwd ? 2 : 1, wa = bwd ? 3 : 1;
-    const int16_t *ref = a.planes[bwd ? a.ref_bwd : a.ref_fwd];
     if (tid == 0) S.row_abort = row > 0 && !wait_progress(a, row - 1, min(col + 1, a.mbw - 1));
     __syncthreads();
     if (S.row_abort) return false;
@@ -2074,18 +2120,21 @@ __device__ bool search_mb(const FrameArgs &a, int row, int col, int n, bool bwd)
     if (tid == 0) {
         setup_mb(a, idx, px, py, false, nullptr);
         pred_gather(a, idx, a.type == EVXG_FRAME_INTER, S.pin);
-        req_window(wa, ref, px, py);
+        for (int k = 0; k < ns; k++) req_window(1 + 2 * k, ref[k], px, py);
     }
     __syncthreads();
     load_windows(a.W, a.H);
     __syncthreads();
-    first_candidates(G_ALL, a, si, wa, wa + 1, px, py, true, false);
+    const int k = ns == 2 && tid >= NT / 2 ? 1 : 0;   // this thread's search
+    const Grp g = ns == 2 ? Grp{5 + k, k * (NT / 2), NT / 2} : G_ALL;
+    first_candidates(g, a, 1 + k, 1 + 2 * k, 2 + 2 * k, px, py, true, false);
     if (tid == 0) {
         S.row_abort = !wait_mail(&S.mail.dec_seq, n - 1, a);
         if (!S.row_abort) {
             set_predictor(a, idx, px, py, S.pin, col > 0 ? &S.mail.left.d : nullptr);
             S.req.n = 0;
-            if (S.sep) req_window(wa + 1, ref, S.qx, S.qy);
+            if (S.sep)
+                for (int j = 0; j < ns; j++) req_window(2 + 2 * j, ref[j], S.qx, S.qy);
         }
     }
     __syncthreads();
@@ -2094,20 +2143,32 @@ __device__ bool search_mb(const FrameArgs &a, int row, int col, int n, bool bwd)
         load_windows(a.W, a.H);
         __syncthreads();
     }
-    inter_search(G_ALL, a, si, wa, wa + 1, px, py, S.pred[si], true);
+    inter_search(g, a, 1 + k, 1 + 2 * k, 2 + 2 * k, px, py, S.pred[1 + k], true);
+    __syncthreads();
     Inbox *in = peer(&S.mail.in[n & 1], 0);
-    copy_block(bwd ? in->b_pred : in->f_pred, S.pred[si]);
-    if (tid == 0) {
-        if (bwd) { in->b_out = S.srch[si].out; in->b_sad = S.srch[si].out_sad; }
-        else { in->f_out = S.srch[si].out; in->f_sad = S.srch[si].out_sad; }
+    for (int j = 0; j < ns; j++) {
+        int16_t *to = out[j] == 0 ? in->f_pred : (out[j] == 1 ? in->b_pred : in->x_pred);
+        copy_block(to, S.pred[1 + j]);
+        if (tid == 0) {
+            Desc &d = out[j] == 0 ? in->f_out : (out[j] == 1 ? in->b_out : in->x_out);
+            int &sad = out[j] == 0 ? in->f_sad : (out[j] == 1 ? in->b_sad : in->x_sad);
+            d = S.srch[1 + j].out;
+            sad = S.srch[1 + j].out_sad;
+        }
     }
     return true;
 }
 
-__device__ bool fwd_mb(const FrameArgs &a, int row, int col, int n)   // rank 1
+// Rank 1: the forward search (B frames), the nearest reference's (P frames),
+// and with three references also the third one's.
+__device__ bool fwd_mb(const FrameArgs &a, int row, int col, int n)
 {
     if (a.type == EVXG_FRAME_INTRA) return true;
-    if (!search_mb(a, row, col, n, false)) return false;
+    const bool p = a.type == EVXG_FRAME_INTER;
+    const int ns = p && a.nref >= 3 ? 2 : 1;
+    const int16_t *const ref[2] = {a.planes[p ? a.ref_slot[0] : a.ref_fwd], a.planes[p ? a.ref_slot[2] : 0]};
+    const int out[2] = {0, 2};
+    if (!search_mb(a, row, col, n, ns, ref, out)) return false;
     __syncthreads();
     if (threadIdx.x == 0) st_release_cl(peer(&SM().mail.f_seq, 0), n);
     return true;
@@ -2118,14 +2179,21 @@ __device__ bool aux_mb(const FrameArgs &a, int row, int col, int n)   // rank 2
     MbShared &S = SM();
     const int tid = threadIdx.x;
     const int px = col * 16, py = row * 16;
-    if (a.type == EVXG_FRAME_BIDIR && !search_mb(a, row, col, n, true)) return false;
+    // B frames: the backward search; P frames with several references: the
+    // second reference's search (window pair 1 / 2 of this CTA).
+    const bool searched = a.type == EVXG_FRAME_BIDIR || (a.type == EVXG_FRAME_INTER && a.nref >= 2);
+    if (searched) {
+        const int16_t *const ref[2] = {a.planes[a.type == EVXG_FRAME_BIDIR ? a.ref_bwd : a.ref_slot[1]], nullptr};
+        const int out[2] = {1, 1};
+        if (!search_mb(a, row, col, n, 1, ref, out)) return false;
+    }
     // Directional intra reads row r-1 up to column c from the destination
     // slot (the search has waited for column c+1) and the right column of
     // MB (r, c-1), which the leader hands over in lcol with wr_seq.
-    if (tid == 0) S.row_abort = a.type != EVXG_FRAME_BIDIR && row > 0 && !wait_progress(a, row - 1, col);
+    if (tid == 0) S.row_abort = !searched && row > 0 && !wait_progress(a, row - 1, col);
     __syncthreads();
     if (S.row_abort) return false;
-    if (a.type != EVXG_FRAME_BIDIR) {
+    if (!searched) {
         load_src(a, px, py);
         if (tid == 0) setup_mb(a, row * a.mbw + col, px, py, false, nullptr);
     }

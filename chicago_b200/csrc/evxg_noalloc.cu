@@ -79,6 +79,7 @@ extern "C" int evxg_mb_pass_noalloc(uint32_t aligned_w, uint32_t aligned_h, cons
     a.vis_w = a.W; a.vis_h = a.H;
     a.type = f->type; a.quality = f->quality; a.dpb = f->dpb_slot;
     a.ref_fwd = f->ref_slot_fwd; a.ref_bwd = f->ref_slot_bwd;
+    a.nref = 1; a.ref_slot[0] = f->ref_slot_fwd;   // the default build: P frames search the forward slot
     a.lambda = evxg_lambda(f->quality);
     for (int i = 0; i < 4; i++) a.planes[i] = dpb[i];
     a.src = const_cast<int16_t *>(src);

@@ -276,6 +276,12 @@ int evxg_server_create(uint64_t hbm_budget_bytes, uint32_t max_streams, evxg_res
 
 int evxg_server_open(evxg_server *v, uint32_t width, uint32_t height, uint8_t quality, uint32_t *stream_id)
 {
+    return evxg_server_open_config(v, width, height, quality, nullptr, stream_id);
+}
+
+int evxg_server_open_config(evxg_server *v, uint32_t width, uint32_t height, uint8_t quality, const evxg_config *cfg,
+                            uint32_t *stream_id)
+{
     if (!v || !stream_id) return fail(EVXG_ERROR_INVALIDARG, "evxg_server_open: bad argument");
     const size_t bytes = stream_bytes(width, height);
     {
@@ -291,8 +297,8 @@ int evxg_server_open(evxg_server *v, uint32_t width, uint32_t height, uint8_t qu
     }
     Slot *s = new Slot();
     s->w = width; s->h = height; s->bytes = bytes;
-    int rc = evxg_stream_create(width, height, &s->st);
-    if (!rc) rc = evxg_encoder_create(nullptr, nullptr, &s->planner);
+    int rc = evxg_stream_create_config(width, height, cfg, &s->st);
+    if (!rc) rc = evxg_encoder_create_config(nullptr, nullptr, cfg, &s->planner);
     if (!rc) { encoder_set_sink(s->planner, sink, s); rc = evxg_encoder_set_quality(s->planner, quality); }
     std::lock_guard<std::mutex> lk(v->mu);
     if (rc) {

@@ -98,6 +98,34 @@ typedef struct evxg_sao_info {
 typedef struct evxg_stream evxg_stream;
 
 /*
+ * The reference's encoder is configured at compile time (src/video/config.h,
+ * motion.cpp:29); a stream reproduces one such build, chosen when it is
+ * created:
+ *   b_frames      EVX_ENABLE_B_FRAMES (config.h:120).  1 (default): the
+ *                 hierarchical P / reference-B / B GOP (evx3enc.cpp:167-383),
+ *                 frames carry their DPB slots in evxg_frame.  0: an I/P GOP
+ *                 encoded in arrival order (evx3enc.cpp:137-160); the slots
+ *                 follow from evxg_frame.index (query_prediction_index_by_offset,
+ *                 common.cpp:256-259; the slot fields are ignored) and each P
+ *                 frame searches the references at offsets 1 .. ref_count-1,
+ *                 its descriptors naming the offset (encode.cpp:211-247).  The
+ *                 reference's evx_frame / evx_block_desc of such a build are the
+ *                 first 10 / 18 bytes of evxg_frame / evxg_block_desc.
+ *   ref_count     EVX_REFERENCE_FRAME_COUNT (config.h:39): 4 with B frames;
+ *                 2 (one reference) or 4 (three) without.
+ *   search_radius EVX_MOTION_SEARCH_RADIUS (motion.cpp:29): 16.
+ * Other combinations are refused with EVXG_ERROR_INVALIDARG.
+ */
+typedef struct evxg_config {
+    uint8_t b_frames;
+    uint8_t ref_count;
+    uint8_t search_radius;
+    uint8_t reserved;          /* 0 */
+} evxg_config;
+/* The default build: b_frames 1, ref_count 4, search_radius 16. */
+void evxg_config_default(evxg_config *cfg);
+
+/*
  * Create the device state of one encoding stream for frames of width x height
  * (visible size; the context is 16-aligned like initialize_context,
  * common.cpp:106-202): source, level and 4 DPB plane sets, block / previous
@@ -105,6 +133,9 @@ typedef struct evxg_stream evxg_stream;
  * initialize (evx3enc.cpp:84-103) on the device side.
  */
 int evxg_stream_create(uint32_t width, uint32_t height, evxg_stream **out);
+/* The same for the build cfg describes (NULL = the default build). */
+int evxg_stream_create_config(uint32_t width, uint32_t height, const evxg_config *cfg, evxg_stream **out);
+int evxg_stream_config(const evxg_stream *s, evxg_config *out);
 int evxg_stream_destroy(evxg_stream *s);
 
 /* Aligned context size and macroblock grid of a stream. */
@@ -245,6 +276,9 @@ int evxg_server_create(uint64_t hbm_budget_bytes, uint32_t max_streams, evxg_res
                        evxg_server **out);
 int evxg_server_destroy(evxg_server *srv);
 int evxg_server_open(evxg_server *srv, uint32_t width, uint32_t height, uint8_t quality, uint32_t *stream_id);
+/* evxg_server_open for a stream of the build cfg describes (NULL = default). */
+int evxg_server_open_config(evxg_server *srv, uint32_t width, uint32_t height, uint8_t quality, const evxg_config *cfg,
+                            uint32_t *stream_id);
 int evxg_server_submit(evxg_server *srv, uint32_t stream_id, const uint8_t *rgb, uint64_t arrival_ns);
 int evxg_server_insert_intra(evxg_server *srv, uint32_t stream_id);
 int evxg_server_close(evxg_server *srv, uint32_t stream_id);
@@ -298,6 +332,9 @@ typedef void (*evxg_frame_callback)(void *user, const evxg_frame *frame,
                                     const evxg_sao_info *sao, const int16_t *levels);
 
 int evxg_encoder_create(evxg_frame_callback cb, void *user, evxg_encoder **out);
+/* An encoder of the build cfg describes (NULL = the default build); without B
+ * frames every frame is encoded as it arrives and flush has nothing to do. */
+int evxg_encoder_create_config(evxg_frame_callback cb, void *user, const evxg_config *cfg, evxg_encoder **out);
 int evxg_encoder_destroy(evxg_encoder *e);
 int evxg_encoder_clear(evxg_encoder *e);                     /* evx3enc.cpp:35-55 */
 int evxg_encoder_insert_intra(evxg_encoder *e);              /* evx3enc.cpp:57-62 */

@@ -8,7 +8,8 @@ import numpy as np
 import pytest
 
 from chicago_b200.synth import generate
-from oracle_py import compare_blocks, pack_frame, plan_gop, split_stream, unpack_frame
+from oracle_py import (REF_VARIANTS, Ref, compare_blocks, join_ip_stream, pack_frame, plan_gop, plan_ip, split_stream,
+                       unpack_frame)
 
 pytestmark = pytest.mark.gpu
 
@@ -27,12 +28,18 @@ CASES = [  # (w, h, frames, quality, vmax, intra_at)
 FORMS = ("cluster", "single")   # three CTAs per macroblock row / one
 
 
-def check_stream(oracle, w, h, T, q, vmax, intra_at, form="cluster"):
+def check_stream(oracle, w, h, T, q, vmax, intra_at, form="cluster", cfg="default", seed=None):
+    """Encode a seeded clip through the C ABI and compare every stage of every
+    frame with the oracle restating the same reference build (cfg: "default",
+    or the I/P builds "ip1" / "ip3")."""
     import chicago_b200 as cb
-    frames = generate(w, h, T, seed=w * 7 + h, vmax=vmax)
-    oc, st = oracle.context(w, h), cb.Stream(w, h)
+    b_frames, ref_count, radius = cb.CONFIGS[cfg]
+    frames = generate(w, h, T, seed=w * 7 + h if seed is None else seed, vmax=vmax)
+    oc = oracle.context(w, h, b_frames=b_frames, ref_count=ref_count, radius=radius)
+    st = cb.Stream(w, h, cfg)
     st.mb_form = cb.MB_FORM_CLUSTER if form == "cluster" else cb.MB_FORM_SINGLE
-    for k, (ti, f18) in enumerate(plan_gop(T, quality=q, intra_at=intra_at)):
+    plan = plan_gop(T, quality=q, intra_at=intra_at) if b_frames else plan_ip(T, q, intra_at, ref_count)
+    for k, (ti, f18) in enumerate(plan):
         fr = unpack_frame(f18)
         od = oc.encode_frame(frames[ti], f18)
         st.encode_frame(frames[ti], f18)
@@ -43,6 +50,7 @@ def check_stream(oracle, w, h, T, q, vmax, intra_at, form="cluster"):
         assert np.array_equal(tb["sao"], od.sao), f"frame {k}: SAO table"
         assert np.array_equal(st.fetch_planes(4), od.src), f"frame {k}: converted source"
         assert np.array_equal(st.fetch_planes(fr["dpb_slot"]), od.final), f"frame {k}: reconstruction"
+    return st
 
 
 @pytest.mark.parametrize("form", FORMS)
@@ -55,6 +63,54 @@ def test_gpu_matches_oracle(oracle, w, h, T, q, vmax, intra_at, form):
 def test_gpu_matches_oracle_1080p(oracle, form):
     """Full-size frames: I, P, reference-B and B at 1920x1080 (120x68 MBs)."""
     check_stream(oracle, 1920, 1080, 4, 8, 24.0, (), form)
+
+
+IP_CASES = [  # (cfg, w, h, frames, quality, vmax, intra_at, seed)
+    ("ip1", 64, 48, 6, 8, 6.0, (), None),
+    ("ip1", 96, 64, 6, 1, 20.0, (), None),
+    ("ip3", 176, 144, 8, 8, 3.0, (7,), 176 * 5 + 144 + 4),   # uses all three references
+    ("ip3", 100, 60, 7, 4, 12.0, (4,), None),
+    ("ip3", 352, 288, 5, 16, 6.0, (), None),
+    ("ip3", 48, 32, 6, 31, 3.0, (), None),
+]
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("cfg,w,h,T,q,vmax,intra_at,seed", IP_CASES)
+def test_gpu_matches_oracle_ip(oracle, cfg, w, h, T, q, vmax, intra_at, seed, form):
+    """I/P builds (EVX_ENABLE_B_FRAMES 0): P frames search one or three
+    references by offset from the frame index, with the distance bias."""
+    check_stream(oracle, w, h, T, q, vmax, intra_at, form, cfg, seed)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_gpu_matches_oracle_ip3_1080p(oracle, form):
+    """Full-size I/P frames with three references: I and three P frames."""
+    check_stream(oracle, 1920, 1080, 4, 8, 24.0, (), form, "ip3")
+
+
+@pytest.mark.parametrize("variant", ["ip1", "ip3"])
+def test_evx_bytes_match_stock_reference_ip(variant):
+    """GOP-level encoder of an I/P configuration (C ABI) -> that reference
+    build's entropy coder -> its stock .evx stream, byte for byte."""
+    import chicago_b200 as cb
+    if not __import__("os").path.exists(REF_VARIANTS[variant][0]):
+        pytest.skip(f"reference variant {variant} not built")
+    ref = Ref(variant=variant)
+    w, h, T, q = 144, 96, 9, 8
+    frames = generate(w, h, T, seed=6, vmax=6.0)
+    stock = ref.encode_stream(frames, quality=q, intra_at=(5,))
+    enc = cb.Encoder(quality=q, cfg=variant)
+    for t in range(T):
+        if t == 5:
+            enc.insert_intra()
+        enc.encode(frames[t])
+    enc.flush()
+    assert len(enc.records) == T
+    ctx = ref.context(w, h)
+    parts = [(r["frame18"], ctx.serialize(r["frame18"], r["blocks"], r["prev_blocks"], r["sao"], r["levels"]))
+             for r in enc.records]
+    assert join_ip_stream(stock[:14], parts) == stock
 
 
 def test_evx_bytes_match_stock_reference(ref):
