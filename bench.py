@@ -3,22 +3,32 @@
 Workload (the plain one-stream configuration): a seeded 1920x1080 RGB24
 sequence of 120 frames (sinusoid background, global pan with per-frame
 velocity in [-24, 24] px at quarter-pel, moving textured rectangles, noise
-sigma 3, scene cut at frame 60 where insert_intra() starts a new GOP),
-quality 8, deblocking and SAO on, encoded with the reference encoder's own GOP
-structure (I, then hierarchical P / reference-B / B groups of 4).
+sigma 3, scene cut at frame 60), quality 8, deblocking and SAO on, encoded as
+an I/P GOP of 60 (insert_intra() at the cut) by the reference's I/P build with
+three references (EVX_ENABLE_B_FRAMES 0, EVX_REFERENCE_FRAME_COUNT 4): every P
+frame searches the last three reconstructed frames.  An I/P GOP with exactly
+two references is not expressible in the reference (a reference count of 3
+breaks its bitstream), so three stand in for two.
 
 A step is one frame of engine_encode_frame minus serialization in encode
-order: RGB->YUV, the macroblock wavefront (mode decision, transform,
-quantisation, trellis, reconstruction), deblocking, SAO.  `value` times the
-steps on the device with the RGB frames already resident in HBM and L2
-flushed between steps; `e2e` times the same steps through the C ABI with
-pinned host RGB in and the serializer's tables (block, previous block, SAO
-tables and level planes) out, copies inside the timed region.
+order: RGB->YUV, the macroblock wavefront (mode decision over three
+references, transform, quantisation, trellis, reconstruction), deblocking,
+SAO.  `value` times the steps on the device with the RGB frames already
+resident in HBM and L2 flushed between steps; `e2e` times the same steps
+through the C ABI with pinned host RGB in and the serializer's tables (block,
+previous block, SAO tables and level planes) out, copies inside the timed
+region.  Extra legs: quality 4 and 16, the reference's default GOP
+(hierarchical P/B), the batched 16-stream mix and the served request loop.
+
+Parity: the cpu_baseline leg encodes the same frames with the reference's own
+I/P build and checks that the GPU arm's tables of every warm-up and timed
+frame, serialized by that build's entropy coder, give its .evx bytes exactly
+(`parity` in the line).
 
 Multi-GPU (torchrun): every rank encodes its own stream (own seed), no
 collective on the data path (weak scaling); time is the max over ranks.
-`--impl reference` times the unmodified reference encoder (oracle/_ref, built
-from the reference's sources) through its public API on the host cores.
+`--impl reference` times the reference encoder of the same build (oracle/_ref,
+built from the reference's sources) through its public API on the host cores.
 """
 from __future__ import annotations
 
@@ -38,11 +48,13 @@ sys.path.insert(0, ROOT)
 METRIC = "1080p-eq frames/s & p99 frame latency, batched vs plain GPU, bit-exact output"
 UNIT = "1080p-eq frames/s"
 W, H, FRAMES, QUALITY, VMAX, CUT = 1920, 1080, 120, 8, 24.0, 60
+CFG = "ip3"          # reference build: I/P GOP, three references
+GOP_DESC = "I/P GOP of 60 (insert_intra at the cut), 3 references standing in for 2"
 EQ = (W * H) / (1920 * 1080)
 HBM_PEAK_FALLBACK = 6650.0
-# dram__bytes_read.sum + dram__bytes_write.sum of one k_mb_cluster launch
-# (a 1080p B frame of this workload), profiles/mb_cluster_1080p.md
-MB_TRAFFIC_BYTES = 25_386_496 + 257_792
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_mb_cluster launch on a
+# 1920x1080 P frame with three references of this workload (ncu capture)
+MB_TRAFFIC_BYTES = 31_906_304 + 365_568
 
 
 def peaks():
@@ -72,9 +84,9 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
-def plan(seed_offset: int):
+def plan(quality: int = QUALITY, cfg: str = CFG):
     from chicago_b200.gop import plan as gop_plan
-    return gop_plan(FRAMES, quality=QUALITY, intra_at=(CUT,))
+    return gop_plan(FRAMES, quality=quality, intra_at=(CUT,), cfg=cfg)
 
 
 def rank_seed(rank: int) -> int:
@@ -82,9 +94,19 @@ def rank_seed(rank: int) -> int:
     return 1000 + rank
 
 
-def frames_for(rank: int):
+def frames_for(rank: int, n: int = FRAMES):
     from chicago_b200.synth import generate
-    return generate(W, H, FRAMES, seed=rank_seed(rank), vmax=VMAX, n_rects=4, cut_at=CUT)
+    return generate(W, H, n, seed=rank_seed(rank), vmax=VMAX, n_rects=4, cut_at=CUT)
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
 
 
 class Clocks:
@@ -130,76 +152,109 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def algorithmic_bytes(ftype: int, aw: int, ah: int) -> int:
+def algorithmic_bytes(ftype: int, aw: int, ah: int, nref: int) -> int:
     """Compulsory HBM bytes of one macroblock-wavefront launch: the source plane
     set read once, every reference slot read once (the intra block-copy search
     reads the destination slot too), reconstruction and levels written once,
     block table written (28 B per MB)."""
     planeset = (aw * ah + 2 * (aw // 2) * (ah // 2)) * 2
-    refs = {0: 1, 1: 2, 2: 3}[ftype]
+    refs = {0: 1, 1: 1 + nref, 2: 3}[ftype]
     return planeset * (1 + refs + 2) + (aw // 16) * (ah // 16) * 28
+
+
+def device_steps(stream, frames_dev, sched, warmup, cfg, flush, profile=False):
+    """Encode sched's frames on a fresh stream from device-resident RGB; time
+    the steps after the warm-up ones with CUDA events on the launching stream,
+    L2 flushed before each.  Returns (stream, step_ms, per-kernel ms list)."""
+    import torch
+    import chicago_b200 as cb
+    sp = stream.cuda_stream
+    st = cb.Stream(W, H, cfg)
+    if profile:
+        st.profile(True)
+    for ti, f18 in sched[:warmup]:
+        st.encode_frame(frames_dev[ti].data_ptr(), f18, on_device=True, cuda_stream=sp)
+    st.sync(sp)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step_ms, kms = [], []
+    for ti, f18 in sched[warmup:]:
+        flush.zero_()
+        ev0.record(stream)
+        st.encode_frame(frames_dev[ti].data_ptr(), f18, on_device=True, cuda_stream=sp)
+        ev1.record(stream)
+        ev1.synchronize()
+        step_ms.append(ev0.elapsed_time(ev1))
+        if profile:
+            kms.append(st.kernel_ms())
+    st.sync(sp)
+    return st, step_ms, kms
 
 
 def run_gpu(args):
     import torch
     import chicago_b200 as cb
+    from chicago_b200.gop import unpack_frame
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=600))
-    sched = plan(rank)
+    sched = plan()
     K = min(args.steps, len(sched) - args.warmup)
+    order = sched[:args.warmup + K]
     frames = frames_for(rank)
     dev_frames = torch.from_numpy(frames).cuda()                       # 746 MB resident in HBM
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")   # > 126 MB L2
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
-    st = cb.Stream(W, H)
-    st.profile(True)
-    from chicago_b200.gop import unpack_frame
-    # warm-up steps, then K timed steps; state (DPB, tables) carries across steps
-    order = sched[:args.warmup + K]
-    for ti, f18 in order[:args.warmup]:
-        st.encode_frame(dev_frames[ti].data_ptr(), f18, on_device=True, cuda_stream=sp)
-    st.sync(sp)
+    nref = cb.CONFIGS[CFG][1] - 1
+
+    # headline: device-resident steps at quality 8, per-kernel times
     clocks = Clocks(local)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    step_ms, mb_ms, mb_bytes = [], [], 0
-    kernel_tot = {k: 0.0 for k in cb.Stream.KERNELS}
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for ti, f18 in order[args.warmup:]:
-        flush.zero_()
-        ev0.record(stream)
-        st.encode_frame(dev_frames[ti].data_ptr(), f18, on_device=True, cuda_stream=sp)
-        ev1.record(stream)
-        ev1.synchronize()
-        step_ms.append(ev0.elapsed_time(ev1))
-        km = st.kernel_ms()
-        for k, v in km.items():
-            kernel_tot[k] += v
-        mb_ms.append(km["mb_wavefront"])
-        mb_bytes += algorithmic_bytes(unpack_frame(f18)["type"], st.aw, st.ah)
-    st.sync(sp)
+    st, step_ms, kms = device_steps(stream, dev_frames, order, args.warmup, CFG, flush, profile=True)
     torch.cuda.synchronize()
     clk = clocks.stop()
     total_ms = max_over_ranks(sum(step_ms), world)
     value = job_value(world, K, total_ms)
+    kernel_tot = {k: sum(m[k] for m in kms) for k in cb.Stream.KERNELS}
+    mb_ms = [m["mb_wavefront"] for m in kms]
+    mb_bytes = sum(algorithmic_bytes(unpack_frame(f18)["type"], st.aw, st.ah, nref) for _, f18 in order[args.warmup:])
+    launches = st.launch_count() * K
+    form = st.mb_form
+    st.close()
+
+    # quality 4 and 16, and the reference's default GOP, on fresh streams
+    legs = {}
+    for q in (4, 16):
+        s_, ms, _ = device_steps(stream, dev_frames, plan(q)[:args.warmup + K], args.warmup, CFG, flush)
+        s_.close()
+        t = max_over_ranks(sum(ms), world)
+        legs[f"q{q}"] = {"value": round(job_value(world, K, t), 3), "ms_per_step": round(t / K, 3),
+                         "p99_frame_ms": round(float(np.percentile(ms, 99)), 3)}
+    s_, ms, _ = device_steps(stream, dev_frames, plan(QUALITY, "default")[:args.warmup + K], args.warmup, "default", flush)
+    s_.close()
+    t = max_over_ranks(sum(ms), world)
+    default_gop = {"value": round(job_value(world, K, t), 3), "ms_per_step": round(t / K, 3),
+                   "p99_frame_ms": round(float(np.percentile(ms, 99)), 3),
+                   "workload": "same frames, the reference's default build: I + hierarchical P/B groups of 4"}
 
     # end to end through the C ABI: pinned host RGB in, serializer tables out
-    nblk = st.mbw * st.mbh
+    import ctypes as C
+    st2 = cb.Stream(W, H, CFG)
+    nblk = st2.mbw * st2.mbh
     host_rgb = torch.from_numpy(frames).pin_memory()
     out_bt = torch.empty(nblk * 28, dtype=torch.uint8).pin_memory()
     out_prev = torch.empty(nblk * 28, dtype=torch.uint8).pin_memory()
     out_sao = torch.empty(nblk * 16, dtype=torch.uint8).pin_memory()
-    out_lev = torch.empty(st.plane_elems, dtype=torch.int16).pin_memory()
-    st2 = cb.Stream(W, H)
+    out_lev = torch.empty(st2.plane_elems, dtype=torch.int16).pin_memory()
     L = cb.lib()
-    import ctypes as C
-    e2e_ms = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_ms, records = [], []
     for i, (ti, f18) in enumerate(order):
         ev0.record(stream)
         cb._check(L.evxg_encode_frame(st2.h, C.c_void_p(host_rgb[ti].data_ptr()), 0, f18, C.c_void_p(sp)))
@@ -209,14 +264,18 @@ def run_gpu(args):
         ev1.synchronize()
         if i >= args.warmup:
             e2e_ms.append(ev0.elapsed_time(ev1))
+        # kept (outside the timed span) for the parity check against the reference
+        records.append((f18, out_bt.numpy().copy(), out_prev.numpy().copy(), out_sao.numpy().copy(),
+                        out_lev.numpy().copy()))
+    st2.close()
     e2e_total = max_over_ranks(sum(e2e_ms), world)
     e2e_value = job_value(world, K, e2e_total)
     h2d = W * H * 3
-    d2h = nblk * 28 * 2 + nblk * 16 + st.plane_elems * 2
+    d2h = nblk * 28 * 2 + nblk * 16 + st2.plane_elems * 2
 
     batched = run_batched(args, stream) if args.batch > 1 and world == 1 else None
     served = run_served(args) if args.serve_streams > 0 and world == 1 else None
-    served_light = (run_served(args, n=8, per=12, sizes_from=[(640, 360), (1280, 720)], seed=11)
+    served_light = (run_served(args, n=8, per=args.serve_frames, sizes_from=[(640, 360), (1280, 720)], seed=11)
                     if args.serve_streams > 0 and world == 1 else None)
 
     peak, peak_kind = peaks()
@@ -226,28 +285,33 @@ def run_gpu(args):
         "warmup": args.warmup, "ms_per_step": round(total_ms / K, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic (seeded generator)",
         "config": {"workload": "plain GPU path, one stream per GPU: 1920x1080 RGB24, 120 frames, pan +-24 px, "
-                               "scene cut at 60, quality 8, reference GOP (I + hierarchical P/B of 4), deblock+SAO",
+                               f"scene cut at 60, quality 8, {GOP_DESC}, quarter-pel search over +-32 px, "
+                               "deblock+SAO",
+                   "reference_build": "EVX_ENABLE_B_FRAMES 0, EVX_REFERENCE_FRAME_COUNT 4",
                    "frames": FRAMES, "quality": QUALITY, "l2": "flushed (256 MB write) between timed steps",
                    "parallelism": f"{world} independent streams, no collective"},
         "p50_frame_ms": round(float(np.percentile(step_ms, 50)), 3),
         "p99_frame_ms": round(float(np.percentile(step_ms, 99)), 3),
         "kernel_ms_per_step": {k: round(v / K, 4) for k, v in kernel_tot.items()},
-        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "roofline": {"kernel": "k_mb_cluster" if st.mb_form == cb.MB_FORM_CLUSTER else "k_mb_wavefront",
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "note": "tables out for the host entropy coder; the reference arm's time includes its entropy coding"},
+        "roofline": {"kernel": "k_mb_cluster" if form == cb.MB_FORM_CLUSTER else "k_mb_wavefront",
                      "bound": "hbm", "achieved": round(achieved, 3), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 6),
-                     "traffic": MB_TRAFFIC_BYTES if st.mb_form == cb.MB_FORM_CLUSTER else None,
+                     "traffic": MB_TRAFFIC_BYTES if form == cb.MB_FORM_CLUSTER else None,
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "note": "dependency-latency bound: macroblock wavefront whose critical path is "
                              "cols + 3*(rows-1) MB steps (321 at 1080p), each one MB's dependent chain"},
-        "gpu_launches": st.launch_count() * K,
+        "gpu_launches": launches,
+        "quality_legs": legs,
+        "default_gop": default_gop,
         "batched": batched,
         "served": served,
         "served_light": served_light,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline()
+        line["cpu_baseline"], line["parity"] = cpu_baseline(order, records, frames)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -255,8 +319,9 @@ def run_gpu(args):
 
 
 # The batched configuration: 16 streams -- 4 x 1920x1080, 6 x 1280x720,
-# 6 x 640x360 -- each with its own seed, at its own GOP position (stream k
-# starts k % 4 ticks late and cuts to a new GOP at its own frame), quality 8.
+# 6 x 640x360 -- each with its own seed and GOP phase (I/P GOP of 30, three
+# references standing in for two, an intra frame every 30 frames from its own
+# start), quality 8.
 BATCH_MIX = [(1920, 1080)] * 4 + [(1280, 720)] * 6 + [(640, 360)] * 6
 
 
@@ -269,7 +334,7 @@ def run_batched(args, stream):
     parities while the host fills the next one."""
     import torch
     import chicago_b200 as cb
-    from chicago_b200.gop import plan as gop_plan, unpack_frame
+    from chicago_b200.gop import plan as gop_plan
     from chicago_b200.synth import generate
     mix = BATCH_MIX[:args.batch] if args.batch < len(BATCH_MIX) else BATCH_MIX
     warm, K = args.warmup, args.batch_ticks
@@ -277,8 +342,9 @@ def run_batched(args, stream):
     seqs = []
     for k, (w, h) in enumerate(mix):
         frames = generate(w, h, nfr, seed=2000 + k, vmax=max(6.0, 24.0 * w / 1920), n_rects=4)
-        seqs.append((frames, gop_plan(nfr, quality=QUALITY, intra_at=(5 + (3 * k) % 7,))))
-    streams = [cb.Stream(w, h) for w, h in mix]
+        phase = (7 * k) % 30   # this stream's GOP position: its next intra frame
+        seqs.append((frames, gop_plan(nfr, quality=QUALITY, intra_at=tuple(range(phase, nfr, 30)), cfg=CFG)))
+    streams = [cb.Stream(w, h, CFG) for w, h in mix]
     b = cb.Batch(streams)
     sp = stream.cuda_stream
     tuned_ms = b.autotune(sp)
@@ -318,6 +384,7 @@ def run_batched(args, stream):
     for w, h in mix:
         sizes[f"{w}x{h}"] = sizes.get(f"{w}x{h}", 0) + 1
     res = {"streams": len(mix), "sizes": " + ".join(f"{n}x{k}" for k, n in sizes.items()),
+           "gop": "I/P GOP of 30 per stream (own phase), 3 references standing in for 2, quality 8",
            "value": round(sum(eq) / (span_ms / 1e3), 3), "unit": UNIT, "ticks": K,
            "ms_per_tick": round(span_ms / K, 3),
            "p50_frame_ms": round(float(np.percentile(tick_ms, 50)), 3),
@@ -336,7 +403,8 @@ def run_batched(args, stream):
 
 # The serving configuration: 64 streams at 60 fps, sizes drawn uniformly from
 # 640x360 / 1280x720 / 1920x1080 / 3840x2160, arrivals every 1/60 s with
-# +-2 ms jitter from a random phase, quality 8.
+# +-2 ms jitter from a random phase, each stream an I/P GOP of 60 with one or
+# three references (three standing in for two), quality 8.
 SERVE_SIZES = [(640, 360), (1280, 720), (1920, 1080), (3840, 2160)]
 
 
@@ -344,9 +412,8 @@ def run_served(args, n=None, per=None, sizes_from=None, seed=7):
     """The request loop (evxg_server_*): all streams admitted by the device
     memory budget, frames submitted at their arrival times by this thread, the
     server's worker batching whatever is ready.  A frame's latency is its done
-    time (results seen by the host) minus its arrival time, so it includes the
-    reference GOP's reorder wait (a B frame waits for its anchor) and queueing;
-    each stream sends `serve_frames` frames and then closes (flushing)."""
+    time (results seen by the host) minus its arrival time, queueing included;
+    each stream sends `serve_frames` frames and then closes."""
     import chicago_b200 as cb
     from chicago_b200.synth import generate
     rng = np.random.default_rng(seed)
@@ -354,10 +421,11 @@ def run_served(args, n=None, per=None, sizes_from=None, seed=7):
     per = args.serve_frames if per is None else per
     choices = SERVE_SIZES if sizes_from is None else sizes_from
     sizes = [choices[i] for i in rng.integers(0, len(choices), n)]
+    cfgs = ["ip1" if i else "ip3" for i in rng.integers(0, 2, n)]
     pool = {sz: generate(sz[0], sz[1], per + 3, seed=3000 + k, vmax=max(4.0, 24.0 * sz[0] / 1920))
             for k, sz in enumerate(SERVE_SIZES) if sz in sizes}
     srv = cb.Server(hbm_budget_bytes=96 << 30, max_streams=n, keep_tables=False)
-    ids = [srv.open(w, h, QUALITY) for w, h in sizes]
+    ids = [srv.open(w, h, QUALITY, cfg=c) for (w, h), c in zip(sizes, cfgs)]
     srv.drain()   # the batch over every admitted stream exists before the first arrival
     phase = rng.uniform(0, 1 / 60, n)
     events = sorted((phase[k] + t / 60 + rng.uniform(-0.002, 0.002), k, t) for k in range(n) for t in range(per))
@@ -368,6 +436,8 @@ def run_served(args, n=None, per=None, sizes_from=None, seed=7):
         while cb.Server.now_ns() < due:
             time.sleep(min(0.0005, (due - cb.Server.now_ns()) / 1e9))
         off = k % 3   # streams of a size class start at different frames of its pool
+        if t > 0 and t % 60 == 0:
+            srv.insert_intra(ids[k])   # GOP of 60
         srv.submit(ids[k], pool[sizes[k]][off + t], arrival_ns=cb.Server.now_ns())
         sent[k] += 1
         if sent[k] == per:
@@ -387,7 +457,8 @@ def run_served(args, n=None, per=None, sizes_from=None, seed=7):
     srv.close()
     offered = sum(w * h for w, h in sizes) / (1920 * 1080) * 60
     counts = {f"{w}x{h}": sizes.count((w, h)) for w, h in SERVE_SIZES if (w, h) in sizes}
-    return {"streams": n, "sizes": counts, "frames": len(lat), "frames_per_stream": per,
+    return {"streams": n, "sizes": counts, "references": {"1": cfgs.count("ip1"), "3": cfgs.count("ip3")},
+            "frames": len(lat), "frames_per_stream": per,
             "value": round(eq / ((last - first) / 1e9), 3), "unit": UNIT,
             "offered_1080p_eq_fps": round(offered, 1),
             "p50_frame_ms": round(float(np.percentile(lat, 50)), 3),
@@ -395,24 +466,46 @@ def run_served(args, n=None, per=None, sizes_from=None, seed=7):
             "p999_frame_ms": round(float(np.percentile(lat, 99.9)), 3),
             "ready_to_done_ms": {q: round(float(np.percentile(work, v)), 3) for q, v in (("p50", 50), ("p99", 99), ("p999", 99.9))},
             "ticks": st["ticks"], "batch_rebuilds": st["rebuilds"],
-            "note": "latency = results seen by the host minus arrival: includes the reference GOP's reorder wait "
-                    "(a B frame waits for its anchor, 3 frames later) and any queueing; ready_to_done starts when "
-                    "the frame's encode order is known"}
+            "note": "latency = results seen by the host minus arrival (I/P GOP: no reorder wait), queueing included"}
 
 
-def cpu_baseline(n_frames: int = 8):
-    """The unmodified reference encoder (built here from its sources) with its
-    WPP threads on all host cores, on the first n_frames of the same workload."""
+def cpu_baseline(order, records, frames):
+    """The reference encoder of the same build (I/P, three references; built
+    here from its sources) on the host cores, over the GPU arm's warm-up and
+    timed frames: with its WPP threads on all cores, and single-threaded
+    (EVX_ENABLE_WPP 0) on the first two frames.  Also the parity check: the
+    GPU arm's tables of every one of those frames, serialized by the same
+    build's entropy coder, must give its stock .evx stream byte for byte."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from chicago_b200.synth import generate
-    from oracle_py import Ref
-    frames = generate(W, H, n_frames, seed=1000, vmax=VMAX)
-    ref = Ref()
+    from oracle_py import REF_VARIANTS, Ref, join_ip_stream
+    n = len(order)
+    if not os.path.exists(REF_VARIANTS[CFG][0]):
+        return None, {"checked": False, "why": "reference I/P build not present"}
+    ref = Ref(variant=CFG)
     t0 = time.perf_counter()
-    ref.encode_stream(frames, quality=QUALITY)
+    stock = ref.encode_stream(frames[:n], quality=QUALITY, intra_at=tuple(t for t in (CUT,) if t < n))
     dt = time.perf_counter() - t0
-    return {"value": round(n_frames * EQ / dt, 4), "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-            "sample": f"first {n_frames} frames of the workload through create_encoder/encode/flush (WPP threads)"}
+    base = {"value": round(n * EQ / dt, 4), "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+            "cpu_model": cpu_model(),
+            "sample": f"frames 0..{n - 1} of the workload (the GPU arm's warm-up and timed frames) through "
+                      "create_encoder/encode of the reference's I/P build (3 references), its WPP threads on every "
+                      "core; host entropy coding included"}
+    if os.path.exists(REF_VARIANTS["ip3seq"][0]):
+        seq = Ref(variant="ip3seq")
+        m = 2
+        t0 = time.perf_counter()
+        s2 = seq.encode_stream(frames[:m], quality=QUALITY)
+        d1 = time.perf_counter() - t0
+        base["single_thread"] = {"value": round(m * EQ / d1, 4), "unit": UNIT, "cores": 1,
+                                 "sample": f"frames 0..{m - 1}, the same build with EVX_ENABLE_WPP 0",
+                                 "same_bytes_as_wpp": s2 == stock[:len(s2)]}
+    ctx = ref.context(W, H)
+    parts = [(f18, ctx.serialize(f18, bt, pv, sao, lev)) for f18, bt, pv, sao, lev in records]
+    mine = join_ip_stream(stock[:14], parts)
+    parity = {"frames": len(records), "match": mine == stock, "bytes": len(stock),
+              "how": "GPU tables of every warm-up and timed frame (e2e leg) serialized by the reference build's entropy "
+                     "coder vs its stock stream of the same frames"}
+    return base, parity
 
 
 def run_reference(args):
@@ -420,12 +513,12 @@ def run_reference(args):
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from oracle_py import REF_SO, Ref
-    if not os.path.exists(REF_SO):
-        print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref/libevxref.so not built"}))
+    from oracle_py import REF_VARIANTS, Ref
+    if not os.path.exists(REF_VARIANTS[CFG][0]):
+        print(json.dumps({"impl": "reference", "unavailable": f"reference build {REF_VARIANTS[CFG][0]} not present"}))
         return
     import ctypes as C
-    ref = Ref()
+    ref = Ref(variant=CFG)
     K = min(args.steps, FRAMES - args.warmup)
     frames = frames_for(0)[:args.warmup + K]
     L = ref.lib
@@ -450,9 +543,13 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
             "steps": K, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / K, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic (seeded generator)",
-            "config": {"workload": "same sequence as the GPU arm, stream 0", "frames": FRAMES, "quality": QUALITY},
+            "config": {"workload": "same sequence as the GPU arm, stream 0: 1920x1080, quality 8, " + GOP_DESC,
+                       "reference_build": "EVX_ENABLE_B_FRAMES 0, EVX_REFERENCE_FRAME_COUNT 4",
+                       "frames": FRAMES, "quality": QUALITY},
             "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                             "sample": f"{K} frames after {args.warmup} warm-up frames, WPP threads"},
+                             "cpu_model": cpu_model(),
+                             "sample": f"{K} frames after {args.warmup} warm-up frames, WPP threads, "
+                                       "host entropy coding included"},
             "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -460,14 +557,14 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=117)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=16, help="streams of the batched measurement (1 = skip)")
     ap.add_argument("--batch-ticks", type=int, default=12, help="timed ticks of the batched measurement")
     ap.add_argument("--serve-streams", type=int, default=64, help="streams of the serving measurement (0 = skip)")
-    ap.add_argument("--serve-frames", type=int, default=4, help="frames each served stream sends")
+    ap.add_argument("--serve-frames", type=int, default=12, help="frames each served stream sends")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

@@ -2,8 +2,10 @@
 the per-frame C ABI (evxg_encode_frame) themselves, e.g. the benchmark and
 batched drivers.  Mirrors evx3_encoder_impl::encode / encode_gop / flush
 (reference src/video/evx3enc.cpp:105-414) with the default build constants
-EVX_B_FRAME_COUNT 3 and EVX_PERIODIC_INTRA_RATE 3600 (config.h:41, :121); the
-C++ encoder behind evxg_encoder_* implements the same logic natively.
+EVX_B_FRAME_COUNT 3 and EVX_PERIODIC_INTRA_RATE 3600 (config.h:41, :121), and
+its I/P path (EVX_ENABLE_B_FRAMES 0, evx3enc.cpp:137-160: every frame encoded
+as it arrives, slots chosen by the frame index); the C++ encoder behind
+evxg_encoder_* implements the same logic natively.
 """
 from __future__ import annotations
 
@@ -30,10 +32,13 @@ def quality_to_qp(q: int) -> int:
 
 
 class Schedule:
-    """Incremental planner: feed input frame indices, get (input index, frame18) in encode order."""
+    """Incremental planner: feed input frame indices, get (input index, frame18)
+    in encode order.  b_frames=False plans the I/P build with ref_count DPB
+    slots (the frame's slots follow from its index)."""
 
-    def __init__(self, quality: int = 8):
+    def __init__(self, quality: int = 8, b_frames: bool = True, ref_count: int = 4):
         self.qp = quality_to_qp(quality)
+        self.b_frames, self.ref_count = b_frames, ref_count
         self.type, self.index, self.doc, self.ip, self.first = FRAME_INTRA, 0, 0, 0, True
         self.reorder = []
 
@@ -66,6 +71,13 @@ class Schedule:
 
     def push(self, t: int):
         out = []
+        if not self.b_frames:   # evx3enc.cpp:137-160
+            R, i = self.ref_count, self.index
+            out.append((t, pack_frame(self.type, i, self.qp, self.doc, 1, i % R, (i + R - 1) % R, 0)))
+            self.doc += 1
+            self.type = FRAME_INTRA if (i + 1) % INTRA_RATE == 0 else FRAME_INTER
+            self.index += 1
+            return out
         if self.doc > 0 and self.doc % INTRA_RATE == 0:
             if self.reorder:
                 self._gop(out)
@@ -102,9 +114,14 @@ class Schedule:
         return out
 
 
-def plan(n_frames: int, quality: int = 8, intra_at=()):
-    """Whole-sequence schedule; insert_intra() is called before each index in intra_at."""
-    s, out = Schedule(quality), []
+CONFIG_GOP = {"default": (True, 4), "ip1": (False, 2), "ip3": (False, 4)}
+
+
+def plan(n_frames: int, quality: int = 8, intra_at=(), cfg: str = "default"):
+    """Whole-sequence schedule of the build cfg names ("default", "ip1",
+    "ip3"); insert_intra() is called before each index in intra_at."""
+    b_frames, ref_count = CONFIG_GOP[cfg]
+    s, out = Schedule(quality, b_frames, ref_count), []
     for t in range(n_frames):
         if t in intra_at:
             s.insert_intra()

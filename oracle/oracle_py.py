@@ -13,7 +13,7 @@
 
 Build variants of the reference (oracle/variants/, ``REF_VARIANTS``): "ip1"
 (I/P GOP, one reference), "ip3" (I/P GOP, three references), "seq" (default
-GOP, one thread).  ``Ref(variant=...)`` loads one; ``Oracle.context(...,
+GOP, one thread), "ip3seq" ("ip3", one thread).  ``Ref(variant=...)`` loads one; ``Oracle.context(...,
 config=...)`` restates the same switches.
 """
 from __future__ import annotations
@@ -31,6 +31,7 @@ REF_VARIANTS = {
     "ip1": (os.path.join(HERE, "_ref", "libevxref_ip1.so"), 0, 2),
     "ip3": (os.path.join(HERE, "_ref", "libevxref_ip3.so"), 0, 4),
     "seq": (os.path.join(HERE, "_ref", "libevxref_seq.so"), 1, 4),
+    "ip3seq": (os.path.join(HERE, "_ref", "libevxref_ip3seq.so"), 0, 4),
 }
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 
