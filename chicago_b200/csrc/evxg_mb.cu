@@ -72,7 +72,7 @@ constexpr int NW = NT / 32;
 constexpr int GT = 128;        // threads per warp group
 constexpr int MB_N = 384;      // 16x16 luma + 2 x 8x8 chroma, MB buffer layout Y | U | V
 constexpr int MAXC = 5;        // RDO candidates (encode.cpp:279-364)
-constexpr int NWIN = 5;        // 0 intra (destination slot), 1/2 forward at MB / predictor, 3/4 backward
+constexpr int NWIN = 6;        // 0 intra (destination slot), 1/2 forward at MB / predictor, 3/4 backward, 5 third reference
 
 struct alignas(16) Win {
     int16_t y[WL_ROWS * WL];
@@ -1710,9 +1710,9 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
     __syncthreads();
     if (a.type == EVXG_FRAME_INTER && tid == 0) {
         for (int k = 0; k < 2 && k < a.nref; k++) { S.rout[k] = S.srch[1 + k].out; S.rsad[k] = S.srch[1 + k].out_sad; S.rpred[k] = 1 + k; }
-        if (a.nref >= 3) {   // the third reference: windows 1 / 2 again, prediction into pred[3]
+        if (a.nref >= 3) {   // the third reference: window 5 at the MB, window 2 again at the predictor; pred[3]
             S.req.n = 0; S.req.fy0 = S.req.fy1 = S.req.fcy0 = S.req.fcy1 = 0; S.req.staged = 0;
-            req_window(1, a.planes[a.ref_slot[2]], px, py);
+            req_window(5, a.planes[a.ref_slot[2]], px, py);
             if (S.sep) req_window(2, a.planes[a.ref_slot[2]], S.qx, S.qy);
         }
     }
@@ -1720,7 +1720,7 @@ __device__ void process_mb(const FrameArgs &a, int row, int col)
         __syncthreads();
         load_windows(a.W, a.H);
         __syncthreads();
-        inter_search(G_ALL, a, 1, 1, 2, px, py, S.pred[3], false);
+        inter_search(G_ALL, a, 1, 5, 2, px, py, S.pred[3], false);
         if (tid == 0) { S.rout[2] = S.srch[1].out; S.rsad[2] = S.srch[1].out_sad; S.rpred[2] = 3; }
     }
     if (a.type == EVXG_FRAME_BIDIR) bi_prediction();
@@ -2098,17 +2098,32 @@ __device__ bool leader_mb(const FrameArgs &a, int row, int col, int n)
     return true;
 }
 
-// Ranks 1 and 2: one or two inter searches of the n-th MB, handed to the
-// leader's inbox (the caller releases the sequence flag).  Search k runs in
-// srch[1 + k] over windows 1 + 2k (at the MB) and 2 + 2k (at the predictor)
-// of reference plane set ref[k] and goes to the inbox's result slot out[k]
-// (0 forward, 1 backward, 2 third reference); two searches run side by side
-// on two six-warp groups.  What does not depend on the left neighbour's
-// decision -- the source, the predictor's other inputs (row r-1 has finished
-// column c+1), the windows around the MB and their metrics -- comes before
-// the wait for the leader's decision of the previous MB.
-__device__ bool search_mb(const FrameArgs &a, int row, int col, int n, int ns, const int16_t *const ref[2],
-                          const int out[2])
+// Search k of search_mb: its state, its windows at the MB and at the
+// predictor, its prediction buffer.  Searches 0 and 1 use the forward and
+// backward resources; search 2 (a third reference) the intra search's state
+// and window 0 (unused on ranks 1 and 2), window 5 and the bi-prediction buffer.
+__device__ __forceinline__ int sm_srch(int k) { return k == 2 ? 0 : 1 + k; }
+__device__ __forceinline__ int sm_wa(int k) { return k == 2 ? 5 : 1 + 2 * k; }
+__device__ __forceinline__ int sm_wb(int k) { return k == 2 ? 0 : 2 + 2 * k; }
+__device__ __forceinline__ int sm_pred(int k) { return k == 2 ? 3 : 1 + k; }
+
+// The reference plane set of search k and its result slot in the leader's
+// inbox (0 forward / nearest, 1 backward / second, 2 third reference): with
+// bwd the backward search, else B frames' forward search or P frames' k-th
+// reference.
+__device__ __forceinline__ const int16_t *sm_ref(const FrameArgs &a, int k, bool bwd)
+{
+    return a.planes[bwd ? a.ref_bwd : (a.type == EVXG_FRAME_INTER ? a.ref_slot[k] : a.ref_fwd)];
+}
+__device__ __forceinline__ int sm_out(int k, bool bwd) { return bwd ? 1 : k; }
+
+// Ranks 1 and 2: ns inter searches of the n-th MB (see sm_ref), handed to the
+// leader's inbox (the caller releases the sequence flag); several searches
+// run side by side on equal warp groups.  What does not depend on the left
+// neighbour's decision -- the source, the predictor's other inputs (row r-1
+// has finished column c+1), the windows around the MB and their metrics --
+// comes before the wait for the leader's decision of the previous MB.
+__device__ bool search_mb(const FrameArgs &a, int row, int col, int n, int ns, bool bwd)
 {
     MbShared &S = SM();
     const int tid = threadIdx.x;
@@ -2120,21 +2135,21 @@ __device__ bool search_mb(const FrameArgs &a, int row, int col, int n, int ns, c
     if (tid == 0) {
         setup_mb(a, idx, px, py, false, nullptr);
         pred_gather(a, idx, a.type == EVXG_FRAME_INTER, S.pin);
-        for (int k = 0; k < ns; k++) req_window(1 + 2 * k, ref[k], px, py);
+        for (int k = 0; k < ns; k++) req_window(sm_wa(k), sm_ref(a, k, bwd), px, py);
     }
     __syncthreads();
     load_windows(a.W, a.H);
     __syncthreads();
-    const int k = ns == 2 && tid >= NT / 2 ? 1 : 0;   // this thread's search
-    const Grp g = ns == 2 ? Grp{5 + k, k * (NT / 2), NT / 2} : G_ALL;
-    first_candidates(g, a, 1 + k, 1 + 2 * k, 2 + 2 * k, px, py, true, false);
+    const int gsz = NT / ns, k = tid / gsz;   // this thread's search and its group (named barriers 5..7)
+    const Grp g = ns == 1 ? G_ALL : Grp{5 + k, k * gsz, gsz};
+    first_candidates(g, a, sm_srch(k), sm_wa(k), sm_wb(k), px, py, true, false);
     if (tid == 0) {
         S.row_abort = !wait_mail(&S.mail.dec_seq, n - 1, a);
         if (!S.row_abort) {
             set_predictor(a, idx, px, py, S.pin, col > 0 ? &S.mail.left.d : nullptr);
             S.req.n = 0;
             if (S.sep)
-                for (int j = 0; j < ns; j++) req_window(2 + 2 * j, ref[j], S.qx, S.qy);
+                for (int j = 0; j < ns; j++) req_window(sm_wb(j), sm_ref(a, j, bwd), S.qx, S.qy);
         }
     }
     __syncthreads();
@@ -2143,32 +2158,29 @@ __device__ bool search_mb(const FrameArgs &a, int row, int col, int n, int ns, c
         load_windows(a.W, a.H);
         __syncthreads();
     }
-    inter_search(g, a, 1 + k, 1 + 2 * k, 2 + 2 * k, px, py, S.pred[1 + k], true);
+    inter_search(g, a, sm_srch(k), sm_wa(k), sm_wb(k), px, py, S.pred[sm_pred(k)], true);
     __syncthreads();
     Inbox *in = peer(&S.mail.in[n & 1], 0);
     for (int j = 0; j < ns; j++) {
-        int16_t *to = out[j] == 0 ? in->f_pred : (out[j] == 1 ? in->b_pred : in->x_pred);
-        copy_block(to, S.pred[1 + j]);
+        const int o = sm_out(j, bwd);
+        int16_t *to = o == 0 ? in->f_pred : (o == 1 ? in->b_pred : in->x_pred);
+        copy_block(to, S.pred[sm_pred(j)]);
         if (tid == 0) {
-            Desc &d = out[j] == 0 ? in->f_out : (out[j] == 1 ? in->b_out : in->x_out);
-            int &sad = out[j] == 0 ? in->f_sad : (out[j] == 1 ? in->b_sad : in->x_sad);
-            d = S.srch[1 + j].out;
-            sad = S.srch[1 + j].out_sad;
+            Desc &d = o == 0 ? in->f_out : (o == 1 ? in->b_out : in->x_out);
+            int &sad = o == 0 ? in->f_sad : (o == 1 ? in->b_sad : in->x_sad);
+            d = S.srch[sm_srch(j)].out;
+            sad = S.srch[sm_srch(j)].out_sad;
         }
     }
     return true;
 }
 
-// Rank 1: the forward search (B frames), the nearest reference's (P frames),
-// and with three references also the third one's.
+// Rank 1: the forward search (B frames), or every reference's search (P
+// frames: one to three, side by side).
 __device__ bool fwd_mb(const FrameArgs &a, int row, int col, int n)
 {
     if (a.type == EVXG_FRAME_INTRA) return true;
-    const bool p = a.type == EVXG_FRAME_INTER;
-    const int ns = p && a.nref >= 3 ? 2 : 1;
-    const int16_t *const ref[2] = {a.planes[p ? a.ref_slot[0] : a.ref_fwd], a.planes[p ? a.ref_slot[2] : 0]};
-    const int out[2] = {0, 2};
-    if (!search_mb(a, row, col, n, ns, ref, out)) return false;
+    if (!search_mb(a, row, col, n, a.type == EVXG_FRAME_INTER ? a.nref : 1, false)) return false;
     __syncthreads();
     if (threadIdx.x == 0) st_release_cl(peer(&SM().mail.f_seq, 0), n);
     return true;
@@ -2179,14 +2191,9 @@ __device__ bool aux_mb(const FrameArgs &a, int row, int col, int n)   // rank 2
     MbShared &S = SM();
     const int tid = threadIdx.x;
     const int px = col * 16, py = row * 16;
-    // B frames: the backward search; P frames with several references: the
-    // second reference's search (window pair 1 / 2 of this CTA).
-    const bool searched = a.type == EVXG_FRAME_BIDIR || (a.type == EVXG_FRAME_INTER && a.nref >= 2);
-    if (searched) {
-        const int16_t *const ref[2] = {a.planes[a.type == EVXG_FRAME_BIDIR ? a.ref_bwd : a.ref_slot[1]], nullptr};
-        const int out[2] = {1, 1};
-        if (!search_mb(a, row, col, n, 1, ref, out)) return false;
-    }
+    // B frames: the backward search.
+    const bool searched = a.type == EVXG_FRAME_BIDIR;
+    if (searched && !search_mb(a, row, col, n, 1, true)) return false;
     // Directional intra reads row r-1 up to column c from the destination
     // slot (the search has waited for column c+1) and the right column of
     // MB (r, c-1), which the leader hands over in lcol with wr_seq.
