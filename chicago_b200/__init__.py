@@ -54,7 +54,8 @@ EXPORTS = [
     "evxg_server_create", "evxg_server_destroy", "evxg_server_open", "evxg_server_submit", "evxg_server_insert_intra",
     "evxg_server_close", "evxg_server_drain", "evxg_server_stats", "evxg_server_now_ns",
     "evxg_config_default", "evxg_stream_create_config", "evxg_stream_config", "evxg_encoder_create_config",
-    "evxg_server_open_config",
+    "evxg_server_open_config", "evxg_stream_set_timeout_ns", "evxg_stream_reset", "evxg_batch_set_timeout_ns",
+    "evxg_mb_pass_noalloc_set_timeout_ns", "evxg_server_cancel", "evxg_inject_alloc_failures",
 ]
 MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
 
@@ -109,6 +110,10 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_fetch_tables.argtypes = [vp, vp, vp, vp, vp, i32, vp]
     L.evxg_fetch_planes.argtypes = [vp, u32, vp, i32, vp]
     L.evxg_stream_sync.argtypes = [vp, vp]
+    L.evxg_stream_set_timeout_ns.argtypes = [vp, C.c_int64]
+    L.evxg_stream_reset.argtypes = [vp, vp]
+    L.evxg_batch_set_timeout_ns.argtypes = [vp, C.c_int64]
+    L.evxg_mb_pass_noalloc_set_timeout_ns.argtypes = [C.c_int64]
     L.evxg_last_launch_count.argtypes = [vp]
     L.evxg_last_launch_count.restype = u32
     L.evxg_stream_profile.argtypes = [vp, i32]
@@ -148,6 +153,8 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_server_insert_intra.argtypes = [vp, u32]
     L.evxg_server_close.argtypes = [vp, u32]
     L.evxg_server_drain.argtypes = [vp]
+    L.evxg_server_cancel.argtypes = [vp, u32]
+    L.evxg_inject_alloc_failures.argtypes = [u32]
     L.evxg_server_stats.argtypes = [vp] + [C.POINTER(u64)] * 4
     L.evxg_server_now_ns.restype = u64
     return L
@@ -224,6 +231,14 @@ class Stream:
 
     def sync(self, cuda_stream=None):
         _check(lib().evxg_stream_sync(self.h, _ptr(cuda_stream)))
+
+    def set_timeout_ns(self, ns: int):
+        """Bound on every device-side wait of this stream's kernels (5 s by default)."""
+        _check(lib().evxg_stream_set_timeout_ns(self.h, int(ns)))
+
+    def reset(self, cuda_stream=None):
+        """Back to the state at creation (zero DPB slots and tables)."""
+        _check(lib().evxg_stream_reset(self.h, _ptr(cuda_stream)))
 
     def fetch_tables(self, cuda_stream=None):
         bt = np.zeros(self.nblk * 28, np.uint8)
@@ -317,6 +332,9 @@ class Batch:
     def launch_count(self) -> int:
         return lib().evxg_batch_launch_count(self.h)
 
+    def set_timeout_ns(self, ns: int):
+        _check(lib().evxg_batch_set_timeout_ns(self.h, int(ns)))
+
     @property
     def shape(self):
         v = [C.c_int() for _ in range(3)]
@@ -386,6 +404,10 @@ class Server:
 
     def drain(self):
         _check(lib().evxg_server_drain(self.h))
+
+    def cancel(self, sid: int):
+        """Drop the stream's frames not yet in a tick; those in flight are delivered."""
+        _check(lib().evxg_server_cancel(self.h, sid))
 
     def stats(self) -> dict:
         v = [C.c_uint64() for _ in range(4)]

@@ -4,9 +4,11 @@
 // (src/video/evx3enc.cpp:35-414) on top of it.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -29,11 +31,29 @@ int cuda_fail(cudaError_t e, const char *where)
 }
 }  // namespace evxg
 
+// Host-side fault injection: the next n device allocations of stream
+// creation report cudaErrorMemoryAllocation without allocating.
+static std::atomic<uint32_t> g_inject_alloc{0};
+template <class T>
+static cudaError_t dev_alloc(T **p, size_t n)
+{
+    uint32_t k = g_inject_alloc.load();
+    while (k > 0)
+        if (g_inject_alloc.compare_exchange_weak(k, k - 1)) return cudaErrorMemoryAllocation;
+    return cudaMalloc(p, n);
+}
+
 extern "C" {
 
 float evxg_lambda(uint16_t q) { return 0.85f * powf(2.0f, ((float)q - 12.0f) / 3.0f); }   // common.h:264-266
 
 const char *evxg_last_error(void) { return g_last_error.c_str(); }
+
+int evxg_inject_alloc_failures(uint32_t n)
+{
+    g_inject_alloc.store(n);
+    return EVXG_SUCCESS;
+}
 
 void evxg_config_default(evxg_config *cfg)
 {
@@ -93,19 +113,19 @@ int evxg_stream_create_config(uint32_t width, uint32_t height, const evxg_config
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess) e = cudaMalloc(&s->src, pb);
-    if (e == cudaSuccess) e = cudaMalloc(&s->lev, pb);
-    for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaMalloc(&s->dpb[i], pb);
-    if (e == cudaSuccess) e = cudaMalloc(&s->bt, nblk * sizeof(evxg_block_desc));
-    if (e == cudaSuccess) e = cudaMalloc(&s->prev, nblk * sizeof(evxg_block_desc));
-    if (e == cudaSuccess) e = cudaMalloc(&s->prev_ser, nblk * sizeof(evxg_block_desc));
-    if (e == cudaSuccess) e = cudaMalloc(&s->sao, nblk * sizeof(evxg_sao_info));
-    if (e == cudaSuccess) e = cudaMalloc(&s->sao_cost, nblk * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&s->sao_orig, pb);
-    if (e == cudaSuccess) e = cudaMalloc(&s->sao_flags, kSaoPasses * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&s->sao_mail, nblk * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMalloc(&s->rgb, (size_t)width * height * 3);
-    if (e == cudaSuccess) e = cudaMalloc(&s->sync, (3 * s->mbh + 5) * sizeof(int));
+    if (e == cudaSuccess) e = dev_alloc(&s->src, pb);
+    if (e == cudaSuccess) e = dev_alloc(&s->lev, pb);
+    for (int i = 0; i < 4 && e == cudaSuccess; i++) e = dev_alloc(&s->dpb[i], pb);
+    if (e == cudaSuccess) e = dev_alloc(&s->bt, nblk * sizeof(evxg_block_desc));
+    if (e == cudaSuccess) e = dev_alloc(&s->prev, nblk * sizeof(evxg_block_desc));
+    if (e == cudaSuccess) e = dev_alloc(&s->prev_ser, nblk * sizeof(evxg_block_desc));
+    if (e == cudaSuccess) e = dev_alloc(&s->sao, nblk * sizeof(evxg_sao_info));
+    if (e == cudaSuccess) e = dev_alloc(&s->sao_cost, nblk * sizeof(float));
+    if (e == cudaSuccess) e = dev_alloc(&s->sao_orig, pb);
+    if (e == cudaSuccess) e = dev_alloc(&s->sao_flags, kSaoPasses * sizeof(int));
+    if (e == cudaSuccess) e = dev_alloc(&s->sao_mail, nblk * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = dev_alloc(&s->rgb, (size_t)width * height * 3);
+    if (e == cudaSuccess) e = dev_alloc(&s->sync, (3 * s->mbh + 5) * sizeof(int));
     // Zeroing on a private stream, synchronised alone: no device-wide
     // synchronisation, which another thread capturing a graph would forbid.
     cudaStream_t zs = nullptr;
@@ -157,6 +177,23 @@ int evxg_stream_dims(const evxg_stream *s, uint32_t *aw, uint32_t *ah, uint32_t 
 
 uint32_t evxg_last_launch_count(const evxg_stream *s) { return s ? s->launches : 0; }
 
+int evxg_stream_set_timeout_ns(evxg_stream *s, int64_t ns)
+{
+    if (!s || ns <= 0) return fail(EVXG_ERROR_INVALIDARG, "evxg_stream_set_timeout_ns: null stream or ns <= 0");
+    s->timeout_ns = ns;
+    return EVXG_SUCCESS;
+}
+
+int evxg_stream_reset(evxg_stream *s, void *cuda_stream)
+{
+    if (!s) return fail(EVXG_ERROR_INVALIDARG, "evxg_stream_reset: null stream");
+    const cudaStream_t st = (cudaStream_t)cuda_stream;
+    const int rc = reset_stream(s, st);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(st));
+    return EVXG_SUCCESS;
+}
+
 int evxg_stream_set_mb_form(evxg_stream *s, int form)
 {
     if (!s || (form != EVXG_MB_FORM_SINGLE && form != EVXG_MB_FORM_CLUSTER))
@@ -192,13 +229,8 @@ int evxg::reset_stream(evxg_stream *s, cudaStream_t st)
 // Shared-memory limits of the macroblock kernels (once per process and device)
 // and the number of three-CTA clusters the device co-schedules; 0 when the
 // cluster form cannot run.
-int evxg::max_active_clusters()
+static int cluster_setup()   // with the device current, once per device
 {
-    static int cached[64];
-    static bool done[64];
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
-    if (done[dev]) return cached[dev];
     const int smem = (int)mb_shared_bytes();
     cudaFuncSetAttribute(k_sao_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(k_deblock, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -218,8 +250,16 @@ int evxg::max_active_clusters()
         if (cudaOccupancyMaxActiveClusters(&n, (void *)k_mb_cluster, &cfg) != cudaSuccess) n = 0;
     }
     cudaGetLastError();   // the cluster form is optional: fall back to one CTA per row
-    cached[dev] = n; done[dev] = true;
     return n;
+}
+int evxg::max_active_clusters()
+{
+    static int cached[64];
+    static std::once_flag once[64];   // streams may be created on several threads at once
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    std::call_once(once[dev], [&] { cached[dev] = cluster_setup(); });
+    return cached[dev];
 }
 
 // Frame descriptor checks shared by the single and the batched path.  Without

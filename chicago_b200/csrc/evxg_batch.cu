@@ -337,6 +337,13 @@ int evxg_batch_encode(evxg_batch *b, const evxg_frame *frames, uint32_t parity, 
 
 uint32_t evxg_batch_launch_count(const evxg_batch *b) { return b ? (uint32_t)kTickKernels : 0; }
 
+int evxg_batch_set_timeout_ns(evxg_batch *b, int64_t ns)
+{
+    if (!b || ns <= 0) return fail(EVXG_ERROR_INVALIDARG, "evxg_batch_set_timeout_ns: null batch or ns <= 0");
+    b->timeout_ns = ns;   // copied into every stream's parameters at the next tick
+    return EVXG_SUCCESS;
+}
+
 int evxg_batch_set_shape(evxg_batch *b, int form, int grid, int policy)
 {
     if (!b || (form != EVXG_MB_FORM_SINGLE && form != EVXG_MB_FORM_CLUSTER) || grid < 1 || policy < 0 || policy > 1)

@@ -351,6 +351,20 @@ int evxg_server_close(evxg_server *v, uint32_t stream_id)
     return rc;
 }
 
+int evxg_server_cancel(evxg_server *v, uint32_t stream_id)
+{
+    if (!v) return EVXG_ERROR_INVALIDARG;
+    std::lock_guard<std::mutex> lk(v->mu);
+    auto it = v->slots.find(stream_id);
+    if (it == v->slots.end() || it->second->closing) return fail(EVXG_ERROR_INVALID_INDEX, "evxg_server_cancel: no such open stream");
+    Slot *s = it->second;
+    s->ready.clear();     // frames not yet in a tick are dropped; those in flight are delivered
+    s->arrival.clear();
+    s->closing = true;    // no flush: frames still waiting for their anchor are dropped too
+    v->cv_work.notify_all();
+    return EVXG_SUCCESS;
+}
+
 int evxg_server_drain(evxg_server *v)
 {
     if (!v) return EVXG_ERROR_INVALIDARG;

@@ -172,6 +172,21 @@ int evxg_fetch_planes(evxg_stream *s, uint32_t slot, int16_t *out, int to_device
  * up waiting (EVXG_ERROR_OPERATION_TIMEDOUT) or a launch failed. */
 int evxg_stream_sync(evxg_stream *s, void *cuda_stream);
 
+/* Failure detection (no counterpart in the reference, whose WPP threads wait
+ * for each other without a bound, encode.cpp:866-877).  Every wait of a
+ * stream's kernels on other CTAs -- wavefront progress, the cluster form's
+ * hand-over, the SAO merge and raster-order application -- gives up after
+ * timeout_ns, sets the stream's device error word and lets every CTA of the
+ * frame run to its end; evxg_stream_sync (and evxg_fetch_* with host
+ * destinations) then return EVXG_ERROR_OPERATION_TIMEDOUT and clear the
+ * word.  The frame's results and the stream's reference state are undefined
+ * after that: evxg_stream_reset returns the stream to its state at creation
+ * (what the reference's clear() does to its context, evx3enc.cpp:35-55), so
+ * the next frame should be an intra frame.  The default bound is 5 s;
+ * ns must be > 0. */
+int evxg_stream_set_timeout_ns(evxg_stream *s, int64_t ns);
+int evxg_stream_reset(evxg_stream *s, void *cuda_stream);
+
 /* Number of kernels launched by the last evxg_encode_frame call. */
 uint32_t evxg_last_launch_count(const evxg_stream *s);
 
@@ -227,6 +242,10 @@ int evxg_batch_encode(evxg_batch *b, const evxg_frame *frames, uint32_t parity, 
 int evxg_batch_wait(evxg_batch *b, uint32_t parity);
 int evxg_batch_output(evxg_batch *b, uint32_t i, uint32_t parity, const evxg_block_desc **blocks,
                       const evxg_block_desc **prev_blocks, const evxg_sao_info **sao, const int16_t **levels);
+/* The wait bound of the batch's ticks (see evxg_stream_set_timeout_ns); one
+ * wait that gives up fails the whole tick (evxg_batch_wait returns
+ * EVXG_ERROR_OPERATION_TIMEDOUT) and leaves every stream of it to be reset. */
+int evxg_batch_set_timeout_ns(evxg_batch *b, int64_t ns);
 /* Kernels one tick launches (the same for any number of streams). */
 uint32_t evxg_batch_launch_count(const evxg_batch *b);
 /* Shape of the tick's macroblock pass: form (EVXG_MB_FORM_*), persistent grid
@@ -283,8 +302,19 @@ int evxg_server_submit(evxg_server *srv, uint32_t stream_id, const uint8_t *rgb,
 int evxg_server_insert_intra(evxg_server *srv, uint32_t stream_id);
 int evxg_server_close(evxg_server *srv, uint32_t stream_id);
 int evxg_server_drain(evxg_server *srv);
+/* Cancel a stream mid-GOP: frames submitted but not yet in a tick (and those
+ * still waiting for their anchor) are dropped without being encoded, frames
+ * already in a tick are delivered, and the stream's memory is released like a
+ * closed stream's.  The other streams' results are not affected. */
+int evxg_server_cancel(evxg_server *srv, uint32_t stream_id);
 int evxg_server_stats(evxg_server *srv, uint64_t *frames, uint64_t *ticks, uint64_t *rebuilds, uint64_t *bytes_in_use);
 uint64_t evxg_server_now_ns(void);
+
+/* Host-side fault injection for tests of callers' error paths (no counterpart
+ * in the reference): the next n device allocations made when a stream is
+ * created fail as if the device were out of memory (the creation returns
+ * EVXG_ERROR_OUTOFMEMORY and frees what it had), without allocating. */
+int evxg_inject_alloc_failures(uint32_t n);
 
 /* lambda = 0.85 * 2^((q-12)/3) in float, as the reference computes it (common.h:264-266). */
 float evxg_lambda(uint16_t quality);
@@ -320,6 +350,10 @@ const char *evxg_last_error(void);
 int evxg_mb_pass_noalloc(uint32_t aligned_w, uint32_t aligned_h, const evxg_frame *frame, const int16_t *src,
                          int16_t *const dpb[4], int16_t *levels, evxg_block_desc *blocks,
                          const evxg_block_desc *prev_blocks, void *cuda_stream);
+/* The wait bound of evxg_mb_pass_noalloc's wavefront (see
+ * evxg_stream_set_timeout_ns), for every later call in the process; 5 s by
+ * default, ns > 0. */
+int evxg_mb_pass_noalloc_set_timeout_ns(int64_t ns);
 
 /* ---- GOP-level encoder: evx3_encoder (evx3.h:67-100) over the stream API ---- */
 

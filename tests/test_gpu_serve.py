@@ -87,3 +87,78 @@ def test_server_admission_by_memory_budget():
     assert len(srv.results[a]) == 1 and len(srv.results[c]) == 1 and len(srv.results[b]) == 0
     assert srv.stats()["bytes_in_use"] == 0
     srv.close()
+
+
+@pytest.mark.timeout(300)
+def test_server_admission_survives_allocation_failure():
+    """Host-side fault injection: a device allocation fails while a stream is
+    admitted.  The admission reports EVXG_ERROR_OUTOFMEMORY and gives its
+    budget reservation back; the stream already running is unaffected and a
+    later admission succeeds."""
+    import chicago_b200 as cb
+    srv = cb.Server(hbm_budget_bytes=1 << 34, max_streams=4)
+    fa = generate(96, 64, 6, seed=51, vmax=4.0)
+    fb = generate(64, 48, 5, seed=52, vmax=3.0)
+    a = srv.open(96, 64, 8)
+    for f in fa[:3]:
+        srv.submit(a, f)
+    used = srv.stats()["bytes_in_use"]
+    cb.lib().evxg_inject_alloc_failures(1)   # the next stream creation's first device allocation fails
+    with pytest.raises(cb.EvxgError) as e:
+        srv.open(64, 48, 8)
+    assert e.value.code == 3                  # EVXG_ERROR_OUTOFMEMORY
+    assert srv.stats()["bytes_in_use"] == used
+    for f in fa[3:]:
+        srv.submit(a, f)
+    b = srv.open(64, 48, 8)                   # no failure pending: admitted
+    for f in fb:
+        srv.submit(b, f)
+    srv.close_stream(a)
+    srv.close_stream(b)
+    srv.drain()
+    for sid, frames in ((a, fa), (b, fb)):
+        want = alone(*((96, 64) if sid == a else (64, 48)), 8, frames, ())
+        got = srv.results[sid]
+        assert len(got) == len(want)
+        for g, w_ in zip(got, want):
+            assert g["frame18"] == w_["frame18"]
+            for key in ("blocks", "prev_blocks", "sao", "levels"):
+                assert np.array_equal(g[key], w_[key])
+    assert srv.stats()["bytes_in_use"] == 0
+    srv.close()
+
+
+@pytest.mark.timeout(300)
+def test_server_cancel_mid_gop_leaves_other_streams_alone():
+    """A stream cancelled in the middle of its GOP: what it got delivered is a
+    prefix of its results alone; the other streams' results equal theirs alone."""
+    import chicago_b200 as cb
+    srv = cb.Server(hbm_budget_bytes=1 << 34, max_streams=4)
+    spec = [(96, 64, 8, 10), (64, 48, 4, 10), (80, 48, 12, 9)]
+    seqs = [generate(w, h, n, seed=60 + k, vmax=4.0) for k, (w, h, q, n) in enumerate(spec)]
+    ids = [srv.open(w, h, q) for (w, h, q, n) in spec]
+    for t in range(10):
+        for k, (w, h, q, n) in enumerate(spec):
+            if k == 1 and t == 6:
+                srv.cancel(ids[1])            # mid-GOP: its last frames wait for their P anchor
+            if t < n and not (k == 1 and t >= 6):
+                srv.submit(ids[k], seqs[k][t])
+        time.sleep(0.002)
+    for k in (0, 2):
+        srv.close_stream(ids[k])
+    srv.drain()
+    for k, (w, h, q, n) in enumerate(spec):
+        want = alone(w, h, q, seqs[k] if k != 1 else seqs[k][:n], ())
+        got = srv.results[ids[k]]
+        if k == 1:
+            assert len(got) <= 6
+        else:
+            assert len(got) == len(want) == n
+        for i, g in enumerate(got):
+            assert g["frame18"] == want[i]["frame18"], f"stream {k} record {i}"
+            for key in ("blocks", "prev_blocks", "sao", "levels"):
+                assert np.array_equal(g[key], want[i][key]), f"stream {k} record {i}: {key}"
+    with pytest.raises(cb.EvxgError):
+        srv.submit(ids[1], seqs[1][0])       # a cancelled stream takes no more frames
+    assert srv.stats()["bytes_in_use"] == 0
+    srv.close()
