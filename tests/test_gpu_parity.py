@@ -4,6 +4,8 @@ reference encoder (GPU tables serialized by the reference's entropy coder).
 
 Bit-exact is the bar: integer pixel work, mode decisions, motion vectors,
 levels and the float RD costs (no FMA contraction, same operation order)."""
+import functools
+
 import numpy as np
 import pytest
 
@@ -28,20 +30,38 @@ CASES = [  # (w, h, frames, quality, vmax, intra_at)
 FORMS = ("cluster", "single")   # three CTAs per macroblock row / one
 
 
-def check_stream(oracle, w, h, T, q, vmax, intra_at, form="cluster", cfg="default", seed=None):
+def clip(w, h, T, vmax, seed=None, window=None):
+    """The seeded test content; window=(first, cut) takes frames first.. of a
+    longer sequence with a scene cut (the benchmark's generator)."""
+    if window is None:
+        return generate(w, h, T, seed=w * 7 + h if seed is None else seed, vmax=vmax)
+    first, cut = window
+    return generate(w, h, first + T, seed=seed, vmax=vmax, n_rects=4, cut_at=cut)[first:]
+
+
+@functools.lru_cache(maxsize=8)
+def oracle_run(w, h, T, q, vmax, intra_at, cfg, seed=None, window=None):
+    """The oracle's stage dumps of a clip (cached: the large cases serve both
+    macroblock-pass forms)."""
+    import chicago_b200 as cb
+    from oracle_py import Oracle
+    b_frames, ref_count, radius = cb.CONFIGS[cfg]
+    frames = clip(w, h, T, vmax, seed, window)
+    oc = Oracle().context(w, h, b_frames=b_frames, ref_count=ref_count, radius=radius)
+    plan = plan_gop(T, quality=q, intra_at=intra_at) if b_frames else plan_ip(T, q, intra_at, ref_count)
+    return frames, [(ti, f18, oc.encode_frame(frames[ti], f18)) for ti, f18 in plan]
+
+
+def check_stream(oracle, w, h, T, q, vmax, intra_at, form="cluster", cfg="default", seed=None, window=None):
     """Encode a seeded clip through the C ABI and compare every stage of every
     frame with the oracle restating the same reference build (cfg: "default",
     or the I/P builds "ip1" / "ip3")."""
     import chicago_b200 as cb
-    b_frames, ref_count, radius = cb.CONFIGS[cfg]
-    frames = generate(w, h, T, seed=w * 7 + h if seed is None else seed, vmax=vmax)
-    oc = oracle.context(w, h, b_frames=b_frames, ref_count=ref_count, radius=radius)
+    frames, runs = oracle_run(w, h, T, q, vmax, tuple(intra_at), cfg, seed, window)
     st = cb.Stream(w, h, cfg)
     st.mb_form = cb.MB_FORM_CLUSTER if form == "cluster" else cb.MB_FORM_SINGLE
-    plan = plan_gop(T, quality=q, intra_at=intra_at) if b_frames else plan_ip(T, q, intra_at, ref_count)
-    for k, (ti, f18) in enumerate(plan):
+    for k, (ti, f18, od) in enumerate(runs):
         fr = unpack_frame(f18)
-        od = oc.encode_frame(frames[ti], f18)
         st.encode_frame(frames[ti], f18)
         tb = st.fetch_tables()
         bad = compare_blocks(tb["blocks"], od.blocks)
@@ -87,6 +107,38 @@ def test_gpu_matches_oracle_ip(oracle, cfg, w, h, T, q, vmax, intra_at, seed, fo
 def test_gpu_matches_oracle_ip3_1080p(oracle, form):
     """Full-size I/P frames with three references: I and three P frames."""
     check_stream(oracle, 1920, 1080, 4, 8, 24.0, (), form, "ip3")
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_gpu_matches_oracle_4k(oracle, form):
+    """3840x2160 (240x135 MBs), the served form's largest size: I, P,
+    reference-B and B frames of the default build."""
+    check_stream(oracle, 3840, 2160, 4, 8, 24.0, (), form, seed=4321)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_gpu_matches_oracle_ip3_4k(oracle, form):
+    """3840x2160 I/P frames with three references: I and two P frames."""
+    check_stream(oracle, 3840, 2160, 3, 8, 24.0, (), form, "ip3", seed=4322)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("q", [4, 16])
+def test_gpu_matches_oracle_1080p_scene_cut(oracle, q, form):
+    """The benchmark's 1080p content around its scene cut (frames 58-62, cut at
+    60) at quality 4 and 16, I/P with three references: I 58, P 59, the cut's
+    I 60, P 61, P 62."""
+    check_stream(oracle, 1920, 1080, 5, q, 24.0, (2,), form, "ip3", seed=1000, window=(58, 60))
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_gpu_matches_oracle_wide_frames(oracle, form):
+    """Frames wider than the filters' shared-memory paths: at 16400 px the
+    deblocking strips exceed their shared-memory window (in-place form); at
+    54640 x 528 the SAO merge's hand-over words exceed shared memory too
+    (memory-word form)."""
+    check_stream(oracle, 16400, 32, 3, 8, 6.0, (), form, seed=77)
+    check_stream(oracle, 54640, 528, 1, 8, 6.0, (), form, seed=78)
 
 
 @pytest.mark.parametrize("variant", ["ip1", "ip3"])
