@@ -56,6 +56,7 @@ EXPORTS = [
     "evxg_config_default", "evxg_stream_create_config", "evxg_stream_config", "evxg_encoder_create_config",
     "evxg_server_open_config", "evxg_stream_set_timeout_ns", "evxg_stream_reset", "evxg_batch_set_timeout_ns",
     "evxg_mb_pass_noalloc_set_timeout_ns", "evxg_server_cancel", "evxg_inject_alloc_failures",
+    "evxg_serialize_slice", "evxg_stream_header", "evxg_encoder_set_output",
 ]
 MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
 
@@ -78,6 +79,7 @@ def config(name_or_tuple="default") -> Config:
     return Config(v[0], v[1], v[2], 0)
 
 FRAME_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
+BYTES_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_uint64)
 
 
 class FrameTimes(C.Structure):
@@ -129,6 +131,7 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_encoder_encode.argtypes = [vp, vp, u32, u32]
     L.evxg_encoder_stream.argtypes = [vp]
     L.evxg_encoder_stream.restype = vp
+    L.evxg_encoder_set_output.argtypes = [vp, BYTES_CB, vp]
     L.evxg_mb_pass_noalloc.argtypes = [u32, u32, C.c_char_p, vp, C.POINTER(vp), vp, vp, vp, vp]
     L.evxg_stream_set_mb_form.argtypes = [vp, i32]
     L.evxg_stream_mb_form.argtypes = [vp]
@@ -155,6 +158,9 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_server_drain.argtypes = [vp]
     L.evxg_server_cancel.argtypes = [vp, u32]
     L.evxg_inject_alloc_failures.argtypes = [u32]
+    L.evxg_serialize_slice.argtypes = [C.POINTER(Config), u32, u32, C.c_char_p, vp, vp, vp, vp, vp, u64,
+                                       C.POINTER(u64)]
+    L.evxg_stream_header.argtypes = [C.POINTER(Config), u32, u32, vp]
     L.evxg_server_stats.argtypes = [vp] + [C.POINTER(u64)] * 4
     L.evxg_server_now_ns.restype = u64
     return L
@@ -192,6 +198,26 @@ def lam(quality: int) -> float:
 def pack_frame(ftype, index, quality, display_order, is_reference, dpb_slot, ref_fwd, ref_bwd) -> bytes:
     """18-byte evx_frame (reference src/video/common.h:72-87)."""
     return struct.pack("<iIHIBBBB", ftype, index, quality, display_order, is_reference, dpb_slot, ref_fwd, ref_bwd)
+
+
+def serialize_slice(cfg, aligned_w: int, aligned_h: int, frame18: bytes, blocks, prev_blocks, sao, levels) -> bytes:
+    """The frame's slice bytes from its tables (host entropy coder, evxg_serialize_slice)."""
+    c = config(cfg)
+    cap = max(1 << 16, aligned_w * aligned_h * 4)
+    out = np.empty(cap, np.uint8)
+    n = C.c_uint64(0)
+    _check(lib().evxg_serialize_slice(C.byref(c), aligned_w, aligned_h, frame18, _ptr(np.ascontiguousarray(blocks)),
+                                      _ptr(np.ascontiguousarray(prev_blocks)), _ptr(np.ascontiguousarray(sao)),
+                                      _ptr(np.ascontiguousarray(levels)), _ptr(out), cap, C.byref(n)))
+    return out[:n.value].tobytes()
+
+
+def stream_header(cfg, width: int, height: int) -> bytes:
+    """The 14-byte stream header (evxg_stream_header)."""
+    c = config(cfg)
+    out = np.zeros(14, np.uint8)
+    _check(lib().evxg_stream_header(C.byref(c), width, height, _ptr(out)))
+    return out.tobytes()
 
 
 class Stream:
@@ -433,13 +459,18 @@ class Server:
 class Encoder:
     """evx3_encoder mirror: frames in, per-frame table records out (bitstream order)."""
 
-    def __init__(self, quality: int | None = None, cfg="default"):
+    def __init__(self, quality: int | None = None, cfg="default", bitstream: bool = False):
+        """bitstream=True: the encoder also emits the .evx stream into self.stream."""
         self.records = []
+        self.stream = bytearray()
         self.cfg = config(cfg)
         self._cb = FRAME_CB(self._on_frame)
         h = C.c_void_p()
         _check(lib().evxg_encoder_create_config(self._cb, None, C.byref(self.cfg), C.byref(h)))
         self.h = h
+        if bitstream:
+            self._out = BYTES_CB(lambda user, p, n: self.stream.extend(C.string_at(p, n)))
+            _check(lib().evxg_encoder_set_output(self.h, self._out, None))
         if quality is not None:
             self.set_quality(quality)
 

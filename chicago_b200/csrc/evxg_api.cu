@@ -470,6 +470,11 @@ struct evxg_encoder {
     // it for a batched tick; the encoder then has no stream of its own).
     evxg::FrameSink sink = nullptr;
     void *sink_ctx = nullptr;
+    // Bitstream output (evxg_encoder_set_output): the stream's bytes in order.
+    evxg_bytes_callback out_cb = nullptr;
+    void *out_user = nullptr;
+    bool header_done = false;
+    std::vector<uint8_t> slice;
 };
 
 void evxg::encoder_set_sink(evxg_encoder *e, FrameSink sink, void *ctx) { e->sink = sink; e->sink_ctx = ctx; }
@@ -491,6 +496,26 @@ static int encode_one(evxg_encoder *e, const uint8_t *px, const evxg_frame &f)
     rc = evxg_fetch_tables(e->stream, e->h_bt.data(), e->h_prev.data(), e->h_sao.data(), e->h_lev.data(), 0, nullptr);
     if (rc) return rc;
     if (e->cb) e->cb(e->user, &f, e->h_bt.data(), e->h_prev.data(), e->h_sao.data(), e->h_lev.data());
+    if (e->out_cb) {   // the reference's bytes for this frame (evx3enc.cpp:137-160, :249-277)
+        if (!e->header_done) {
+            uint8_t h[14];
+            if ((rc = evxg_stream_header(&e->cfg, e->width, e->height, h))) return rc;
+            e->out_cb(e->out_user, h, sizeof h);
+            e->header_done = true;
+        }
+        const size_t fb = e->cfg.b_frames ? sizeof(evxg_frame) : 10, pre = e->cfg.b_frames ? 4 : 0;
+        if (e->slice.size() < (size_t)e->stream->W * e->stream->H * 4) e->slice.resize((size_t)e->stream->W * e->stream->H * 4);
+        uint64_t n = 0;
+        rc = evxg_serialize_slice(&e->cfg, e->stream->W, e->stream->H, &f, e->h_bt.data(), e->h_prev.data(),
+                                  e->h_sao.data(), e->h_lev.data(), e->slice.data() + pre + fb, e->slice.size() - pre - fb, &n);
+        if (rc) return rc;
+        if (pre) {   // default build: a 4-byte size before the frame record
+            const uint32_t size = (uint32_t)(fb + n);
+            memcpy(e->slice.data(), &size, 4);
+        }
+        memcpy(e->slice.data() + pre, &f, fb);   // evx_frame of the build: the first fb bytes
+        e->out_cb(e->out_user, e->slice.data(), pre + fb + n);
+    }
     return EVXG_SUCCESS;
 }
 
@@ -574,6 +599,7 @@ int evxg_encoder_clear(evxg_encoder *e)   // evx3enc.cpp:35-55
     if (!e) return EVXG_ERROR_INVALIDARG;
     if (e->stream) evxg_stream_destroy(e->stream);
     e->stream = nullptr;
+    e->header_done = false;   // the next frame starts a new stream
     clear_frame(e->frame);
     e->reorder_count = 0; e->display_counter = 0; e->ip_index = 0; e->first = true;
     return EVXG_SUCCESS;
@@ -604,6 +630,15 @@ int evxg_encoder_set_quality(evxg_encoder *e, uint8_t q)   // evx3enc.cpp:64-82
 }
 
 evxg_stream *evxg_encoder_stream(evxg_encoder *e) { return e ? e->stream : nullptr; }
+
+int evxg_encoder_set_output(evxg_encoder *e, evxg_bytes_callback cb, void *user)
+{
+    if (!e) return fail(EVXG_ERROR_INVALIDARG, "evxg_encoder_set_output: null encoder");
+    if (e->sink) return fail(EVXG_ERROR_INVALID_RESOURCE, "evxg_encoder_set_output: a served stream's encoder has no output");
+    e->out_cb = cb;
+    e->out_user = user;
+    return EVXG_SUCCESS;
+}
 
 int evxg_encoder_encode(evxg_encoder *e, const uint8_t *rgb, uint32_t width, uint32_t height)
 {

@@ -319,6 +319,33 @@ int evxg_inject_alloc_failures(uint32_t n);
 /* lambda = 0.85 * 2^((q-12)/3) in float, as the reference computes it (common.h:264-266). */
 float evxg_lambda(uint16_t quality);
 
+/* ---- Host entropy coder ----
+ *
+ * The part of engine_encode_frame that stays on the CPU: serialize_slice
+ * (serialize.cpp:624-686) -- the block table (block types, intra modes with
+ * most-probable-mode prediction, prediction targets, motion-vector
+ * differences, sub-pel fields, QP deltas), the SAO table and the residual
+ * levels (significance maps in scan order), all through the adaptive binary
+ * arithmetic coder (abac.cpp) with exponential-Golomb binarisation
+ * (golomb.cpp, stream.cpp:996-1075).  The inputs are exactly what
+ * evxg_fetch_tables returns for the frame (host memory), for a stream of the
+ * build cfg describes (NULL = default); the output is the frame's slice
+ * bytes, identical to the reference's, byte-aligned.  *out_len receives the
+ * size even when capacity is too small (EVXG_ERROR_CAPACITY_LIMIT).  Keeps no
+ * state: slices of different frames may be coded on different threads at once. */
+int evxg_serialize_slice(const evxg_config *cfg, uint32_t aligned_w, uint32_t aligned_h, const evxg_frame *frame,
+                         const evxg_block_desc *blocks, const evxg_block_desc *prev_blocks, const evxg_sao_info *sao,
+                         const int16_t *levels, uint8_t *out, uint64_t capacity, uint64_t *out_len);
+/* The 14-byte stream header (evx_header, common.h:55-64) for visible size
+ * width x height: "EVX1", size 14, DPB slot count, version 3.11, width,
+ * height; its padding byte (offset 7) is 0 (the reference leaves it
+ * uninitialised).  A stream is the header followed, per frame in bitstream
+ * order, by -- default build -- a 4-byte little-endian size and that many
+ * bytes: the 18-byte evxg_frame and the slice (evx3enc.cpp:249-277), or --
+ * without B frames -- the first 10 bytes of evxg_frame and the slice
+ * (evx3enc.cpp:141-147). */
+int evxg_stream_header(const evxg_config *cfg, uint32_t width, uint32_t height, uint8_t out[14]);
+
 /* Human-readable text of the last error on this thread. */
 const char *evxg_last_error(void);
 
@@ -378,6 +405,14 @@ int evxg_encoder_encode(evxg_encoder *e, const uint8_t *rgb, uint32_t width, uin
 int evxg_encoder_flush(evxg_encoder *e);                     /* evx3enc.cpp:385-414 */
 /* The stream under an encoder (NULL before the first frame). */
 evxg_stream *evxg_encoder_stream(evxg_encoder *e);
+/* Bitstream output: once set, the encoder also codes every frame on the host
+ * (evxg_serialize_slice) and hands the stream's bytes to cb in order, on the
+ * calling thread -- the 14-byte header before the first frame, then each
+ * frame's record (see evxg_stream_header) -- the bytes the reference's
+ * encode / flush write into their bit_stream (evx3enc.cpp:105-414).  cb NULL
+ * turns it off. */
+typedef void (*evxg_bytes_callback)(void *user, const uint8_t *bytes, uint64_t n);
+int evxg_encoder_set_output(evxg_encoder *e, evxg_bytes_callback cb, void *user);
 
 #ifdef __cplusplus
 }

@@ -227,3 +227,29 @@ def test_deterministic_repeat():
     for a, b in zip(*res):
         for key in a:
             assert np.array_equal(a[key], b[key])
+
+
+@pytest.mark.parametrize("cfg", ["default", "ip1", "ip3"])
+def test_encoder_bitstream_equals_stock_stream(cfg):
+    """The GOP-level encoder with its bitstream output on: GPU pixel pipeline,
+    then the library's own host entropy coder -- no reference code -- give the
+    stock encoder's .evx stream byte for byte (but the header's padding byte,
+    which the reference leaves uninitialised)."""
+    import os
+    import chicago_b200 as cb
+    path = REF_VARIANTS[cfg][0] if cfg != "default" else None
+    if path and not os.path.exists(path):
+        pytest.skip(f"reference variant {cfg} not built")
+    ref = Ref(variant=None if cfg == "default" else cfg)
+    w, h, T, q = 160, 96, 11, 8
+    frames = generate(w, h, T, seed=12, vmax=6.0)
+    stock = ref.encode_stream(frames, quality=q, intra_at=(6,))
+    enc = cb.Encoder(quality=q, cfg=cfg, bitstream=True)
+    for t in range(T):
+        if t == 6:
+            enc.insert_intra()
+        enc.encode(frames[t])
+    enc.flush()
+    mine = bytes(enc.stream)
+    assert len(mine) == len(stock)
+    assert mine[:7] == stock[:7] and mine[8:] == stock[8:]
