@@ -227,15 +227,17 @@ class Ref:
         L.evxref_enc_encode.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
                                         C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]
         L.evxref_enc_flush.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]
-        L.evxref_ctx_create.restype = C.c_void_p
-        L.evxref_ctx_create.argtypes = [C.c_uint32, C.c_uint32]
-        L.evxref_ctx_destroy.argtypes = [C.c_void_p]
-        L.evxref_ctx_encode_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
-                                              C.c_char_p, C.c_int] + [C.c_void_p] * 8 + \
-                                             [C.c_uint32, C.POINTER(C.c_uint32)]
-        L.evxref_ctx_serialize.argtypes = [C.c_void_p, C.c_char_p] + [C.c_void_p] * 5 + \
-                                          [C.c_uint32, C.POINTER(C.c_uint32)]
-        L.evxref_ctx_get_slot.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        self.staged = hasattr(L, "evxref_ctx_create")   # builds without encode.cpp have the stock API only
+        if self.staged:
+            L.evxref_ctx_create.restype = C.c_void_p
+            L.evxref_ctx_create.argtypes = [C.c_uint32, C.c_uint32]
+            L.evxref_ctx_destroy.argtypes = [C.c_void_p]
+            L.evxref_ctx_encode_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                                  C.c_char_p, C.c_int] + [C.c_void_p] * 8 + \
+                                                 [C.c_uint32, C.POINTER(C.c_uint32)]
+            L.evxref_ctx_serialize.argtypes = [C.c_void_p, C.c_char_p] + [C.c_void_p] * 5 + \
+                                              [C.c_uint32, C.POINTER(C.c_uint32)]
+            L.evxref_ctx_get_slot.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
         L.evxref_lambda.restype = C.c_float
         L.evxref_lambda.argtypes = [C.c_uint16]
 

@@ -144,6 +144,7 @@ int evxref_enc_flush(void *p, uint8_t *out, uint32_t cap, uint32_t *out_len)
     return 0;
 }
 
+#ifndef EVXREF_STOCK_ONLY   /* the staged driver needs encode.cpp; builds without it keep the stock API */
 /* ---------------- 2. staged per-frame driver ---------------- */
 
 struct evxref_ctx {
@@ -282,6 +283,8 @@ int evxref_ctx_get_slot(void *p, uint32_t slot, int16_t *out)
     copy_set(c->ctx.cache_bank.prediction_cache[slot], out, c->w, c->h);
     return 0;
 }
+
+#endif /* EVXREF_STOCK_ONLY */
 
 float evxref_lambda(uint16_t q) { return compute_lambda(q); }
 
