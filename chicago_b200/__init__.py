@@ -56,7 +56,7 @@ EXPORTS = [
     "evxg_config_default", "evxg_stream_create_config", "evxg_stream_config", "evxg_encoder_create_config",
     "evxg_server_open_config", "evxg_stream_set_timeout_ns", "evxg_stream_reset", "evxg_batch_set_timeout_ns",
     "evxg_mb_pass_noalloc_set_timeout_ns", "evxg_server_cancel", "evxg_inject_alloc_failures",
-    "evxg_serialize_slice", "evxg_stream_header", "evxg_encoder_set_output",
+    "evxg_serialize_slice", "evxg_stream_header", "evxg_encoder_set_output", "evxg_server_create_lanes",
 ]
 MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
 
@@ -149,6 +149,7 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_batch_autotune.argtypes = [vp, vp, C.POINTER(C.c_float)]
     u64 = C.c_uint64
     L.evxg_server_create.argtypes = [u64, u32, RESULT_CB, vp, C.POINTER(vp)]
+    L.evxg_server_create_lanes.argtypes = [u64, u32, u32, RESULT_CB, vp, C.POINTER(vp)]
     L.evxg_server_destroy.argtypes = [vp]
     L.evxg_server_open.argtypes = [vp, u32, u32, C.c_uint8, C.POINTER(u32)]
     L.evxg_server_open_config.argtypes = [vp, u32, u32, C.c_uint8, C.POINTER(Config), C.POINTER(u32)]
@@ -385,7 +386,7 @@ class Server:
     frame18 and times (arrival, ready, launch, done in ns), plus the
     serializer's tables when keep_tables is set."""
 
-    def __init__(self, hbm_budget_bytes: int, max_streams: int, keep_tables: bool = True):
+    def __init__(self, hbm_budget_bytes: int, max_streams: int, keep_tables: bool = True, lanes: int | None = None):
         import threading
         self.keep_tables = keep_tables
         self.results = {}
@@ -393,7 +394,11 @@ class Server:
         self._lock = threading.Lock()
         self._cb = RESULT_CB(self._on_result)
         h = C.c_void_p()
-        _check(lib().evxg_server_create(int(hbm_budget_bytes), int(max_streams), self._cb, None, C.byref(h)))
+        if lanes is None:
+            _check(lib().evxg_server_create(int(hbm_budget_bytes), int(max_streams), self._cb, None, C.byref(h)))
+        else:
+            _check(lib().evxg_server_create_lanes(int(hbm_budget_bytes), int(max_streams), int(lanes), self._cb, None,
+                                                  C.byref(h)))
         self.h = h
 
     def _on_result(self, user, sid, frame, bt, pv, sao, lev, times):

@@ -244,6 +244,15 @@ int evxg_batch_create(evxg_stream *const *streams, uint32_t n, evxg_batch **out)
         evxg_batch_destroy(b);
         return rc;
     }
+    // Both parities' tick graphs now: they do not depend on the frames, and the
+    // first ticks then do not pay for the capture.
+    for (int p = 0; p < 2; p++) {
+        const int rc = build_graph(b, p);
+        if (rc) {
+            evxg_batch_destroy(b);
+            return rc;
+        }
+    }
     *out = b;
     return EVXG_SUCCESS;
 }
@@ -356,6 +365,10 @@ int evxg_batch_set_shape(evxg_batch *b, int form, int grid, int policy)
     b->grid = std::min(grid, cap);   // every CTA / cluster of the persistent grid must be resident
     b->policy = policy;
     drop_graphs(b);
+    for (int p = 0; p < 2; p++) {
+        const int rc = build_graph(b, p);
+        if (rc) return rc;
+    }
     return EVXG_SUCCESS;
 }
 

@@ -6,12 +6,18 @@
 // live.  Callers submit RGB frames as they arrive; each stream's GOP logic is
 // the reference encoder's (evx3enc.cpp:105-414, the same planner evxg_encoder
 // runs), so a frame becomes ready to encode once the frames it depends on
-// have arrived.  A worker thread batches whatever is ready -- at most one
-// frame per stream per tick -- into batched ticks (evxg_batch.cu), building
-// tick t+1 while tick t runs on the device, and delivers every frame's
-// serializer inputs, with its arrival / ready / launch / done times, through a
-// callback.  Streams that join or leave change the batch at the next tick
-// boundary; the others' device state is untouched.
+// have arrived.  Streams are spread over lanes -- a stream joins the lane
+// whose streams are closest to its size -- and each lane has its own worker
+// thread, CUDA stream and batch: the worker batches whatever of its streams'
+// frames is ready -- at most one frame per stream per tick -- into batched
+// ticks (evxg_batch.cu), building tick t+1 while tick t runs, and delivers
+// every frame's serializer inputs, with its arrival / ready / launch / done
+// times, through a callback.  Lanes tick independently and their ticks run
+// on the device side by side (their streams are disjoint and each tick's
+// persistent kernels claim only their own rows), so a small stream's frame
+// does not wait for a large stream's wavefront.  Streams that join or leave
+// change their lane's batch at its next tick boundary; the others' device
+// state is untouched.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -51,6 +57,7 @@ struct Ready {
 
 struct Slot {
     uint32_t id = 0, w = 0, h = 0;
+    int lane = 0;
     size_t bytes = 0;
     evxg_stream *st = nullptr;
     evxg_encoder *planner = nullptr;
@@ -63,6 +70,23 @@ struct Slot {
 
 }  // namespace
 
+struct Pending {
+    bool used = false;
+    std::vector<Ready> frames;                 // per batch index; f.type < 0 = none
+};
+
+// One lane: a set of streams with its own worker thread, CUDA stream and batch.
+struct Lane {
+    int index = 0;
+    bool set_dirty = true;                     // its stream set changed (under the server lock)
+    // worker-owned
+    evxg_batch *batch = nullptr;
+    std::vector<Slot *> bslots;                // batch order
+    Pending pend[2];
+    cudaStream_t cs = nullptr;
+    std::thread worker;
+};
+
 struct evxg_server {
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -71,19 +95,11 @@ struct evxg_server {
     uint64_t budget = 0, used = 0;
     evxg_result_callback cb = nullptr;
     void *user = nullptr;
-    std::thread worker;
-    bool stop = false, set_dirty = true;
+    std::vector<Lane *> lanes;
+    bool stop = false;
     int drainers = 0;                          // threads waiting in evxg_server_drain
     int error = 0;
     uint64_t frames_done = 0, ticks = 0, rebuilds = 0;
-    // worker-owned
-    evxg_batch *batch = nullptr;
-    std::vector<Slot *> bslots;                // batch order
-    struct Pending {
-        bool used = false;
-        std::vector<Ready> frames;             // per batch index; f.type < 0 = none
-    } pend[2];
-    cudaStream_t cs = nullptr;
     int device = 0;
 };
 
@@ -117,13 +133,13 @@ size_t dead_bytes(const evxg_server *v)
     return b;
 }
 
-// Deliver tick q's results (worker thread, without the lock).
-int complete(evxg_server *v, int q)
+// Deliver lane l's tick q's results (its worker thread, without the lock).
+int complete(evxg_server *v, Lane *l, int q)
 {
-    evxg_server::Pending &pd = v->pend[q];
+    Pending &pd = l->pend[q];
     if (!pd.used) return EVXG_SUCCESS;
     pd.used = false;
-    int rc = evxg_batch_wait(v->batch, (uint32_t)q);
+    int rc = evxg_batch_wait(l->batch, (uint32_t)q);
     const uint64_t done = now_ns();
     for (size_t i = 0; i < pd.frames.size() && !rc; i++) {
         Ready &r = pd.frames[i];
@@ -132,12 +148,12 @@ int complete(evxg_server *v, int q)
         const evxg_block_desc *bt, *pv;
         const evxg_sao_info *sao;
         const int16_t *lev;
-        rc = evxg_batch_output(v->batch, (uint32_t)i, (uint32_t)q, &bt, &pv, &sao, &lev);
-        if (!rc && v->cb) v->cb(v->user, v->bslots[i]->id, &r.f, bt, pv, sao, lev, &r.t);
+        rc = evxg_batch_output(l->batch, (uint32_t)i, (uint32_t)q, &bt, &pv, &sao, &lev);
+        if (!rc && v->cb) v->cb(v->user, l->bslots[i]->id, &r.f, bt, pv, sao, lev, &r.t);
     }
     std::lock_guard<std::mutex> lk(v->mu);
     for (size_t i = 0; i < pd.frames.size(); i++)
-        if (pd.frames[i].f.type >= 0) { v->bslots[i]->in_flight--; v->frames_done++; }
+        if (pd.frames[i].f.type >= 0) { l->bslots[i]->in_flight--; v->frames_done++; }
     if (rc && !v->error) v->error = rc;
     pd.frames.clear();
     v->cv_done.notify_all();
@@ -148,9 +164,10 @@ int complete(evxg_server *v, int q)
 
 namespace {
 
-// Worker: rebuild the batch when the stream set changed (with no tick in
-// flight), launch a tick of whatever is ready, then deliver the tick before it.
-void work(evxg_server *v)
+// Worker of lane l: rebuild the lane's batch when its stream set changed
+// (with no tick in flight), launch a tick of whatever is ready, then deliver
+// the tick before it.
+void work(evxg_server *v, Lane *l)
 {
     cudaSetDevice(v->device);   // the caller's device
     int p = 0;
@@ -158,13 +175,13 @@ void work(evxg_server *v)
         std::unique_lock<std::mutex> lk(v->mu);
         auto any_ready = [&] {
             for (auto &kv : v->slots)
-                if (!kv.second->ready.empty()) return true;
+                if (kv.second->lane == l->index && !kv.second->ready.empty()) return true;
             return false;
         };
         v->cv_work.wait(lk, [&] {
             // a changed stream set is rebuilt when there is work for it or a drain waits on it, so a
             // burst of admissions costs one rebuild
-            return v->stop || (v->set_dirty && v->drainers > 0) || any_ready() || v->pend[0].used || v->pend[1].used;
+            return v->stop || (l->set_dirty && v->drainers > 0) || any_ready() || l->pend[0].used || l->pend[1].used;
         });
         if (v->error) {   // a tick failed: deliver nothing more, let callers see the error
             v->cv_done.notify_all();
@@ -172,17 +189,17 @@ void work(evxg_server *v)
             v->cv_work.wait(lk, [&] { return v->stop; });
             break;
         }
-        if (v->stop && !any_ready() && !v->pend[0].used && !v->pend[1].used) break;
-        if (v->set_dirty) {
-            if (v->pend[0].used || v->pend[1].used) {   // finish the batch's ticks first, oldest first
+        if (v->stop && !any_ready() && !l->pend[0].used && !l->pend[1].used) break;
+        if (l->set_dirty) {
+            if (l->pend[0].used || l->pend[1].used) {   // finish the batch's ticks first, oldest first
                 lk.unlock();
-                complete(v, p ^ 1);
-                complete(v, p);
+                complete(v, l, p ^ 1);
+                complete(v, l, p);
                 continue;
             }
             for (auto it = v->slots.begin(); it != v->slots.end();) {
                 Slot *s = it->second;
-                if (s->closing && drained(s)) {
+                if (s->lane == l->index && s->closing && drained(s)) {
                     evxg_encoder_destroy(s->planner);
                     evxg_stream_destroy(s->st);
                     v->used -= s->bytes;
@@ -192,25 +209,26 @@ void work(evxg_server *v)
                     ++it;
                 }
             }
-            if (v->batch) { evxg_batch_destroy(v->batch); v->batch = nullptr; }
-            v->bslots.clear();
+            if (l->batch) { evxg_batch_destroy(l->batch); l->batch = nullptr; }
+            l->bslots.clear();
             std::vector<evxg_stream *> sts;
-            for (auto &kv : v->slots) { v->bslots.push_back(kv.second); sts.push_back(kv.second->st); }
+            for (auto &kv : v->slots)
+                if (kv.second->lane == l->index) { l->bslots.push_back(kv.second); sts.push_back(kv.second->st); }
             if (!sts.empty()) {
-                const int rc = evxg_batch_create(sts.data(), (uint32_t)sts.size(), &v->batch);
+                const int rc = evxg_batch_create(sts.data(), (uint32_t)sts.size(), &l->batch);
                 if (rc) { v->error = rc; continue; }   // the batch's default shape: its tick model (evxg_batch.cu)
             }
-            v->set_dirty = false;
+            l->set_dirty = false;
             v->rebuilds++;
             p = 0;
             v->cv_done.notify_all();
             continue;
         }
         // a tick of whatever is ready: at most one frame per stream, its oldest
-        std::vector<Ready> frames(v->bslots.size());
+        std::vector<Ready> frames(l->bslots.size());
         bool any = false;
-        for (size_t i = 0; i < v->bslots.size(); i++) {
-            Slot *s = v->bslots[i];
+        for (size_t i = 0; i < l->bslots.size(); i++) {
+            Slot *s = l->bslots[i];
             if (s->ready.empty()) { frames[i].f.type = -1; continue; }
             frames[i] = std::move(s->ready.front());
             s->ready.pop_front();
@@ -219,35 +237,63 @@ void work(evxg_server *v)
         }
         lk.unlock();
         if (!any) {   // nothing new: deliver what is in flight
-            complete(v, p ^ 1);
-            complete(v, p);
+            complete(v, l, p ^ 1);
+            complete(v, l, p);
             continue;
         }
-        if (complete(v, p)) continue;   // this parity's buffers are free again
+        if (complete(v, l, p)) continue;   // this parity's buffers are free again
         std::vector<evxg_frame> fr(frames.size());
         const uint64_t launch = now_ns();
         for (size_t i = 0; i < frames.size(); i++) {
             fr[i] = frames[i].f;
             if (frames[i].f.type < 0) continue;
-            memcpy(evxg_batch_input(v->batch, (uint32_t)i, (uint32_t)p), frames[i].px.data(), frames[i].px.size());
+            memcpy(evxg_batch_input(l->batch, (uint32_t)i, (uint32_t)p), frames[i].px.data(), frames[i].px.size());
             frames[i].t.launch_ns = launch;
             frames[i].px.clear();
             frames[i].px.shrink_to_fit();
         }
-        int rc = evxg_batch_encode(v->batch, fr.data(), (uint32_t)p, v->cs);
+        int rc = evxg_batch_encode(l->batch, fr.data(), (uint32_t)p, l->cs);
         {
             std::lock_guard<std::mutex> g(v->mu);
             if (rc && !v->error) v->error = rc;
             v->ticks++;
         }
         if (rc) continue;
-        v->pend[p].used = true;
-        v->pend[p].frames = std::move(frames);
-        complete(v, p ^ 1);   // the tick before runs ahead of this one; deliver it while this one runs
+        l->pend[p].used = true;
+        l->pend[p].frames = std::move(frames);
+        complete(v, l, p ^ 1);   // the tick before runs ahead of this one; deliver it while this one runs
         p ^= 1;
     }
-    complete(v, p ^ 1);
-    complete(v, p);
+    complete(v, l, p ^ 1);
+    complete(v, l, p);
+}
+
+// The lane a new stream of w x h joins: one whose streams have the closest
+// size (macroblock count within a factor of two), else an empty lane, else
+// the one with the fewest macroblocks.
+int pick_lane(const evxg_server *v, uint32_t w, uint32_t h)
+{
+    const size_t n = v->lanes.size();
+    std::vector<double> load(n, 0.0), closest(n, 1e30);
+    const double mbs = (double)((w + 15) / 16) * ((h + 15) / 16);
+    for (const auto &kv : v->slots) {
+        const Slot *s = kv.second;
+        if (s->closing && drained(s)) continue;
+        const double m = (double)((s->w + 15) / 16) * ((s->h + 15) / 16);
+        load[s->lane] += m;
+        const double r = m > mbs ? m / mbs : mbs / m;
+        closest[s->lane] = std::min(closest[s->lane], r);
+    }
+    int best = -1;
+    for (size_t i = 0; i < n; i++)   // same size class, least loaded
+        if (closest[i] < 2.0 && (best < 0 || load[i] < load[best])) best = (int)i;
+    if (best >= 0) return best;
+    for (size_t i = 0; i < n; i++)
+        if (load[i] == 0.0) return (int)i;
+    best = 0;
+    for (size_t i = 1; i < n; i++)
+        if (load[i] < load[best]) best = (int)i;
+    return best;
 }
 
 }  // namespace
@@ -259,17 +305,35 @@ uint64_t evxg_server_now_ns(void) { return now_ns(); }
 int evxg_server_create(uint64_t hbm_budget_bytes, uint32_t max_streams, evxg_result_callback cb, void *user,
                        evxg_server **out)
 {
-    if (!out || !max_streams || !hbm_budget_bytes) return fail(EVXG_ERROR_INVALIDARG, "evxg_server_create: bad argument");
+    return evxg_server_create_lanes(hbm_budget_bytes, max_streams, max_streams < 8 ? max_streams : 8, cb, user, out);
+}
+
+int evxg_server_create_lanes(uint64_t hbm_budget_bytes, uint32_t max_streams, uint32_t lanes, evxg_result_callback cb,
+                             void *user, evxg_server **out)
+{
+    if (!out || !max_streams || !hbm_budget_bytes || !lanes || lanes > max_streams)
+        return fail(EVXG_ERROR_INVALIDARG, "evxg_server_create: bad argument");
     evxg_server *v = new evxg_server();
     v->budget = hbm_budget_bytes;
     v->max_streams = max_streams;
     v->cb = cb;
     v->user = user;
-    if (cudaGetDevice(&v->device) != cudaSuccess || cudaStreamCreateWithFlags(&v->cs, cudaStreamNonBlocking) != cudaSuccess) {
+    bool ok = cudaGetDevice(&v->device) == cudaSuccess;
+    for (uint32_t i = 0; i < lanes && ok; i++) {
+        Lane *l = new Lane();
+        l->index = (int)i;
+        v->lanes.push_back(l);
+        ok = cudaStreamCreateWithFlags(&l->cs, cudaStreamNonBlocking) == cudaSuccess;
+    }
+    if (!ok) {
+        for (Lane *l : v->lanes) {
+            if (l->cs) cudaStreamDestroy(l->cs);
+            delete l;
+        }
         delete v;
         return fail(EVXG_ERROR_EXECUTION_FAILURE, "evxg_server_create: stream creation failed");
     }
-    v->worker = std::thread(work, v);
+    for (Lane *l : v->lanes) l->worker = std::thread(work, v, l);
     *out = v;
     return EVXG_SUCCESS;
 }
@@ -309,8 +373,9 @@ int evxg_server_open_config(evxg_server *v, uint32_t width, uint32_t height, uin
         return rc;
     }
     s->id = v->next_id++;
+    s->lane = pick_lane(v, width, height);
     v->slots[s->id] = s;
-    v->set_dirty = true;
+    v->lanes[s->lane]->set_dirty = true;
     *stream_id = s->id;
     v->cv_work.notify_all();
     return EVXG_SUCCESS;
@@ -373,10 +438,11 @@ int evxg_server_drain(evxg_server *v)
     v->cv_work.notify_all();
     v->cv_done.wait(lk, [&] {
         if (v->error) return true;
-        if (v->pend[0].used || v->pend[1].used) return false;
+        for (const Lane *l : v->lanes)   // pend is read without the worker's ownership: only as a hint, in_flight decides
+            if (l->set_dirty) return false;
         for (auto &kv : v->slots)
             if (!kv.second->ready.empty() || kv.second->in_flight) return false;
-        return !v->set_dirty;
+        return true;
     });
     v->drainers--;
     return v->error ? fail(v->error, "evxg_server_drain: a tick failed") : EVXG_SUCCESS;
@@ -403,14 +469,17 @@ int evxg_server_destroy(evxg_server *v)
         v->stop = true;
         v->cv_work.notify_all();
     }
-    v->worker.join();
-    if (v->batch) evxg_batch_destroy(v->batch);
+    for (Lane *l : v->lanes) l->worker.join();
+    for (Lane *l : v->lanes) {
+        if (l->batch) evxg_batch_destroy(l->batch);
+        cudaStreamDestroy(l->cs);
+        delete l;
+    }
     for (auto &kv : v->slots) {
         evxg_encoder_destroy(kv.second->planner);
         evxg_stream_destroy(kv.second->st);
         delete kv.second;
     }
-    cudaStreamDestroy(v->cs);
     delete v;
     return EVXG_SUCCESS;
 }

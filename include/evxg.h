@@ -270,11 +270,12 @@ int evxg_batch_autotune(evxg_batch *b, void *cuda_stream, float *best_ms);
  * evxg_server_submit copies one RGB24 frame in (arrival_ns on the
  * evxg_server_now_ns clock; 0 = now).  Each stream follows the reference
  * encoder's GOP (evx3enc.cpp:105-414), so a frame is ready to encode once the
- * frames it depends on have arrived; a worker thread batches whatever is ready
+ * frames it depends on have arrived; each lane's worker thread (see
+ * evxg_server_create_lanes) batches whatever of its streams' frames is ready
  * (at most one frame per stream per tick, see Batched encoding) while the
  * previous tick runs, and calls cb on that thread, in each stream's bitstream
- * order, with the frame's serializer inputs (valid during the call) and its
- * times.  evxg_server_close flushes a stream (its last frames are encoded);
+ * order (streams of different lanes concurrently), with the frame's
+ * serializer inputs (valid during the call) and its times.  evxg_server_close flushes a stream (its last frames are encoded);
  * once they are delivered its memory counts as free for admissions and is
  * released when the next admission rebuilds the batch.  evxg_server_drain
  * waits until every frame that can be encoded has been delivered (and the
@@ -293,6 +294,14 @@ typedef void (*evxg_result_callback)(void *user, uint32_t stream_id, const evxg_
                                      const evxg_sao_info *sao, const int16_t *levels, const evxg_frame_times *times);
 int evxg_server_create(uint64_t hbm_budget_bytes, uint32_t max_streams, evxg_result_callback cb, void *user,
                        evxg_server **out);
+/* evxg_server_create spreads the streams over min(max_streams, 8) lanes; this
+ * form sets the count (1..max_streams).  A lane is a set of streams with its
+ * own worker thread, CUDA stream and batched ticks; a new stream joins the
+ * lane whose streams are closest to its size (else an empty lane, else the
+ * least loaded), lanes tick independently and their ticks share the device,
+ * so a small stream's frames do not wait for a large stream's. */
+int evxg_server_create_lanes(uint64_t hbm_budget_bytes, uint32_t max_streams, uint32_t lanes, evxg_result_callback cb,
+                             void *user, evxg_server **out);
 int evxg_server_destroy(evxg_server *srv);
 int evxg_server_open(evxg_server *srv, uint32_t width, uint32_t height, uint8_t quality, uint32_t *stream_id);
 /* evxg_server_open for a stream of the build cfg describes (NULL = default). */
