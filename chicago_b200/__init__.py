@@ -57,6 +57,8 @@ EXPORTS = [
     "evxg_server_open_config", "evxg_stream_set_timeout_ns", "evxg_stream_reset", "evxg_batch_set_timeout_ns",
     "evxg_mb_pass_noalloc_set_timeout_ns", "evxg_server_cancel", "evxg_inject_alloc_failures",
     "evxg_serialize_slice", "evxg_stream_header", "evxg_encoder_set_output", "evxg_server_create_lanes",
+    "evxg_decoder_create", "evxg_decoder_destroy", "evxg_decode_frame", "evxg_decoder_sync",
+    "evxg_decoder_fetch_planes", "evxg_decoder_set_timeout_ns", "evxg_decoder_reset",
 ]
 MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
 
@@ -164,6 +166,13 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_stream_header.argtypes = [C.POINTER(Config), u32, u32, vp]
     L.evxg_server_stats.argtypes = [vp] + [C.POINTER(u64)] * 4
     L.evxg_server_now_ns.restype = u64
+    L.evxg_decoder_create.argtypes = [u32, u32, C.POINTER(Config), C.POINTER(vp)]
+    L.evxg_decoder_destroy.argtypes = [vp]
+    L.evxg_decode_frame.argtypes = [vp, C.c_char_p, vp, vp, vp, i32, vp, i32, vp]
+    L.evxg_decoder_sync.argtypes = [vp, vp]
+    L.evxg_decoder_fetch_planes.argtypes = [vp, u32, vp, i32, vp]
+    L.evxg_decoder_set_timeout_ns.argtypes = [vp, C.c_int64]
+    L.evxg_decoder_reset.argtypes = [vp, vp]
     return L
 
 
@@ -303,6 +312,59 @@ class Stream:
     @mb_form.setter
     def mb_form(self, form: int):
         _check(lib().evxg_stream_set_mb_form(self.h, int(form)))
+
+
+class Decoder:
+    """The decoder's pixel half on the device (engine_decode_frame after
+    unserialize_slice, src/video/decode.cpp:560-612) for one stream of the
+    reference build ``cfg`` names: ``decode_frame`` takes a frame's descriptor
+    and the tables the entropy decoder produces (the layouts of
+    :meth:`Stream.fetch_tables`) and returns the visible RGB24 frame."""
+
+    def __init__(self, width: int, height: int, cfg="default"):
+        self.width, self.height = int(width), int(height)
+        self.cfg = config(cfg)
+        h = C.c_void_p()
+        _check(lib().evxg_decoder_create(self.width, self.height, C.byref(self.cfg), C.byref(h)))
+        self.h = h
+        self.aw, self.ah = (self.width + 15) & ~15, (self.height + 15) & ~15
+        self.plane_elems = self.aw * self.ah + 2 * (self.aw // 2) * (self.ah // 2)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().evxg_decoder_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def decode_frame(self, frame18: bytes, blocks, sao, levels, rgb: bool = True, cuda_stream=None):
+        """Decode one frame (host tables); returns the (H, W, 3) RGB24 frame, or None with rgb=False."""
+        bt = np.ascontiguousarray(blocks)
+        sa = np.ascontiguousarray(sao)
+        lv = np.ascontiguousarray(levels, dtype=np.int16)
+        out = np.empty((self.height, self.width, 3), np.uint8) if rgb else None
+        _check(lib().evxg_decode_frame(self.h, frame18, _ptr(bt), _ptr(sa), _ptr(lv), 0, _ptr(out), 0,
+                                       _ptr(cuda_stream)))
+        self.sync(cuda_stream)
+        return out
+
+    def sync(self, cuda_stream=None):
+        _check(lib().evxg_decoder_sync(self.h, _ptr(cuda_stream)))
+
+    def set_timeout_ns(self, ns: int):
+        _check(lib().evxg_decoder_set_timeout_ns(self.h, int(ns)))
+
+    def reset(self, cuda_stream=None):
+        _check(lib().evxg_decoder_reset(self.h, _ptr(cuda_stream)))
+
+    def fetch_planes(self, slot: int, cuda_stream=None) -> np.ndarray:
+        out = np.zeros(self.plane_elems, np.int16)
+        _check(lib().evxg_decoder_fetch_planes(self.h, slot, _ptr(out), 0, _ptr(cuda_stream)))
+        return out
 
 
 NO_FRAME = struct.pack("<iIHIBBBB", -1, 0, 0, 0, 0, 0, 0, 0)   # a stream without a frame in a batch tick

@@ -43,6 +43,22 @@ static cudaError_t dev_alloc(T **p, size_t n)
     return cudaMalloc(p, n);
 }
 
+int evxg::check_config(const evxg_config *c, const char *who)
+{
+    static thread_local char msg[200];
+    const bool ok = (c->b_frames == 1 && c->ref_count == 4) || (c->b_frames == 0 && (c->ref_count == 2 || c->ref_count == 4));
+    if (!ok) {
+        snprintf(msg, sizeof msg, "%s: unsupported configuration (b_frames %u, ref_count %u): B frames need 4 DPB slots, "
+                 "I/P streams 2 or 4", who, c->b_frames, c->ref_count);
+        return fail(EVXG_ERROR_INVALIDARG, msg);
+    }
+    if (c->search_radius != 16 || c->reserved) {
+        snprintf(msg, sizeof msg, "%s: unsupported search radius %u (16)", who, c->search_radius);
+        return fail(EVXG_ERROR_INVALIDARG, msg);
+    }
+    return EVXG_SUCCESS;
+}
+
 extern "C" {
 
 float evxg_lambda(uint16_t q) { return 0.85f * powf(2.0f, ((float)q - 12.0f) / 3.0f); }   // common.h:264-266
@@ -60,22 +76,6 @@ void evxg_config_default(evxg_config *cfg)
     if (!cfg) return;
     *cfg = evxg_config{};
     cfg->b_frames = 1; cfg->ref_count = 4; cfg->search_radius = 16;
-}
-
-static int check_config(const evxg_config *c, const char *who)
-{
-    static thread_local char msg[200];
-    const bool ok = (c->b_frames == 1 && c->ref_count == 4) || (c->b_frames == 0 && (c->ref_count == 2 || c->ref_count == 4));
-    if (!ok) {
-        snprintf(msg, sizeof msg, "%s: unsupported configuration (b_frames %u, ref_count %u): B frames need 4 DPB slots, "
-                 "I/P streams 2 or 4", who, c->b_frames, c->ref_count);
-        return fail(EVXG_ERROR_INVALIDARG, msg);
-    }
-    if (c->search_radius != 16 || c->reserved) {
-        snprintf(msg, sizeof msg, "%s: unsupported search radius %u (16)", who, c->search_radius);
-        return fail(EVXG_ERROR_INVALIDARG, msg);
-    }
-    return EVXG_SUCCESS;
 }
 
 int evxg_stream_create(uint32_t width, uint32_t height, evxg_stream **out)
@@ -268,6 +268,10 @@ int evxg::max_active_clusters()
 // common.cpp:256-259), and are written into the copy.
 int evxg::check_frame(const evxg_stream *s, const evxg_frame *fin, const char *who, evxg_frame *out)
 {
+    return check_frame_config(s->cfg, fin, who, out);
+}
+int evxg::check_frame_config(const evxg_config &cfg, const evxg_frame *fin, const char *who, evxg_frame *out)
+{
     static thread_local char msg[160];
     auto bad = [&](int code, const char *what) {
         snprintf(msg, sizeof msg, "%s: %s", who, what);
@@ -276,9 +280,9 @@ int evxg::check_frame(const evxg_stream *s, const evxg_frame *fin, const char *w
     evxg_frame g = *fin;
     const evxg_frame *f = &g;
     if (f->type < EVXG_FRAME_INTRA || f->type > EVXG_FRAME_BIDIR) return bad(EVXG_ERROR_INVALIDARG, "bad frame type");
-    if (!s->cfg.b_frames) {
+    if (!cfg.b_frames) {
         if (f->type == EVXG_FRAME_BIDIR) return bad(EVXG_ERROR_INVALIDARG, "B frame in a stream without B frames");
-        const uint32_t R = s->cfg.ref_count;
+        const uint32_t R = cfg.ref_count;
         g.dpb_slot = (uint8_t)(f->index % R);
         g.ref_slot_fwd = (uint8_t)((f->index + R - 1) % R);
         g.ref_slot_bwd = 0;

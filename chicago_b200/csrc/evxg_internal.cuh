@@ -49,6 +49,9 @@ int cuda_fail(cudaError_t e, const char *where);
 // streams without B frames, derives its DPB slots from the index (out may be
 // the same as f).
 int check_frame(const evxg_stream *s, const evxg_frame *f, const char *who, evxg_frame *out);
+int check_frame_config(const evxg_config &cfg, const evxg_frame *f, const char *who, evxg_frame *out);
+// A build configuration the library reproduces (EVXG_ERROR_INVALIDARG otherwise).
+int check_config(const evxg_config *c, const char *who);
 int max_active_clusters();
 }  // namespace evxg
 

@@ -355,6 +355,40 @@ int evxg_serialize_slice(const evxg_config *cfg, uint32_t aligned_w, uint32_t al
  * (evx3enc.cpp:141-147). */
 int evxg_stream_header(const evxg_config *cfg, uint32_t width, uint32_t height, uint8_t out[14]);
 
+/* ---- Decoder pixel half ----
+ *
+ * engine_decode_frame (decode.cpp:560-612) after unserialize_slice: per
+ * macroblock decode_block (decode.cpp:31-432) into the destination slot,
+ * deblock_image_filter, sao_filter_image, and the conversion to RGB24
+ * (convert.cpp:162-223).  A decoder holds the DPB of one stream of the build
+ * cfg describes (NULL = default), zero-initialised like the reference's
+ * context (common.cpp:106-202).  evxg_decode_frame takes one frame in
+ * bitstream order: its evxg_frame (the record's descriptor; without B frames
+ * the slots follow from the index), block and SAO tables and level planes as
+ * the entropy decoder produces them -- the same layouts evxg_fetch_tables
+ * returns (host memory, or device memory with tables_on_device != 0) -- and
+ * writes the visible width*height*3 bytes of RGB24 to rgb (NULL: none; device
+ * memory with rgb_on_device != 0).  Decoding the tables an evxg_stream encoded
+ * reproduces its reconstruction exactly.  Asynchronous on cuda_stream;
+ * evxg_decoder_sync waits and reports EVXG_ERROR_INVALID_RESOURCE for a block
+ * descriptor the reference rejects (an unknown block type, a reference that
+ * is not a DPB slot other than the destination) and
+ * EVXG_ERROR_OPERATION_TIMEDOUT when the intra wavefront gave up waiting (the
+ * bound as in evxg_stream_set_timeout_ns; evxg_decoder_reset then restores the
+ * state at creation).  Host tables must stay valid until the call returns;
+ * a host rgb buffer until the frame is synchronised. */
+typedef struct evxg_decoder evxg_decoder;
+int evxg_decoder_create(uint32_t width, uint32_t height, const evxg_config *cfg, evxg_decoder **out);
+int evxg_decoder_destroy(evxg_decoder *d);
+int evxg_decode_frame(evxg_decoder *d, const evxg_frame *frame, const evxg_block_desc *blocks,
+                      const evxg_sao_info *sao, const int16_t *levels, int tables_on_device, uint8_t *rgb,
+                      int rgb_on_device, void *cuda_stream);
+int evxg_decoder_sync(evxg_decoder *d, void *cuda_stream);
+/* Copy one DPB slot (plane-set layout) out. */
+int evxg_decoder_fetch_planes(evxg_decoder *d, uint32_t slot, int16_t *out, int to_device, void *cuda_stream);
+int evxg_decoder_set_timeout_ns(evxg_decoder *d, int64_t ns);
+int evxg_decoder_reset(evxg_decoder *d, void *cuda_stream);
+
 /* Human-readable text of the last error on this thread. */
 const char *evxg_last_error(void);
 

@@ -177,6 +177,25 @@ static i32 variance2(mbv a) /* analysis.h:251-275, int32 wrapping kept */
     return cnt > 0 ? (i32)((u32)sq - (u32)rdiv(wmul(sum, sum), cnt)) : 0;
 }
 
+/* ---------- YUV 4:2:0 -> RGB24 (convert.cpp:15-18, :75-93, :162-223) ----------
+ * Each chroma sample colours a 2x2 quad; (256(Y-16) + k(C-128) + 128) >> 8
+ * saturated to 0..255; the frame is cropped to w x h (the visible size). */
+static u8 sat8(i32 v) { return (u8)(v < 0 ? 0 : (v > 255 ? 255 : v)); }
+void orc_yuv_to_rgb(const i16 *planes, u32 aw, u32 ah, u32 w, u32 h, u8 *rgb)
+{
+    pset p = pset_wrap((i16 *)planes, (i32)aw, (i32)ah);
+    u32 cw = w < aw ? w : aw, ch = h < ah ? h : ah;
+    for (u32 y = 0; y < ch; y++) for (u32 x = 0; x < cw; x++) {
+        i32 l = 256 * ((i32)p.y[(size_t)y * aw + x] - 16);
+        i32 u = (i32)p.u[(size_t)(y / 2) * (aw / 2) + x / 2] - 128;
+        i32 v = (i32)p.v[(size_t)(y / 2) * (aw / 2) + x / 2] - 128;
+        u8 *o = rgb + ((size_t)y * w + x) * 3;
+        o[0] = sat8((l + 358 * v + 128) >> 8);
+        o[1] = sat8((l - 88 * u - 182 * v + 128) >> 8);
+        o[2] = sat8((l + 452 * u + 128) >> 8);
+    }
+}
+
 /* ---------- colour conversion (convert.cpp:11-14, :30-73, :95-160) ---------- */
 void orc_convert(const u8 *rgb, u32 w, u32 h, i16 *planes, u32 aw, u32 ah)
 {

@@ -61,6 +61,7 @@ void orc_mv_predictor(const uint8_t *blocks, const uint8_t *prev_blocks, uint32_
                       uint32_t index, int16_t *px, int16_t *py);
 uint8_t orc_deblock_strength(int32_t mb_boundary, const uint8_t *left_desc, const uint8_t *right_desc);
 void orc_convert(const uint8_t *rgb, uint32_t w, uint32_t h, int16_t *planes, uint32_t aw, uint32_t ah);
+void orc_yuv_to_rgb(const int16_t *planes, uint32_t aw, uint32_t ah, uint32_t w, uint32_t h, uint8_t *rgb);
 
 #ifdef __cplusplus
 }

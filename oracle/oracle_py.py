@@ -240,6 +240,15 @@ class Ref:
             L.evxref_ctx_get_slot.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
         L.evxref_lambda.restype = C.c_float
         L.evxref_lambda.argtypes = [C.c_uint16]
+        L.evxref_decode_stream.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+                                           C.c_uint32, C.POINTER(C.c_uint32)]
+        L.evxref_decode_records.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                            C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]
+        L.evxref_dctx_create.restype = C.c_void_p
+        L.evxref_dctx_create.argtypes = [C.c_uint32, C.c_uint32]
+        L.evxref_dctx_destroy.argtypes = [C.c_void_p]
+        L.evxref_dctx_decode_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32] + \
+            [C.c_void_p] * 6
 
     # --- stock API ---
     def encode_stream(self, frames: np.ndarray, quality: int = 8, intra_at=()) -> bytes:
@@ -268,12 +277,74 @@ class Ref:
             self.lib.evxref_enc_destroy(h)
         return bytes(out)
 
+    def decode_stream(self, data: bytes, width: int, height: int, max_frames: int = 256) -> np.ndarray:
+        """Decode a whole .evx stream with the stock decoder; (T,H,W,3) frames in display order."""
+        out = np.zeros((max_frames, height, width, 3), np.uint8)
+        n = C.c_uint32(0)
+        buf = np.frombuffer(data, np.uint8).copy()
+        rc = self.lib.evxref_decode_stream(_p(buf), len(data), width, height, _p(out), max_frames, C.byref(n))
+        if rc:
+            raise RuntimeError(f"reference decode failed: {rc}")
+        return out[:min(n.value, max_frames)]
+
+    def decode_records(self, records, width: int, height: int) -> np.ndarray:
+        """The stock decoder fed one record per call (records[0] starts with the
+        stream header); (T,H,W,3) frames in display order."""
+        data = np.frombuffer(b"".join(records), np.uint8).copy()
+        offs = np.cumsum([0] + [len(r) for r in records]).astype(np.uint32)
+        out = np.zeros((len(records), height, width, 3), np.uint8)
+        n = C.c_uint32(0)
+        rc = self.lib.evxref_decode_records(_p(data), _p(offs), len(records), width, height, _p(out), len(records),
+                                            C.byref(n))
+        if rc:
+            raise RuntimeError(f"reference decode failed: {rc} after {n.value} frames")
+        return out[:n.value]
+
     # --- staged engine ---
     def context(self, width: int, height: int):
         return RefContext(self, align16(width), align16(height))
 
+    def decoder(self, width: int, height: int):
+        """Staged engine_decode_frame with dumps (see RefDecodeContext)."""
+        return RefDecodeContext(self, width, height)
+
     def lam(self, q: int) -> float:
         return self.lib.evxref_lambda(q)
+
+
+class RefDecodeContext:
+    """The reference's engine_decode_frame step by step (decode.cpp:560-612):
+    decode_frame(record) takes one frame record (evx_frame + slice) and returns
+    what unserialize_slice produced -- descriptor (18-byte layout), block table
+    (28-byte layout), SAO table, level planes -- plus the final reconstruction
+    and the RGB24 frame."""
+
+    def __init__(self, ref: Ref, width: int, height: int):
+        self.ref, self.w, self.h = ref, width, height
+        self.aw, self.ah = align16(width), align16(height)
+        self.hd = ref.lib.evxref_dctx_create(self.aw, self.ah)
+        if not self.hd:
+            raise RuntimeError("reference decoder context creation failed")
+
+    def __del__(self):
+        if getattr(self, "hd", None):
+            self.ref.lib.evxref_dctx_destroy(self.hd)
+            self.hd = None
+
+    def decode_frame(self, record: bytes) -> dict:
+        n = self.aw * self.ah + 2 * (self.aw // 2) * (self.ah // 2)
+        nblk = (self.aw // 16) * (self.ah // 16)
+        out = dict(frame18=np.zeros(18, np.uint8), blocks=np.zeros(nblk * 28, np.uint8),
+                   sao=np.zeros(nblk * 16, np.uint8), levels=np.zeros(n, np.int16), final=np.zeros(n, np.int16),
+                   rgb=np.zeros((self.h, self.w, 3), np.uint8))
+        buf = np.frombuffer(record, np.uint8).copy()
+        rc = self.ref.lib.evxref_dctx_decode_frame(self.hd, _p(buf), len(record), self.w, self.h,
+                                                   *[_p(out[k]) for k in ("frame18", "blocks", "sao", "levels",
+                                                                          "final", "rgb")])
+        if rc:
+            raise RuntimeError(f"reference staged decode failed: {rc}")
+        out["frame18"] = out["frame18"].tobytes()
+        return out
 
 
 class RefContext:
@@ -347,6 +418,14 @@ class Oracle:
         L.orc_deblock_strength.restype = C.c_uint8
         L.orc_deblock_strength.argtypes = [C.c_int32, C.c_void_p, C.c_void_p]
         L.orc_convert.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32]
+        L.orc_yuv_to_rgb.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p]
+
+    def yuv_to_rgb(self, planes: np.ndarray, aw: int, ah: int, width: int, height: int) -> np.ndarray:
+        """RGB24 (H,W,3) of an int16 plane set (convert.cpp:162-223)."""
+        p = np.ascontiguousarray(planes, dtype=np.int16)
+        out = np.zeros((height, width, 3), np.uint8)
+        self.lib.orc_yuv_to_rgb(_p(p), aw, ah, width, height, _p(out))
+        return out
 
     def context(self, width: int, height: int, b_frames: int = 1, ref_count: int = 4, radius: int = 16):
         """A stream context restating the reference build with these switches

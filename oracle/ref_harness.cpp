@@ -38,6 +38,11 @@ evx_status deblock_image_filter(evx_block_desc *block_table, image_set *target_i
 evx_status serialize_slice(const evx_frame &frame, evx_context *context, bit_stream *output);
 evx_status encode_slice(const evx_frame &frame, evx_context *context);
 evx_status encode_slice_wpp(const evx_frame &frame, evx_context *context);
+evx_status unserialize_slice(bit_stream *input, const evx_frame &frame, evx_context *context);
+evx_status decode_slice(const evx_frame &frame, evx_context *context);
+#if EVX_ENABLE_WPP
+evx_status decode_slice_wpp(const evx_frame &frame, evx_context *context);
+#endif
 }
 
 /*
@@ -144,6 +149,169 @@ int evxref_enc_flush(void *p, uint8_t *out, uint32_t cap, uint32_t *out_len)
     return 0;
 }
 
+/* Decode a whole .evx stream with the reference's public decoder
+ * (create_decoder / decode / has_output / flush, src/video/evx3.h:103-127),
+ * the way its own round-trip test drives it (tests/test_codec_roundtrip.cpp:
+ * 211-231): frames come out in display order, w*h*3 bytes each; at most
+ * max_frames are stored, *n_out counts all of them. */
+int evxref_decode_stream(const uint8_t *data, uint32_t len, uint32_t w, uint32_t h, uint8_t *out,
+                         uint32_t max_frames, uint32_t *n_out)
+{
+    evx3_decoder *dec = nullptr;
+    if (create_decoder(&dec) != EVX_SUCCESS) return EVX_ERROR_EXECUTION_FAILURE;
+    bit_stream bs;
+    bs.resize_capacity((len + 64) * 8u);
+    bs.write_bytes((void *)data, len);
+    const size_t fb = (size_t)w * h * 3;
+    std::vector<uint8_t> buf(fb);
+    uint32_t n = 0;
+    int rc = 0;
+    auto keep = [&]() {
+        if (n < max_frames) memcpy(out + n * fb, buf.data(), fb);
+        n++;
+    };
+    while (bs.query_byte_occupancy() > 0) {
+        const evx_status s = dec->decode(&bs, buf.data());
+        if (s != EVX_SUCCESS) { rc = s; break; }
+#if EVX_ENABLE_B_FRAMES
+        if (!dec->has_output()) continue;
+#endif
+        keep();
+    }
+#if EVX_ENABLE_B_FRAMES
+    while (rc == 0) {
+        dec->flush(buf.data());
+        if (!dec->has_output()) break;
+        keep();
+    }
+#endif
+    destroy_decoder(dec);
+    *n_out = n;
+    return rc;
+}
+
+/* The same decoder fed one frame record per decode() call, each in a bit
+ * stream of its own (record k = data[offsets[k] .. offsets[k+1]), the first
+ * one with the stream header in front), as a container delivers packets.
+ * Builds without B frames need this: their records carry no size prefix and
+ * the arithmetic decoder reads past a frame's end (decode.cpp's reason for
+ * the prefix, evx3dec.cpp:116-135), so a concatenated stream decodes only its
+ * first frame. */
+int evxref_decode_records(const uint8_t *data, const uint32_t *offsets, uint32_t n_records, uint32_t w, uint32_t h,
+                          uint8_t *out, uint32_t max_frames, uint32_t *n_out)
+{
+    evx3_decoder *dec = nullptr;
+    if (create_decoder(&dec) != EVX_SUCCESS) return EVX_ERROR_EXECUTION_FAILURE;
+    const size_t fb = (size_t)w * h * 3;
+    std::vector<uint8_t> buf(fb);
+    uint32_t n = 0;
+    int rc = 0;
+    auto keep = [&]() {
+        if (n < max_frames) memcpy(out + n * fb, buf.data(), fb);
+        n++;
+    };
+    for (uint32_t k = 0; k < n_records && rc == 0; k++) {
+        const uint32_t len = offsets[k + 1] - offsets[k];
+        bit_stream bs;
+        bs.resize_capacity((len + 64) * 8u);
+        bs.write_bytes((void *)(data + offsets[k]), len);
+        const evx_status s = dec->decode(&bs, buf.data());
+        if (s != EVX_SUCCESS) { rc = s; break; }
+#if EVX_ENABLE_B_FRAMES
+        if (!dec->has_output()) continue;
+#endif
+        keep();
+    }
+#if EVX_ENABLE_B_FRAMES
+    while (rc == 0) {
+        dec->flush(buf.data());
+        if (!dec->has_output()) break;
+        keep();
+    }
+#endif
+    destroy_decoder(dec);
+    *n_out = n;
+    return rc;
+}
+
+static void copy_set(const image_set &s, int16_t *dst, uint32_t w, uint32_t h)
+{
+    if (!dst) return;
+    memcpy(dst, s.query_y_image()->query_data(), (size_t)w * h * 2);
+    memcpy(dst + (size_t)w * h, s.query_u_image()->query_data(), (size_t)(w / 2) * (h / 2) * 2);
+    memcpy(dst + (size_t)w * h + (size_t)(w / 2) * (h / 2), s.query_v_image()->query_data(),
+           (size_t)(w / 2) * (h / 2) * 2);
+}
+
+/* ---------------- staged decoder ----------------
+ * engine_decode_frame (src/video/decode.cpp:560-612) step by step with the
+ * reference's own functions, dumping what unserialize_slice produced (block
+ * table, SAO table, level planes) and the final reconstruction: the tables a
+ * GPU decoder is given and the pixels it must reach. */
+struct evxref_dctx {
+    evx_context ctx;
+    uint32_t w, h;       /* aligned (context) dimensions */
+};
+
+void *evxref_dctx_create(uint32_t aligned_w, uint32_t aligned_h)
+{
+    evxref_dctx *c = new evxref_dctx;
+    if (initialize_context(aligned_w, aligned_h, &c->ctx) != EVX_SUCCESS) { delete c; return nullptr; }
+    c->w = aligned_w; c->h = aligned_h;
+    return c;
+}
+
+void evxref_dctx_destroy(void *p)
+{
+    evxref_dctx *c = (evxref_dctx *)p;
+    if (!c) return;
+    clear_context(&c->ctx);
+    delete c;
+}
+
+/* record = the frame's evx_frame (native size) followed by its slice; the
+ * descriptor is returned in the default build's 18-byte layout. */
+int evxref_dctx_decode_frame(void *p, const uint8_t *record, uint32_t len, uint32_t vis_w, uint32_t vis_h,
+                             uint8_t *frame18_out, uint8_t *dump_blocks, uint8_t *dump_sao, int16_t *dump_levels,
+                             int16_t *dump_final, uint8_t *rgb_out)
+{
+    evxref_dctx *c = (evxref_dctx *)p;
+    const uint32_t nblk = c->ctx.width_in_blocks * c->ctx.height_in_blocks;
+    bit_stream bs;
+    bs.resize_capacity((len + 64) * 8u);
+    bs.write_bytes((void *)record, len);
+    evx_frame frame;
+    if (bs.read_bytes(&frame, sizeof(evx_frame)) != EVX_SUCCESS) return 110;
+    if (frame18_out) {
+        memset(frame18_out, 0, WIDE_FRAME);
+        memcpy(frame18_out, &frame, sizeof(evx_frame));
+    }
+    if (unserialize_slice(&bs, frame, &c->ctx) != EVX_SUCCESS) return 111;
+    if (dump_blocks) blocks_to_wide(c->ctx.block_table, nblk, dump_blocks);
+    if (dump_sao) memcpy(dump_sao, c->ctx.sao_table, (size_t)nblk * 16);
+    copy_set(c->ctx.cache_bank.input_cache, dump_levels, c->w, c->h);
+#if EVX_ENABLE_WPP
+    if (decode_slice_wpp(frame, &c->ctx) != EVX_SUCCESS) return 112;
+#else
+    if (decode_slice(frame, &c->ctx) != EVX_SUCCESS) return 112;
+#endif
+    image_set &dest = c->ctx.cache_bank.prediction_cache[dest_slot(frame)];
+    if (deblock_image_filter(c->ctx.block_table, &dest) != EVX_SUCCESS) return 113;
+    if (sao_filter_image(c->ctx.sao_table, c->ctx.width_in_blocks, c->ctx.height_in_blocks, &dest) != EVX_SUCCESS)
+        return 114;
+    copy_set(dest, dump_final, c->w, c->h);
+    if (rgb_out) {
+        image out;
+        if (create_image(EVX_IMAGE_FORMAT_R8G8B8, rgb_out, vis_w, vis_h, &out) != EVX_SUCCESS) return 115;
+        if (convert_image(dest, &out) != EVX_SUCCESS) return 116;
+    }
+#if EVX_ENABLE_B_FRAMES
+    if (frame.type != EVX_FRAME_BIDIR)   /* decode.cpp:601-609 */
+#endif
+        memcpy(c->ctx.prev_block_table, c->ctx.block_table, (size_t)nblk * sizeof(evx_block_desc));
+    return 0;
+}
+
 #ifndef EVXREF_STOCK_ONLY   /* the staged driver needs encode.cpp; builds without it keep the stock API */
 /* ---------------- 2. staged per-frame driver ---------------- */
 
@@ -170,14 +338,6 @@ void evxref_ctx_destroy(void *p)
     delete c;
 }
 
-static void copy_set(const image_set &s, int16_t *dst, uint32_t w, uint32_t h)
-{
-    if (!dst) return;
-    memcpy(dst, s.query_y_image()->query_data(), (size_t)w * h * 2);
-    memcpy(dst + (size_t)w * h, s.query_u_image()->query_data(), (size_t)(w / 2) * (h / 2) * 2);
-    memcpy(dst + (size_t)w * h + (size_t)(w / 2) * (h / 2), s.query_v_image()->query_data(),
-           (size_t)(w / 2) * (h / 2) * 2);
-}
 
 static void load_set(image_set *s, const int16_t *src, uint32_t w, uint32_t h)
 {

@@ -101,3 +101,71 @@ def test_sequential_build_equals_wpp_build(ref):
     # Byte 7 of the stream header is a struct pad byte that the reference never
     # initialises, so it differs between runs.
     assert len(a) == len(b) and a[:7] == b[:7] and a[8:] == b[8:]
+
+
+DEC_CASES = [  # (variant, w, h, frames, quality, vmax, intra_at); None = the default build
+    (None, 100, 60, 9, 8, 8.0, ()),
+    (None, 176, 144, 8, 16, 6.0, (5,)),
+    ("ip1", 64, 48, 7, 16, 6.0, ()),
+    ("ip3", 176, 144, 8, 4, 8.0, (6,)),
+]
+
+
+def reference_records(ref, variant, frames, q, intra_at):
+    """The stock stream, its frame records in bitstream order (payload =
+    evx_frame + slice; record = what one decode() call reads, the first with
+    the header in front) and the encoder's final reconstruction of each frame
+    by display order."""
+    T, h, w, _ = frames.shape
+    stock = ref.encode_stream(frames, quality=q, intra_at=intra_at)
+    rc = ref.context(w, h)
+    if variant is None:
+        plan = plan_gop(T, quality=q, intra_at=intra_at)
+    else:
+        plan = plan_ip(T, quality=q, intra_at=intra_at, ref_count=REF_VARIANTS[variant][2])
+    final, payloads = {}, []
+    for ti, f18 in plan:
+        d, sl = rc.encode_frame(frames[ti], f18)
+        payloads.append(bytes(f18[:len(f18) if variant is None else 10]) + sl)
+        final[unpack_frame(f18)["display_order"] if variant is None else ti] = d.final
+    if variant is None:
+        assert split_stream(stock)[1] == payloads
+        records = [len(p).to_bytes(4, "little") + p for p in payloads]
+    else:
+        assert stock[:14] + b"".join(payloads) == stock
+        records = list(payloads)
+    records[0] = stock[:14] + records[0]
+    return stock, payloads, records, final
+
+
+@pytest.mark.parametrize("variant,w,h,T,q,vmax,intra_at", DEC_CASES)
+def test_staged_reference_decoder_equals_stock_decoder(oracle, variant, w, h, T, q, vmax, intra_at):
+    """The staged engine_decode_frame (unserialize, decode_slice, deblock, SAO,
+    YUV -> RGB) gives the stock evx3_decoder's frames; its RGB is the restated
+    conversion of its final reconstruction.  Without an inserted intra frame in
+    the default build the decoder reproduces the encoder's reconstruction; with
+    one, the reference's decoder departs from its encoder: unserialize_slice
+    writes only the fields it codes, so the intra frame's descriptors keep the
+    previous B frame's prediction fields, which the next P frame's motion
+    vector prediction reads (the encoder cleared them)."""
+    ref = Ref() if variant is None else variant_ref(variant)
+    frames = generate(w, h, T, seed=w + 3 * h + q, vmax=vmax)
+    stock, payloads, records, final = reference_records(ref, variant, frames, q, intra_at)
+    dec = ref.decode_records(records, w, h)
+    assert len(dec) == T
+    if variant is None:   # the default build's records carry sizes: the whole stream decodes in one go
+        assert np.array_equal(ref.decode_stream(stock, w, h), dec)
+    dc = ref.decoder(w, h)
+    aw, ah = (w + 15) & ~15, (h + 15) & ~15
+    staged = {}
+    for k, p in enumerate(payloads):
+        d = dc.decode_frame(p)
+        assert np.array_equal(d["rgb"], oracle.yuv_to_rgb(d["final"], aw, ah, w, h)), f"record {k}: YUV -> RGB"
+        staged[unpack_frame(d["frame18"])["display_order"] if variant is None else k] = d
+    for k in range(T):
+        assert np.array_equal(dec[k], staged[k]["rgb"]), f"frame {k} (display order)"
+    same = [np.array_equal(staged[k]["final"], final[k]) for k in range(T)]
+    if variant is not None or not intra_at:
+        assert all(same)
+    else:
+        assert not all(same)
