@@ -255,6 +255,7 @@ def run_gpu(args):
     h2d = W * H * 3
     d2h = nblk * 28 * 2 + nblk * 16 + plane_elems * 2
 
+    decode, decoded = run_decode(args, slices, stream) if world == 1 else (None, None)
     batched = run_batched(args, stream) if args.batch > 1 and world == 1 else None
     served = run_served(args) if args.serve_streams > 0 and world == 1 else None
     served_light = (run_served(args, n=8, per=args.serve_frames, sizes_from=[(640, 360), (1280, 720)], seed=11)
@@ -290,13 +291,14 @@ def run_gpu(args):
         "gpu_launches": launches,
         "quality_legs": legs,
         "default_gop": default_gop,
+        "decode": decode,
         "batched": batched,
         "served": served,
         "served_light": served_light,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"], line["parity"] = cpu_baseline(order, slices, frames)
+        line["cpu_baseline"], line["parity"] = cpu_baseline(order, slices, frames, decoded)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -356,6 +358,98 @@ def run_e2e(args, frames, order, stream):
         t1 = time.perf_counter()
     st.close()
     return t1 - t0, slices, threads
+
+
+def decode_bytes_per_frame(aw: int, ah: int) -> int:
+    """Algorithmic HBM bytes of one decoded frame: the macroblock reconstruction
+    reads a reference plane set and the level planes and writes the
+    destination; deblocking reads and writes it; the SAO pass copies it, then
+    reads the copy and reads and writes the slot; the conversion reads it and
+    writes RGB24 (one plane set = aw*ah*3/2 int16 samples)."""
+    ps = aw * ah * 3
+    return 3 * ps + 2 * ps + 2 * ps + 3 * ps + ps + aw * ah * 3
+
+
+def run_decode(args, slices, stream):
+    """The decoder on the GPU arm's own stream (its e2e leg's records: I/P,
+    three references, 1080p), frames 0..warmup-1 decoded untimed first (the
+    DPB needs them):
+      device -- the tables entropy-decoded beforehand and resident in HBM, each
+                frame's evxg_decode_frame (macroblock reconstruction,
+                deblocking, SAO, RGB24 into HBM) timed with CUDA events, L2
+                flushed between frames;
+      e2e    -- record bytes in host memory to RGB24 in pinned host memory
+                through evxg_decoder_decode_record (host entropy decoding,
+                copies, the same kernels), wall clock.
+    Returns the leg's JSON object and the e2e leg's frames (decode order)."""
+    import ctypes as C
+    import torch
+    import chicago_b200 as cb
+    L = cb.lib()
+    sp = C.c_void_p(stream.cuda_stream)
+    aw, ah = W, (H + 15) & ~15
+    nblk, ne = (aw // 16) * (ah // 16), aw * ah * 3 // 2
+    blocks, prev = np.zeros(nblk * 28, np.uint8), np.zeros(nblk * 28, np.uint8)
+    sao, lev = np.zeros(nblk * 16, np.uint8), np.zeros(ne, np.int16)
+    tabs, ent_s = [], 0.0
+    for f18, sl in slices:   # I/P build: every frame updates the temporal table
+        t0 = time.perf_counter()
+        cb.unserialize_slice(CFG, aw, ah, f18, sl, blocks, prev, sao, lev)
+        ent_s += time.perf_counter() - t0
+        prev[:] = blocks
+        tabs.append(tuple(torch.from_numpy(a.copy()).cuda() for a in (blocks, sao, lev)))
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    rgb = torch.empty(H * W * 3, dtype=torch.uint8, device="cuda")
+    dec = cb.Decoder(W, H, CFG)
+    evs = []
+    for i, ((f18, _), (bt, sa, lv)) in enumerate(zip(slices, tabs)):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        cb._check(L.evxg_decode_frame(dec.h, f18, C.c_void_p(bt.data_ptr()), C.c_void_p(sa.data_ptr()),
+                                      C.c_void_p(lv.data_ptr()), 1, C.c_void_p(rgb.data_ptr()), 1, sp))
+        e1.record()
+        if i >= args.warmup:
+            evs.append((e0, e1))
+    dec.sync(stream.cuda_stream)
+    ms = [a.elapsed_time(b) for a, b in evs]
+    device_last = rgb.cpu().numpy().reshape(H, W, 3)
+    dec.close()
+    # e2e: the .evx bytes, record by record
+    data = np.frombuffer(cb.stream_header(CFG, W, H) + b"".join(bytes(f18[:10]) + sl for f18, sl in slices), np.uint8)
+    out = torch.empty(H * W * 3, dtype=torch.uint8).pin_memory()
+    dec = cb.Decoder(W, H, CFG)
+    f = (C.c_uint8 * 18)()
+    n = C.c_uint64(0)
+    pos, frames_out, t0 = 14, [], None
+    for i in range(len(slices)):
+        if i == args.warmup:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+        cb._check(L.evxg_decoder_decode_record(dec.h, C.c_void_p(data.ctypes.data + pos), len(data) - pos,
+                                               C.c_void_p(out.data_ptr()), f, C.byref(n), sp))
+        pos += n.value
+        frames_out.append(out.numpy().reshape(H, W, 3).copy())
+    e2e_s = time.perf_counter() - t0
+    dec.close()
+    K = len(slices) - args.warmup
+    dbytes = decode_bytes_per_frame(aw, ah)
+    peak, peak_kind = peaks()
+    line = {
+        "value": round(K * EQ / (sum(ms) / 1e3), 3), "unit": UNIT, "ms_per_step": round(sum(ms) / K, 3),
+        "p99_frame_ms": round(float(np.percentile(ms, 99)), 3),
+        "roofline": {"bound": "hbm", "algorithmic_bytes_per_frame": dbytes,
+                     "achieved": round(dbytes * K / (sum(ms) / 1e3) / 1e9, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(dbytes * K / (sum(ms) / 1e3) / 1e9 / peak, 4), "peak_source": f"{peak_kind} hbm_gbs"},
+        "e2e": {"value": round(K * EQ / e2e_s, 3), "unit": UNIT, "ms_per_step": round(e2e_s * 1e3 / K, 3),
+                "entropy_ms_per_frame": round(ent_s * 1e3 / len(slices), 3),
+                "h2d_bytes_per_step": int(np.mean([len(sl) + 10 for _, sl in slices])) + nblk * 44 + ne * 2,
+                "d2h_bytes_per_step": W * H * 3},
+        "device_equals_e2e": bool(np.array_equal(device_last, frames_out[-1])),
+        "workload": f"decoding the GPU arm's own {CFG} stream of frames 0..{len(slices) - 1} (1920x1080, quality "
+                    f"{QUALITY}); timed frames {args.warmup}..{len(slices) - 1}",
+    }
+    return line, frames_out
 
 
 # The batched configuration: 16 streams -- 4 x 1920x1080, 6 x 1280x720,
@@ -514,7 +608,7 @@ def run_served(args, n=None, per=None, sizes_from=None, seed=7):
             "note": "latency = results seen by the host minus arrival (I/P GOP: no reorder wait), queueing included"}
 
 
-def cpu_baseline(order, slices, frames):
+def cpu_baseline(order, slices, frames, decoded=None):
     """The reference encoder of the same build (I/P, three references; built
     here from its sources) on the host cores, over the GPU arm's warm-up and
     timed frames: with its WPP threads on all cores, and single-threaded
@@ -552,6 +646,16 @@ def cpu_baseline(order, slices, frames):
               "bytes": len(stock),
               "how": "the .evx stream of every warm-up and timed frame from the GPU arm's e2e leg (GPU pixel pipeline + "
                      "the library's host entropy coder) vs the reference build's stock stream of the same frames"}
+    if decoded is not None:   # the reference decoder on the same records, one per call (its I/P build's framing)
+        records = [bytes(f18[:10]) + sl for f18, sl in slices]
+        records[0] = cb.stream_header(CFG, W, H) + records[0]
+        t0 = time.perf_counter()
+        want = ref.decode_records(records, W, H)
+        dt = time.perf_counter() - t0
+        base["decode"] = {"value": round(len(records) * EQ / dt, 4), "unit": UNIT, "cores": os.cpu_count(),
+                          "sample": f"frames 0..{len(records) - 1}: the reference decoder (evx3_decoder, WPP threads) "
+                                    "on the GPU arm's records, entropy decoding included"}
+        parity["decode_match"] = len(want) == len(decoded) and all(np.array_equal(a, b) for a, b in zip(want, decoded))
     return base, parity
 
 

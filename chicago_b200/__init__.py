@@ -59,6 +59,7 @@ EXPORTS = [
     "evxg_serialize_slice", "evxg_stream_header", "evxg_encoder_set_output", "evxg_server_create_lanes",
     "evxg_decoder_create", "evxg_decoder_destroy", "evxg_decode_frame", "evxg_decoder_sync",
     "evxg_decoder_fetch_planes", "evxg_decoder_set_timeout_ns", "evxg_decoder_reset",
+    "evxg_unserialize_slice", "evxg_decoder_decode_record",
 ]
 MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
 
@@ -173,6 +174,9 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_decoder_fetch_planes.argtypes = [vp, u32, vp, i32, vp]
     L.evxg_decoder_set_timeout_ns.argtypes = [vp, C.c_int64]
     L.evxg_decoder_reset.argtypes = [vp, vp]
+    L.evxg_unserialize_slice.argtypes = [C.POINTER(Config), u32, u32, C.c_char_p, vp, u64, vp, vp, vp, vp,
+                                         C.POINTER(u64)]
+    L.evxg_decoder_decode_record.argtypes = [vp, vp, u64, vp, vp, C.POINTER(u64), vp]
     return L
 
 
@@ -220,6 +224,22 @@ def serialize_slice(cfg, aligned_w: int, aligned_h: int, frame18: bytes, blocks,
                                       _ptr(np.ascontiguousarray(prev_blocks)), _ptr(np.ascontiguousarray(sao)),
                                       _ptr(np.ascontiguousarray(levels)), _ptr(out), cap, C.byref(n)))
     return out[:n.value].tobytes()
+
+
+def unserialize_slice(cfg, aligned_w: int, aligned_h: int, frame18: bytes, data: bytes, blocks, prev_blocks, sao,
+                      levels) -> int:
+    """Entropy-decode one slice into blocks / sao / levels in place (the tables
+    persist across frames: only coded fields are written); returns the slice's
+    length in bytes (evxg_unserialize_slice)."""
+    c = config(cfg)
+    for a in (blocks, prev_blocks, sao, levels):
+        if not (isinstance(a, np.ndarray) and a.flags.c_contiguous):
+            raise ValueError("tables must be C-contiguous arrays")
+    buf = np.frombuffer(data, np.uint8)
+    n = C.c_uint64(0)
+    _check(lib().evxg_unserialize_slice(C.byref(c), aligned_w, aligned_h, frame18, _ptr(buf), len(data), _ptr(blocks),
+                                        _ptr(prev_blocks), _ptr(sao), _ptr(levels), C.byref(n)))
+    return n.value
 
 
 def stream_header(cfg, width: int, height: int) -> bytes:
@@ -352,6 +372,17 @@ class Decoder:
         self.sync(cuda_stream)
         return out
 
+    def decode_record(self, data, rgb: bool = True, cuda_stream=None):
+        """Decode the frame record at the start of data (bitstream order):
+        returns (rgb frame or None, 18-byte descriptor, bytes the record used)."""
+        buf = np.frombuffer(data, np.uint8)
+        out = np.empty((self.height, self.width, 3), np.uint8) if rgb else None
+        f = (C.c_uint8 * 18)()
+        n = C.c_uint64(0)
+        _check(lib().evxg_decoder_decode_record(self.h, _ptr(buf), len(buf), _ptr(out), f, C.byref(n),
+                                                _ptr(cuda_stream)))
+        return out, bytes(f), n.value
+
     def sync(self, cuda_stream=None):
         _check(lib().evxg_decoder_sync(self.h, _ptr(cuda_stream)))
 
@@ -365,6 +396,39 @@ class Decoder:
         out = np.zeros(self.plane_elems, np.int16)
         _check(lib().evxg_decoder_fetch_planes(self.h, slot, _ptr(out), 0, _ptr(cuda_stream)))
         return out
+
+
+class StreamDecoder:
+    """The reference's evx3_decoder (src/video/evx3.h:103-127) for a whole
+    .evx stream of the build ``cfg`` names: ``decode(data)`` reads the 14-byte
+    header (evxg_stream_header) and every frame record after it, and returns
+    the frames in display order -- the default build reorders its B frames
+    like evx3dec.cpp:137-185 -- as (H, W, 3) RGB24 arrays.  Records need no
+    size prefix: the entropy decoder finds each slice's end, so the I/P builds'
+    concatenated records decode too."""
+
+    def __init__(self, cfg="default"):
+        self.cfg = cfg
+        self.dec = None
+
+    def decode(self, data: bytes):
+        data = bytes(data)
+        if len(data) < 14 or data[:4] != b"EVX1":
+            raise EvxgError(8, "not an .evx stream (header)")
+        width, height = struct.unpack_from("<HH", data, 10)
+        self.width, self.height = width, height
+        self.dec = Decoder(width, height, self.cfg)
+        frames, pending, nxt, pos = [], {}, 0, 14
+        while pos < len(data):
+            rgb, f18, used = self.dec.decode_record(data[pos:])
+            pos += used
+            order = struct.unpack_from("<I", f18, 10)[0] if config(self.cfg).b_frames else len(frames) + len(pending)
+            pending[order] = rgb
+            while nxt in pending:
+                frames.append(pending.pop(nxt))
+                nxt += 1
+        frames.extend(pending[k] for k in sorted(pending))
+        return frames
 
 
 NO_FRAME = struct.pack("<iIHIBBBB", -1, 0, 0, 0, 0, 0, 0, 0)   # a stream without a frame in a batch tick

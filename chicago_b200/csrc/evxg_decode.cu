@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "evxg_internal.cuh"
 
@@ -494,6 +495,13 @@ struct evxg_decoder {
     uint8_t *rgb;
     int num_sms;
     long long timeout_ns;
+    // Entropy-decoded state of the host side (evx_context of the reference's
+    // decoder): the tables persist from frame to frame, since a slice
+    // rewrites only the fields it codes.
+    std::vector<evxg_block_desc> hbt, hprev;
+    std::vector<evxg_sao_info> hsao;
+    std::vector<int16_t> hlev;
+    uint32_t next_index;
 };
 
 static int decoder_zero(evxg_decoder *d, cudaStream_t st)   // every plane and table zero, like a new context
@@ -530,6 +538,15 @@ int evxg_decoder_create(uint32_t width, uint32_t height, const evxg_config *cfg,
     d->plane_elems = (size_t)d->W * d->H + 2 * (size_t)(d->W / 2) * (d->H / 2);
     d->timeout_ns = 5000000000LL;
     const size_t pb = d->plane_elems * sizeof(int16_t), nblk = (size_t)d->mbw * d->mbh;
+    try {
+        d->hbt.assign(nblk, evxg_block_desc{});
+        d->hprev.assign(nblk, evxg_block_desc{});
+        d->hsao.assign(nblk, evxg_sao_info{});
+        d->hlev.assign(d->plane_elems, 0);
+    } catch (const std::bad_alloc &) {
+        delete d;
+        return fail(EVXG_ERROR_OUTOFMEMORY, "evxg_decoder_create: host allocation");
+    }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&d->num_sms, cudaDevAttrMultiProcessorCount, dev);
@@ -554,6 +571,7 @@ int evxg_decoder_create(uint32_t width, uint32_t height, const evxg_config *cfg,
         evxg_decoder_destroy(d);
         return rc;
     }
+    d->next_index = 0;
     *out = d;
     return EVXG_SUCCESS;
 }
@@ -581,7 +599,45 @@ int evxg_decoder_reset(evxg_decoder *d, void *cuda_stream)
     const cudaStream_t st = (cudaStream_t)cuda_stream;
     const int rc = decoder_zero(d, st);
     if (rc) return rc;
+    std::fill(d->hbt.begin(), d->hbt.end(), evxg_block_desc{});
+    std::fill(d->hprev.begin(), d->hprev.end(), evxg_block_desc{});
+    std::fill(d->hsao.begin(), d->hsao.end(), evxg_sao_info{});
+    std::fill(d->hlev.begin(), d->hlev.end(), (int16_t)0);
+    d->next_index = 0;
     CK(cudaStreamSynchronize(st));
+    return EVXG_SUCCESS;
+}
+
+int evxg_decoder_decode_record(evxg_decoder *d, const uint8_t *data, uint64_t len, uint8_t *rgb, evxg_frame *frame_out,
+                               uint64_t *consumed, void *cuda_stream)
+{
+    if (!d || !data) return fail(EVXG_ERROR_INVALIDARG, "evxg_decoder_decode_record: null argument");
+    // default build: u32 size, 18-byte evx_frame, slice; without B frames: 10-byte evx_frame, slice
+    const bool sized = d->cfg.b_frames;
+    const uint64_t fbytes = sized ? 18 : 10, head = sized ? 4 : 0;
+    if (len < head + fbytes) return fail(EVXG_ERROR_INVALID_RESOURCE, "evxg_decoder_decode_record: record truncated");
+    uint64_t body = len - head;
+    if (sized) {
+        uint32_t n = 0;
+        std::memcpy(&n, data, 4);
+        if (n < fbytes || n > body) return fail(EVXG_ERROR_INVALID_RESOURCE, "evxg_decoder_decode_record: bad record size");
+        body = n;
+    }
+    evxg_frame f{};
+    std::memcpy(&f, data + head, fbytes);
+    if (f.index != d->next_index)   // evx3dec.cpp:86-96
+        return fail(EVXG_ERROR_INVALID_RESOURCE, "evxg_decoder_decode_record: frame index out of sequence");
+    uint64_t used = 0;
+    int rc = evxg_unserialize_slice(&d->cfg, d->W, d->H, &f, data + head + fbytes, body - fbytes, d->hbt.data(),
+                                    d->hprev.data(), d->hsao.data(), d->hlev.data(), &used);
+    if (rc) return rc;
+    rc = evxg_decode_frame(d, &f, d->hbt.data(), d->hsao.data(), d->hlev.data(), 0, rgb, 0, cuda_stream);
+    if (!rc) rc = evxg_decoder_sync(d, cuda_stream);
+    if (rc) return rc;
+    if (!(d->cfg.b_frames && f.type == EVXG_FRAME_BIDIR)) d->hprev = d->hbt;   // decode.cpp:601-609
+    d->next_index++;
+    if (frame_out) *frame_out = f;
+    if (consumed) *consumed = sized ? head + body : fbytes + used;
     return EVXG_SUCCESS;
 }
 

@@ -375,6 +375,234 @@ void code_plane(Coder &c, Model *sets, const evxg_block_desc *bt, const int16_t 
         }
 }
 
+// ------------------------------------------------------------- decoding
+
+// The arithmetic decoder of abac.cpp:165-559: a 32-bit window on the input,
+// read most significant bit first (after 32 leading bits; past the end of the
+// input the last bit read repeats), the interval split exactly as the coder
+// splits it, and the same rescalings, each pulling one more input bit.  The
+// coder emits one bit per rescaling plus two to close, so the slice's length
+// follows from the decoder's own count.
+class SliceDecoder {
+public:
+    SliceDecoder(const uint8_t *d, uint64_t n) : d_(d), nbits_(n * 8)
+    {
+        uint32_t b = 0;
+        for (int i = 0; i < 32; i++) {
+            if (pos_ < nbits_) b = bit_at(pos_++);
+            value_ = (value_ << 1) | b;
+        }
+    }
+    unsigned decode(Model &m)
+    {
+        const uint32_t mid = lo_ + (uint32_t)((uint64_t)(hi_ - lo_) * m.c[0] / (m.c[0] + m.c[1]));
+        unsigned bit;
+        if (value_ >= lo_ && value_ <= mid) { hi_ = mid; bit = 0; }
+        else if (value_ > mid && value_ <= hi_) { lo_ = mid + 1; bit = 1; }
+        else { bad_ = true; return 0; }   // outside the interval: not a slice of this format
+        if (++m.c[bit] + m.c[bit ^ 1u] >= 65536u) {
+            m.c[0] = (m.c[0] >> 1) | 1u;
+            m.c[1] = (m.c[1] >> 1) | 1u;
+        }
+        rescale();
+        return bit;
+    }
+    unsigned decode_own() { return decode(own_); }
+    uint32_t decode_bits(int n, Model &m)   // least significant bit first
+    {
+        uint32_t v = 0;
+        for (int i = 0; i < n; i++) v |= decode(m) << i;
+        return v;
+    }
+    // Exponential-Golomb code: the number k + 1 whose leading zeros precede it
+    // (stream.cpp:713-778).  Returns k + 1; more than 32 leading zeros is no
+    // code of this format.
+    uint32_t decode_golomb_number(Model &m)
+    {
+        int zeros = 0;
+        unsigned b = decode(m);
+        while (!b) {
+            if (++zeros > 32 || bad_) { bad_ = true; return 1; }
+            b = decode(m);
+        }
+        uint32_t v = 1;
+        for (int i = 0; i < zeros; i++) v = (v << 1) | decode(m);
+        return v;
+    }
+    uint16_t decode_unsigned(Model &m) { return (uint16_t)(decode_golomb_number(m) - 1u); }
+    int16_t decode_signed(Model &m)   // stream.cpp:780-857: low bit the sign, the rest the magnitude
+    {
+        int zeros = 0;
+        unsigned b = decode(m);
+        while (!b) {
+            if (++zeros > 32 || bad_) { bad_ = true; return 0; }
+            b = decode(m);
+        }
+        int16_t r = 1;
+        for (int i = 0; i < zeros; i++) r = (int16_t)((r << 1) | (int)decode(m));
+        const int16_t sign = (int16_t)(1 - 2 * (r & 1));
+        int16_t out = (int16_t)(sign * ((r >> 1) & 0x7FFF));
+        if (2 * zeros + 1 > 32) out = (int16_t)(out | 0x8000);
+        return out;
+    }
+    bool bad() const { return bad_; }
+    uint64_t bytes_used() const { return (shifts_ + 2 + 7) / 8; }
+
+private:
+    static constexpr uint32_t kHalf = 0x7FFFFFFFu, kQuarter = 0x3FFFFFFFu, kThreeQuarters = 0xBFFFFFFDu;
+    unsigned bit_at(uint64_t i) const { return (d_[i >> 3] >> (i & 7)) & 1u; }
+    void rescale()
+    {
+        uint32_t b = 0;
+        for (;;) {
+            if (hi_ <= kHalf) {
+            } else if (lo_ > kHalf) {
+                hi_ -= kHalf + 1; lo_ -= kHalf + 1; value_ -= kHalf + 1;
+            } else if (hi_ <= kThreeQuarters && lo_ > kQuarter) {
+                hi_ -= kQuarter + 1; lo_ -= kQuarter + 1; value_ -= kQuarter + 1;
+            } else {
+                return;
+            }
+            if (pos_ < nbits_) b = bit_at(pos_++);
+            hi_ = (hi_ << 1) | 1u;
+            lo_ <<= 1;
+            value_ = (value_ << 1) | b;
+            shifts_++;
+        }
+    }
+    const uint8_t *d_;
+    uint64_t nbits_, pos_ = 0, shifts_ = 0;
+    uint32_t lo_ = 0, hi_ = 0xFFFFFFFFu, value_ = 0;
+    Model own_;
+    bool bad_ = false;
+};
+
+// One 8x8 block: levels in raster order into blk (row stride `stride`), the
+// DC coded as the difference to pred_dc (unserialize.cpp:13-29,
+// stream.cpp:1077-1158).
+bool decode_block(SliceDecoder &c, Model *set, int16_t *blk, int stride, int16_t pred_dc, int kind)
+{
+    int16_t v[64] = {};
+    const uint16_t n = c.decode_unsigned(set[kLast]);
+    if (n > 64) return false;
+    if (n) {
+        const int last = n - 1;
+        uint8_t sig[64] = {};
+        for (int pos = 0; pos < last; pos++) sig[pos] = (uint8_t)c.decode(set[pos]);
+        sig[last] = 1;
+        int above1 = 0;
+        for (int pos = 0; pos <= last; pos++) {
+            if (!sig[pos]) continue;
+            const int grp = position_group(pos), st = above1;
+            uint16_t m = 1;
+            if (c.decode(set[kGt1 + 2 * grp + st])) {
+                above1 = 1;
+                m = 2;
+                if (c.decode(set[kGt2 + 2 * grp + st])) m = (uint16_t)(c.decode_unsigned(set[kRem + grp]) + 3);
+            }
+            int16_t x = (int16_t)m;
+            if (c.decode_own()) x = (int16_t)-x;
+            v[scan_at(kind, pos)] = x;
+        }
+    }
+    v[0] = (int16_t)(v[0] + pred_dc);
+    for (int r = 0; r < 8; r++) std::memcpy(blk + (size_t)r * stride, v + 8 * r, 16);
+    return !c.bad();
+}
+
+// unserialize_block_table_unified (unserialize.cpp:181-308): writes only the
+// fields the slice codes; the rest keep the values of earlier frames.
+void decode_metadata(SliceDecoder &c, MetaModels &mm, evxg_block_desc *bt, const evxg_block_desc *prev, uint32_t mbw,
+                     uint32_t n, int tbits, bool bidir)
+{
+    int16_t last_q = 0;
+    for (uint32_t i = 0; i < n && !c.bad(); i++) {
+        evxg_block_desc &d = bt[i];
+        d.block_type = (int32_t)c.decode_bits(3, mm.block_type);
+        if (d.block_type == INTRA_DEFAULT) {
+            const uint32_t bx = i % mbw, by = i / mbw;
+            const int left = (bx > 0 && bt[i - 1].block_type == INTRA_DEFAULT) ? bt[i - 1].intra_mode : 0;
+            const int top = (by > 0 && bt[i - mbw].block_type == INTRA_DEFAULT) ? bt[i - mbw].intra_mode : 0;
+            const int m0 = left, m1 = left == top ? (left == 0 ? 1 : 0) : top;
+            if (c.decode(mm.mpm_flag)) d.intra_mode = (uint8_t)(c.decode(mm.mpm_idx) ? m1 : m0);
+            else d.intra_mode = (uint8_t)c.decode_bits(3, mm.intra_mode);
+        }
+        if (!(d.block_type & BT_INTRA)) d.prediction_target = (uint8_t)c.decode_bits(tbits, mm.target);
+        if (d.block_type & BT_MOTION) {
+            int16_t px, py;
+            mv_predictor(bt, prev, mbw, i, px, py);
+            d.motion_x = (int16_t)(c.decode_signed(mm.mvd_x) + px);
+            d.motion_y = (int16_t)(c.decode_signed(mm.mvd_y) + py);
+            d.sp_pred = (uint8_t)c.decode(mm.sp_pred);
+            if (d.sp_pred) {
+                d.sp_amount = (uint8_t)c.decode(mm.sp_amount);
+                d.sp_index = (uint8_t)c.decode_bits(3, mm.sp_index);
+            }
+        }
+        if (bidir && !(d.block_type & BT_INTRA)) {
+            d.prediction_mode = (uint8_t)c.decode_bits(2, mm.b_mode);
+            if (d.prediction_mode == 2) {
+                d.prediction_target_b = (uint8_t)c.decode_bits(tbits, mm.b_target);
+                d.motion_x_b = c.decode_signed(mm.b_mvd_x);
+                d.motion_y_b = c.decode_signed(mm.b_mvd_y);
+                d.sp_pred_b = (uint8_t)c.decode(mm.b_sp_pred);
+                if (d.sp_pred_b) {
+                    d.sp_amount_b = (uint8_t)c.decode(mm.b_sp_amount);
+                    d.sp_index_b = (uint8_t)c.decode_bits(3, mm.b_sp_index);
+                }
+            }
+        }
+        if (!(d.block_type & BT_COPY)) {
+            d.q_index = (uint8_t)(c.decode_signed(mm.qdelta) + last_q);
+            last_q = d.q_index;
+        }
+    }
+}
+
+void decode_sao(SliceDecoder &c, MetaModels &mm, evxg_sao_info *sao, uint32_t mbw, uint32_t n)   // unserialize.cpp:573-632
+{
+    for (uint32_t i = 0; i < n && !c.bad(); i++) {
+        evxg_sao_info &s = sao[i];
+        s = evxg_sao_info{};
+        if (i % mbw > 0) s.merge_left = (uint8_t)c.decode(mm.sao_merge);
+        if (!s.merge_left && i / mbw > 0) s.merge_above = (uint8_t)c.decode(mm.sao_merge);
+        if (s.merge_left || s.merge_above) continue;
+        for (evxg_sao_params *p : {&s.luma, &s.chroma}) {
+            p->type = (uint8_t)c.decode_bits(2, mm.sao_type);
+            if (p->type == 1) p->eo_class = (uint8_t)c.decode_bits(2, mm.sao_eo_class);
+            else if (p->type == 2) p->band_position = (uint8_t)c.decode_signed(mm.sao_band);
+            if (p->type != 0)
+                for (int k = 0; k < 4; k++) p->offsets[k] = (int8_t)c.decode_signed(mm.sao_offset);
+        }
+    }
+}
+
+// Residuals of one plane (unserialize.cpp:43-148), the mirror of code_plane.
+bool decode_plane(SliceDecoder &c, Model *sets, const evxg_block_desc *bt, int16_t *pl, int w, int h, bool luma)
+{
+    const int n = luma ? 16 : 8;
+    uint32_t i = 0;
+    for (int y = 0; y < h; y += n)
+        for (int x = 0; x < w; x += n, i++) {
+            const evxg_block_desc &d = bt[i];
+            if (d.block_type & BT_COPY) continue;
+            int16_t pdc = 0;
+            if (x >= n) pdc = pl[(size_t)y * w + x - 8];
+            else if (y >= n) pdc = pl[(size_t)(y - 8) * w + x];
+            Model *set = sets + (d.block_type == INTRA_DEFAULT ? 0 : kSetSize);
+            const int kind = scan_kind_of(d);
+            int16_t *b = pl + (size_t)y * w + x;
+            if (!decode_block(c, set, b, w, pdc, kind)) return false;
+            if (luma) {
+                if (!decode_block(c, set, b + 8, w, b[0], kind) ||
+                    !decode_block(c, set, b + 8 * (size_t)w, w, b[0], kind) ||
+                    !decode_block(c, set, b + 8 * (size_t)w + 8, w, b[8 * (size_t)w], kind))
+                    return false;
+            }
+        }
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -425,6 +653,38 @@ int evxg_stream_header(const evxg_config *cfg, uint32_t width, uint32_t height, 
     const uint8_t h[14] = {'E', 'V', 'X', '1', 14, 0, c.ref_count, 0, 11, 3, (uint8_t)(width & 0xFF), (uint8_t)(width >> 8),
                            (uint8_t)(height & 0xFF), (uint8_t)(height >> 8)};
     std::memcpy(out, h, 14);
+    return EVXG_SUCCESS;
+}
+
+int evxg_unserialize_slice(const evxg_config *cfg, uint32_t aligned_w, uint32_t aligned_h, const evxg_frame *frame,
+                           const uint8_t *data, uint64_t len, evxg_block_desc *blocks,
+                           const evxg_block_desc *prev_blocks, evxg_sao_info *sao, int16_t *levels, uint64_t *consumed)
+{
+    using evxg::fail;
+    if (!frame || !data || !blocks || !prev_blocks || !sao || !levels)
+        return fail(EVXG_ERROR_INVALIDARG, "evxg_unserialize_slice: null argument");
+    if (!aligned_w || !aligned_h || (aligned_w & 15) || (aligned_h & 15))
+        return fail(EVXG_ERROR_INVALIDARG, "evxg_unserialize_slice: aligned size must be a non-zero multiple of 16");
+    evxg_config c;
+    evxg_config_default(&c);
+    if (cfg) c = *cfg;
+    if (c.ref_count < 1 || c.ref_count > 4)
+        return fail(EVXG_ERROR_INVALIDARG, "evxg_unserialize_slice: bad reference count");
+    const uint32_t mbw = aligned_w / 16, n = mbw * (aligned_h / 16);
+    SliceDecoder dec(data, len);
+    MetaModels mm;
+    std::vector<Model> sets(2 * kSetSize);
+    decode_metadata(dec, mm, blocks, prev_blocks, mbw, n, target_bits(c.ref_count),
+                    c.b_frames && frame->type == EVXG_FRAME_BIDIR);
+    decode_sao(dec, mm, sao, mbw, n);
+    const size_t ny = (size_t)aligned_w * aligned_h, nc = (size_t)(aligned_w / 2) * (aligned_h / 2);
+    const bool ok = !dec.bad() &&
+                    decode_plane(dec, sets.data(), blocks, levels, (int)aligned_w, (int)aligned_h, true) &&
+                    decode_plane(dec, sets.data(), blocks, levels + ny, (int)aligned_w / 2, (int)aligned_h / 2, false) &&
+                    decode_plane(dec, sets.data(), blocks, levels + ny + nc, (int)aligned_w / 2, (int)aligned_h / 2, false);
+    if (consumed) *consumed = dec.bytes_used();
+    if (!ok) return fail(EVXG_ERROR_INVALID_RESOURCE, "evxg_unserialize_slice: not a slice of this format");
+    if (dec.bytes_used() > len) return fail(EVXG_ERROR_INVALID_RESOURCE, "evxg_unserialize_slice: slice truncated");
     return EVXG_SUCCESS;
 }
 

@@ -389,6 +389,37 @@ int evxg_decoder_fetch_planes(evxg_decoder *d, uint32_t slot, int16_t *out, int 
 int evxg_decoder_set_timeout_ns(evxg_decoder *d, int64_t ns);
 int evxg_decoder_reset(evxg_decoder *d, void *cuda_stream);
 
+/* The host entropy decoder: unserialize_slice (unserialize.cpp:634-696), the
+ * inverse of evxg_serialize_slice.  Decodes one slice (data, len bytes; bytes
+ * after the slice may follow) into tables that persist from frame to frame
+ * the way the reference decoder's context does: a block descriptor gets only
+ * the fields the slice codes (block type; intra mode of intra-default blocks;
+ * prediction target of inter blocks; vector and sub-pel fields of motion
+ * blocks; the second reference's fields of inter blocks in B frames; QP of
+ * blocks that are not copies), the others keep earlier frames' values; every
+ * SAO entry is cleared and then decoded; the level planes of blocks that are
+ * not copies are rewritten.  prev_blocks is the temporal predictor table (the
+ * block table after the last frame that is not a B frame, zero before the
+ * first).  *consumed receives the slice's length in bytes, known from the
+ * arithmetic decoder itself, so records without a size prefix can be cut.
+ * EVXG_ERROR_INVALID_RESOURCE for data that is not such a slice. */
+int evxg_unserialize_slice(const evxg_config *cfg, uint32_t aligned_w, uint32_t aligned_h, const evxg_frame *frame,
+                           const uint8_t *data, uint64_t len, evxg_block_desc *blocks,
+                           const evxg_block_desc *prev_blocks, evxg_sao_info *sao, int16_t *levels,
+                           uint64_t *consumed);
+/* One frame record of a stream, the reference decoder's decode() without its
+ * display reorder (evx3dec.cpp:104-215): default build -- a 4-byte size, the
+ * 18-byte evxg_frame, the slice; without B frames -- the first 10 bytes of
+ * evxg_frame and the slice.  Entropy-decodes on the host into the decoder's
+ * own tables, runs evxg_decode_frame and waits for it, and updates the
+ * temporal predictor table after frames that are not B frames.  Frames must
+ * come in bitstream order (index 0, 1, ...; EVXG_ERROR_INVALID_RESOURCE
+ * otherwise).  rgb (host, may be NULL) receives the frame in decode order;
+ * *frame_out its descriptor; *consumed the record's length, so concatenated
+ * records of either build can be cut. */
+int evxg_decoder_decode_record(evxg_decoder *d, const uint8_t *data, uint64_t len, uint8_t *rgb, evxg_frame *frame_out,
+                               uint64_t *consumed, void *cuda_stream);
+
 /* Human-readable text of the last error on this thread. */
 const char *evxg_last_error(void);
 
