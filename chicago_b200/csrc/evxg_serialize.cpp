@@ -385,7 +385,7 @@ void code_plane(Coder &c, Model *sets, const evxg_block_desc *bt, const int16_t 
 // follows from the decoder's own count.
 class SliceDecoder {
 public:
-    SliceDecoder(const uint8_t *d, uint64_t n) : d_(d), nbits_(n * 8)
+    SliceDecoder(const uint8_t *d, uint64_t n) : d_(d), nbits_(n * 8), rcp_(reciprocals().r)
     {
         uint32_t b = 0;
         for (int i = 0; i < 32; i++) {
@@ -395,11 +395,13 @@ public:
     }
     unsigned decode(Model &m)
     {
-        const uint32_t mid = lo_ + (uint32_t)((uint64_t)(hi_ - lo_) * m.c[0] / (m.c[0] + m.c[1]));
-        unsigned bit;
-        if (value_ >= lo_ && value_ <= mid) { hi_ = mid; bit = 0; }
-        else if (value_ > mid && value_ <= hi_) { lo_ = mid + 1; bit = 1; }
-        else { bad_ = true; return 0; }   // outside the interval: not a slice of this format
+        const uint32_t mid = lo_ + (uint32_t)div_small((uint64_t)(hi_ - lo_) * m.c[0], m.c[0] + m.c[1], rcp_);
+        // The value lies in [low, high] for any slice of this format; outside
+        // it the data is something else (flagged; the caller stops).
+        bad_ |= (value_ < lo_) | (value_ > hi_);
+        const unsigned bit = value_ > mid;   // selects, not branches: the decisions are unpredictable
+        hi_ = bit ? hi_ : mid;
+        lo_ = bit ? mid + 1 : lo_;
         if (++m.c[bit] + m.c[bit ^ 1u] >= 65536u) {
             m.c[0] = (m.c[0] >> 1) | 1u;
             m.c[1] = (m.c[1] >> 1) | 1u;
@@ -449,29 +451,47 @@ public:
     uint64_t bytes_used() const { return (shifts_ + 2 + 7) / 8; }
 
 private:
-    static constexpr uint32_t kHalf = 0x7FFFFFFFu, kQuarter = 0x3FFFFFFFu, kThreeQuarters = 0xBFFFFFFDu;
+    static constexpr uint32_t kQuarter = 0x3FFFFFFFu, kThreeQuarters = 0xBFFFFFFDu;
     unsigned bit_at(uint64_t i) const { return (d_[i >> 3] >> (i & 7)) & 1u; }
+    // The next input bit; within one rescaling, past the end of the input the
+    // last bit read repeats (0 if none was read yet), as abac.cpp:306-349 reads.
+    unsigned next_bit()
+    {
+        if (pos_ < nbits_) last_ = bit_at(pos_++);
+        return last_;
+    }
+    // abac.cpp:306-349.  When low and high share their k leading bits, k
+    // rescalings in a row shift them out (a lower-half one doubles the
+    // interval, an upper-half one subtracts the half first -- the bit the
+    // shift drops anyway, since the value lies in the interval and shares
+    // those bits), so they happen at once; middle-half rescalings one by one.
     void rescale()
     {
-        uint32_t b = 0;
+        last_ = 0;
         for (;;) {
-            if (hi_ <= kHalf) {
-            } else if (lo_ > kHalf) {
-                hi_ -= kHalf + 1; lo_ -= kHalf + 1; value_ -= kHalf + 1;
+            const uint32_t same = ~(hi_ ^ lo_);
+            if (same & 0x80000000u) {   // low < high, so k < 32
+                const int k = __builtin_clz(~same);
+                uint32_t in = 0;
+                for (int i = 0; i < k; i++) in = (in << 1) | next_bit();
+                hi_ = (hi_ << k) | ((1u << k) - 1u);
+                lo_ <<= k;
+                value_ = (value_ << k) | in;
+                shifts_ += (uint64_t)k;
             } else if (hi_ <= kThreeQuarters && lo_ > kQuarter) {
-                hi_ -= kQuarter + 1; lo_ -= kQuarter + 1; value_ -= kQuarter + 1;
+                hi_ = ((hi_ - (kQuarter + 1)) << 1) | 1u;
+                lo_ = (lo_ - (kQuarter + 1)) << 1;
+                value_ = ((value_ - (kQuarter + 1)) << 1) | next_bit();
+                shifts_++;
             } else {
                 return;
             }
-            if (pos_ < nbits_) b = bit_at(pos_++);
-            hi_ = (hi_ << 1) | 1u;
-            lo_ <<= 1;
-            value_ = (value_ << 1) | b;
-            shifts_++;
         }
     }
     const uint8_t *d_;
     uint64_t nbits_, pos_ = 0, shifts_ = 0;
+    const uint64_t *rcp_;
+    unsigned last_ = 0;
     uint32_t lo_ = 0, hi_ = 0xFFFFFFFFu, value_ = 0;
     Model own_;
     bool bad_ = false;
