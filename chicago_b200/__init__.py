@@ -60,6 +60,9 @@ EXPORTS = [
     "evxg_decoder_create", "evxg_decoder_destroy", "evxg_decode_frame", "evxg_decoder_sync",
     "evxg_decoder_fetch_planes", "evxg_decoder_set_timeout_ns", "evxg_decoder_reset",
     "evxg_unserialize_slice", "evxg_decoder_decode_record",
+    "evxg_muxer_open", "evxg_muxer_add_video_stream", "evxg_muxer_add_audio_stream", "evxg_muxer_write_header",
+    "evxg_muxer_write_packet", "evxg_muxer_close", "evxg_demuxer_open", "evxg_demuxer_stream_count",
+    "evxg_demuxer_stream", "evxg_demuxer_read_packet", "evxg_demuxer_close",
 ]
 MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
 
@@ -91,6 +94,18 @@ class FrameTimes(C.Structure):
 
 RESULT_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                         C.POINTER(FrameTimes))
+
+
+class StreamDesc(C.Structure):
+    """evxg_stream_desc: one stream of a container (video: size and frame
+    rate; audio: sample rate, channels, bit depth, quality)."""
+    _fields_ = [("stream_type", C.c_uint8), ("stream_id", C.c_uint8), ("width", C.c_uint16), ("height", C.c_uint16),
+                ("frame_rate", C.c_float), ("sample_rate", C.c_uint32), ("channels", C.c_uint8),
+                ("bit_depth", C.c_uint8), ("quality", C.c_uint8)]
+
+
+STREAM_TYPE_VIDEO, STREAM_TYPE_AUDIO = 0, 1
+OPERATION_COMPLETED, CAPACITY_LIMIT = 16, 7
 
 
 class EvxgError(RuntimeError):
@@ -177,6 +192,19 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_unserialize_slice.argtypes = [C.POINTER(Config), u32, u32, C.c_char_p, vp, u64, vp, vp, vp, vp,
                                          C.POINTER(u64)]
     L.evxg_decoder_decode_record.argtypes = [vp, vp, u64, vp, vp, C.POINTER(u64), vp]
+    L.evxg_muxer_open.argtypes = [C.c_char_p, C.POINTER(vp)]
+    L.evxg_muxer_add_video_stream.argtypes = [vp, C.c_uint16, C.c_uint16, C.c_float, C.POINTER(C.c_uint8)]
+    L.evxg_muxer_add_audio_stream.argtypes = [vp, u32, C.c_uint8, C.c_uint8, C.c_uint8, C.POINTER(C.c_uint8)]
+    L.evxg_muxer_write_header.argtypes = [vp]
+    L.evxg_muxer_write_packet.argtypes = [vp, C.c_uint8, C.c_uint8, u64, vp, u32]
+    L.evxg_muxer_close.argtypes = [vp]
+    L.evxg_demuxer_open.argtypes = [C.c_char_p, C.POINTER(vp)]
+    L.evxg_demuxer_stream_count.argtypes = [vp]
+    L.evxg_demuxer_stream_count.restype = u32
+    L.evxg_demuxer_stream.argtypes = [vp, u32, C.POINTER(StreamDesc)]
+    L.evxg_demuxer_read_packet.argtypes = [vp, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8), C.POINTER(u64), vp, u32,
+                                           C.POINTER(u32)]
+    L.evxg_demuxer_close.argtypes = [vp]
     return L
 
 
@@ -396,6 +424,84 @@ class Decoder:
         out = np.zeros(self.plane_elems, np.int16)
         _check(lib().evxg_decoder_fetch_planes(self.h, slot, _ptr(out), 0, _ptr(cuda_stream)))
         return out
+
+
+class Muxer:
+    """The packet container writer (evxg_muxer_*; the reference's evx_muxer)."""
+
+    def __init__(self, path: str):
+        h = C.c_void_p()
+        _check(lib().evxg_muxer_open(os.fsencode(path), C.byref(h)))
+        self.h = h
+
+    def add_video_stream(self, width: int, height: int, frame_rate: float) -> int:
+        sid = C.c_uint8()
+        _check(lib().evxg_muxer_add_video_stream(self.h, width, height, frame_rate, C.byref(sid)))
+        return sid.value
+
+    def add_audio_stream(self, sample_rate: int, channels: int, bit_depth: int, quality: int) -> int:
+        sid = C.c_uint8()
+        _check(lib().evxg_muxer_add_audio_stream(self.h, sample_rate, channels, bit_depth, quality, C.byref(sid)))
+        return sid.value
+
+    def write_header(self):
+        _check(lib().evxg_muxer_write_header(self.h))
+
+    def write_packet(self, stream_id: int, stream_type: int, timestamp_us: int, payload: bytes):
+        buf = np.frombuffer(bytes(payload), np.uint8)
+        _check(lib().evxg_muxer_write_packet(self.h, stream_id, stream_type, timestamp_us, _ptr(buf), len(buf)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            h, self.h = self.h, None
+            _check(lib().evxg_muxer_close(h))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Demuxer:
+    """The packet container reader (evxg_demuxer_*; the reference's evx_demuxer):
+    ``streams`` lists the descriptors, iterating yields (stream_id, stream_type,
+    timestamp_us, payload) per packet."""
+
+    def __init__(self, path: str):
+        h = C.c_void_p()
+        _check(lib().evxg_demuxer_open(os.fsencode(path), C.byref(h)))
+        self.h = h
+        self.streams = []
+        for i in range(lib().evxg_demuxer_stream_count(self.h)):
+            d = StreamDesc()
+            _check(lib().evxg_demuxer_stream(self.h, i, C.byref(d)))
+            self.streams.append(d)
+
+    def __iter__(self):
+        buf = np.empty(1 << 20, np.uint8)
+        sid, stype, ts, n = C.c_uint8(), C.c_uint8(), C.c_uint64(), C.c_uint32()
+        while True:
+            rc = lib().evxg_demuxer_read_packet(self.h, C.byref(sid), C.byref(stype), C.byref(ts), _ptr(buf), len(buf),
+                                                C.byref(n))
+            if rc == OPERATION_COMPLETED:
+                return
+            if rc == CAPACITY_LIMIT:
+                buf = np.empty(n.value, np.uint8)
+                continue
+            _check(rc)
+            yield sid.value, stype.value, ts.value, buf[:n.value].tobytes()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().evxg_demuxer_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class StreamDecoder:

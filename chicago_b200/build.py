@@ -17,7 +17,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libevxg.so")
 SOURCES = ["evxg_mb.cu", "evxg_filters.cu", "evxg_api.cu", "evxg_batch.cu", "evxg_serve.cu", "evxg_noalloc.cu", "evxg_decode.cu",
-           "evxg_serialize.cpp"]
+           "evxg_serialize.cpp", "evxg_mux.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 

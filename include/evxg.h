@@ -37,6 +37,9 @@ extern "C" {
 #define EVXG_ERROR_INVALID_RESOURCE 8
 #define EVXG_ERROR_OPERATION_TIMEDOUT 9
 #define EVXG_ERROR_EXECUTION_FAILURE 10
+#define EVXG_ERROR_IO_FAILURE     12
+#define EVXG_ERROR_NOT_READY      15
+#define EVXG_ERROR_OPERATION_COMPLETED 16
 
 /* Frame types (reference types.h:45-53). */
 #define EVXG_FRAME_INTRA 0
@@ -419,6 +422,51 @@ int evxg_unserialize_slice(const evxg_config *cfg, uint32_t aligned_w, uint32_t 
  * records of either build can be cut. */
 int evxg_decoder_decode_record(evxg_decoder *d, const uint8_t *data, uint64_t len, uint8_t *rgb, evxg_frame *frame_out,
                                uint64_t *consumed, void *cuda_stream);
+
+/* ---- Container ----
+ *
+ * The reference's packet container (evx_muxer / evx_demuxer, muxer.h:53-160,
+ * muxer.cpp), byte for byte: a 10-byte header ("EVX3", u32 header size,
+ * version 1, stream count), an 18-byte descriptor per stream (type, id,
+ * width, height, f32 frame rate, u32 sample rate, channels, bit depth,
+ * quality, a zero pad byte), then packets of a 16-byte header ("EP", stream
+ * id, stream type, u64 timestamp in microseconds, u32 payload size) and the
+ * payload; all little-endian.  A video stream's packets carry the .evx
+ * stream as the reference's encoder tool cuts it (tools/evx_encode.cpp:
+ * 185-275): the stream header with the first frame record, then one frame
+ * record per packet. */
+#define EVXG_STREAM_TYPE_VIDEO 0
+#define EVXG_STREAM_TYPE_AUDIO 1
+typedef struct evxg_stream_desc {
+    uint8_t stream_type;
+    uint8_t stream_id;
+    uint16_t width, height;    /* video */
+    float frame_rate;          /* video */
+    uint32_t sample_rate;      /* audio */
+    uint8_t channels, bit_depth, quality;   /* audio */
+} evxg_stream_desc;
+typedef struct evxg_muxer evxg_muxer;
+/* Creates (truncates) the file; streams are added before the header is written. */
+int evxg_muxer_open(const char *path, evxg_muxer **out);
+int evxg_muxer_add_video_stream(evxg_muxer *m, uint16_t width, uint16_t height, float frame_rate, uint8_t *stream_id);
+int evxg_muxer_add_audio_stream(evxg_muxer *m, uint32_t sample_rate, uint8_t channels, uint8_t bit_depth,
+                                uint8_t quality, uint8_t *stream_id);
+int evxg_muxer_write_header(evxg_muxer *m);
+int evxg_muxer_write_packet(evxg_muxer *m, uint8_t stream_id, uint8_t stream_type, uint64_t timestamp_us,
+                            const void *payload, uint32_t size);
+/* Flushes and closes the file and frees m. */
+int evxg_muxer_close(evxg_muxer *m);
+typedef struct evxg_demuxer evxg_demuxer;
+/* Opens the file and reads its header and stream descriptors. */
+int evxg_demuxer_open(const char *path, evxg_demuxer **out);
+uint32_t evxg_demuxer_stream_count(const evxg_demuxer *d);
+int evxg_demuxer_stream(const evxg_demuxer *d, uint32_t index, evxg_stream_desc *out);
+/* The next packet: EVXG_ERROR_OPERATION_COMPLETED at the end of the file;
+ * EVXG_ERROR_CAPACITY_LIMIT (with *size set, the packet left unread) when
+ * capacity is too small. */
+int evxg_demuxer_read_packet(evxg_demuxer *d, uint8_t *stream_id, uint8_t *stream_type, uint64_t *timestamp_us,
+                             uint8_t *payload, uint32_t capacity, uint32_t *size);
+int evxg_demuxer_close(evxg_demuxer *d);
 
 /* Human-readable text of the last error on this thread. */
 const char *evxg_last_error(void);

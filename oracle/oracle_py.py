@@ -244,6 +244,12 @@ class Ref:
                                            C.c_uint32, C.POINTER(C.c_uint32)]
         L.evxref_decode_records.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
                                             C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]
+        L.evxref_mux_file.argtypes = [C.c_char_p, C.c_uint16, C.c_uint16, C.c_float, C.c_int, C.c_uint32, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]
+        L.evxref_encode_container.argtypes = [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double,
+                                              C.c_uint8]
+        L.evxref_demux_file.argtypes = [C.c_char_p, C.POINTER(C.c_uint32), C.c_void_p, C.c_uint64, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]
         L.evxref_dctx_create.restype = C.c_void_p
         L.evxref_dctx_create.argtypes = [C.c_uint32, C.c_uint32]
         L.evxref_dctx_destroy.argtypes = [C.c_void_p]
@@ -251,14 +257,15 @@ class Ref:
             [C.c_void_p] * 6
 
     # --- stock API ---
-    def encode_stream(self, frames: np.ndarray, quality: int = 8, intra_at=()) -> bytes:
-        """Encode (T,H,W,3) uint8 frames through create_encoder/encode/flush."""
+    def encode_stream(self, frames: np.ndarray, quality: int = 8, intra_at=(), chunks: bool = False):
+        """Encode (T,H,W,3) uint8 frames through create_encoder/encode/flush;
+        chunks=True: each encode() call's output and flush()'s, as a list."""
         T, H, W, _ = frames.shape
         cap = max(1 << 22, W * H * 3 * 8)
         h = self.lib.evxref_enc_create(cap)
         buf = np.zeros(cap, np.uint8)
         n = C.c_uint32(0)
-        out = bytearray()
+        out = []
         try:
             self.lib.evxref_enc_set_quality(h, quality)
             for t in range(T):
@@ -268,14 +275,14 @@ class Ref:
                 rc = self.lib.evxref_enc_encode(h, _p(f), W, H, _p(buf), cap, C.byref(n))
                 if rc:
                     raise RuntimeError(f"reference encode failed: {rc}")
-                out += buf[:n.value].tobytes()
+                out.append(buf[:n.value].tobytes())
             rc = self.lib.evxref_enc_flush(h, _p(buf), cap, C.byref(n))
             if rc:
                 raise RuntimeError(f"reference flush failed: {rc}")
-            out += buf[:n.value].tobytes()
+            out.append(buf[:n.value].tobytes())
         finally:
             self.lib.evxref_enc_destroy(h)
-        return bytes(out)
+        return out if chunks else b"".join(out)
 
     def decode_stream(self, data: bytes, width: int, height: int, max_frames: int = 256) -> np.ndarray:
         """Decode a whole .evx stream with the stock decoder; (T,H,W,3) frames in display order."""
@@ -299,6 +306,43 @@ class Ref:
         if rc:
             raise RuntimeError(f"reference decode failed: {rc} after {n.value} frames")
         return out[:n.value]
+
+    # --- container (evx_muxer / evx_demuxer) ---
+    def mux_file(self, path: str, width: int, height: int, fps: float, packets, with_audio: bool = False):
+        """Write packets [(timestamp_us, payload)] of one video stream with evx_muxer."""
+        data = np.frombuffer(b"".join(p for _, p in packets) or b"\0", np.uint8).copy()
+        offs = np.cumsum([0] + [len(p) for _, p in packets]).astype(np.uint32)
+        ts = np.array([t for t, _ in packets] or [0], np.uint64)
+        rc = self.lib.evxref_mux_file(os.fsencode(path), width, height, fps, int(with_audio), len(packets), _p(data),
+                                      _p(offs), _p(ts))
+        if rc:
+            raise RuntimeError(f"reference muxer failed: {rc}")
+
+    def encode_container(self, path: str, frames: np.ndarray, fps: float, quality: int):
+        """The reference encoder tool's video path over raw RGB24 frames (T,H,W,3)."""
+        T, H, W, _ = frames.shape
+        f = np.ascontiguousarray(frames)
+        rc = self.lib.evxref_encode_container(os.fsencode(path), _p(f), T, W, H, fps, quality)
+        if rc:
+            raise RuntimeError(f"reference container encode failed: {rc}")
+
+    def demux_file(self, path: str, max_packets: int = 4096):
+        """(stream count, [(stream_id, timestamp_us, payload)]) read with evx_demuxer."""
+        cap = os.path.getsize(path)
+        data = np.zeros(max(cap, 1), np.uint8)
+        sizes = np.zeros(max_packets, np.uint32)
+        ids = np.zeros(max_packets, np.uint8)
+        ts = np.zeros(max_packets, np.uint64)
+        ns, n = C.c_uint32(0), C.c_uint32(0)
+        rc = self.lib.evxref_demux_file(os.fsencode(path), C.byref(ns), _p(data), cap, _p(sizes), _p(ids), _p(ts),
+                                        max_packets, C.byref(n))
+        if rc:
+            raise RuntimeError(f"reference demuxer failed: {rc}")
+        out, pos = [], 0
+        for k in range(min(n.value, max_packets)):
+            out.append((int(ids[k]), int(ts[k]), data[pos:pos + sizes[k]].tobytes()))
+            pos += int(sizes[k])
+        return ns.value, out
 
     # --- staged engine ---
     def context(self, width: int, height: int):

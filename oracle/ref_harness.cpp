@@ -26,6 +26,7 @@
 #include "imageset.h"
 #include "sao.h"
 #include "bitstream.h"
+#include "muxer.h"
 
 #include <cstring>
 #include <cstdint>
@@ -241,6 +242,125 @@ static void copy_set(const image_set &s, int16_t *dst, uint32_t w, uint32_t h)
     memcpy(dst + (size_t)w * h, s.query_u_image()->query_data(), (size_t)(w / 2) * (h / 2) * 2);
     memcpy(dst + (size_t)w * h + (size_t)(w / 2) * (h / 2), s.query_v_image()->query_data(),
            (size_t)(w / 2) * (h / 2) * 2);
+}
+
+/* ---------------- container (src/muxer.cpp) ---------------- */
+
+/* A container written by the reference's evx_muxer: a video stream (w x h at
+ * fps; and an audio stream after it when with_audio), then n packets of the
+ * video stream, packet k = data[offsets[k] .. offsets[k+1]) at timestamp ts[k]. */
+int evxref_mux_file(const char *path, uint16_t w, uint16_t h, float fps, int with_audio, uint32_t n,
+                    const uint8_t *data, const uint32_t *offsets, const uint64_t *ts)
+{
+    evx_muxer mux;
+    uint8 vid = 0, aud = 0;
+    if (mux.open(path) != EVX_SUCCESS) return EVX_ERROR_IO_FAILURE;
+    mux.add_video_stream(w, h, fps, &vid);
+    if (with_audio) mux.add_audio_stream(48000, 2, 16, 5, &aud);
+    if (mux.write_header() != EVX_SUCCESS) return EVX_ERROR_IO_FAILURE;
+    for (uint32_t k = 0; k < n; k++)
+        if (mux.write_packet(vid, EVX_STREAM_TYPE_VIDEO, ts[k], data + offsets[k], offsets[k + 1] - offsets[k]) !=
+            EVX_SUCCESS)
+            return EVX_ERROR_IO_FAILURE;
+    mux.close();
+    return 0;
+}
+
+/* The reference encoder tool's video path (tools/evx_encode.cpp:143-275) on n
+ * raw RGB24 frames instead of FFmpeg's decoder: set_quality, encode() every
+ * frame into one bit stream, cut each call's output into packets as the tool
+ * does (with B frames: the first output whole -- stream header and the first
+ * record -- then one size-prefixed record per packet, flush() included;
+ * without: one packet per call), timestamps count * 10^6 / fps. */
+int evxref_encode_container(const char *path, const uint8_t *frames, uint32_t n, uint32_t w, uint32_t h, double fps,
+                            uint8_t quality)
+{
+    evx_muxer mux;
+    uint8 vid = 0;
+    if (mux.open(path) != EVX_SUCCESS) return EVX_ERROR_IO_FAILURE;
+    mux.add_video_stream((uint16)w, (uint16)h, (float32)fps, &vid);
+    mux.write_header();
+    evx3_encoder *enc = nullptr;
+    if (create_encoder(&enc) != EVX_SUCCESS) return EVX_ERROR_EXECUTION_FAILURE;
+    enc->set_quality(quality);
+    bit_stream coded;
+    coded.resize_capacity((w * h * 3 * 4 + (1u << 20)) * 8u);
+    uint64_t count = 0;
+    bool header_written = false;
+    auto packet = [&](const uint8_t *p, uint32_t len) {
+        mux.write_packet(vid, EVX_STREAM_TYPE_VIDEO, (uint64)(count * 1000000.0 / fps), p, len);
+        count++;
+    };
+    auto records = [&]() {   /* size-prefixed records of one output */
+        const uint8_t *base = coded.query_data();
+        uint32_t pos = 0, total = coded.query_byte_occupancy();
+        while (pos + 4 <= total) {
+            uint32_t size;
+            memcpy(&size, base + pos, 4);
+            if (pos + 4 + size > total) break;
+            packet(base + pos, 4 + size);
+            pos += 4 + size;
+        }
+    };
+    int rc = 0;
+    for (uint32_t i = 0; i < n && rc == 0; i++) {
+        coded.empty();
+        rc = enc->encode((void *)(frames + (size_t)i * w * h * 3), w, h, &coded);
+        if (rc) break;
+#if EVX_ENABLE_B_FRAMES && (EVX_B_FRAME_COUNT > 0)
+        if (coded.query_byte_occupancy() > 0) {
+            if (!header_written) {
+                packet(coded.query_data(), coded.query_byte_occupancy());
+                header_written = true;
+            } else {
+                records();
+            }
+        }
+#else
+        (void)header_written;
+        packet(coded.query_data(), coded.query_byte_occupancy());
+#endif
+    }
+#if EVX_ENABLE_B_FRAMES
+    if (rc == 0) {
+        coded.empty();
+        rc = enc->flush(&coded);
+        records();
+    }
+#else
+    (void)records;
+#endif
+    destroy_encoder(enc);
+    mux.close();
+    return rc;
+}
+
+/* A container read by the reference's evx_demuxer: the stream count and every
+ * packet's stream id, timestamp and payload (payloads concatenated into data,
+ * at most max packets). */
+int evxref_demux_file(const char *path, uint32_t *n_streams, uint8_t *data, uint64_t cap, uint32_t *sizes,
+                      uint8_t *ids, uint64_t *ts, uint32_t max, uint32_t *n)
+{
+    evx_demuxer dmx;
+    if (dmx.open(path) != EVX_SUCCESS || dmx.read_header() != EVX_SUCCESS) return EVX_ERROR_IO_FAILURE;
+    *n_streams = dmx.query_stream_count();
+    evx_demux_packet pkt;
+    uint64_t used = 0;
+    uint32_t k = 0;
+    evx_status s;
+    while ((s = dmx.read_packet(&pkt)) == EVX_SUCCESS) {
+        if (k < max && used + pkt.payload.size() <= cap) {
+            memcpy(data + used, pkt.payload.data(), pkt.payload.size());
+            used += pkt.payload.size();
+            sizes[k] = (uint32_t)pkt.payload.size();
+            ids[k] = pkt.stream_id;
+            ts[k] = pkt.timestamp;
+        }
+        k++;
+    }
+    dmx.close();
+    *n = k;
+    return s == EVX_ERROR_OPERATION_COMPLETED ? 0 : s;
 }
 
 /* ---------------- staged decoder ----------------

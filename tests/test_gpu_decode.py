@@ -186,3 +186,33 @@ def test_stream_decoder_matches_reference_decoder(variant, w, h, T, q, vmax, int
     assert len(mine) == len(want) == T
     for k in range(T):
         assert np.array_equal(mine[k], want[k]), f"frame {k} (display order)"
+
+
+@pytest.mark.parametrize("cfg", ["default", "ip3"])
+def test_tools_round_trip_matches_reference_tool(tmp_path, cfg):
+    """Raw RGB file -> tools encode (GPU encoder, container) -> the reference
+    tool's container byte for byte (but the stream header's uninitialised
+    padding byte); tools decode -> the reference decoder's frames."""
+    import chicago_b200 as cb
+    from chicago_b200 import tools
+    variant = None if cfg == "default" else cfg
+    ref = ref_for(variant)
+    w, h, T, fps, q = 176, 144, 9, 30.0, 8
+    frames = generate(w, h, T, seed=21, vmax=6.0)
+    src, mine, theirs, out = (str(tmp_path / n) for n in ("in.rgb", "mine.evx3", "ref.evx3", "out.rgb"))
+    frames.tofile(src)
+    tools.encode_file(src, mine, w, h, fps, q, cfg)
+    ref.encode_container(theirs, frames, fps, q)
+    a, b = open(mine, "rb").read(), open(theirs, "rb").read()
+    pad = 10 + 18 + 16 + 7
+    assert len(a) == len(b) and a[:pad] == b[:pad] and a[pad + 1:] == b[pad + 1:]
+    tools.decode_file(mine, out, cfg)
+    got = np.fromfile(out, np.uint8).reshape(-1, h, w, 3)
+    stock = ref.encode_stream(frames, quality=q)
+    if variant is None:
+        want = ref.decode_stream(stock, w, h)
+    else:
+        records = stock_payloads(ref, variant, frames, q, ())
+        records[0] = stock[:14] + records[0]
+        want = ref.decode_records(records, w, h)
+    assert got.shape[0] == T and np.array_equal(got, want)
