@@ -12,6 +12,12 @@
  * table, the SAO table and the quantised level planes, byte-identical to the
  * reference's for the same inputs.
  *
+ * Around it, for a drop-in codec: the host entropy coder and decoder
+ * (serialize_slice / unserialize_slice), the decoder's pixel half on the GPU
+ * (engine_decode_frame after unserialize_slice, decode.cpp:560-612), the GOP
+ * level encoder (evx3_encoder), batched and served encoding of many streams,
+ * and the packet container (evx_muxer / evx_demuxer, muxer.h:53-160).
+ *
  * All entry points return an evx_status-compatible code (reference
  * src/base.h:168-185); no exceptions cross the ABI.  One stream handle is one
  * encoder context (reference evx_context, common.h:209-240); a handle is not
