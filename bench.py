@@ -716,12 +716,31 @@ def main():
     ap.add_argument("--batch-ticks", type=int, default=12, help="timed ticks of the batched measurement")
     ap.add_argument("--serve-streams", type=int, default=64, help="streams of the serving measurement (0 = skip)")
     ap.add_argument("--serve-frames", type=int, default=60, help="frames each served stream sends (a GOP)")
+    ap.add_argument("--decode-only", action="store_true",
+                    help="only the decode leg (its stream from the e2e leg) -- for profiling the decoder")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         run_reference(args)
+    elif args.decode_only:
+        run_decode_only(args)
     else:
         run_gpu(args)
+
+
+def run_decode_only(args):
+    """The e2e leg to make the stream, then the decode leg alone; prints the
+    decode leg's JSON object (not a bench line)."""
+    import torch
+    torch.cuda.set_device(0)
+    sched = plan()
+    K = min(args.steps, len(sched) - args.warmup)
+    order = sched[:args.warmup + K]
+    frames = frames_for(0)
+    stream = torch.cuda.current_stream()
+    _, slices, _ = run_e2e(args, frames, order, stream)
+    line, _ = run_decode(args, slices, stream)
+    print(json.dumps({"decode": line}), flush=True)
 
 
 if __name__ == "__main__":
