@@ -63,6 +63,8 @@ EXPORTS = [
     "evxg_muxer_open", "evxg_muxer_add_video_stream", "evxg_muxer_add_audio_stream", "evxg_muxer_write_header",
     "evxg_muxer_write_packet", "evxg_muxer_close", "evxg_demuxer_open", "evxg_demuxer_stream_count",
     "evxg_demuxer_stream", "evxg_demuxer_read_packet", "evxg_demuxer_close",
+    "evxg_stream_decoder_create", "evxg_stream_decoder_destroy", "evxg_stream_decoder_clear",
+    "evxg_stream_decoder_dims", "evxg_stream_decoder_decode", "evxg_stream_decoder_flush",
 ]
 MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
 
@@ -205,6 +207,12 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_demuxer_read_packet.argtypes = [vp, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8), C.POINTER(u64), vp, u32,
                                            C.POINTER(u32)]
     L.evxg_demuxer_close.argtypes = [vp]
+    L.evxg_stream_decoder_create.argtypes = [C.POINTER(Config), C.POINTER(vp)]
+    L.evxg_stream_decoder_destroy.argtypes = [vp]
+    L.evxg_stream_decoder_clear.argtypes = [vp]
+    L.evxg_stream_decoder_dims.argtypes = [vp, C.POINTER(u32), C.POINTER(u32)]
+    L.evxg_stream_decoder_decode.argtypes = [vp, vp, u64, C.POINTER(u64), vp, C.POINTER(C.c_int)]
+    L.evxg_stream_decoder_flush.argtypes = [vp, vp, C.POINTER(C.c_int)]
     return L
 
 
@@ -506,35 +514,49 @@ class Demuxer:
 
 class StreamDecoder:
     """The reference's evx3_decoder (src/video/evx3.h:103-127) for a whole
-    .evx stream of the build ``cfg`` names: ``decode(data)`` reads the 14-byte
-    header (evxg_stream_header) and every frame record after it, and returns
-    the frames in display order -- the default build reorders its B frames
-    like evx3dec.cpp:137-185 -- as (H, W, 3) RGB24 arrays.  Records need no
-    size prefix: the entropy decoder finds each slice's end, so the I/P builds'
-    concatenated records decode too."""
+    .evx stream of the build ``cfg`` names (evxg_stream_decoder_*, C++):
+    ``decode(data)`` feeds the header and every frame record and drains the
+    display buffer, returning the frames in display order as (H, W, 3) RGB24
+    arrays.  Records need no size prefix: the entropy decoder finds each
+    slice's end, so the I/P builds' concatenated records decode too."""
 
     def __init__(self, cfg="default"):
-        self.cfg = cfg
-        self.dec = None
+        self.cfg = config(cfg)
+        h = C.c_void_p()
+        _check(lib().evxg_stream_decoder_create(C.byref(self.cfg), C.byref(h)))
+        self.h = h
 
     def decode(self, data: bytes):
-        data = bytes(data)
-        if len(data) < 14 or data[:4] != b"EVX1":
+        buf = np.frombuffer(bytes(data), np.uint8)
+        if len(buf) < 14 or buf[:4].tobytes() != b"EVX1":
             raise EvxgError(8, "not an .evx stream (header)")
-        width, height = struct.unpack_from("<HH", data, 10)
-        self.width, self.height = width, height
-        self.dec = Decoder(width, height, self.cfg)
-        frames, pending, nxt, pos = [], {}, 0, 14
-        while pos < len(data):
-            rgb, f18, used = self.dec.decode_record(data[pos:])
-            pos += used
-            order = struct.unpack_from("<I", f18, 10)[0] if config(self.cfg).b_frames else len(frames) + len(pending)
-            pending[order] = rgb
-            while nxt in pending:
-                frames.append(pending.pop(nxt))
-                nxt += 1
-        frames.extend(pending[k] for k in sorted(pending))
-        return frames
+        self.width, self.height = struct.unpack_from("<HH", buf.tobytes()[:14], 10)
+        _check(lib().evxg_stream_decoder_clear(self.h))
+        frames, pos = [], 0
+        out = np.empty((self.height, self.width, 3), np.uint8)
+        used, ready = C.c_uint64(0), C.c_int(0)
+        while pos < len(buf):
+            _check(lib().evxg_stream_decoder_decode(self.h, C.c_void_p(buf.ctypes.data + pos), len(buf) - pos,
+                                                    C.byref(used), _ptr(out), C.byref(ready)))
+            pos += used.value
+            if ready.value:
+                frames.append(out.copy())
+        while True:
+            _check(lib().evxg_stream_decoder_flush(self.h, _ptr(out), C.byref(ready)))
+            if not ready.value:
+                return frames
+            frames.append(out.copy())
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().evxg_stream_decoder_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 NO_FRAME = struct.pack("<iIHIBBBB", -1, 0, 0, 0, 0, 0, 0, 0)   # a stream without a frame in a batch tick

@@ -728,3 +728,137 @@ int evxg_decoder_fetch_planes(evxg_decoder *d, uint32_t slot, int16_t *out, int 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------- whole streams
+
+// The reference's evx3_decoder_impl (evx3dec.cpp:12-260) over the decoder
+// above: the stream header on the first call, then one frame record per
+// decode(); with B frames a display buffer of B-frame-count + 2 = 5 frames,
+// of which each decode() and flush() hands out at most the next one in
+// display order (evx3dec.cpp:137-185, :219-241).
+struct evxg_stream_decoder {
+    evxg_config cfg;
+    evxg_decoder *dec = nullptr;
+    uint32_t width = 0, height = 0;
+    struct Held {
+        std::vector<uint8_t> rgb;
+        uint32_t display_order = 0;
+        bool valid = false;
+    };
+    std::vector<Held> held;   // the display buffer
+    uint32_t next_display = 0;
+    std::vector<uint8_t> frame;
+};
+
+static constexpr uint32_t kDisplaySlots = 5;   // EVX_B_FRAME_COUNT + 2
+
+// Hands out the next frame in display order if the buffer has it.
+static bool emit_next(evxg_stream_decoder *sd, uint8_t *rgb)
+{
+    for (auto &h : sd->held)
+        if (h.valid && h.display_order == sd->next_display) {
+            if (rgb) std::memcpy(rgb, h.rgb.data(), h.rgb.size());
+            h.valid = false;
+            sd->next_display++;
+            return true;
+        }
+    return false;
+}
+
+extern "C" {
+
+int evxg_stream_decoder_create(const evxg_config *cfg, evxg_stream_decoder **out)
+{
+    if (!out) return fail(EVXG_ERROR_INVALIDARG, "evxg_stream_decoder_create: null argument");
+    *out = nullptr;
+    evxg_config c;
+    evxg_config_default(&c);
+    if (cfg) {
+        const int rc = check_config(cfg, "evxg_stream_decoder_create");
+        if (rc) return rc;
+        c = *cfg;
+    }
+    evxg_stream_decoder *sd = new (std::nothrow) evxg_stream_decoder();
+    if (!sd) return fail(EVXG_ERROR_OUTOFMEMORY, "evxg_stream_decoder_create: host allocation");
+    sd->cfg = c;
+    *out = sd;
+    return EVXG_SUCCESS;
+}
+
+int evxg_stream_decoder_destroy(evxg_stream_decoder *sd)
+{
+    if (!sd) return EVXG_ERROR_INVALIDARG;
+    if (sd->dec) evxg_decoder_destroy(sd->dec);
+    delete sd;
+    return EVXG_SUCCESS;
+}
+
+int evxg_stream_decoder_clear(evxg_stream_decoder *sd)   // evx3dec.cpp:25-48
+{
+    if (!sd) return fail(EVXG_ERROR_INVALIDARG, "evxg_stream_decoder_clear: null decoder");
+    if (sd->dec) evxg_decoder_destroy(sd->dec);
+    sd->dec = nullptr;
+    sd->width = sd->height = 0;
+    sd->held.clear();
+    sd->next_display = 0;
+    return EVXG_SUCCESS;
+}
+
+int evxg_stream_decoder_dims(const evxg_stream_decoder *sd, uint32_t *width, uint32_t *height)
+{
+    if (!sd || !sd->dec) return fail(EVXG_ERROR_NOT_READY, "evxg_stream_decoder_dims: no header read yet");
+    if (width) *width = sd->width;
+    if (height) *height = sd->height;
+    return EVXG_SUCCESS;
+}
+
+int evxg_stream_decoder_decode(evxg_stream_decoder *sd, const uint8_t *data, uint64_t len, uint64_t *consumed,
+                               uint8_t *rgb, int *has_output)
+{
+    if (!sd || !data || !consumed) return fail(EVXG_ERROR_INVALIDARG, "evxg_stream_decoder_decode: null argument");
+    *consumed = 0;
+    if (has_output) *has_output = 0;
+    uint64_t used = 0;
+    if (!sd->dec) {   // evx3dec.cpp:50-79: the header, then the context for its size
+        if (len < 14 || std::memcmp(data, "EVX1", 4) != 0)
+            return fail(EVXG_ERROR_INVALID_RESOURCE, "evxg_stream_decoder_decode: no stream header");
+        const uint32_t w = data[10] | (data[11] << 8), h = data[12] | (data[13] << 8);
+        const int rc = evxg_decoder_create(w, h, &sd->cfg, &sd->dec);
+        if (rc) return rc;
+        sd->width = w;
+        sd->height = h;
+        used = 14;
+    }
+    const size_t fb = (size_t)sd->width * sd->height * 3;
+    sd->frame.resize(fb);
+    evxg_frame f{};
+    uint64_t rec = 0;
+    const int rc = evxg_decoder_decode_record(sd->dec, data + used, len - used, sd->frame.data(), &f, &rec, nullptr);
+    if (rc) return rc;
+    *consumed = used + rec;
+    if (!sd->cfg.b_frames) {   // no reorder: every frame is output as decoded
+        if (rgb) std::memcpy(rgb, sd->frame.data(), fb);
+        if (has_output) *has_output = 1;
+        return EVXG_SUCCESS;
+    }
+    size_t slot = sd->held.size();
+    for (size_t s = 0; s < sd->held.size(); s++)
+        if (!sd->held[s].valid) { slot = s; break; }
+    if (slot >= kDisplaySlots) return fail(EVXG_ERROR_EXECUTION_FAILURE, "evxg_stream_decoder_decode: display buffer full");
+    if (slot == sd->held.size()) sd->held.emplace_back();
+    sd->held[slot].rgb.swap(sd->frame);
+    sd->held[slot].display_order = f.display_order;
+    sd->held[slot].valid = true;
+    const bool out = emit_next(sd, rgb);
+    if (has_output) *has_output = out;
+    return EVXG_SUCCESS;
+}
+
+int evxg_stream_decoder_flush(evxg_stream_decoder *sd, uint8_t *rgb, int *has_output)
+{
+    if (!sd || !has_output) return fail(EVXG_ERROR_INVALIDARG, "evxg_stream_decoder_flush: null argument");
+    *has_output = sd->cfg.b_frames ? emit_next(sd, rgb) : 0;
+    return EVXG_SUCCESS;
+}
+
+}  // extern "C"

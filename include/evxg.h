@@ -429,6 +429,25 @@ int evxg_unserialize_slice(const evxg_config *cfg, uint32_t aligned_w, uint32_t 
 int evxg_decoder_decode_record(evxg_decoder *d, const uint8_t *data, uint64_t len, uint8_t *rgb, evxg_frame *frame_out,
                                uint64_t *consumed, void *cuda_stream);
 
+/* The reference's evx3_decoder (evx3.h:103-127) for a whole stream of the
+ * build cfg describes (NULL = default), over evxg_decoder: the first decode
+ * call reads the 14-byte stream header (and creates the device state for its
+ * size), every call one frame record (records need no size prefix: the
+ * entropy decoder finds each slice's end), *consumed the bytes used.  With B
+ * frames the frames go through a display buffer of 5 like evx3dec.cpp:137-185
+ * and each decode / flush call hands out at most the next frame in display
+ * order (*has_output); without them every call outputs its frame.  rgb: host
+ * memory of width*height*3 bytes (evxg_stream_decoder_dims after the first
+ * call).  clear returns to the state before the header (evx3dec.cpp:25-48). */
+typedef struct evxg_stream_decoder evxg_stream_decoder;
+int evxg_stream_decoder_create(const evxg_config *cfg, evxg_stream_decoder **out);
+int evxg_stream_decoder_destroy(evxg_stream_decoder *d);
+int evxg_stream_decoder_clear(evxg_stream_decoder *d);
+int evxg_stream_decoder_dims(const evxg_stream_decoder *d, uint32_t *width, uint32_t *height);
+int evxg_stream_decoder_decode(evxg_stream_decoder *d, const uint8_t *data, uint64_t len, uint64_t *consumed,
+                               uint8_t *rgb, int *has_output);
+int evxg_stream_decoder_flush(evxg_stream_decoder *d, uint8_t *rgb, int *has_output);
+
 /* ---- Container ----
  *
  * The reference's packet container (evx_muxer / evx_demuxer, muxer.h:53-160,
