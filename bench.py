@@ -578,12 +578,14 @@ def run_served(args, n=None, per=None, sizes_from=None, seed=7):
         if sent[k] == per:
             srv.close_stream(ids[k])
     srv.drain()
-    lat, work, steady, eq, first, last = [], [], [], 0.0, None, 0
+    lat, work, steady, wait, run, eq, first, last = [], [], [], [], [], 0.0, None, 0
     for k, sid in enumerate(ids):
         w, h = sizes[k]
         for j, r in enumerate(srv.results[sid]):
-            a, rd, _, d = r["times"]
+            a, rd, ln, d = r["times"]
             lat.append((d - a) / 1e6)
+            wait.append((ln - a) / 1e6)
+            run.append((d - ln) / 1e6)
             if j > 0:   # after the stream's first frame (its I frame, its lane's first tick)
                 steady.append((d - a) / 1e6)
             work.append((d - rd) / 1e6)
@@ -603,6 +605,8 @@ def run_served(args, n=None, per=None, sizes_from=None, seed=7):
             "p999_frame_ms": round(float(np.percentile(lat, 99.9)), 3),
             "ready_to_done_ms": {q: round(float(np.percentile(work, v)), 3) for q, v in (("p50", 50), ("p99", 99), ("p999", 99.9))},
             "after_first_frame_ms": {q: round(float(np.percentile(steady, v)), 3) for q, v in (("p50", 50), ("p99", 99), ("p999", 99.9))},
+            "arrival_to_launch_ms": {q: round(float(np.percentile(wait, v)), 3) for q, v in (("p50", 50), ("p99", 99))},
+            "launch_to_done_ms": {q: round(float(np.percentile(run, v)), 3) for q, v in (("p50", 50), ("p99", 99))},
             "target_ms": round(1000 / 60, 1), "lanes": min(n, 8),
             "ticks": st["ticks"], "batch_rebuilds": st["rebuilds"],
             "note": "latency = results seen by the host minus arrival (I/P GOP: no reorder wait), queueing included"}

@@ -268,9 +268,10 @@ void work(evxg_server *v, Lane *l)
     complete(v, l, p);
 }
 
-// The lane a new stream of w x h joins: one whose streams have the closest
-// size (macroblock count within a factor of two), else an empty lane, else
-// the one with the fewest macroblocks.
+// The lane a new stream of w x h joins: an empty lane while there is one (a
+// stream alone in its lane is launched as soon as its frame arrives), else
+// the least loaded lane whose streams have the closest size (macroblock count
+// within a factor of two), else the one with the fewest macroblocks.
 int pick_lane(const evxg_server *v, uint32_t w, uint32_t h)
 {
     const size_t n = v->lanes.size();
@@ -284,12 +285,12 @@ int pick_lane(const evxg_server *v, uint32_t w, uint32_t h)
         const double r = m > mbs ? m / mbs : mbs / m;
         closest[s->lane] = std::min(closest[s->lane], r);
     }
+    for (size_t i = 0; i < n; i++)
+        if (load[i] == 0.0) return (int)i;
     int best = -1;
     for (size_t i = 0; i < n; i++)   // same size class, least loaded
         if (closest[i] < 2.0 && (best < 0 || load[i] < load[best])) best = (int)i;
     if (best >= 0) return best;
-    for (size_t i = 0; i < n; i++)
-        if (load[i] == 0.0) return (int)i;
     best = 0;
     for (size_t i = 1; i < n; i++)
         if (load[i] < load[best]) best = (int)i;
