@@ -47,7 +47,11 @@ __constant__ int16_t d_qm[2][64] = {
 
 constexpr int MB_N = 384;            // 16x16 luma + 2 x 8x8 chroma; MB buffers are Y | U | V
 constexpr int INTER_WARPS = 8;       // k_dec_inter: warps per CTA, one macroblock each
-constexpr int INTRA_THREADS = 128;   // k_dec_intra: one CTA per macroblock row
+constexpr int INTRA_THREADS = 256;   // k_dec_intra: one CTA per macroblock row
+// Block-copy source staged in shared memory by k_dec_intra: the 16x16 luma
+// block with the 6-tap margin (-3 .. +18) and the two 8x8 chroma blocks with
+// theirs (-3 .. +10).
+constexpr int WIN_L = 22, WIN_C = 14, WIN_N = WIN_L * WIN_L + 2 * WIN_C * WIN_C;
 
 // Kernel parameters of one decoded frame.
 struct DecArgs {
@@ -107,6 +111,14 @@ struct CurReader {
         const size_t k = (size_t)y * v.w + x;
         return (y >> sh) * mbw + (x >> sh) < m ? __ldcg(v.p + k) : __ldg(old.p + k);
     }
+};
+
+// Reads of a staged window whose cell (i, j) holds the sample the frame
+// reader gives at (x0 + j, y0 + i); every read of a prediction stays inside.
+struct WinReader {
+    const int16_t *p;
+    int n, x0, y0;
+    __device__ __forceinline__ int operator()(int x, int y) const { return p[(y - y0) * n + (x - x0)]; }
 };
 
 // One predicted sample at (c, r) of an n x n block whose integer position is
@@ -222,14 +234,31 @@ __device__ __forceinline__ int ref_slot(const DecArgs &a, int target)
 // threads of a group (t = thread index in it; sync() = the group's barrier):
 // prediction into pred, inverse quantisation and the inverse transform in
 // buf (2 x 384 samples), the sum written into the destination slot.
-template <int NTH, class Sync>
-__device__ void decode_mb(const DecArgs &a, int row, int col, int t, int16_t *pred, int16_t *buf, Nbrs &nb, Sync sync)
+template <int NTH, bool STAGE, class Sync>
+__device__ void decode_mb(const DecArgs &a, int row, int col, int t, int16_t *pred, int16_t *buf, Nbrs &nb,
+                          int16_t *win, Sync sync)
 {
     const int m = row * a.mbw + col, px = col * 16, py = row * 16;
     const evxg_block_desc d = a.bt[m];
     const int bt = d.block_type;
     const bool intra = bt & 1, motion = bt & 2, copy = bt & 4;
     if (bt > 7 || bt == 5) { if (t == 0) set_error(a, EVXG_ERROR_INVALID_RESOURCE); return; }   // decode.cpp:429
+    // this thread's levels, loaded now so that they arrive while the prediction is built
+    constexpr int PER = (MB_N + NTH - 1) / NTH;
+    int16_t lv[PER];
+    if (!copy) {
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const int e = t + k * NTH;
+            if (e < MB_N) {
+                int pl, r, c;
+                mb_pos(e, pl, r, c);
+                const size_t ny = (size_t)a.W * a.H, nc = (size_t)(a.W / 2) * (a.H / 2);
+                lv[k] = __ldg(pl == 0 ? a.lev + (size_t)(py + r) * a.W + px + c
+                                      : a.lev + ny + (pl - 1) * nc + (size_t)((py >> 1) + r) * (a.W / 2) + (px >> 1) + c);
+            }
+        }
+    }
     bool has_pred = true;
     if (bt == 1) {   // intra default: directional prediction, or none
         has_pred = d.intra_mode != 7;
@@ -264,13 +293,37 @@ __device__ void decode_mb(const DecArgs &a, int row, int col, int t, int16_t *pr
     } else if (intra) {   // intra block copy from the frame itself
         int dx = 0, dy = 0;
         if (d.sp_pred) dir_of_frac(d.sp_index, dx, dy);
-        for (int e = t; e < MB_N; e += NTH) {
-            int pl, r, c;
-            mb_pos(e, pl, r, c);
-            const CurReader rd{plane_of(a.planes[a.dest], a.W, a.H, pl), plane_of(a.snap, a.W, a.H, pl), pl ? 3 : 4,
-                               a.mbw, m};
-            const int bx = px + d.motion_x, by = py + d.motion_y;
-            pred[e] = mc_sample(rd, pl ? bx >> 1 : bx, pl ? by >> 1 : by, r, c, d.sp_pred, dx, dy, d.sp_amount);
+        const int bx = px + d.motion_x, by = py + d.motion_y;
+        if constexpr (STAGE) {   // the source with its taps, once, then the prediction from shared memory
+            for (int k = t; k < WIN_N; k += NTH) {
+                int pl, r, c, x0, y0;
+                if (k < WIN_L * WIN_L) { pl = 0; r = k / WIN_L; c = k % WIN_L; x0 = bx - 3; y0 = by - 3; }
+                else {
+                    const int q = k - WIN_L * WIN_L;
+                    pl = 1 + q / (WIN_C * WIN_C); r = (q % (WIN_C * WIN_C)) / WIN_C; c = q % WIN_C;
+                    x0 = (bx >> 1) - 3; y0 = (by >> 1) - 3;
+                }
+                const CurReader rd{plane_of(a.planes[a.dest], a.W, a.H, pl), plane_of(a.snap, a.W, a.H, pl),
+                                   pl ? 3 : 4, a.mbw, m};
+                win[k] = (int16_t)rd(x0 + c, y0 + r);
+            }
+            sync();
+            for (int e = t; e < MB_N; e += NTH) {
+                int pl, r, c;
+                mb_pos(e, pl, r, c);
+                const WinReader wr = pl == 0 ? WinReader{win, WIN_L, bx - 3, by - 3}
+                                             : WinReader{win + WIN_L * WIN_L + (pl - 1) * WIN_C * WIN_C, WIN_C,
+                                                         (bx >> 1) - 3, (by >> 1) - 3};
+                pred[e] = mc_sample(wr, pl ? bx >> 1 : bx, pl ? by >> 1 : by, r, c, d.sp_pred, dx, dy, d.sp_amount);
+            }
+        } else {
+            for (int e = t; e < MB_N; e += NTH) {
+                int pl, r, c;
+                mb_pos(e, pl, r, c);
+                const CurReader rd{plane_of(a.planes[a.dest], a.W, a.H, pl), plane_of(a.snap, a.W, a.H, pl),
+                                   pl ? 3 : 4, a.mbw, m};
+                pred[e] = mc_sample(rd, pl ? bx >> 1 : bx, pl ? by >> 1 : by, r, c, d.sp_pred, dx, dy, d.sp_amount);
+            }
         }
     } else if (a.type == EVXG_FRAME_BIDIR && d.prediction_mode == 2) {   // bi-prediction: (fwd + bwd + 1) >> 1
         const int sf = ref_slot(a, d.prediction_target), sb = ref_slot(a, d.prediction_target_b);
@@ -318,12 +371,14 @@ __device__ void decode_mb(const DecArgs &a, int row, int col, int t, int16_t *pr
     int16_t *coef = buf, *tmp = buf + MB_N;
     const bool iq = intra && !motion;   // quantize.cpp:457
     const int qy = d.q_index, qc = min(d.q_index + 2, 63);
-    for (int e = t; e < MB_N; e += NTH) {   // levels sit at the MB's own position of the level planes
-        const int16_t lv = __ldg(out_at(e) - Y + a.lev);
+#pragma unroll
+    for (int k = 0; k < PER; k++) {   // the levels loaded at the start
+        const int e = t + k * NTH;
+        if (e >= MB_N) break;
         int pl, r, c;
         mb_pos(e, pl, r, c);
         const int o = (r & 7) * 8 + (c & 7);
-        coef[e] = dequant(lv, pl ? qc : qy, o, iq, pl != 0);
+        coef[e] = dequant(lv[k], pl ? qc : qy, o, iq, pl != 0);
     }
     sync();
     for (int q = t; q < MB_N; q += NTH) {   // columns: coef -> tmp (int16)
@@ -353,18 +408,24 @@ __global__ void __launch_bounds__(32 * INTER_WARPS) k_dec_inter(DecArgs a)
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nmb = a.mbw * a.mbh;
     for (int m = blockIdx.x * INTER_WARPS + w; m < nmb; m += gridDim.x * INTER_WARPS) {
         if (a.bt[m].block_type & 1) continue;
-        decode_mb<32>(a, m / a.mbw, m % a.mbw, lane, s_pred[w], s_buf[w], s_nb[w], [] { __syncwarp(); });
+        decode_mb<32, false>(a, m / a.mbw, m % a.mbw, lane, s_pred[w], s_buf[w], s_nb[w], nullptr, [] { __syncwarp(); });
         __syncwarp();
     }
 }
 
 // Thread 0: wait until rows lo .. hi have decoded their intra macroblocks up
 // to column col; false (and the error word set) when the bound ran out.
-__device__ bool wait_rows(const DecArgs &a, int lo, int hi, int col)
+// seen[k] caches the last progress read of row hi - k (progress only grows),
+// so rows already known to be far enough are not read again.
+constexpr int kSeenRows = 8;
+__device__ bool wait_rows(const DecArgs &a, int lo, int hi, int col, int *seen)
 {
     unsigned long long t0 = 0;
     for (int r = max(lo, 0); r <= hi; r++) {
-        while (ld_acquire(&a.progress[r]) < col) {
+        const int k = hi - r;
+        if (k < kSeenRows && seen[k] >= col) continue;
+        int v;
+        while ((v = ld_acquire(&a.progress[r])) < col) {
             if (!t0) t0 = globaltimer_ns();
             else if ((long long)(globaltimer_ns() - t0) > a.timeout_ns) {
                 set_error(a, EVXG_ERROR_OPERATION_TIMEDOUT);
@@ -372,6 +433,7 @@ __device__ bool wait_rows(const DecArgs &a, int lo, int hi, int col)
             }
             __nanosleep(200);
         }
+        if (k < kSeenRows) seen[k] = v;
     }
     return true;
 }
@@ -401,6 +463,7 @@ __global__ void __launch_bounds__(INTRA_THREADS) k_dec_intra(DecArgs a)
     __shared__ int16_t s_pred[MB_N];
     __shared__ int16_t s_buf[2 * MB_N];
     __shared__ Nbrs s_nb;
+    __shared__ int16_t s_win[WIN_N];
     __shared__ unsigned s_mask[128];   // intra columns of the row (mbw <= 4096)
     __shared__ int s_row, s_ok;
     const int t = threadIdx.x, words = (a.mbw + 31) >> 5;
@@ -421,16 +484,19 @@ __global__ void __launch_bounds__(INTRA_THREADS) k_dec_intra(DecArgs a)
             return a.mbw;
         };
         int c = next_intra(0);
+        int seen[kSeenRows];   // thread 0: progress of rows row-1, row-2, ... as last read
+#pragma unroll
+        for (int k = 0; k < kSeenRows; k++) seen[k] = -1;
         if (t == 0) st_release(&a.progress[row], c - 1);
         while (c < a.mbw) {
             if (t == 0) {
                 int lo, need;
                 intra_reach(a, a.bt[row * a.mbw + c], row, c, lo, need);
-                s_ok = need < 0 || lo >= row || wait_rows(a, lo, row - 1, need);
+                s_ok = need < 0 || lo >= row || wait_rows(a, lo, row - 1, need, seen);
             }
             __syncthreads();
             if (!s_ok) return;   // the error word is set; rows below give up in turn
-            decode_mb<INTRA_THREADS>(a, row, c, t, s_pred, s_buf, s_nb, [] { __syncthreads(); });
+            decode_mb<INTRA_THREADS, true>(a, row, c, t, s_pred, s_buf, s_nb, s_win, [] { __syncthreads(); });
             __threadfence();
             __syncthreads();
             c = next_intra(c + 1);
