@@ -306,11 +306,13 @@ def run_gpu(args):
 
 
 def run_e2e(args, frames, order, stream):
-    """Encode the frames of `order` through the C ABI from pinned host RGB,
-    fetch each frame's tables into one of a ring of pinned host buffers and
-    hand them to a pool of host threads running the library's entropy coder
-    (ctypes releases the interpreter lock during the call); a buffer is reused
-    once its frame's slice is done.  Returns the wall time of the frames after
+    """Encode the frames of `order` through the C ABI from pinned host RGB
+    (evxg_encode_frame_pipelined: uploads and table downloads on the stream's
+    copy stream, off the frames' critical path), each frame's tables into one
+    of a ring of pinned host buffers, handed to a pool of host threads that
+    wait for the frame (evxg_stream_output_wait) and run the library's entropy
+    coder (ctypes releases the interpreter lock during the calls); a buffer is
+    reused once its frame's slice is done.  Returns the wall time of the frames after
     the warm-up ones (their slices included), every frame's (frame18, slice)
     and the thread count."""
     import ctypes as C
@@ -329,7 +331,8 @@ def run_e2e(args, frames, order, stream):
     cfg = cb.config(CFG)
     cap = st.aw * st.ah * 4
 
-    def serialize(f18, bufs):
+    def serialize(f18, bufs, ticket):
+        cb._check(L.evxg_stream_output_wait(st.h, ticket))   # the frame's tables are in bufs
         out = np.empty(cap, np.uint8)
         n = C.c_uint64(0)
         cb._check(L.evxg_serialize_slice(C.byref(cfg), st.aw, st.ah, f18, *[C.c_void_p(b.data_ptr()) for b in bufs],
@@ -349,10 +352,12 @@ def run_e2e(args, frames, order, stream):
             for j in [j for j in pending if j % len(ring) == k]:   # this buffer's previous frame must be coded
                 slices[j] = (slices[j][0], pending.pop(j).result())
             bufs = ring[k]
-            cb._check(L.evxg_encode_frame(st.h, C.c_void_p(host_rgb[ti].data_ptr()), 0, f18, C.c_void_p(sp)))
-            cb._check(L.evxg_fetch_tables(st.h, *[C.c_void_p(b.data_ptr()) for b in bufs], 0, C.c_void_p(sp)))
+            ticket = C.c_uint64()
+            cb._check(L.evxg_encode_frame_pipelined(st.h, C.c_void_p(host_rgb[ti].data_ptr()), f18,
+                                                    *[C.c_void_p(b.data_ptr()) for b in bufs], C.c_void_p(sp),
+                                                    C.byref(ticket)))
             slices.append((f18, None))
-            pending[i] = pool.submit(serialize, f18, bufs)
+            pending[i] = pool.submit(serialize, f18, bufs, ticket.value)
         for j in list(pending):
             slices[j] = (slices[j][0], pending.pop(j).result())
         t1 = time.perf_counter()
@@ -712,7 +717,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

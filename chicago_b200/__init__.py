@@ -65,6 +65,7 @@ EXPORTS = [
     "evxg_demuxer_stream", "evxg_demuxer_read_packet", "evxg_demuxer_close",
     "evxg_stream_decoder_create", "evxg_stream_decoder_destroy", "evxg_stream_decoder_clear",
     "evxg_stream_decoder_dims", "evxg_stream_decoder_decode", "evxg_stream_decoder_flush",
+    "evxg_encode_frame_pipelined", "evxg_stream_output_wait",
 ]
 MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
 
@@ -213,6 +214,8 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_stream_decoder_dims.argtypes = [vp, C.POINTER(u32), C.POINTER(u32)]
     L.evxg_stream_decoder_decode.argtypes = [vp, vp, u64, C.POINTER(u64), vp, C.POINTER(C.c_int)]
     L.evxg_stream_decoder_flush.argtypes = [vp, vp, C.POINTER(C.c_int)]
+    L.evxg_encode_frame_pipelined.argtypes = [vp, vp, C.c_char_p, vp, vp, vp, vp, vp, C.POINTER(u64)]
+    L.evxg_stream_output_wait.argtypes = [vp, u64]
     return L
 
 
@@ -323,6 +326,19 @@ class Stream:
 
     def sync(self, cuda_stream=None):
         _check(lib().evxg_stream_sync(self.h, _ptr(cuda_stream)))
+
+    def encode_pipelined(self, rgb, frame18: bytes, out: dict, cuda_stream=None) -> int:
+        """evxg_encode_frame_pipelined: encode a host RGB24 frame without waiting;
+        its tables land in out (arrays as fetch_tables returns them, kept alive by
+        the caller) once output_wait(ticket) returns.  Returns the ticket."""
+        t = C.c_uint64()
+        _check(lib().evxg_encode_frame_pipelined(self.h, _ptr(rgb), frame18, _ptr(out["blocks"]),
+                                                 _ptr(out["prev_blocks"]), _ptr(out["sao"]), _ptr(out["levels"]),
+                                                 _ptr(cuda_stream), C.byref(t)))
+        return t.value
+
+    def output_wait(self, ticket: int):
+        _check(lib().evxg_stream_output_wait(self.h, ticket))
 
     def set_timeout_ns(self, ns: int):
         """Bound on every device-side wait of this stream's kernels (5 s by default)."""

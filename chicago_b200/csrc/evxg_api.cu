@@ -31,6 +31,8 @@ int cuda_fail(cudaError_t e, const char *where)
 }
 }  // namespace evxg
 
+static void pipeline_free(evxg_stream *s);
+
 // Host-side fault injection: the next n device allocations of stream
 // creation report cudaErrorMemoryAllocation without allocating.
 static std::atomic<uint32_t> g_inject_alloc{0};
@@ -161,6 +163,7 @@ int evxg_stream_destroy(evxg_stream *s)
     cudaFree(s->sao_orig); cudaFree(s->sao_flags); cudaFree(s->sao_mail);
     if (s->profile)
         for (int i = 0; i < 7; i++) cudaEventDestroy(s->ev[i]);
+    pipeline_free(s);
     delete s;
     return EVXG_SUCCESS;
 }
@@ -326,16 +329,16 @@ void evxg::fill_args(evxg_stream *s, const evxg_frame *f, const uint8_t *drgb, F
     a.prev_tab = s->prev; a.prev_ser = s->prev_ser; a.plane_elems = s->plane_elems;
 }
 
-extern "C" {
-
-int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, const evxg_frame *fin, void *cuda_stream)
+// The frame's work on stream st; after_convert (optional) is recorded once the
+// conversion has read the RGB input.
+static int encode_impl(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, const evxg_frame *fin, cudaStream_t st,
+                       cudaEvent_t after_convert)
 {
     if (!s || !rgb || !fin) return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame: null argument");
     evxg_frame fr;
     int rc = check_frame(s, fin, "evxg_encode_frame", &fr);
     if (rc) return rc;
     const evxg_frame *f = &fr;
-    cudaStream_t st = (cudaStream_t)cuda_stream;
     const uint8_t *drgb = rgb;
     if (!rgb_on_device) {
         CK(cudaMemcpyAsync(s->rgb, rgb, (size_t)s->vw * s->vh * 3, cudaMemcpyHostToDevice, st));
@@ -354,6 +357,7 @@ int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, con
     auto mark = [&](int i) { if (s->profile) cudaEventRecord(s->ev[i], st); };
     mark(0);
     k_convert<<<cg, 128, 0, st>>>(a);
+    if (after_convert) CK(cudaEventRecord(after_convert, st));
     mark(1);
     if (s->mb_form == EVXG_MB_FORM_CLUSTER)
         k_mb_cluster<<<3 * s->mb_clusters, mb_threads(), mb_shared_bytes(), st>>>(a);
@@ -376,6 +380,113 @@ int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, con
     CK(cudaGetLastError());
     if (f->type != EVXG_FRAME_BIDIR)   // temporal MV predictor table (encode.cpp:990-998)
         CK(cudaMemcpyAsync(s->prev, s->bt, nblk * sizeof(evxg_block_desc), cudaMemcpyDeviceToDevice, st));
+    return EVXG_SUCCESS;
+}
+
+// Device bytes of one table snapshot: block table, previous table, SAO table,
+// level planes, the error word.
+static size_t snapshot_bytes(const evxg_stream *s)
+{
+    const size_t nblk = (size_t)s->mbw * s->mbh;
+    return 2 * nblk * sizeof(evxg_block_desc) + nblk * sizeof(evxg_sao_info) + s->plane_elems * sizeof(int16_t) + 16;
+}
+
+static int pipeline_setup(evxg_stream *s)
+{
+    if (s->copy) return EVXG_SUCCESS;
+    cudaError_t e = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking);
+    for (int p = 0; p < 2 && e == cudaSuccess; p++) {
+        e = dev_alloc(&s->prgb[p], (size_t)s->vw * s->vh * 3);
+        if (e == cudaSuccess) e = dev_alloc(&s->snap[p], snapshot_bytes(s));
+        for (cudaEvent_t *ev : {&s->ev_up[p], &s->ev_conv[p], &s->ev_snap[p], &s->ev_free[p]})
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    }
+    for (int k = 0; k < evxg_stream::kRing && e == cudaSuccess; k++)
+        e = cudaEventCreateWithFlags(&s->done[k], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMallocHost(&s->herr, evxg_stream::kRing * sizeof(int));
+    if (e != cudaSuccess) return cuda_fail(e, "evxg_encode_frame_pipelined: set-up");
+    return EVXG_SUCCESS;
+}
+
+static void pipeline_free(evxg_stream *s)
+{
+    if (!s->copy) return;
+    cudaStreamSynchronize(s->copy);
+    if (s->down) cudaStreamSynchronize(s->down);
+    for (int p = 0; p < 2; p++) {
+        cudaFree(s->prgb[p]);
+        cudaFree(s->snap[p]);
+        for (cudaEvent_t ev : {s->ev_up[p], s->ev_conv[p], s->ev_snap[p], s->ev_free[p]})
+            if (ev) cudaEventDestroy(ev);
+    }
+    for (int k = 0; k < evxg_stream::kRing; k++)
+        if (s->done[k]) cudaEventDestroy(s->done[k]);
+    cudaFreeHost(s->herr);
+    cudaStreamDestroy(s->copy);
+    if (s->down) cudaStreamDestroy(s->down);
+}
+
+extern "C" {
+
+int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, const evxg_frame *fin, void *cuda_stream)
+{
+    return encode_impl(s, rgb, rgb_on_device, fin, (cudaStream_t)cuda_stream, nullptr);
+}
+
+// Frame t uses buffer pair t & 1.  Upload stream: into prgb[p] once frame
+// t-2's conversion read it; compute stream: the frame, then (once frame t-2's
+// download read it) the snapshot of its tables into snap[p]; download
+// stream: the snapshot, then done[t % kRing].  Uploads and downloads on
+// streams of their own, so the next frame's upload never queues behind this
+// frame's download.
+int evxg_encode_frame_pipelined(evxg_stream *s, const uint8_t *rgb, const evxg_frame *frame, evxg_block_desc *blocks,
+                                evxg_block_desc *prev_blocks, evxg_sao_info *sao, int16_t *levels, void *cuda_stream,
+                                uint64_t *ticket)
+{
+    if (!s || !rgb || !frame || !ticket) return fail(EVXG_ERROR_INVALIDARG, "evxg_encode_frame_pipelined: null argument");
+    int rc = pipeline_setup(s);
+    if (rc) return rc;
+    const uint64_t t = s->tickets.load();
+    const int p = (int)(t & 1), k = (int)(t % evxg_stream::kRing);
+    if (t >= (uint64_t)evxg_stream::kRing) CK(cudaEventSynchronize(s->done[k]));   // the ring entry is free again
+    cudaStream_t st = (cudaStream_t)cuda_stream, cp = s->copy, dn = s->down;
+    CK(cudaStreamWaitEvent(cp, s->ev_conv[p], 0));
+    CK(cudaMemcpyAsync(s->prgb[p], rgb, (size_t)s->vw * s->vh * 3, cudaMemcpyHostToDevice, cp));
+    CK(cudaEventRecord(s->ev_up[p], cp));
+    CK(cudaStreamWaitEvent(st, s->ev_up[p], 0));
+    if ((rc = encode_impl(s, s->prgb[p], 1, frame, st, s->ev_conv[p]))) return rc;
+    const size_t nblk = (size_t)s->mbw * s->mbh, tb = nblk * sizeof(evxg_block_desc),
+                 sb = nblk * sizeof(evxg_sao_info), lb = s->plane_elems * sizeof(int16_t);
+    uint8_t *sn = s->snap[p];
+    CK(cudaStreamWaitEvent(st, s->ev_free[p], 0));
+    CK(cudaMemcpyAsync(sn, s->bt, tb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(sn + tb, s->prev_ser, tb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(sn + 2 * tb, s->sao, sb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(sn + 2 * tb + sb, s->lev, lb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(sn + 2 * tb + sb + lb, s->sync + 3 * s->mbh + 4, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    CK(cudaEventRecord(s->ev_snap[p], st));
+    CK(cudaStreamWaitEvent(dn, s->ev_snap[p], 0));
+    if (blocks) CK(cudaMemcpyAsync(blocks, sn, tb, cudaMemcpyDeviceToHost, dn));
+    if (prev_blocks) CK(cudaMemcpyAsync(prev_blocks, sn + tb, tb, cudaMemcpyDeviceToHost, dn));
+    if (sao) CK(cudaMemcpyAsync(sao, sn + 2 * tb, sb, cudaMemcpyDeviceToHost, dn));
+    if (levels) CK(cudaMemcpyAsync(levels, sn + 2 * tb + sb, lb, cudaMemcpyDeviceToHost, dn));
+    CK(cudaMemcpyAsync(&s->herr[k], sn + 2 * tb + sb + lb, sizeof(int), cudaMemcpyDeviceToHost, dn));
+    CK(cudaEventRecord(s->ev_free[p], dn));
+    CK(cudaEventRecord(s->done[k], dn));
+    s->tickets.store(t + 1);
+    *ticket = t;
+    return EVXG_SUCCESS;
+}
+
+int evxg_stream_output_wait(evxg_stream *s, uint64_t ticket)
+{
+    const uint64_t issued = s ? s->tickets.load() : 0;
+    if (!s || ticket >= issued || issued - ticket > (uint64_t)evxg_stream::kRing)
+        return fail(EVXG_ERROR_INVALID_INDEX, "evxg_stream_output_wait: not one of the last 16 pipelined frames");
+    const int k = (int)(ticket % evxg_stream::kRing);
+    CK(cudaEventSynchronize(s->done[k]));
+    if (s->herr[k]) return fail(s->herr[k], "evxg_stream_output_wait: the frame's wavefront gave up waiting (timeout)");
     return EVXG_SUCCESS;
 }
 

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <string>
 
 #include "evxg.h"
@@ -81,6 +82,17 @@ struct evxg_stream {
     evxg_config cfg;                    // reference build configuration the stream reproduces
     bool profile;
     cudaEvent_t ev[7];
+    // Pipelined encoding from host memory (evxg_encode_frame_pipelined), set
+    // up on first use: an upload and a download stream, two device RGB
+    // buffers and two table snapshots, the events that order uploads / frames
+    // / downloads across the three streams, and a ring of per-frame
+    // completion events with the frames' error words.
+    static constexpr int kRing = 16;
+    cudaStream_t copy, down;
+    uint8_t *prgb[2], *snap[2];
+    cudaEvent_t ev_up[2], ev_conv[2], ev_snap[2], ev_free[2], done[kRing];
+    int *herr;                          // pinned, one error word per ring entry
+    std::atomic<uint64_t> tickets{0};   // frames issued; read by output waits on other threads
 };
 
 namespace evxg {

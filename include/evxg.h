@@ -173,6 +173,24 @@ int evxg_encode_frame(evxg_stream *s, const uint8_t *rgb, int rgb_on_device,
 int evxg_fetch_tables(evxg_stream *s, evxg_block_desc *blocks, evxg_block_desc *prev_blocks,
                       evxg_sao_info *sao, int16_t *levels, int to_device, void *cuda_stream);
 
+/* Pipelined encoding from host memory (no counterpart in the reference):
+ * evxg_encode_frame plus evxg_fetch_tables for one frame, returning at once,
+ * with the copies off the frame's critical path -- the RGB upload runs on
+ * an upload stream of the stream's own while earlier frames compute, the
+ * frame's tables are snapshotted on the device when its kernels end and
+ * downloaded on a download stream while the next frame computes.  Frames run in call
+ * order on cuda_stream like evxg_encode_frame; results are identical.
+ * *ticket names the frame: evxg_stream_output_wait(s, ticket) returns once
+ * its tables are in the host buffers (any of which may be NULL), with the
+ * frame's error (EVXG_ERROR_OPERATION_TIMEDOUT) if a wait gave up.  rgb and
+ * the output buffers must stay valid until then (pinned memory keeps the
+ * copies asynchronous); at most the last 16 frames can be waited for, and a
+ * 17th call waits for the oldest itself. */
+int evxg_encode_frame_pipelined(evxg_stream *s, const uint8_t *rgb, const evxg_frame *frame, evxg_block_desc *blocks,
+                                evxg_block_desc *prev_blocks, evxg_sao_info *sao, int16_t *levels, void *cuda_stream,
+                                uint64_t *ticket);
+int evxg_stream_output_wait(evxg_stream *s, uint64_t ticket);
+
 /* Copy one DPB slot (plane-set layout) or the converted source
  * (slot = 4) out; supports the reference's peek() views (evx3enc.cpp:417-547). */
 int evxg_fetch_planes(evxg_stream *s, uint32_t slot, int16_t *out, int to_device, void *cuda_stream);

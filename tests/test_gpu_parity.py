@@ -253,3 +253,28 @@ def test_encoder_bitstream_equals_stock_stream(cfg):
     mine = bytes(enc.stream)
     assert len(mine) == len(stock)
     assert mine[:7] == stock[:7] and mine[8:] == stock[8:]
+
+
+@pytest.mark.parametrize("cfg,w,h,T", [("default", 176, 144, 9), ("ip3", 352, 288, 8)])
+def test_pipelined_frames_equal_synchronous_frames(cfg, w, h, T):
+    """evxg_encode_frame_pipelined (uploads and downloads on the stream's copy
+    stream, several frames in flight) gives every frame's tables exactly as
+    evxg_encode_frame + evxg_fetch_tables do."""
+    import chicago_b200 as cb
+    b_frames, ref_count, _ = cb.CONFIGS[cfg]
+    frames = generate(w, h, T, seed=w + T, vmax=8.0)
+    plan = plan_gop(T, quality=8) if b_frames else plan_ip(T, 8, (), ref_count)
+    a, b = cb.Stream(w, h, cfg), cb.Stream(w, h, cfg)
+    want = []
+    for ti, f18 in plan:
+        a.encode_frame(frames[ti], f18)
+        want.append(a.fetch_tables())
+    outs, tickets = [], []
+    for ti, f18 in plan:   # every frame issued before any is waited for
+        o = {k: np.zeros_like(v) for k, v in want[0].items()}
+        outs.append(o)
+        tickets.append(b.encode_pipelined(np.ascontiguousarray(frames[ti]), f18, o))
+    for k, t in enumerate(tickets):
+        b.output_wait(t)
+        for key in want[k]:
+            assert np.array_equal(outs[k][key], want[k][key]), f"frame {k}: {key}"
