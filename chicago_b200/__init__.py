@@ -65,7 +65,7 @@ EXPORTS = [
     "evxg_demuxer_stream", "evxg_demuxer_read_packet", "evxg_demuxer_close",
     "evxg_stream_decoder_create", "evxg_stream_decoder_destroy", "evxg_stream_decoder_clear",
     "evxg_stream_decoder_dims", "evxg_stream_decoder_decode", "evxg_stream_decoder_flush",
-    "evxg_encode_frame_pipelined", "evxg_stream_output_wait",
+    "evxg_encode_frame_pipelined", "evxg_stream_output_wait", "evxg_encoder_peek",
 ]
 MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
 
@@ -216,6 +216,7 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_stream_decoder_flush.argtypes = [vp, vp, C.POINTER(C.c_int)]
     L.evxg_encode_frame_pipelined.argtypes = [vp, vp, C.c_char_p, vp, vp, vp, vp, vp, C.POINTER(u64)]
     L.evxg_stream_output_wait.argtypes = [vp, u64]
+    L.evxg_encoder_peek.argtypes = [vp, i32, vp]
     return L
 
 
@@ -775,6 +776,16 @@ class Encoder:
 
     def flush(self):
         _check(lib().evxg_encoder_flush(self.h))
+
+    PEEK = {"source": 0, "prediction": 1, "block_table": 2, "quant_table": 3, "spmp_table": 4,
+            "block_variance": 5, "destination": 6}
+
+    def peek(self, which, width: int, height: int) -> np.ndarray:
+        """evx3_encoder::peek: the (H, W, 3) RGB24 view ``which`` (a name of PEEK
+        or its number) of the encoder's state after the last encode call."""
+        out = np.zeros((height, width, 3), np.uint8)
+        _check(lib().evxg_encoder_peek(self.h, self.PEEK.get(which, which), _ptr(out)))
+        return out
 
     def clear(self):
         _check(lib().evxg_encoder_clear(self.h))

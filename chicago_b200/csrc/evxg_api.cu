@@ -822,6 +822,27 @@ int evxg_encoder_encode(evxg_encoder *e, const uint8_t *rgb, uint32_t width, uin
     return EVXG_SUCCESS;
 }
 
+int evxg_encoder_peek(evxg_encoder *e, int which, uint8_t *rgb)   // evx3enc.cpp:417-547
+{
+    if (!e || !rgb) return fail(EVXG_ERROR_INVALIDARG, "evxg_encoder_peek: null argument");
+    if (!e->stream) return EVXG_SUCCESS;   // nothing encoded yet (evx3enc.cpp:428-431)
+    if (which < EVXG_PEEK_SOURCE || which > EVXG_PEEK_DESTINATION || which == EVXG_PEEK_PREDICTION)
+        return fail(EVXG_ERROR_NOTIMPL, "evxg_encoder_peek: not a view the reference draws");
+    evxg_stream *s = e->stream;
+    const int16_t *planes = nullptr;
+    if (which == EVXG_PEEK_SOURCE) {
+        planes = s->src;
+    } else if (which == EVXG_PEEK_DESTINATION) {   // evx3enc.cpp:444-452
+        const uint32_t R = e->cfg.ref_count;
+        planes = s->dpb[e->cfg.b_frames ? e->frame.dpb_slot % 4 : (e->frame.index + R - 1) % R];
+    }
+    // the stream's RGB staging buffer is free between frames; the encoder's work is on the legacy stream
+    int rc = peek_rgb(planes, s->bt, which, (int)s->W, (int)s->H, (int)s->mbw, (int)s->vw, (int)s->vh, s->rgb, nullptr);
+    if (rc) return rc;
+    CK(cudaMemcpy(rgb, s->rgb, (size_t)s->vw * s->vh * 3, cudaMemcpyDeviceToHost));
+    return evxg_stream_sync(s, nullptr);
+}
+
 int evxg_encoder_flush(evxg_encoder *e)   // evx3enc.cpp:385-414
 {
     if (!e) return EVXG_ERROR_INVALIDARG;

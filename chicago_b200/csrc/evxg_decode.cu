@@ -545,7 +545,49 @@ __global__ void k_dec_rgb(const int16_t *set, int W, int H, int w, int h, uint8_
         }
 }
 
+// The encoder's peek() maps (evx3enc.cpp:454-543), one thread per visible
+// pixel, from the block of the block table it lies in.
+__global__ void k_peek_map(const evxg_block_desc *bt, int mbw, int w, int h, int which, uint8_t *rgb)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    const evxg_block_desc &d = bt[(x / 16) + (y / 16) * mbw];
+    const int bt_ = d.block_type;
+    const bool copy = bt_ & 4;
+    int r = 0, g = 0, b = 0;
+    switch (which) {
+    case EVXG_PEEK_BLOCK_TABLE: r = 255 * (bt_ & 1); g = 255 * ((bt_ >> 1) & 1); b = 255 * ((bt_ >> 2) & 1); break;
+    case EVXG_PEEK_QUANT_TABLE:
+        if (copy) r = 255;
+        else r = g = b = 255 - 15 * d.q_index;
+        break;
+    case EVXG_PEEK_BLOCK_VARIANCE:
+        if (copy) r = 255;
+        else r = g = b = min(max(d.variance / 30, 0), 255);
+        break;
+    case EVXG_PEEK_SPMP_TABLE:
+        if (d.sp_pred) { g = 255 * d.sp_amount; b = 255 * !d.sp_amount; }
+        break;
+    default: break;
+    }
+    uint8_t *o = rgb + ((size_t)y * w + x) * 3;
+    o[0] = (uint8_t)r; o[1] = (uint8_t)g; o[2] = (uint8_t)b;
+}
+
 }  // namespace
+
+int peek_rgb(const int16_t *planes, const evxg_block_desc *bt, int which, int W, int H, int mbw, int w, int h,
+             uint8_t *out, cudaStream_t st)
+{
+    if (which == EVXG_PEEK_SOURCE || which == EVXG_PEEK_DESTINATION) {
+        const int cw = std::min(w, W), ch = std::min(h, H);
+        k_dec_rgb<<<dim3((cw / 2 + 127) / 128, ch / 2), 128, 0, st>>>(planes, W, H, w, h, out);
+    } else {
+        k_peek_map<<<dim3((w + 127) / 128, h), 128, 0, st>>>(bt, mbw, w, h, which, out);
+    }
+    CK(cudaGetLastError());
+    return EVXG_SUCCESS;
+}
 }  // namespace evxg
 
 using namespace evxg;

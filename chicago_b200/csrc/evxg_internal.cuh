@@ -54,6 +54,10 @@ int check_frame_config(const evxg_config &cfg, const evxg_frame *f, const char *
 // A build configuration the library reproduces (EVXG_ERROR_INVALIDARG otherwise).
 int check_config(const evxg_config *c, const char *who);
 int max_active_clusters();
+// RGB24 of an int16 plane set (EVXG_PEEK_SOURCE / _DESTINATION) or one of the
+// block-table maps of the encoder's peek() into device memory out (w x h).
+int peek_rgb(const int16_t *planes, const evxg_block_desc *bt, int which, int W, int H, int mbw, int w, int h,
+             uint8_t *out, cudaStream_t st);
 }  // namespace evxg
 
 #define CK(call)                                                     \

@@ -37,6 +37,7 @@ extern "C" {
 /* Status codes: same values as the reference's evx_status (base.h:168-185). */
 #define EVXG_SUCCESS              0
 #define EVXG_ERROR_INVALIDARG     1
+#define EVXG_ERROR_NOTIMPL        2
 #define EVXG_ERROR_OUTOFMEMORY    3
 #define EVXG_ERROR_INVALID_INDEX  6
 #define EVXG_ERROR_CAPACITY_LIMIT 7
@@ -570,6 +571,23 @@ int evxg_encoder_encode(evxg_encoder *e, const uint8_t *rgb, uint32_t width, uin
 int evxg_encoder_flush(evxg_encoder *e);                     /* evx3enc.cpp:385-414 */
 /* The stream under an encoder (NULL before the first frame). */
 evxg_stream *evxg_encoder_stream(evxg_encoder *e);
+/* evx3_encoder::peek (evx3enc.cpp:417-547): an RGB24 image of the visible
+ * size into host memory -- the converted source, the reference slot the
+ * reference's own encoder state names (its running frame's dpb_slot, which
+ * its GOP logic never sets in the default build, so slot 0; without B frames
+ * the slot one index back from the next frame), or per macroblock of the
+ * last encoded frame: block type (R intra, G motion, B copy), QP
+ * (255 - 15 q, copies red), variance (variance / 30, copies red), sub-pel
+ * (G quarter, B half).  EVXG_PEEK_PREDICTION is EVXG_ERROR_NOTIMPL, as in the
+ * reference; before the first frame nothing is written. */
+#define EVXG_PEEK_SOURCE         0
+#define EVXG_PEEK_PREDICTION     1
+#define EVXG_PEEK_BLOCK_TABLE    2
+#define EVXG_PEEK_QUANT_TABLE    3
+#define EVXG_PEEK_SPMP_TABLE     4
+#define EVXG_PEEK_BLOCK_VARIANCE 5
+#define EVXG_PEEK_DESTINATION    6
+int evxg_encoder_peek(evxg_encoder *e, int which, uint8_t *rgb);
 /* Bitstream output: once set, the encoder also codes every frame on the host
  * (evxg_serialize_slice) and hands the stream's bytes to cb in order, on the
  * calling thread -- the 14-byte header before the first frame, then each

@@ -227,6 +227,7 @@ class Ref:
         L.evxref_enc_encode.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
                                         C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]
         L.evxref_enc_flush.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]
+        L.evxref_enc_peek.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         self.staged = hasattr(L, "evxref_ctx_create")   # builds without encode.cpp have the stock API only
         if self.staged:
             L.evxref_ctx_create.restype = C.c_void_p
@@ -283,6 +284,31 @@ class Ref:
         finally:
             self.lib.evxref_enc_destroy(h)
         return out if chunks else b"".join(out)
+
+    def peeks(self, frames: np.ndarray, quality: int, states) -> list:
+        """Encode (T,H,W,3) frames with the stock encoder and after every
+        encode() call take peek(state) for each state: [{state: (H,W,3)}]."""
+        T, H, W, _ = frames.shape
+        cap = max(1 << 22, W * H * 3 * 8)
+        h = self.lib.evxref_enc_create(cap)
+        buf = np.zeros(cap, np.uint8)
+        n = C.c_uint32(0)
+        out = []
+        try:
+            self.lib.evxref_enc_set_quality(h, quality)
+            for t in range(T):
+                f = np.ascontiguousarray(frames[t])
+                if self.lib.evxref_enc_encode(h, _p(f), W, H, _p(buf), cap, C.byref(n)):
+                    raise RuntimeError("reference encode failed")
+                views = {}
+                for st in states:
+                    img = np.zeros((H, W, 3), np.uint8)
+                    rc = self.lib.evxref_enc_peek(h, st, _p(img))
+                    views[st] = img if rc == 0 else rc
+                out.append(views)
+        finally:
+            self.lib.evxref_enc_destroy(h)
+        return out
 
     def decode_stream(self, data: bytes, width: int, height: int, max_frames: int = 256) -> np.ndarray:
         """Decode a whole .evx stream with the stock decoder; (T,H,W,3) frames in display order."""

@@ -133,6 +133,12 @@ int evxref_enc_encode(void *p, const uint8_t *rgb, uint32_t w, uint32_t h,
     return 0;
 }
 
+/* evx3_encoder::peek (evx3enc.cpp:417-547) into out (visible size RGB24). */
+int evxref_enc_peek(void *p, int state, uint8_t *out)
+{
+    return ((evxref_enc *)p)->enc->peek((EVX_PEEK_STATE)state, out);
+}
+
 int evxref_enc_flush(void *p, uint8_t *out, uint32_t cap, uint32_t *out_len)
 {
     evxref_enc *e = (evxref_enc *)p;

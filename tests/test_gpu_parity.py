@@ -278,3 +278,30 @@ def test_pipelined_frames_equal_synchronous_frames(cfg, w, h, T):
         b.output_wait(t)
         for key in want[k]:
             assert np.array_equal(outs[k][key], want[k][key]), f"frame {k}: {key}"
+
+
+@pytest.mark.parametrize("cfg", ["default", "ip3"])
+def test_encoder_peek_views_match_reference(cfg):
+    """evxg_encoder_peek gives the stock encoder's peek() images after every
+    encode() call: source, destination slot, block types, QP, sub-pel and
+    variance maps; the prediction view is not implemented in either."""
+    import os
+    import chicago_b200 as cb
+    if cfg != "default" and not os.path.exists(REF_VARIANTS[cfg][0]):
+        pytest.skip("reference variant not built")
+    ref = Ref() if cfg == "default" else Ref(variant=cfg)
+    w, h, T = 100, 60, 7
+    frames = generate(w, h, T, seed=17, vmax=8.0)
+    want = ref.peeks(frames, 8, range(7))
+    enc = cb.Encoder(quality=8, cfg=cfg)
+    for t in range(T):
+        enc.encode(frames[t])
+        for st in range(7):
+            if st == 1:
+                assert want[t][st] == 2
+                with pytest.raises(cb.EvxgError) as e:
+                    enc.peek(st, w, h)
+                assert e.value.code == 2
+                continue
+            assert np.array_equal(enc.peek(st, w, h), want[t][st]), f"call {t}: view {st}"
+    enc.close()
