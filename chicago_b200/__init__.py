@@ -66,6 +66,7 @@ EXPORTS = [
     "evxg_stream_decoder_create", "evxg_stream_decoder_destroy", "evxg_stream_decoder_clear",
     "evxg_stream_decoder_dims", "evxg_stream_decoder_decode", "evxg_stream_decoder_flush",
     "evxg_encode_frame_pipelined", "evxg_stream_output_wait", "evxg_encoder_peek",
+    "evxg_stream_state_bytes", "evxg_stream_save", "evxg_stream_restore", "evxg_server_evict", "evxg_server_restore",
 ]
 MB_FORM_SINGLE, MB_FORM_CLUSTER = 0, 1
 
@@ -217,6 +218,12 @@ def _load(path: str = LIB_PATH) -> C.CDLL:
     L.evxg_encode_frame_pipelined.argtypes = [vp, vp, C.c_char_p, vp, vp, vp, vp, vp, C.POINTER(u64)]
     L.evxg_stream_output_wait.argtypes = [vp, u64]
     L.evxg_encoder_peek.argtypes = [vp, i32, vp]
+    L.evxg_stream_state_bytes.argtypes = [vp]
+    L.evxg_stream_state_bytes.restype = u64
+    L.evxg_stream_save.argtypes = [vp, vp, u64, vp]
+    L.evxg_stream_restore.argtypes = [vp, vp, u64, vp]
+    L.evxg_server_evict.argtypes = [vp, u32]
+    L.evxg_server_restore.argtypes = [vp, u32]
     return L
 
 
@@ -340,6 +347,16 @@ class Stream:
 
     def output_wait(self, ticket: int):
         _check(lib().evxg_stream_output_wait(self.h, ticket))
+
+    def save(self, cuda_stream=None) -> bytes:
+        """evxg_stream_save: the stream's device state, to continue it later."""
+        buf = np.empty(lib().evxg_stream_state_bytes(self.h), np.uint8)
+        _check(lib().evxg_stream_save(self.h, _ptr(buf), len(buf), _ptr(cuda_stream)))
+        return buf.tobytes()
+
+    def restore(self, state: bytes, cuda_stream=None):
+        buf = np.frombuffer(state, np.uint8)
+        _check(lib().evxg_stream_restore(self.h, _ptr(buf), len(buf), _ptr(cuda_stream)))
 
     def set_timeout_ns(self, ns: int):
         """Bound on every device-side wait of this stream's kernels (5 s by default)."""
@@ -710,6 +727,14 @@ class Server:
     def cancel(self, sid: int):
         """Drop the stream's frames not yet in a tick; those in flight are delivered."""
         _check(lib().evxg_server_cancel(self.h, sid))
+
+    def evict(self, sid: int):
+        """Move the stream's device state to host memory, freeing its device memory."""
+        _check(lib().evxg_server_evict(self.h, sid))
+
+    def restore(self, sid: int):
+        """Bring an evicted stream back onto the device; it continues bit-identically."""
+        _check(lib().evxg_server_restore(self.h, sid))
 
     def stats(self) -> dict:
         v = [C.c_uint64() for _ in range(4)]

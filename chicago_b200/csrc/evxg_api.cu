@@ -197,6 +197,76 @@ int evxg_stream_reset(evxg_stream *s, void *cuda_stream)
     return EVXG_SUCCESS;
 }
 
+// Saved stream state: a 48-byte header (magic "EVXS", format version, aligned
+// size, build, SAO epoch, sizes of what follows), then the four DPB plane
+// sets, the level planes, the temporal predictor table and the block table --
+// everything a later frame of the stream reads (the source, the SAO scratch
+// and the serializer's snapshot are rewritten by every frame).
+struct SavedHeader {
+    char magic[4];
+    uint32_t version, W, H;
+    evxg_config cfg;
+    int32_t epoch;
+    uint64_t plane_bytes, table_bytes;
+    uint32_t reserved[2];
+};
+static_assert(sizeof(SavedHeader) == 48, "saved-state header");
+
+uint64_t evxg_stream_state_bytes(const evxg_stream *s)
+{
+    if (!s) return 0;
+    const uint64_t pb = s->plane_elems * sizeof(int16_t), tb = (uint64_t)s->mbw * s->mbh * sizeof(evxg_block_desc);
+    return sizeof(SavedHeader) + 5 * pb + 2 * tb;
+}
+
+int evxg_stream_save(evxg_stream *s, void *host, uint64_t capacity, void *cuda_stream)
+{
+    if (!s || !host) return fail(EVXG_ERROR_INVALIDARG, "evxg_stream_save: null argument");
+    if (capacity < evxg_stream_state_bytes(s)) return fail(EVXG_ERROR_CAPACITY_LIMIT, "evxg_stream_save: buffer too small");
+    const cudaStream_t st = (cudaStream_t)cuda_stream;
+    const uint64_t pb = s->plane_elems * sizeof(int16_t), tb = (uint64_t)s->mbw * s->mbh * sizeof(evxg_block_desc);
+    SavedHeader h{};
+    memcpy(h.magic, "EVXS", 4);
+    h.version = 1; h.W = s->W; h.H = s->H; h.cfg = s->cfg; h.epoch = s->epoch;
+    h.plane_bytes = pb; h.table_bytes = tb;
+    uint8_t *o = static_cast<uint8_t *>(host);
+    memcpy(o, &h, sizeof h);
+    o += sizeof h;
+    for (int i = 0; i < 4; i++, o += pb) CK(cudaMemcpyAsync(o, s->dpb[i], pb, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(o, s->lev, pb, cudaMemcpyDeviceToHost, st));
+    o += pb;
+    CK(cudaMemcpyAsync(o, s->prev, tb, cudaMemcpyDeviceToHost, st));
+    o += tb;
+    CK(cudaMemcpyAsync(o, s->bt, tb, cudaMemcpyDeviceToHost, st));
+    return evxg_stream_sync(s, cuda_stream);
+}
+
+int evxg_stream_restore(evxg_stream *s, const void *host, uint64_t size, void *cuda_stream)
+{
+    if (!s || !host) return fail(EVXG_ERROR_INVALIDARG, "evxg_stream_restore: null argument");
+    SavedHeader h;
+    if (size < sizeof h) return fail(EVXG_ERROR_INVALID_RESOURCE, "evxg_stream_restore: not a saved stream state");
+    memcpy(&h, host, sizeof h);
+    if (memcmp(h.magic, "EVXS", 4) != 0 || h.version != 1 || size != evxg_stream_state_bytes(s))
+        return fail(EVXG_ERROR_INVALID_RESOURCE, "evxg_stream_restore: not a saved stream state of this size");
+    if (h.W != s->W || h.H != s->H || memcmp(&h.cfg, &s->cfg, sizeof h.cfg) != 0)
+        return fail(EVXG_ERROR_INVALIDARG, "evxg_stream_restore: saved from a stream of another size or build");
+    const cudaStream_t st = (cudaStream_t)cuda_stream;
+    const uint64_t pb = h.plane_bytes, tb = h.table_bytes;
+    const uint8_t *i = static_cast<const uint8_t *>(host) + sizeof h;
+    for (int k = 0; k < 4; k++, i += pb) CK(cudaMemcpyAsync(s->dpb[k], i, pb, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->lev, i, pb, cudaMemcpyHostToDevice, st));
+    i += pb;
+    CK(cudaMemcpyAsync(s->prev, i, tb, cudaMemcpyHostToDevice, st));
+    i += tb;
+    CK(cudaMemcpyAsync(s->bt, i, tb, cudaMemcpyHostToDevice, st));
+    // mail words of frames after the saved one could carry the epochs that
+    // follow it: none may match (a zero word matches no epoch 1..255)
+    CK(cudaMemsetAsync(s->sao_mail, 0, (size_t)s->mbw * s->mbh * sizeof(unsigned long long), st));
+    s->epoch = h.epoch;
+    return evxg_stream_sync(s, cuda_stream);
+}
+
 int evxg_stream_set_mb_form(evxg_stream *s, int form)
 {
     if (!s || (form != EVXG_MB_FORM_SINGLE && form != EVXG_MB_FORM_CLUSTER))

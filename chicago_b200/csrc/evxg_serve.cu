@@ -25,6 +25,7 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <new>
 #include <thread>
 #include <vector>
 
@@ -66,6 +67,11 @@ struct Slot {
     uint32_t next_order = 0;
     bool closing = false;                      // no more input; removed once drained
     int in_flight = 0;                         // frames in ticks not yet delivered
+    evxg_config cfg{};                         // the build the stream reproduces
+    // Evicted: the device state lives in `saved` (evxg_stream_save), st is
+    // gone, its memory is back in the budget; the planner stays.
+    bool evicted = false;
+    std::vector<uint8_t> saved;
 };
 
 }  // namespace
@@ -175,7 +181,7 @@ void work(evxg_server *v, Lane *l)
         std::unique_lock<std::mutex> lk(v->mu);
         auto any_ready = [&] {
             for (auto &kv : v->slots)
-                if (kv.second->lane == l->index && !kv.second->ready.empty()) return true;
+                if (kv.second->lane == l->index && !kv.second->evicted && !kv.second->ready.empty()) return true;
             return false;
         };
         v->cv_work.wait(lk, [&] {
@@ -201,7 +207,7 @@ void work(evxg_server *v, Lane *l)
                 Slot *s = it->second;
                 if (s->lane == l->index && s->closing && drained(s)) {
                     evxg_encoder_destroy(s->planner);
-                    evxg_stream_destroy(s->st);
+                    if (s->st) evxg_stream_destroy(s->st);
                     v->used -= s->bytes;
                     delete s;
                     it = v->slots.erase(it);
@@ -213,7 +219,10 @@ void work(evxg_server *v, Lane *l)
             l->bslots.clear();
             std::vector<evxg_stream *> sts;
             for (auto &kv : v->slots)
-                if (kv.second->lane == l->index) { l->bslots.push_back(kv.second); sts.push_back(kv.second->st); }
+                if (kv.second->lane == l->index && !kv.second->evicted) {
+                    l->bslots.push_back(kv.second);
+                    sts.push_back(kv.second->st);
+                }
             if (!sts.empty()) {
                 const int rc = evxg_batch_create(sts.data(), (uint32_t)sts.size(), &l->batch);
                 if (rc) { v->error = rc; continue; }   // the batch's default shape: its tick model (evxg_batch.cu)
@@ -362,6 +371,8 @@ int evxg_server_open_config(evxg_server *v, uint32_t width, uint32_t height, uin
     }
     Slot *s = new Slot();
     s->w = width; s->h = height; s->bytes = bytes;
+    evxg_config_default(&s->cfg);
+    if (cfg) s->cfg = *cfg;
     int rc = evxg_stream_create_config(width, height, cfg, &s->st);
     if (!rc) rc = evxg_encoder_create_config(nullptr, nullptr, cfg, &s->planner);
     if (!rc) { encoder_set_sink(s->planner, sink, s); rc = evxg_encoder_set_quality(s->planner, quality); }
@@ -390,6 +401,7 @@ int evxg_server_submit(evxg_server *v, uint32_t stream_id, const uint8_t *rgb, u
     auto it = v->slots.find(stream_id);
     if (it == v->slots.end() || it->second->closing) return fail(EVXG_ERROR_INVALID_INDEX, "evxg_server_submit: no such open stream");
     Slot *s = it->second;
+    if (s->evicted) return fail(EVXG_ERROR_NOT_READY, "evxg_server_submit: the stream is evicted (restore it first)");
     s->arrival[s->next_order++] = arrival_ns ? arrival_ns : now_ns();
     const int rc = evxg_encoder_encode(s->planner, rgb, s->w, s->h);
     v->cv_work.notify_all();
@@ -402,6 +414,7 @@ int evxg_server_insert_intra(evxg_server *v, uint32_t stream_id)
     std::lock_guard<std::mutex> lk(v->mu);
     auto it = v->slots.find(stream_id);
     if (it == v->slots.end() || it->second->closing) return fail(EVXG_ERROR_INVALID_INDEX, "evxg_server_insert_intra: no such open stream");
+    if (it->second->evicted) return fail(EVXG_ERROR_NOT_READY, "evxg_server_insert_intra: the stream is evicted");
     return evxg_encoder_insert_intra(it->second->planner);
 }
 
@@ -411,6 +424,7 @@ int evxg_server_close(evxg_server *v, uint32_t stream_id)
     std::lock_guard<std::mutex> lk(v->mu);
     auto it = v->slots.find(stream_id);
     if (it == v->slots.end() || it->second->closing) return fail(EVXG_ERROR_INVALID_INDEX, "evxg_server_close: no such open stream");
+    if (it->second->evicted) return fail(EVXG_ERROR_NOT_READY, "evxg_server_close: the stream is evicted (restore or cancel it)");
     const int rc = evxg_encoder_flush(it->second->planner);   // the frames still waiting for their anchor
     it->second->closing = true;
     v->cv_work.notify_all();
@@ -427,6 +441,92 @@ int evxg_server_cancel(evxg_server *v, uint32_t stream_id)
     s->ready.clear();     // frames not yet in a tick are dropped; those in flight are delivered
     s->arrival.clear();
     s->closing = true;    // no flush: frames still waiting for their anchor are dropped too
+    v->cv_work.notify_all();
+    return EVXG_SUCCESS;
+}
+
+int evxg_server_evict(evxg_server *v, uint32_t stream_id)
+{
+    if (!v) return EVXG_ERROR_INVALIDARG;
+    std::unique_lock<std::mutex> lk(v->mu);
+    auto it = v->slots.find(stream_id);
+    if (it == v->slots.end() || it->second->closing || it->second->evicted)
+        return fail(EVXG_ERROR_INVALID_INDEX, "evxg_server_evict: no such resident stream");
+    Slot *s = it->second;
+    Lane *l = v->lanes[s->lane];
+    // The frames it already has are encoded and delivered first; then its lane
+    // rebuilds its batch without it, so that no tick touches its memory again.
+    v->drainers++;
+    v->cv_work.notify_all();
+    v->cv_done.wait(lk, [&] { return v->error || drained(s); });
+    if (!v->error) {
+        s->evicted = true;
+        l->set_dirty = true;
+        v->cv_work.notify_all();
+        v->cv_done.wait(lk, [&] { return v->error || !l->set_dirty; });
+    }
+    v->drainers--;
+    if (v->error) return fail(v->error, "evxg_server_evict: the server has failed");
+    evxg_stream *st = s->st;
+    s->st = nullptr;
+    lk.unlock();
+    std::vector<uint8_t> saved;
+    int rc = EVXG_SUCCESS;
+    try {
+        saved.resize(evxg_stream_state_bytes(st));
+    } catch (const std::bad_alloc &) {
+        rc = fail(EVXG_ERROR_OUTOFMEMORY, "evxg_server_evict: host allocation");
+    }
+    if (!rc) rc = evxg_stream_save(st, saved.data(), saved.size(), nullptr);
+    lk.lock();
+    if (rc) {   // no copy: keep the stream resident as it was
+        s->st = st;
+        s->evicted = false;
+        l->set_dirty = true;
+        v->cv_work.notify_all();
+        return rc;
+    }
+    lk.unlock();
+    evxg_stream_destroy(st);
+    lk.lock();
+    s->saved = std::move(saved);
+    v->used -= s->bytes;
+    s->bytes = 0;
+    return EVXG_SUCCESS;
+}
+
+int evxg_server_restore(evxg_server *v, uint32_t stream_id)
+{
+    if (!v) return EVXG_ERROR_INVALIDARG;
+    Slot *s = nullptr;
+    size_t bytes = 0;
+    {
+        std::lock_guard<std::mutex> lk(v->mu);
+        if (v->error) return fail(v->error, "evxg_server_restore: the server has failed");
+        auto it = v->slots.find(stream_id);
+        if (it == v->slots.end() || it->second->closing || !it->second->evicted)
+            return fail(EVXG_ERROR_INVALID_INDEX, "evxg_server_restore: no such evicted stream");
+        s = it->second;
+        bytes = stream_bytes(s->w, s->h);
+        if (v->used - dead_bytes(v) + bytes > v->budget)
+            return fail(EVXG_ERROR_CAPACITY_LIMIT, "evxg_server_restore: the device memory budget is spent");
+        v->used += bytes;   // reserved while the stream is created
+    }
+    evxg_stream *st = nullptr;
+    int rc = evxg_stream_create_config(s->w, s->h, &s->cfg, &st);
+    if (!rc) rc = evxg_stream_restore(st, s->saved.data(), s->saved.size(), nullptr);
+    std::lock_guard<std::mutex> lk(v->mu);
+    if (rc) {
+        if (st) evxg_stream_destroy(st);
+        v->used -= bytes;
+        return rc;
+    }
+    s->st = st;
+    s->bytes = bytes;
+    s->saved.clear();
+    s->saved.shrink_to_fit();
+    s->evicted = false;
+    v->lanes[s->lane]->set_dirty = true;
     v->cv_work.notify_all();
     return EVXG_SUCCESS;
 }

@@ -215,6 +215,19 @@ int evxg_stream_sync(evxg_stream *s, void *cuda_stream);
 int evxg_stream_set_timeout_ns(evxg_stream *s, int64_t ns);
 int evxg_stream_reset(evxg_stream *s, void *cuda_stream);
 
+/* Checkpoint of a stream (the device half of the reference's evx_context,
+ * common.h:209-240; the GOP state lives with the caller or the GOP encoder):
+ * evxg_stream_save copies everything later frames read -- the DPB slots, the
+ * level planes (copy blocks keep stale levels that later DC prediction
+ * reads), the temporal predictor and block tables, the SAO epoch -- into
+ * evxg_stream_state_bytes(s) bytes of host memory; evxg_stream_restore loads
+ * it into a stream of the same size and build, after which the stream's next
+ * frames are bit-identical to those of the stream it was saved from.  Both
+ * wait for their copies. */
+uint64_t evxg_stream_state_bytes(const evxg_stream *s);
+int evxg_stream_save(evxg_stream *s, void *host, uint64_t capacity, void *cuda_stream);
+int evxg_stream_restore(evxg_stream *s, const void *host, uint64_t size, void *cuda_stream);
+
 /* Number of kernels launched by the last evxg_encode_frame call. */
 uint32_t evxg_last_launch_count(const evxg_stream *s);
 
@@ -344,6 +357,15 @@ int evxg_server_drain(evxg_server *srv);
  * already in a tick are delivered, and the stream's memory is released like a
  * closed stream's.  The other streams' results are not affected. */
 int evxg_server_cancel(evxg_server *srv, uint32_t stream_id);
+/* Evict a live stream from the device: its frames already submitted are
+ * encoded and delivered, its lane stops ticking it, its device state goes to
+ * host memory (evxg_stream_save) and its device memory back to the budget;
+ * its GOP planner stays.  While evicted, submit / insert_intra / close return
+ * EVXG_ERROR_NOT_READY (cancel drops it).  evxg_server_restore re-admits it
+ * within the budget (EVXG_ERROR_CAPACITY_LIMIT otherwise; try again later)
+ * and it continues bit-identically.  Its id keeps its stream slot. */
+int evxg_server_evict(evxg_server *srv, uint32_t stream_id);
+int evxg_server_restore(evxg_server *srv, uint32_t stream_id);
 int evxg_server_stats(evxg_server *srv, uint64_t *frames, uint64_t *ticks, uint64_t *rebuilds, uint64_t *bytes_in_use);
 uint64_t evxg_server_now_ns(void);
 

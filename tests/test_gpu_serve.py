@@ -162,3 +162,76 @@ def test_server_cancel_mid_gop_leaves_other_streams_alone():
         srv.submit(ids[1], seqs[1][0])       # a cancelled stream takes no more frames
     assert srv.stats()["bytes_in_use"] == 0
     srv.close()
+
+
+@pytest.mark.timeout(300)
+@pytest.mark.parametrize("cfg", ["default", "ip3"])
+def test_stream_checkpoint_continues_bit_identically(cfg):
+    """evxg_stream_save after frame k, evxg_stream_restore into a fresh stream:
+    its following frames equal the uninterrupted stream's."""
+    import chicago_b200 as cb
+    from oracle_py import plan_gop, plan_ip
+    b_frames, ref_count, _ = cb.CONFIGS[cfg]
+    w, h, T, k = 176, 144, 10, 5
+    frames = generate(w, h, T, seed=41, vmax=6.0)
+    plan = plan_gop(T, quality=8) if b_frames else plan_ip(T, 8, (), ref_count)
+    a = cb.Stream(w, h, cfg)
+    want = []
+    for ti, f18 in plan:
+        a.encode_frame(frames[ti], f18)
+        want.append(a.fetch_tables())
+    b = cb.Stream(w, h, cfg)
+    for ti, f18 in plan[:k]:
+        b.encode_frame(frames[ti], f18)
+    state = b.save()
+    b.close()
+    c = cb.Stream(w, h, cfg)
+    c.restore(state)
+    for i, (ti, f18) in enumerate(plan[k:], start=k):
+        c.encode_frame(frames[ti], f18)
+        got = c.fetch_tables()
+        for key in want[i]:
+            assert np.array_equal(got[key], want[i][key]), f"frame {i}: {key}"
+    with pytest.raises(cb.EvxgError):   # another size
+        cb.Stream(w + 16, h, cfg).restore(state)
+
+
+@pytest.mark.timeout(300)
+def test_server_evict_restore_continues_bit_identically():
+    """A served stream evicted mid-sequence frees its device memory, refuses
+    frames while evicted, and after restore its results equal the stream
+    encoded alone; a neighbour keeps running meanwhile."""
+    import chicago_b200 as cb
+    srv = cb.Server(hbm_budget_bytes=1 << 34, max_streams=4)
+    w, h, q, n = 176, 144, 8, 12
+    seq = generate(w, h, n, seed=77, vmax=5.0)
+    other = generate(96, 64, n, seed=78, vmax=4.0)
+    sid, oid = srv.open(w, h, q), srv.open(96, 64, 8)
+    for t in range(6):
+        srv.submit(sid, seq[t])
+        srv.submit(oid, other[t])
+    srv.drain()
+    before = srv.stats()["bytes_in_use"]
+    srv.evict(sid)
+    assert srv.stats()["bytes_in_use"] < before
+    with pytest.raises(cb.EvxgError) as e:
+        srv.submit(sid, seq[6])
+    assert e.value.code == 15   # EVXG_ERROR_NOT_READY
+    for t in range(6, 9):
+        srv.submit(oid, other[t])
+    srv.restore(sid)
+    for t in range(6, n):
+        srv.submit(sid, seq[t])
+    for t in range(9, n):
+        srv.submit(oid, other[t])
+    srv.close_stream(sid)
+    srv.close_stream(oid)
+    srv.drain()
+    for s_, frames, (ww, hh, qq) in ((sid, seq, (w, h, q)), (oid, other, (96, 64, 8))):
+        got, want = srv.results[s_], alone(ww, hh, qq, frames, ())
+        assert len(got) == len(want) == n
+        for i, (g, e_) in enumerate(zip(got, want)):
+            assert g["frame18"] == e_["frame18"], f"stream {s_} record {i}: frame"
+            for key in ("blocks", "prev_blocks", "sao", "levels"):
+                assert np.array_equal(g[key], e_[key]), f"stream {s_} record {i}: {key}"
+    srv.close()
