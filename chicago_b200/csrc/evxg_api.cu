@@ -130,6 +130,8 @@ int evxg_stream_create_config(uint32_t width, uint32_t height, const evxg_config
     if (e == cudaSuccess) e = dev_alloc(&s->sync, (3 * s->mbh + 5) * sizeof(int));
     // Zeroing on a private stream, synchronised alone: no device-wide
     // synchronisation, which another thread capturing a graph would forbid.
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking);
+    for (int i = 0; i < 2 && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&s->ev_aux[i], cudaEventDisableTiming);
     cudaStream_t zs = nullptr;
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&zs, cudaStreamNonBlocking);
     if (e == cudaSuccess && reset_stream(s, zs)) e = cudaErrorUnknown;
@@ -164,6 +166,9 @@ int evxg_stream_destroy(evxg_stream *s)
     if (s->profile)
         for (int i = 0; i < 7; i++) cudaEventDestroy(s->ev[i]);
     pipeline_free(s);
+    if (s->aux) { cudaStreamSynchronize(s->aux); cudaStreamDestroy(s->aux); }
+    for (int i = 0; i < 2; i++)
+        if (s->ev_aux[i]) cudaEventDestroy(s->ev_aux[i]);
     delete s;
     return EVXG_SUCCESS;
 }
@@ -421,6 +426,13 @@ static int encode_impl(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, co
     CK(cudaMemcpyAsync(s->prev_ser, s->prev, nblk * sizeof(evxg_block_desc), cudaMemcpyDeviceToDevice, st));
     CK(cudaMemsetAsync(s->sync, 0xFF, 3 * s->mbh * sizeof(int), st));
     CK(cudaMemsetAsync(s->sync + 3 * s->mbh, 0, 4 * sizeof(int), st));
+    // Deblocking runs beside the cluster-form pass when both fit on the
+    // device at once: it trails the wavefront and writes the deblocked frame
+    // to the SAO pristine copy (later macroblock rows still read the slot's
+    // reconstruction), which then becomes the SAO pass's starting image.
+    const bool overlap = s->aux && s->mb_form == EVXG_MB_FORM_CLUSTER && deblock_shared_bytes((int)s->W) > 0 &&
+                         3 * s->mb_clusters + kDeblockCtas <= s->num_sms;
+    if (overlap) CK(cudaEventRecord(s->ev_aux[0], st));   // the progress words are reset
     const int cw = (int)std::min(s->vw, s->W), ch = (int)std::min(s->vh, s->H);
     dim3 cg((cw / 2 + 127) / 128, ch / 2);
     const unsigned wf = (s->mbh + 7) / 8;
@@ -433,10 +445,24 @@ static int encode_impl(evxg_stream *s, const uint8_t *rgb, int rgb_on_device, co
         k_mb_cluster<<<3 * s->mb_clusters, mb_threads(), mb_shared_bytes(), st>>>(a);
     else
         k_mb_wavefront<<<s->mb_grid, mb_threads(), mb_shared_bytes(), st>>>(a);
+    if (overlap) {   // launched after the pass, so that the pass's clusters are placed first
+        FrameArgs da = a;
+        da.db_out = s->sao_orig;
+        da.db_wait = 1;
+        CK(cudaStreamWaitEvent(s->aux, s->ev_aux[0], 0));
+        k_deblock<<<kDeblockCtas, kDeblockThreads, deblock_shared_bytes((int)s->W), s->aux>>>(da);
+        CK(cudaEventRecord(s->ev_aux[1], s->aux));
+    }
     mark(2);
-    k_deblock<<<kDeblockCtas, kDeblockThreads, deblock_shared_bytes((int)s->W), st>>>(a);
-    mark(3);
-    CK(cudaMemcpyAsync(s->sao_orig, s->dpb[f->dpb_slot], s->plane_elems * sizeof(int16_t), cudaMemcpyDeviceToDevice, st));
+    if (overlap) {
+        CK(cudaStreamWaitEvent(st, s->ev_aux[1], 0));
+        mark(3);
+        CK(cudaMemcpyAsync(s->dpb[f->dpb_slot], s->sao_orig, s->plane_elems * sizeof(int16_t), cudaMemcpyDeviceToDevice, st));
+    } else {
+        k_deblock<<<kDeblockCtas, kDeblockThreads, deblock_shared_bytes((int)s->W), st>>>(a);
+        mark(3);
+        CK(cudaMemcpyAsync(s->sao_orig, s->dpb[f->dpb_slot], s->plane_elems * sizeof(int16_t), cudaMemcpyDeviceToDevice, st));
+    }
     CK(cudaMemsetAsync(s->sao_flags, 0, kSaoPasses * sizeof(int), st));
     k_sao_rdo<<<(unsigned)((nblk + 7) / 8), 256, 0, st>>>(a);   // one warp per MB
     mark(4);

@@ -121,6 +121,10 @@ struct FrameArgs {
     evxg_block_desc *prev_tab;   // temporal predictor table (the frame's update target)
     evxg_block_desc *prev_ser;   // snapshot of it for the serializer
     size_t plane_elems;          // samples in one plane set
+    // deblocking beside the macroblock pass: filtered rows go to db_out
+    // (else in place), each band once the wavefront has finished its rows
+    int16_t *db_out;
+    int db_wait;
 };
 
 // Batched launches: blockIdx.z selects the stream; its parameters are copied

@@ -176,13 +176,44 @@ __device__ __forceinline__ int16_t *db_peer(int16_t *p, unsigned rank)
     asm volatile("mapa.u64 %0, %1, %2;" : "=l"(r) : "l"(p), "r"(rank));
     return r;
 }
+// Deblocking beside the macroblock pass (a.db_wait): before a strip reads
+// plane rows up to y, its thread 0 waits (bounded) until the wavefront has
+// finished the macroblock row holding y -- rows finish in order.  After a
+// wait that gave up (error word set) the strip stops waiting but keeps
+// step with its cluster's barriers, so every CTA still reaches its end.
+__device__ void db_wait(const FrameArgs &a, int y, int mbs, bool &live)
+{
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        int ok = live;
+        const int r = min(y / mbs, a.mbh - 1);
+        if (ok) {
+            const unsigned long long t0 = globaltimer_ns();
+            while (ld_acquire(&a.progress[r]) < a.mbw - 1) {
+                if (*(volatile int *)a.error || (long long)(globaltimer_ns() - t0) > a.timeout_ns) {
+                    atomicCAS(a.error, 0, EVXG_ERROR_OPERATION_TIMEDOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(128);
+            }
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    live = s_ok != 0;
+    __syncthreads();   // s_ok is rewritten by the next wait
+}
 __device__ void deblock_strip_body(const FrameArgs &a, int16_t *buf)
 {
     const int pl = blockIdx.x / DB_STRIPS, sid = (int)db_rank();
     const bool luma = pl == 0;
     const int w = luma ? a.W : a.W / 2, h = luma ? a.H : a.H / 2;
     const int mbs = luma ? 16 : 8, qoff = luma ? 0 : 2;
-    int16_t *d = a.planes[a.dpb] + (pl == 0 ? 0 : (size_t)a.W * a.H + (pl - 1) * (size_t)(a.W / 2) * (a.H / 2));
+    const size_t poff = pl == 0 ? 0 : (size_t)a.W * a.H + (pl - 1) * (size_t)(a.W / 2) * (a.H / 2);
+    const int16_t *d = a.planes[a.dpb] + poff;           // reconstruction read
+    int16_t *o = (a.db_out ? a.db_out : a.planes[a.dpb]) + poff;   // filtered rows written
+    bool live = true;
     const int xs = db_x0(w, sid), xe = sid + 1 < DB_STRIPS ? db_x0(w, sid + 1) : w;
     const int sw = xe - xs, cpr = sw / 8;   // strip width, 16-byte chunks per strip row
     // the strip holding columns xs-4 .. xs-1 (strips are multiples of 8 wide; empty ones hold nothing)
@@ -198,6 +229,7 @@ __device__ void deblock_strip_body(const FrameArgs &a, int16_t *buf)
     const int nvx = sw / 8 - (xs == 0 ? 1 : 0);   // vertical edges owned: x = xs (if > 0), xs + 8, ...
     const int xv0 = xs == 0 ? 8 : xs;
     const int tid = threadIdx.x, nt = blockDim.x;
+    if (a.db_wait) db_wait(a, min(7, h - 1), mbs, live);
     for (int i = tid; i < 8 * cpr; i += nt) {   // band 0
         const int r = i / cpr, c = i % cpr;
         *reinterpret_cast<uint4 *>(buf + db_slot(r) * sw + 8 * c) = __ldcg(reinterpret_cast<const uint4 *>(d + (size_t)r * w + xs + 8 * c));
@@ -206,6 +238,7 @@ __device__ void deblock_strip_body(const FrameArgs &a, int16_t *buf)
     int written = 0;   // rows [0, written) of the strip are back in the slot
     for (int j = 0; j < h; j += 8) {
         const bool more = j + 8 < h;
+        if (more && a.db_wait) db_wait(a, min(j + 15, h - 1), mbs, live);
         constexpr int PF = DB_MAXW / DB_THREADS;   // next band: at most 8 rows x 256 chunks
         uint4 pf[PF];
 #pragma unroll
@@ -245,7 +278,7 @@ __device__ void deblock_strip_body(const FrameArgs &a, int16_t *buf)
         const int upto = more ? j + 5 : h;
         for (int i = tid; i < (upto - written) * cpr; i += nt) {
             const int r = written + i / cpr, c = i % cpr;
-            *reinterpret_cast<uint4 *>(d + (size_t)r * w + xs + 8 * c) = *reinterpret_cast<const uint4 *>(buf + db_slot(r) * sw + 8 * c);
+            *reinterpret_cast<uint4 *>(o + (size_t)r * w + xs + 8 * c) = *reinterpret_cast<const uint4 *>(buf + db_slot(r) * sw + 8 * c);
         }
         written = upto;
 #pragma unroll

@@ -86,6 +86,10 @@ struct evxg_stream {
     evxg_config cfg;                    // reference build configuration the stream reproduces
     bool profile;
     cudaEvent_t ev[7];
+    // deblocking beside the macroblock pass (cluster form): its stream, and
+    // events for "sync words reset" and "deblocking done"
+    cudaStream_t aux;
+    cudaEvent_t ev_aux[2];
     // Pipelined encoding from host memory (evxg_encode_frame_pipelined), set
     // up on first use: an upload and a download stream, two device RGB
     // buffers and two table snapshots, the events that order uploads / frames
