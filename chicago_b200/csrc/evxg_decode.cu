@@ -603,6 +603,8 @@ struct evxg_decoder {
     uint8_t *rgb;
     int num_sms;
     long long timeout_ns;
+    cudaStream_t aux;                  // deblocking beside the intra wavefront
+    cudaEvent_t ev_aux[2];             // inter pass done / deblocking done
     // Entropy-decoded state of the host side (evx_context of the reference's
     // decoder): the tables persist from frame to frame, since a slice
     // rewrites only the fields it codes.
@@ -668,6 +670,8 @@ int evxg_decoder_create(uint32_t width, uint32_t height, const evxg_config *cfg,
     if (e == cudaSuccess) e = cudaMalloc(&d->sao_flags, kSaoPasses * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&d->sync, (3 * d->mbh + 5) * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&d->rgb, (size_t)width * height * 3);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&d->aux, cudaStreamNonBlocking);
+    for (int i = 0; i < 2 && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&d->ev_aux[i], cudaEventDisableTiming);
     cudaStream_t zs = nullptr;
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&zs, cudaStreamNonBlocking);
     if (e == cudaSuccess && decoder_zero(d, zs)) e = cudaErrorUnknown;
@@ -690,6 +694,9 @@ int evxg_decoder_destroy(evxg_decoder *d)
     for (int i = 0; i < 4; i++) cudaFree(d->dpb[i]);
     cudaFree(d->lev); cudaFree(d->snap); cudaFree(d->sao_orig);
     cudaFree(d->bt); cudaFree(d->sao); cudaFree(d->sao_res); cudaFree(d->sao_flags); cudaFree(d->sync); cudaFree(d->rgb);
+    if (d->aux) { cudaStreamSynchronize(d->aux); cudaStreamDestroy(d->aux); }
+    for (int i = 0; i < 2; i++)
+        if (d->ev_aux[i]) cudaEventDestroy(d->ev_aux[i]);
     delete d;
     return EVXG_SUCCESS;
 }
@@ -785,6 +792,12 @@ int evxg_decode_frame(evxg_decoder *d, const evxg_frame *fin, const evxg_block_d
         const unsigned blocks_needed = (unsigned)((nblk + INTER_WARPS - 1) / INTER_WARPS);
         k_dec_inter<<<std::min<unsigned>(blocks_needed, (unsigned)d->num_sms * 8), 32 * INTER_WARPS, 0, st>>>(a);
     }
+    // With an intra wavefront, deblocking trails it on a stream of its own (a
+    // row is final once its progress word reaches the last column) and writes
+    // the deblocked frame to the SAO pristine copy: the wavefront still reads
+    // the slot's unfiltered reconstruction.
+    const bool overlap = any_intra && d->aux && deblock_shared_bytes((int)d->W) > 0;
+    if (overlap) CK(cudaEventRecord(d->ev_aux[0], st));   // the inter macroblocks are in the slot
     if (any_intra) k_dec_intra<<<std::min<unsigned>(d->mbh, (unsigned)d->num_sms * 4), INTRA_THREADS, 0, st>>>(a);
 
     FrameArgs fa{};   // the encoder's in-loop filters on the decoded slot
@@ -794,9 +807,22 @@ int evxg_decode_frame(evxg_decoder *d, const evxg_frame *fin, const evxg_block_d
     fa.lev = d->lev; fa.bt = d->bt; fa.sao = d->sao_res; fa.sao_orig = d->sao_orig; fa.sao_flags = d->sao_flags;
     fa.progress = a.progress; fa.counters = a.counters; fa.error = a.error; fa.timeout_ns = d->timeout_ns;
     fa.active = 1; fa.plane_elems = d->plane_elems;
+    if (overlap) {
+        FrameArgs da = fa;
+        da.db_out = d->sao_orig;
+        da.db_wait = 1;
+        CK(cudaStreamWaitEvent(d->aux, d->ev_aux[0], 0));
+        k_deblock<<<kDeblockCtas, kDeblockThreads, deblock_shared_bytes((int)d->W), d->aux>>>(da);
+        CK(cudaEventRecord(d->ev_aux[1], d->aux));
+    }
     k_dec_sao_resolve<<<(unsigned)((nblk + 255) / 256), 256, 0, st>>>(d->sao, d->sao_res, a.mbw, a.mbh);
-    k_deblock<<<kDeblockCtas, kDeblockThreads, deblock_shared_bytes((int)d->W), st>>>(fa);
-    CK(cudaMemcpyAsync(d->sao_orig, d->dpb[dest], pb, cudaMemcpyDeviceToDevice, st));
+    if (overlap) {
+        CK(cudaStreamWaitEvent(st, d->ev_aux[1], 0));
+        CK(cudaMemcpyAsync(d->dpb[dest], d->sao_orig, pb, cudaMemcpyDeviceToDevice, st));
+    } else {
+        k_deblock<<<kDeblockCtas, kDeblockThreads, deblock_shared_bytes((int)d->W), st>>>(fa);
+        CK(cudaMemcpyAsync(d->sao_orig, d->dpb[dest], pb, cudaMemcpyDeviceToDevice, st));
+    }
     CK(cudaMemsetAsync(d->sao_flags, 0, kSaoPasses * sizeof(int), st));
     for (int p = 0; p < kSaoPasses; p++) k_sao_fix<<<d->num_sms * 8, 256, 0, st>>>(fa, p);
     k_sao_restore<<<d->num_sms * 4, 256, 0, st>>>(fa, kSaoPasses - 1);
