@@ -122,7 +122,7 @@ int evxg_stream_create_config(uint32_t width, uint32_t height, const evxg_config
     if (e == cudaSuccess) e = dev_alloc(&s->prev, nblk * sizeof(evxg_block_desc));
     if (e == cudaSuccess) e = dev_alloc(&s->prev_ser, nblk * sizeof(evxg_block_desc));
     if (e == cudaSuccess) e = dev_alloc(&s->sao, nblk * sizeof(evxg_sao_info));
-    if (e == cudaSuccess) e = dev_alloc(&s->sao_cost, nblk * sizeof(float));
+    if (e == cudaSuccess) e = dev_alloc(&s->sao_stats, nblk * kSaoStatEntries * sizeof(int2));
     if (e == cudaSuccess) e = dev_alloc(&s->sao_orig, pb);
     if (e == cudaSuccess) e = dev_alloc(&s->sao_flags, kSaoPasses * sizeof(int));
     if (e == cudaSuccess) e = dev_alloc(&s->sao_mail, nblk * sizeof(unsigned long long));
@@ -161,7 +161,7 @@ int evxg_stream_destroy(evxg_stream *s)
     cudaFree(s->src); cudaFree(s->lev);
     for (int i = 0; i < 4; i++) cudaFree(s->dpb[i]);
     cudaFree(s->bt); cudaFree(s->prev); cudaFree(s->prev_ser);
-    cudaFree(s->sao); cudaFree(s->sao_cost); cudaFree(s->rgb); cudaFree(s->sync);
+    cudaFree(s->sao); cudaFree(s->sao_stats); cudaFree(s->rgb); cudaFree(s->sync);
     cudaFree(s->sao_orig); cudaFree(s->sao_flags); cudaFree(s->sao_mail);
     if (s->profile)
         for (int i = 0; i < 7; i++) cudaEventDestroy(s->ev[i]);
@@ -394,7 +394,7 @@ void evxg::fill_args(evxg_stream *s, const evxg_frame *f, const uint8_t *drgb, F
     for (int i = 0; i < 4; i++) a.planes[i] = s->dpb[i];
     a.src = s->src; a.lev = s->lev; a.bt = s->bt;
     a.prev = f->type == EVXG_FRAME_INTER ? s->prev : nullptr;
-    a.sao = s->sao; a.sao_cost = s->sao_cost; a.rgb = drgb;
+    a.sao = s->sao; a.sao_stats = s->sao_stats; a.rgb = drgb;
     a.sao_orig = s->sao_orig; a.sao_flags = s->sao_flags; a.sao_mail = s->sao_mail;
     s->epoch = s->epoch % 255 + 1;
     a.epoch = s->epoch;

@@ -81,12 +81,30 @@ __device__ __forceinline__ void st_release64(unsigned long long *p, unsigned lon
 {
     asm volatile("st.release.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
 }
+// 16-byte asynchronous copies global -> shared, in commit groups.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ unsigned long long globaltimer_ns()
 {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
+
+// The SAO RDO's results for one MB, read by the merge: entries 0..31 are the
+// luma bands, 32..47 the luma edge categories (class * 4 + category), each as
+// (sum of source - recon, count | lowest recon sample << 9 | highest << 17);
+// entry 48 is the luma SSD without SAO and a flag set when a recon sample
+// lies outside [0, 255]; 49 the cost of the MB's own parameters (float bits);
+// 50..51 those parameters (evxg_sao_info).  416 bytes, a multiple of 16.
+constexpr int kSaoStatEntries = 52;
 
 // Per-frame parameters shared by all kernels of one encode step.
 struct FrameArgs {
@@ -106,7 +124,7 @@ struct FrameArgs {
     evxg_block_desc *bt;         // block table of this frame
     const evxg_block_desc *prev; // temporal MV predictor table (P frames), else null
     evxg_sao_info *sao;          // final SAO table
-    float *sao_cost;             // per-MB own-parameter SAO cost (RDO -> merge)
+    int2 *sao_stats;             // per MB: kSaoStatEntries entries of RDO results for the merge
     int16_t *sao_orig;           // deblocked, not yet SAO-filtered copy of the destination slot
     int *sao_flags;              // per fixed-point pass: 1 if the pass changed a pixel
     unsigned long long *sao_mail;// per MB: final SAO parameters of this frame, tagged with epoch

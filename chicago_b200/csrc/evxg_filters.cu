@@ -369,10 +369,12 @@ struct SaoScratch {
 // offsets of classes 0..3) and the reference's loop -- take a candidate when
 // it is strictly cheaper than the best so far -- picks the first candidate of
 // that order whose cost is the minimum, which a (cost, index) argmin finds.
-// All sums are of integers, so regrouping them changes nothing.
+// All sums are of integers, so regrouping them changes nothing.  With stats
+// set (luma), the band and edge-category sums and counts, the SSD without SAO
+// and the out-of-range flag are stored for the merge costs (kSaoStatEntries).
 template <int N>
 __device__ void sao_rdo_warp(const int16_t *s, const int16_t *r, int w, int h, int x0, int y0, float lambda, int lane,
-                             SaoScratch &sc, evxg_sao_params &out, long long &out_ssd)
+                             SaoScratch &sc, evxg_sao_params &out, long long &out_ssd, int2 *stats = nullptr)
 {
     constexpr int P = N * N / 32;   // pixels per lane: 8 (luma) or 2 (chroma)
     const int y = y0 + lane * P / N, xs = x0 + (lane * P) % N;
@@ -401,6 +403,23 @@ __device__ void sao_rdo_warp(const int16_t *s, const int16_t *r, int w, int h, i
     }
     base = warp_sum64(base);
     __syncwarp();
+    if (stats) {   // band b's samples lie in [8b, 8b+7]: only bands 0 and 31 need their extremes
+        bool out = false;
+        int mn0 = 255, mx31 = 0;
+#pragma unroll
+        for (int i = 0; i < P; i++) {
+            out |= pv[i] < 0 || pv[i] > 255;
+            const int b = sclamp(pv[i]) >> 3;
+            if (b == 0) mn0 = min(mn0, pv[i]);
+            if (b == 31) mx31 = max(mx31, pv[i]);
+        }
+        out = __any_sync(0xffffffffu, out);
+        mn0 = __reduce_min_sync(0xffffffffu, mn0);
+        mx31 = __reduce_max_sync(0xffffffffu, mx31);
+        const int lo = lane == 0 ? mn0 : 8 * lane, hi = lane == 31 ? mx31 : 8 * lane + 7;
+        stats[lane] = make_int2(sc.bsum[lane], sc.bcnt[lane] | (lo & 255) << 9 | (hi & 255) << 17);
+        if (lane == 0) stats[48] = make_int2((int)base, out ? 1 : 0);
+    }
     // band offsets: lane b owns band b (its offset does not depend on the band position)
     sc.boff[lane] = sc.bcnt[lane] > 0 ? avg_off(sc.bsum[lane], sc.bcnt[lane]) : 0;
     __syncwarp();
@@ -454,6 +473,22 @@ __device__ void sao_rdo_warp(const int16_t *s, const int16_t *r, int w, int h, i
     for (int ec = 0; ec < 4; ec++)
 #pragma unroll
         for (int k = 0; k < 4; k++) { cs[ec][k] = warp_sum(cs[ec][k]); cc[ec][k] = warp_sum(cc[ec][k]); }
+    if (stats) {   // each category's sum, count and sample range
+        int2 e = make_int2(0, 0);
+#pragma unroll
+        for (int ec = 0; ec < 4; ec++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                int mn = 255, mx = 0;
+#pragma unroll
+                for (int i = 0; i < P; i++)
+                    if (cat[ec][i] == k) { mn = min(mn, pv[i]); mx = max(mx, pv[i]); }
+                mn = __reduce_min_sync(0xffffffffu, mn);
+                mx = __reduce_max_sync(0xffffffffu, mx);
+                if (lane == 4 * ec + k) e = make_int2(cs[ec][k], cc[ec][k] | (mn & 255) << 9 | (mx & 255) << 17);
+            }
+        if (lane < 16) stats[32 + lane] = e;
+    }
     long long eo_ssd[4];
     bool eo_nz[4];
     int off[4][4];
@@ -509,7 +544,8 @@ __device__ void sao_rdo_warp(const int16_t *s, const int16_t *r, int w, int h, i
 }
 
 // One warp per MB: own luma and chroma (U plane) parameters and the cost of
-// keeping them, the starting point of the merge decision (sao.cpp:414-557).
+// keeping them, the starting point of the merge decision (sao.cpp:414-557),
+// stored with the luma statistics in the MB's record (kSaoStatEntries).
 __device__ __forceinline__ void sao_rdo_body(const FrameArgs &a, SaoScratch *scratch)
 {
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
@@ -520,7 +556,8 @@ __device__ __forceinline__ void sao_rdo_body(const FrameArgs &a, SaoScratch *scr
     const int cw = a.W / 2, ch = a.H / 2;
     evxg_sao_info info{};
     long long lssd, cssd;
-    sao_rdo_warp<16>(a.src, rec, a.W, a.H, bx * 16, by * 16, a.lambda, lane, scratch[wi], info.luma, lssd);
+    sao_rdo_warp<16>(a.src, rec, a.W, a.H, bx * 16, by * 16, a.lambda, lane, scratch[wi], info.luma, lssd,
+                     a.sao_stats + (size_t)m * kSaoStatEntries);
     sao_rdo_warp<8>(a.src + (size_t)a.W * a.H, rec + (size_t)a.W * a.H, cw, ch, bx * 8, by * 8, a.lambda, lane, scratch[wi],
                     info.chroma, cssd);
     if (lane == 0) {
@@ -528,8 +565,11 @@ __device__ __forceinline__ void sao_rdo_body(const FrameArgs &a, SaoScratch *scr
         if (info.luma.type == 0) cur = __fadd_rn(__ll2float_rn(lssd), __fmul_rn(a.lambda, 2.0f));
         else cur = __fadd_rn(__fsub_rn(__fadd_rn(__ll2float_rn(lssd), __fmul_rn(a.lambda, 1.0f)), __fmul_rn(a.lambda, 1.0f)),
                              __fmul_rn(a.lambda, __uint2float_rn(sao_bits(info.luma))));
-        a.sao[m] = info;
-        a.sao_cost[m] = cur;
+        int2 *r = a.sao_stats + (size_t)m * kSaoStatEntries;
+        uint4 w;
+        memcpy(&w, &info, sizeof w);
+        r[49] = make_int2(__float_as_int(cur), 0);
+        *reinterpret_cast<uint4 *>(r + 50) = w;
     }
 }
 constexpr int SAO_RDO_WARPS = 8;   // MBs per block of the RDO kernels
@@ -576,10 +616,11 @@ __device__ bool wait_row(const FrameArgs &a, const int *progress, int row, int n
 
 // ---- merge decisions (sao.cpp:559-586) ----
 // One warp per MB row in a wavefront: MB (r, c) needs the final parameters of
-// (r-1, c) and (r, c-1).  Merge costs read the deblocked, not yet filtered
-// frame, which does not change during this kernel, so each warp prefetches
-// the next MB's tile (recon rows y0-1..y0+16, columns x0-2..x0+17, and the
-// source block) into registers while it waits for the row above.
+// (r-1, c) and (r, c-1).  A merge cost is the luma SSD of the MB under the
+// neighbour's parameters plus one bit: from the band and edge-category sums
+// k_sao_rdo stored for the MB, or, when those parameters would clamp one of
+// the MB's samples, from its tile of the deblocked, not yet filtered frame
+// (recon rows y0-1..y0+16, columns x0-2..x0+17, and the source block).
 constexpr int MT_W = 20, MT_H = 18;   // recon tile, 10 words per row
 struct MergeTile {
     int16_t rec[MT_H * MT_W];
@@ -704,96 +745,154 @@ __device__ __forceinline__ evxg_sao_params unpack_params(unsigned long long v)
 // hand-over goes through global memory.  Frames whose words would not fit
 // use a.sao_mail for every row.
 constexpr int MERGE_CTAS = kMergeCtas, MERGE_WARPS = kMergeThreads / 32;
-constexpr size_t MERGE_SMEM_MAX = 160 * 1024;
+constexpr int MERGE_RING = 4;   // MB records in a warp's ring: the one decided and three in flight
+constexpr size_t MERGE_WARP_BYTES = sizeof(MergeTile) + MERGE_RING * kSaoStatEntries * sizeof(int2);
+constexpr size_t MERGE_SMEM_MAX = 200 * 1024 - MERGE_WARPS * MERGE_WARP_BYTES;   // hand-over words
 __host__ __device__ __forceinline__ int merge_rpc(int mbh) { return (mbh + MERGE_CTAS - 1) / MERGE_CTAS; }
 __host__ __device__ __forceinline__ size_t merge_words_bytes(int mbw, int mbh) { return (size_t)(merge_rpc(mbh) + 1) * mbw * 8; }
 __host__ __device__ __forceinline__ bool merge_words_fit(int mbw, int mbh) { return merge_words_bytes(mbw, mbh) <= MERGE_SMEM_MAX; }
 size_t merge_shared_bytes(int mbw, int mbh)   // dynamic shared memory of the merge kernels
 {
-    return MERGE_WARPS * 2 * sizeof(MergeTile) + (merge_words_fit(mbw, mbh) ? merge_words_bytes(mbw, mbh) : 0);
+    return MERGE_WARPS * MERGE_WARP_BYTES + (merge_words_fit(mbw, mbh) ? merge_words_bytes(mbw, mbh) : 0);
 }
 
-// Bounded wait of lane 0 for a tagged word; the shared-memory form polls
-// cheaply and looks at the error word and the clock every 256 polls.
+// Bounded wait of the whole warp for a tagged word: every lane reads the same
+// address, so each poll gives all lanes one value and the warp stays
+// converged.  The shared-memory form polls cheaply and looks at the error
+// word and the clock every 256 polls.
 template <bool kShared>
 __device__ __forceinline__ bool wait_word(const FrameArgs &a, const unsigned long long *p, unsigned long long ep,
                                           unsigned long long &v)
 {
-    const unsigned long long t0 = globaltimer_ns();
+    unsigned long long t0 = 0;
     for (unsigned it = 0;; it++) {
         v = kShared ? *(const volatile unsigned long long *)p : ld_acquire64(p);
-        if ((v & 0xFF) == ep) return true;
+        if (__all_sync(0xffffffffu, (v & 0xFF) == ep)) return true;
         if (kShared && (it & 255) != 255) continue;
-        if (*(volatile int *)a.error) return false;
-        if ((long long)(globaltimer_ns() - t0) > a.timeout_ns) {
+        bool stop = *(volatile int *)a.error != 0;
+        const unsigned long long now = globaltimer_ns();
+        if (!t0) {
+            t0 = now;
+        } else if ((long long)(now - t0) > a.timeout_ns) {
             atomicCAS(a.error, 0, EVXG_ERROR_OPERATION_TIMEDOUT);
-            return false;
+            stop = true;
         }
+        if (__any_sync(0xffffffffu, stop)) return false;
     }
 }
 
-// One row of merge decisions (sao.cpp:559-586); false once a wait gave up.
-// With shared words: above = this CTA's word row i (row i-1 of the block, or
-// for i = 0 the previous block's last row), own = word row i+1, and next (if
-// not null) the next CTA's word row 0.
-__device__ bool merge_row(const FrameArgs &a, MergeTile *tiles, unsigned long long *words, unsigned long long *next,
-                          int i, int row)
+// The record of MB m (kSaoStatEntries, 26 x 16 bytes) into a ring slot, by
+// lanes 0..25; one commit group per MB, issued by the whole warp.
+__device__ __forceinline__ void merge_fetch(const FrameArgs &a, int2 *slot, int m, int lane)
+{
+    if (lane < kSaoStatEntries / 2) cp_async16(slot + 2 * lane, a.sao_stats + (size_t)m * kSaoStatEntries + 2 * lane);
+}
+
+// Luma SSD of an MB under p from its record r (read alike by every lane): a
+// corrected sample v + o adds o^2 - 2 o (s - v) to the SSD without SAO,
+// exactly, unless v + o leaves [0, 255], where the correction clamps
+// (sao.cpp:40-97); false then, read from the sample ranges of p's entries.
+// Every term and the sum stay below 2^24 (256 samples, |s - v| <= 255).
+__device__ __forceinline__ bool stat_ssd(const int2 *r, const evxg_sao_params &p, int &ssd)
+{
+    const bool bo = p.type == 2;
+    const int first = bo ? p.band_position : 32 + 4 * p.eo_class, end = bo ? 32 : 48;
+    const int2 h = r[48];
+    int acc = h.x;
+    bool exact = h.y == 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int e = first + k;
+        if (e < end) {
+            const int2 v = r[e];
+            const int o = p.offsets[k], cnt = v.y & 511, lo = (v.y >> 9) & 255, hi = (v.y >> 17) & 255;
+            if (cnt) {
+                acc += cnt * o * o - 2 * o * v.x;
+                exact &= lo + o >= 0 && hi + o <= 255;
+            }
+        }
+    }
+    ssd = acc;
+    return exact;
+}
+
+// One row of merge decisions (sao.cpp:559-586) by one warp, all lanes in
+// step; false once a wait gave up.  With shared words: above = this CTA's
+// word row i (row i-1 of the block, or for i = 0 the previous block's last
+// row), own = word row i+1, and next (if not null) the next CTA's word row
+// 0.  The records of the next three MBs are in flight into the ring while one
+// MB is decided; a cost the statistics cannot give exactly is taken on the
+// MB's tile, loaded then (at most once per MB).
+__device__ bool merge_row(const FrameArgs &a, MergeTile &tile, int2 *ring, unsigned long long *words,
+                          unsigned long long *next, int i, int row)
 {
     const int lane = threadIdx.x & 31;
     const unsigned long long ep = (unsigned long long)a.epoch;
-    TileRegs t;
-    tile_load(a, 0, row, lane, t);
-    tile_store(tiles[0], lane, t);
-    evxg_sao_info own = ld_info_cg(&a.sao[row * a.mbw]);
-    float own_cost = __ldcg(&a.sao_cost[row * a.mbw]);
+    const int m0 = row * a.mbw;
+    for (int k = 0; k < MERGE_RING - 1; k++) {
+        if (k < a.mbw) merge_fetch(a, ring + k * kSaoStatEntries, m0 + k, lane);
+        cp_async_commit();
+    }
     evxg_sao_info left{};
     for (int c = 0; c < a.mbw; c++) {
-        const int m = row * a.mbw + c;
-        evxg_sao_info info = own;   // own RDO parameters, prefetched
-        float cur = own_cost;
-        if (c + 1 < a.mbw) {        // next MB's data is in flight while this one waits
-            tile_load(a, c + 1, row, lane, t);
-            own = ld_info_cg(&a.sao[m + 1]);
-            own_cost = __ldcg(&a.sao_cost[m + 1]);
-        }
+        const int m = m0 + c;
+        if (c + MERGE_RING - 1 < a.mbw)   // into the slot MB c-1 used
+            merge_fetch(a, ring + ((c + MERGE_RING - 1) % MERGE_RING) * kSaoStatEntries, m + MERGE_RING - 1, lane);
+        cp_async_commit();
+        cp_async_wait_group<MERGE_RING - 1>();   // MB c's group has landed
+        __syncwarp();
+        const int2 *r = ring + (c % MERGE_RING) * kSaoStatEntries;
+        evxg_sao_info info;
+        const uint4 own = *reinterpret_cast<const uint4 *>(r + 50);
+        memcpy(&info, &own, sizeof info);
+        float cur = __int_as_float(r[49].x);
+        bool have_tile = false;
+        auto cost = [&](const evxg_sao_params &p) {   // luma SSD of this MB under p, plus one bit
+            int ssd;
+            if (stat_ssd(r, p, ssd)) return __fadd_rn(__int2float_rn(ssd), __fmul_rn(a.lambda, 1.0f));
+            if (!have_tile) {
+                TileRegs t;
+                tile_load(a, c, row, lane, t);
+                __syncwarp();
+                tile_store(tile, lane, t);
+                __syncwarp();
+                have_tile = true;
+            }
+            return __fadd_rn(__ll2float_rn(tile_sao_ssd(a.W, a.H, tile, c, row, lane, p)), __fmul_rn(a.lambda, 1.0f));
+        };
         // The merge-left cost needs only this row's previous MB: it is computed
         // before the wait for the row above, off the wavefront's critical path.
-        __syncwarp();
-        const MergeTile &mt = tiles[c & 1];
         const bool try_left = c > 0 && left.luma.type != 0;
-        float mc_left = 0.0f;
-        if (try_left) mc_left = __fadd_rn(__ll2float_rn(tile_sao_ssd(a.W, a.H, mt, c, row, lane, left.luma)), __fmul_rn(a.lambda, 1.0f));
+        const float mc_left = try_left ? cost(left.luma) : 0.0f;
         unsigned long long above = 0;
         if (row > 0) {   // bounded wait for the final parameters of (r-1, c)
-            bool ok = true;
-            if (lane == 0)
-                ok = words ? wait_word<true>(a, &words[i * a.mbw + c], ep, above)
-                           : wait_word<false>(a, &a.sao_mail[m - a.mbw], ep, above);
-            if (!__shfl_sync(0xffffffffu, ok, 0)) return false;
-            above = __shfl_sync(0xffffffffu, above, 0);
+            const bool ok = words ? wait_word<true>(a, &words[i * a.mbw + c], ep, above)
+                                  : wait_word<false>(a, &a.sao_mail[m - a.mbw], ep, above);
+            if (!ok) {
+                cp_async_wait_all();   // no copy left in flight into the ring
+                return false;
+            }
         }
         if (try_left && mc_left < cur) { info.merge_left = 1; info.luma = left.luma; info.chroma = left.chroma; cur = mc_left; }
         if (!info.merge_left && row > 0) {
             const evxg_sao_params al = unpack_params(above >> 8), ac = unpack_params(above >> 33);
-            if (al.type != 0) {
-                const float mc = __fadd_rn(__ll2float_rn(tile_sao_ssd(a.W, a.H, mt, c, row, lane, al)), __fmul_rn(a.lambda, 1.0f));
-                if (mc < cur) { info.merge_above = 1; info.luma = al; info.chroma = ac; }
-            }
+            if (al.type != 0 && cost(al) < cur) { info.merge_above = 1; info.luma = al; info.chroma = ac; }
         }
         left = info;
-        if (lane == 0) {
-            const unsigned long long word = ep | (pack_params(info.luma) << 8) | (pack_params(info.chroma) << 33);
-            *reinterpret_cast<uint4 *>(&a.sao[m]) = *reinterpret_cast<const uint4 *>(&info);
-            if (words) {
-                *(volatile unsigned long long *)&words[(i + 1) * a.mbw + c] = word;
-                if (next) *(volatile unsigned long long *)&next[c] = word;
-            } else {
-                st_release64(&a.sao_mail[m], word);
-            }
+        // every lane stores the same value to the same address: one store each
+        const unsigned long long word = ep | (pack_params(info.luma) << 8) | (pack_params(info.chroma) << 33);
+        uint4 fin;
+        memcpy(&fin, &info, sizeof fin);
+        *reinterpret_cast<uint4 *>(&a.sao[m]) = fin;
+        if (words) {
+            *(volatile unsigned long long *)&words[(i + 1) * a.mbw + c] = word;
+            if (next) *(volatile unsigned long long *)&next[c] = word;
+        } else {
+            st_release64(&a.sao_mail[m], word);
         }
         __syncwarp();
-        if (c + 1 < a.mbw) tile_store(tiles[(c + 1) & 1], lane, t);
     }
+    cp_async_wait_all();
     return true;
 }
 
@@ -824,8 +923,9 @@ __device__ __forceinline__ void sao_merge_body(const FrameArgs &a, unsigned char
     const int w = threadIdx.x >> 5;
     const int rpc = merge_rpc(a.mbh), r0 = (int)k * rpc, rows = max(0, min(rpc, a.mbh - r0));
     MergeTile *tiles = reinterpret_cast<MergeTile *>(dsm);
+    int2 *rings = reinterpret_cast<int2 *>(dsm + MERGE_WARPS * sizeof(MergeTile));
     unsigned long long *words =
-        merge_words_fit(a.mbw, a.mbh) ? reinterpret_cast<unsigned long long *>(dsm + MERGE_WARPS * 2 * sizeof(MergeTile)) : nullptr;
+        merge_words_fit(a.mbw, a.mbh) ? reinterpret_cast<unsigned long long *>(dsm + MERGE_WARPS * MERGE_WARP_BYTES) : nullptr;
     if (words)
         for (int e = threadIdx.x; e < (rpc + 1) * a.mbw; e += blockDim.x) words[e] = 0;
     merge_cluster_barrier();
@@ -833,15 +933,15 @@ __device__ __forceinline__ void sao_merge_body(const FrameArgs &a, unsigned char
     if (words && r0 + rpc < a.mbh) next = merge_peer(words, k + 1);   // the next block's word row 0
     bool alive = true;
     for (int i = w; i < rows && alive; i += MERGE_WARPS)
-        alive = merge_row(a, tiles + 2 * w, words, i == rpc - 1 ? next : nullptr, i, r0 + i);
+        alive = merge_row(a, tiles[w], rings + w * MERGE_RING * kSaoStatEntries, words, i == rpc - 1 ? next : nullptr, i, r0 + i);
     merge_cluster_barrier();
 }
-__global__ void __cluster_dims__(MERGE_CTAS, 1, 1) __launch_bounds__(32 * MERGE_WARPS) k_sao_merge(FrameArgs a)
+__global__ void __cluster_dims__(MERGE_CTAS, 1, 1) __launch_bounds__(32 * MERGE_WARPS, 1) k_sao_merge(FrameArgs a)
 {
     extern __shared__ __align__(16) unsigned char merge_smem[];
     sao_merge_body(a, merge_smem);
 }
-__global__ void __cluster_dims__(MERGE_CTAS, 1, 1) __launch_bounds__(32 * MERGE_WARPS) k_sao_merge_b(const FrameArgs *args)
+__global__ void __cluster_dims__(MERGE_CTAS, 1, 1) __launch_bounds__(32 * MERGE_WARPS, 1) k_sao_merge_b(const FrameArgs *args)
 {
     extern __shared__ __align__(16) unsigned char merge_smem[];
     __shared__ FrameArgs sa;

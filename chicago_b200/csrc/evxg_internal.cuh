@@ -72,7 +72,7 @@ struct evxg_stream {
     int16_t *src, *lev, *dpb[4];
     evxg_block_desc *bt, *prev, *prev_ser;
     evxg_sao_info *sao;
-    float *sao_cost;
+    int2 *sao_stats;                    // per-MB RDO results for the merge (kSaoStatEntries each)
     int16_t *sao_orig;                  // pristine copy for the SAO fixed-point passes
     int *sao_flags;
     unsigned long long *sao_mail;       // SAO merge hand-over words, epoch-tagged

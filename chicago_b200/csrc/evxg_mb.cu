@@ -367,16 +367,6 @@ __device__ __noinline__ void load_windows(int W, int H)
     }
 }
 
-// 16-byte asynchronous copies global -> shared, in commit groups.
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
 // Rows of window 0 (loaded around (px, py-16)) that show MB row r-1 of the
 // destination slot: window rows [y0, y1) luma and [cy0, cy1) chroma.  For
 // r = 1 the rows clamped to plane row 0 (above the frame) show it too.

@@ -46,7 +46,7 @@ size_t stream_bytes(uint32_t w, uint32_t h)
 {
     const size_t W = (w + 15) & ~15u, H = (h + 15) & ~15u, nblk = (W / 16) * (H / 16);
     const size_t planeset = (W * H + 2 * (W / 2) * (H / 2)) * sizeof(int16_t);
-    return 7 * planeset + (size_t)w * h * 3 + nblk * (3 * sizeof(evxg_block_desc) + sizeof(evxg_sao_info) + 12) +
+    return 7 * planeset + (size_t)w * h * 3 + nblk * (3 * sizeof(evxg_block_desc) + sizeof(evxg_sao_info) + 8 + kSaoStatEntries * sizeof(int2)) +
            (3 * (H / 16) + 5) * sizeof(int) + kSaoPasses * sizeof(int);
 }
 

@@ -30,34 +30,40 @@ CASES = [  # (w, h, frames, quality, vmax, intra_at)
 FORMS = ("cluster", "single")   # three CTAs per macroblock row / one
 
 
-def clip(w, h, T, vmax, seed=None, window=None):
+def clip(w, h, T, vmax, seed=None, window=None, stretch=None):
     """The seeded test content; window=(first, cut) takes frames first.. of a
-    longer sequence with a scene cut (the benchmark's generator)."""
+    longer sequence with a scene cut (the benchmark's generator); stretch
+    scales the contrast about mid-grey, clipping to 0..255."""
     if window is None:
-        return generate(w, h, T, seed=w * 7 + h if seed is None else seed, vmax=vmax)
-    first, cut = window
-    return generate(w, h, first + T, seed=seed, vmax=vmax, n_rects=4, cut_at=cut)[first:]
+        frames = generate(w, h, T, seed=w * 7 + h if seed is None else seed, vmax=vmax)
+    else:
+        first, cut = window
+        frames = generate(w, h, first + T, seed=seed, vmax=vmax, n_rects=4, cut_at=cut)[first:]
+    if stretch is not None:
+        frames = np.clip((frames.astype(np.float32) - 128.0) * stretch + 128.0, 0, 255).astype(np.uint8)
+    return frames
 
 
 @functools.lru_cache(maxsize=8)
-def oracle_run(w, h, T, q, vmax, intra_at, cfg, seed=None, window=None):
+def oracle_run(w, h, T, q, vmax, intra_at, cfg, seed=None, window=None, stretch=None):
     """The oracle's stage dumps of a clip (cached: the large cases serve both
     macroblock-pass forms)."""
     import chicago_b200 as cb
     from oracle_py import Oracle
     b_frames, ref_count, radius = cb.CONFIGS[cfg]
-    frames = clip(w, h, T, vmax, seed, window)
+    frames = clip(w, h, T, vmax, seed, window, stretch)
     oc = Oracle().context(w, h, b_frames=b_frames, ref_count=ref_count, radius=radius)
     plan = plan_gop(T, quality=q, intra_at=intra_at) if b_frames else plan_ip(T, q, intra_at, ref_count)
     return frames, [(ti, f18, oc.encode_frame(frames[ti], f18)) for ti, f18 in plan]
 
 
-def check_stream(oracle, w, h, T, q, vmax, intra_at, form="cluster", cfg="default", seed=None, window=None):
+def check_stream(oracle, w, h, T, q, vmax, intra_at, form="cluster", cfg="default", seed=None, window=None,
+                 stretch=None):
     """Encode a seeded clip through the C ABI and compare every stage of every
     frame with the oracle restating the same reference build (cfg: "default",
     or the I/P builds "ip1" / "ip3")."""
     import chicago_b200 as cb
-    frames, runs = oracle_run(w, h, T, q, vmax, tuple(intra_at), cfg, seed, window)
+    frames, runs = oracle_run(w, h, T, q, vmax, tuple(intra_at), cfg, seed, window, stretch)
     st = cb.Stream(w, h, cfg)
     st.mb_form = cb.MB_FORM_CLUSTER if form == "cluster" else cb.MB_FORM_SINGLE
     for k, (ti, f18, od) in enumerate(runs):
@@ -139,6 +145,22 @@ def test_gpu_matches_oracle_wide_frames(oracle, form):
     (memory-word form)."""
     check_stream(oracle, 16400, 32, 3, 8, 6.0, (), form, seed=77)
     check_stream(oracle, 54640, 528, 1, 8, 6.0, (), form, seed=78)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("cfg", ["default", "ip3"])
+def test_gpu_matches_oracle_saturated(oracle, cfg, form):
+    """Contrast stretched until large areas clip to 0 or 255.  The SAO merge
+    costs an MB whose samples stay in [8, 247] from the RDO's band and
+    edge-category sums, and any other MB on its pixels (where v + o may
+    clamp); both kinds are frequent in every frame of this clip."""
+    w, h, T = 352, 288, 6
+    frames, runs = oracle_run(w, h, T, 8, 6.0, (), cfg, 91, None, 2.5)
+    for _, _, od in runs:
+        mbs = od.final[:w * h].reshape(h // 16, 16, w // 16, 16)
+        near = ((mbs < 8) | (mbs > 247)).any(axis=(1, 3)).mean()
+        assert 0.1 < near < 0.9, near
+    check_stream(oracle, w, h, T, 8, 6.0, (), form, cfg, seed=91, stretch=2.5)
 
 
 @pytest.mark.parametrize("variant", ["ip1", "ip3"])
