@@ -961,12 +961,62 @@ __global__ void __cluster_dims__(MERGE_CTAS, 1, 1) __launch_bounds__(32 * MERGE_
 // flags any change; once a pass changes nothing the frame is exactly x = F(x).
 // Passes after a quiet pass return at once; if the last pass still changed a
 // pixel, k_sao_restore and k_sao_apply redo the frame in raster wavefront order.
-// One work item is 8 consecutive samples of a row (always inside one MB:
-// MBs are 16 luma / 8 chroma samples wide), read and written as 16-byte
-// chunks; the item's row and column come from one 32-bit division.
+// In the first pass one work item is 8 consecutive samples of a row (always
+// inside one MB: MBs are 16 luma / 8 chroma samples wide), read and written
+// as 16-byte chunks; the item's row and column come from one 32-bit division.
+// After it, band offsets and every sample whose edge neighbours lie in its
+// own MB or raster-later ones are final: neighbours are one sample away, so
+// only a sample on its MB's top row or left column can read a raster-earlier
+// MB, and the later passes evaluate those samples of edge-offset MBs alone
+// (luma 16 + 15, chroma 8 + 7 per MB and plane), one thread each.
+// Edge-offset value of sample (x, y) of MB m, unfiltered value v.
+__device__ __forceinline__ int sao_fix_sample(const FrameArgs &a, const evxg_sao_params &p, const int16_t *orig,
+                                              const int16_t *img, int w, int h, int sh, int m, int x, int y, int v)
+{
+    const int ax = x + c_eo[p.eo_class][0], ay = y + c_eo[p.eo_class][1];
+    const int bx = x + c_eo[p.eo_class][2], by = y + c_eo[p.eo_class][3];
+    if (ax < 0 || ax >= w || ay < 0 || ay >= h || bx < 0 || bx >= w || by < 0 || by >= h) return v;
+    const int ma = (ay >> sh) * a.mbw + (ax >> sh), mb = (by >> sh) * a.mbw + (bx >> sh);
+    const size_t ka = (size_t)ay * w + ax, kb = (size_t)by * w + bx;
+    const int va = ma < m ? __ldcg(img + ka) : orig[ka];
+    const int vb = mb < m ? __ldcg(img + kb) : orig[kb];
+    const int ct = eo_cat(v, va, vb);
+    return ct < 4 ? sclamp(v + p.offsets[ct]) : v;
+}
+__device__ __forceinline__ void sao_fix_border(const FrameArgs &a, int pass)
+{
+    constexpr int kLuma = 31, kChroma = 15, kPer = kLuma + 2 * kChroma;
+    const int cw = a.W / 2, ch = a.H / 2;
+    const size_t ny = (size_t)a.W * a.H, nc = (size_t)cw * ch;
+    bool changed = false;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.mbw * a.mbh * kPer; i += gridDim.x * blockDim.x) {
+        const int m = i / kPer, s = i - m * kPer;
+        const int pl = s < kLuma ? 0 : (s < kLuma + kChroma ? 1 : 2);
+        const evxg_sao_params p = pl ? a.sao[m].chroma : a.sao[m].luma;
+        if (p.type != 1) continue;
+        const int t = pl == 0 ? s : (pl == 1 ? s - kLuma : s - kLuma - kChroma);
+        const int n = pl ? 8 : 16, sh = pl ? 3 : 4, w = pl ? cw : a.W, h = pl ? ch : a.H;
+        const int x0 = (m % a.mbw) * n, y0 = (m / a.mbw) * n;
+        const int x = t < n ? x0 + t : x0, y = t < n ? y0 : y0 + t - n + 1;   // top row, then the left column
+        const size_t off = pl == 0 ? 0 : (pl == 1 ? ny : ny + nc);
+        int16_t *img = a.planes[a.dpb] + off;
+        const int16_t *orig = a.sao_orig + off;
+        const size_t k = (size_t)y * w + x;
+        const int corr = sao_fix_sample(a, p, orig, img, w, h, sh, m, x, y, orig[k]);
+        if (__ldcg(img + k) != corr) {   // the sample is this thread's alone
+            img[k] = (int16_t)corr;
+            changed = true;
+        }
+    }
+    if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) atomicOr(&a.sao_flags[pass], 1);
+}
 __device__ __forceinline__ void sao_fix_body(const FrameArgs &a, int pass)
 {
     if (pass > 0 && __ldcg(&a.sao_flags[pass - 1]) == 0) return;
+    if (pass > 0) {
+        sao_fix_border(a, pass);
+        return;
+    }
     const int cw = a.W / 2, ch = a.H / 2;
     const int ly = a.H * (a.W / 8), lc = ch * (cw / 8);   // items per plane
     const size_t ny = (size_t)a.W * a.H, nc = (size_t)cw * ch;
@@ -995,16 +1045,7 @@ __device__ __forceinline__ void sao_fix_body(const FrameArgs &a, int pass)
                 const int idx = (sclamp(v) >> 3) - p.band_position;
                 if (idx >= 0 && idx < 4) corr = sclamp(v + p.offsets[idx]);
             } else {
-                const int ax = x + c_eo[p.eo_class][0], ay = y + c_eo[p.eo_class][1];
-                const int bx = x + c_eo[p.eo_class][2], by = y + c_eo[p.eo_class][3];
-                if (ax >= 0 && ax < w && ay >= 0 && ay < h && bx >= 0 && bx < w && by >= 0 && by < h) {
-                    const int ma = (ay >> sh) * a.mbw + (ax >> sh), mb = (by >> sh) * a.mbw + (bx >> sh);
-                    const size_t ka = (size_t)ay * w + ax, kb = (size_t)by * w + bx;
-                    const int va = ma < m ? __ldcg(img + ka) : orig[ka];
-                    const int vb = mb < m ? __ldcg(img + kb) : orig[kb];
-                    const int ct = eo_cat(v, va, vb);
-                    if (ct < 4) corr = sclamp(v + p.offsets[ct]);
-                }
+                corr = sao_fix_sample(a, p, orig, img, w, h, sh, m, x, y, v);
             }
             if (i8[e] != corr) { i8[e] = (int16_t)corr; any = true; }
         }
