@@ -743,7 +743,8 @@ __device__ __forceinline__ evxg_sao_params unpack_params(unsigned long long v)
 // fence: the parameters are the word -- and at a block boundary the last
 // row stores its words straight into the next CTA's shared memory, so no
 // hand-over goes through global memory.  Frames whose words would not fit
-// use a.sao_mail for every row.
+// use a.sao_mail for every row.  A CTA's dynamic shared memory holds one
+// tile per warp, then one four-record ring per warp, then the words.
 constexpr int MERGE_CTAS = kMergeCtas, MERGE_WARPS = kMergeThreads / 32;
 constexpr int MERGE_RING = 4;   // MB records in a warp's ring: the one decided and three in flight
 constexpr size_t MERGE_WARP_BYTES = sizeof(MergeTile) + MERGE_RING * kSaoStatEntries * sizeof(int2);
